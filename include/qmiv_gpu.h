@@ -1,0 +1,204 @@
+/*
+  qmiv_gpu.h — C ABI of the B200 (sm_100a) implementation of the QMIV metric hot path.
+
+  The entry points replace the pmbb-ivqm metric-calculator calls that the QMIV app makes per frame
+  (apps/QMIV/src/xAppQMIV.cpp:927-1108). Plain pointers, sizes and status codes only: no C++ or
+  torch types cross this boundary. All entry points return a qmiv_status; none throws.
+
+  Ownership: the caller owns every host buffer it passes; the library owns all device memory it
+  allocates (a calc's buffers count against its context's HBM budget). Device-resident frames may
+  also be passed (QMIV_MEM_DEVICE); they stay owned by the caller.
+  Threading: a qmiv_calc is not re-entrant (as a reference processor with its row buffers is not,
+  libs/pmbb-ivqm/src/xMetricCommon.h:23-27); different calcs may be used from different threads.
+
+  Reference interfaces replaced (paths inside the QMIV repository):
+    qmiv_calc_create        xGlobClrDiffProc / xShftCompPicProc / xIVPSNRM / xIVSSIM set-up:
+                            setSearchRange, setCmpWeightsSearch/Average, setUnntcbCoef, initRowBuffers,
+                            initWS, xSSIM::create, setStructSimParams
+                            (apps/QMIV/src/xAppQMIV.cpp:680-744; xCorrespPixelShiftPrms.h:30-32;
+                             xGlobClrDiff.h:24; xMetricCommon.cpp:12-19; xWeightedSpherically.h:21;
+                             xSSIM.h:78-81)
+    qmiv_calc_gcd           xGlobClrDiffProc::CalcGlobalColorDiff (xGlobClrDiff.h:41)
+    qmiv_calc_scp           xShftCompPicProc::GenShftCompPics (xShftCompPic.h:44-47)
+    qmiv_frame_pair_compute one frame of processAllFrames: calcFrameGCD, calcFrameSCP and the
+                            calcFrame* metric calls (apps/QMIV/src/xAppQMIV.cpp:761-827):
+                            xPSNR::calcPicPSNR (xPSNR.h:89), xWSPSNR::calcPicWSPSNR (xWSPSNR.h:22),
+                            xIVPSNR::calcPicIVPSNR (xIVPSNR.h:36), xSSIM::calcPicSSIM / calcPicMSSSIM
+                            (xSSIM.h:83-84), xIVSSIM::calcPicIVSSIM / calcPicIVMSSSIM (xIVSSIM.h:39-40)
+    qmiv_batch_*            no single reference counterpart: the reference processes frames one at a
+                            time (xAppQMIV.cpp:761); the batch runs many frame pairs of uneven shape
+                            per launch.
+    qmiv_server_*           no reference counterpart (the reference has no serving mode).
+*/
+#ifndef QMIV_GPU_H
+#define QMIV_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QMIV_API_VERSION 1
+
+#if defined(__GNUC__)
+#define QMIV_API __attribute__((visibility("default")))
+#else
+#define QMIV_API
+#endif
+
+typedef enum qmiv_status
+{
+  QMIV_OK                 = 0,
+  QMIV_ERR_INVALID_ARG    = 1,  /* null pointer, bad size, bad parameter value */
+  QMIV_ERR_UNSUPPORTED    = 2,  /* valid in the reference but not implemented here */
+  QMIV_ERR_CUDA           = 3,  /* a CUDA runtime call failed (see qmiv_last_error) */
+  QMIV_ERR_OUT_OF_MEMORY  = 4,  /* device allocation failed */
+  QMIV_ERR_INVALID_PIXEL  = 5,  /* a sample exceeds the bit depth's range and the action is STOP */
+  QMIV_ERR_BUDGET         = 6,  /* the request does not fit in the context's HBM budget */
+  QMIV_ERR_TIMEOUT        = 7,  /* a bounded wait ran out */
+  QMIV_ERR_NOT_READY      = 8,  /* asynchronous result not available yet */
+  QMIV_ERR_CANCELLED      = 9,  /* request cancelled before it ran */
+  QMIV_ERR_BUSY           = 10  /* no free slot / queue full */
+} qmiv_status;
+
+/* metric selection bits (apps/QMIV/src/xAppQMIV.cpp:60-63 metric list) */
+enum
+{
+  QMIV_PSNR     = 1u << 0,
+  QMIV_WSPSNR   = 1u << 1,
+  QMIV_IVPSNR   = 1u << 2,
+  QMIV_SSIM     = 1u << 3,
+  QMIV_MSSSIM   = 1u << 4,
+  QMIV_IVSSIM   = 1u << 5,
+  QMIV_IVMSSSIM = 1u << 6,
+  QMIV_ALL      = 0x7Fu
+};
+
+/* where a frame's planes live */
+enum { QMIV_MEM_HOST = 0, QMIV_MEM_DEVICE = 1 };
+
+/* invalid-pixel action (apps/QMIV/src/xAppQMIV.cpp:834-852, README "InvalidPelActn") */
+enum { QMIV_PEL_SKIP = 0, QMIV_PEL_WARN = 1, QMIV_PEL_STOP = 2, QMIV_PEL_CNCL = 3 };
+
+typedef struct qmiv_ctx_s*    qmiv_ctx;
+typedef struct qmiv_calc_s*   qmiv_calc;
+typedef struct qmiv_batch_s*  qmiv_batch;
+typedef struct qmiv_server_s* qmiv_server;
+
+/* Processor parameters. qmiv_params_default() gives the reference defaults:
+   R=2, weights 4:1:1:0 (xCorrespPixelShiftPrms.h:22-24), unnoticeable coef 0.01 (xGlobClrDiff.h:20),
+   BlockAveraged SSIM with 8x8 windows at stride 4 (xSSIM.h:35-37), no ERP, STOP on invalid pixels. */
+typedef struct qmiv_params
+{
+  int32_t search_range;        /* 1..5 */
+  int32_t cws[4];              /* search component weights, cws[3] must be 0 */
+  int32_t cwa[4];              /* averaging component weights */
+  float   unc[4];              /* unnoticeable colour difference coefficients */
+  int32_t erp;                 /* equirectangular (WS) weighting on/off */
+  int32_t lon_range_deg;       /* 360 */
+  int32_t lat_range_deg;       /* 180 */
+  int32_t ssim_window;         /* 8 (BlockAveraged) */
+  int32_t ssim_stride;         /* 4 */
+  int32_t invalid_pel_action;  /* QMIV_PEL_* */
+} qmiv_params;
+
+/* One frame: planar Y, Cb, Cr. Samples are 1 byte for bitdepth <= 8, else 2 bytes little endian.
+   pitch is in bytes. Chroma planes are (W>>1)x(H>>1) for 4:2:0, (W>>1)xH for 4:2:2, WxH for 4:4:4. */
+typedef struct qmiv_frame
+{
+  const void* plane[3];
+  int64_t     pitch[3];
+  int32_t     mem;             /* QMIV_MEM_HOST or QMIV_MEM_DEVICE */
+} qmiv_frame;
+
+/* Results of one frame pair. Fields of metrics that were not requested are left at 0.
+   Direction names follow the reference: R2T searches In0+GCD inside In1, T2R searches In1-GCD
+   inside In0 (xIVPSNR.cpp:115-116); IV-SSIM T2R = SSIM(In0, SCP1), R2T = SSIM(In1, SCP0)
+   (xIVSSIM.cpp:46-47). */
+typedef struct qmiv_result
+{
+  int32_t  gcd_r2t[4];         /* round(mean(In1 - In0)), clipped (xGlobClrDiff.cpp:70-103) */
+  int32_t  exact[4];           /* component identical in both frames (xAppQMIV.cpp:894-897) */
+  int32_t  invalid_pel[2];     /* frame 0/1 held samples above the bit depth's maximum */
+  uint64_t ssd[4];             /* per-component SSD of the 4:4:4 pictures */
+  uint64_t cps_sse_r2t[4];     /* sum over rows of the CPS row SSE, R2T */
+  uint64_t cps_sse_t2r[4];     /* sum over rows of the CPS row SSE, T2R */
+  double   psnr[4];   double psnr_pic;
+  double   wspsnr[4]; double wspsnr_pic;
+  double   ivpsnr;    double ivpsnr_r2t;   double ivpsnr_t2r;
+  double   ssim[4];   double ssim_pic;
+  double   msssim[4]; double msssim_pic;
+  double   ivssim;    double ivssim_r2t;   double ivssim_t2r;
+  double   ivmsssim;  double ivmsssim_r2t; double ivmsssim_t2r;
+} qmiv_result;
+
+/* ---- library / context -------------------------------------------------------------------- */
+QMIV_API int32_t     qmiv_api_version(void);
+QMIV_API const char* qmiv_status_string(qmiv_status status);
+QMIV_API const char* qmiv_last_error(void);          /* thread-local message of the last failure */
+QMIV_API void        qmiv_params_default(qmiv_params* params);
+
+/* device: CUDA ordinal. hbm_budget_bytes: cap on the device memory this context's calcs,
+   batches and servers may hold (0 = no cap). */
+QMIV_API qmiv_status qmiv_ctx_create(int32_t device, uint64_t hbm_budget_bytes, qmiv_ctx* out_ctx);
+QMIV_API qmiv_status qmiv_ctx_destroy(qmiv_ctx ctx);
+QMIV_API qmiv_status qmiv_ctx_memory(qmiv_ctx ctx, uint64_t* used_bytes, uint64_t* budget_bytes);
+
+/* ---- plain form: one frame pair per call -------------------------------------------------- */
+QMIV_API qmiv_status qmiv_calc_create(qmiv_ctx ctx, int32_t width, int32_t height, int32_t bitdepth, int32_t chroma_format,
+                             const qmiv_params* params, qmiv_calc* out_calc);
+QMIV_API qmiv_status qmiv_calc_destroy(qmiv_calc calc);
+
+/* Full per-frame pipeline (GCD, SCP if needed, requested metrics). Blocks until done. */
+QMIV_API qmiv_status qmiv_frame_pair_compute(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1,
+                                    uint32_t metric_mask, qmiv_result* out);
+
+/* Asynchronous form: enqueue on the calc's stream; qmiv_frame_pair_wait() returns the result.
+   One submission in flight per calc; host frames must stay valid until the wait returns. */
+QMIV_API qmiv_status qmiv_frame_pair_submit(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1,
+                                   uint32_t metric_mask);
+QMIV_API qmiv_status qmiv_frame_pair_wait(qmiv_calc calc, int32_t timeout_ms, qmiv_result* out);
+
+/* xGlobClrDiffProc::CalcGlobalColorDiff(Tst=In0, Ref=In1) -> round(mean(In1 - In0)), clipped. */
+QMIV_API qmiv_status qmiv_calc_gcd(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, int32_t gcd_r2t[4]);
+
+/* xShftCompPicProc::GenShftCompPics as called by the app (xAppQMIV.cpp:934-948): writes the
+   shift-compensated pictures SCP0 (In0 resampled onto In1's grid) and SCP1 (In1 onto In0's), planar
+   4:4:4, WxH per component, 2-byte samples, into the caller's host or device buffers
+   (dst_mem = QMIV_MEM_*). Either destination may be NULL. gcd_r2t may be NULL (computed here). */
+QMIV_API qmiv_status qmiv_calc_scp(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, const int32_t* gcd_r2t,
+                          uint16_t* scp0, uint16_t* scp1, int32_t dst_mem);
+
+/* Per-row CPS SSE of the last computed pair: rows_r2t/rows_t2r receive H*3 uint64 values
+   (row-major, component fastest) with the reference's 32-bit-lane accumulation semantics
+   (xCorrespPixelShiftSSE.cpp:29-40). Either pointer may be NULL. */
+QMIV_API qmiv_status qmiv_calc_cps_rows(qmiv_calc calc, uint64_t* rows_r2t, uint64_t* rows_t2r);
+
+/* Device stream (cudaStream_t) the calc enqueues on, for callers that order their own work. */
+QMIV_API qmiv_status qmiv_calc_stream(qmiv_calc calc, void** cuda_stream);
+
+/* ---- batched form: many frame pairs of uneven shape per launch ---------------------------- */
+typedef struct qmiv_pair_desc
+{
+  qmiv_frame in0, in1;
+  int32_t    width, height, bitdepth, chroma_format;
+  int32_t    search_range;     /* 1..5 */
+  uint32_t   metric_mask;
+} qmiv_pair_desc;
+
+/* max_pairs: pairs per qmiv_batch_compute call; max_pixels: sum of W*H over one call's pairs.
+   params: shared weights/coefficients (search_range is taken per pair). use_graph: capture the
+   launch sequence in CUDA graphs keyed by the batch's shape signature. */
+QMIV_API qmiv_status qmiv_batch_create(qmiv_ctx ctx, int32_t max_pairs, int64_t max_pixels, const qmiv_params* params,
+                              int32_t use_graph, qmiv_batch* out_batch);
+QMIV_API qmiv_status qmiv_batch_destroy(qmiv_batch batch);
+QMIV_API qmiv_status qmiv_batch_compute(qmiv_batch batch, const qmiv_pair_desc* pairs, int32_t num_pairs, qmiv_result* out);
+/* Tile shapes picked by the autotuner for (width, height, bitdepth, R): for inspection and tests. */
+QMIV_API qmiv_status qmiv_batch_tuning(qmiv_batch batch, int32_t width, int32_t height, int32_t bitdepth, int32_t search_range,
+                              int32_t* cps_tile_w, int32_t* cps_tile_h, int32_t* cps_rows_per_thread);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QMIV_GPU_H */

@@ -1,0 +1,509 @@
+/*
+  qmiv_oracle.c — CPU restatement of the QMIV metric hot path (see qmiv_oracle.h).
+
+  TEST INFRASTRUCTURE ONLY: the checker for the CUDA library, never part of it.
+  Compiled with -ffp-contract=off so that every floating-point operation is the single IEEE
+  operation written here, in the order the reference writes it.
+  Citations are file:line inside the QMIV repository.
+*/
+#include "qmiv_oracle.h"
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ----------------------------------------------------------------------------------------------- */
+/* helpers                                                                                         */
+/* ----------------------------------------------------------------------------------------------- */
+
+static inline int32_t qo_clampi(int32_t v, int32_t lo, int32_t hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static inline int32_t qo_max_value(int32_t bitdepth) { return (1 << bitdepth) - 1; } /* xCommonDefCORE.h:156 */
+
+/* Round half away from zero by adding +-0.5 and truncating, as xRoundF32ToI32 / xRoundF64ToI32
+   (libs/pmbb-core/src/xHelpersFLT.h:32-33). The addition happens in the source precision. */
+static inline int32_t qo_round_f32(float f) { volatile float t = f + copysignf(0.5f, f); return (int32_t)t; }
+static inline int32_t qo_round_f64(double f) { volatile double t = f + copysign(0.5, f); return (int32_t)t; }
+
+/* Kahan-Babuska-Neumaier summation, libs/pmbb-core/src/xKBNS.h:36-43 (scalar) and
+   libs/pmbb-core/src/xKBNS.cpp (SSE/AVX lane-wise variants compute the same per lane). */
+typedef struct { double s, c; } qo_kbns;
+static inline void qo_kbns_add(qo_kbns* k, double v)
+{
+  double t = k->s + v;
+  if(fabs(k->s) >= fabs(v)) { k->c += ((k->s - t) + v); }
+  else                      { k->c += ((v - t) + k->s); }
+  k->s = t;
+}
+static inline double qo_kbns_result(const qo_kbns* k) { return k->s + k->c; }
+
+/* xPSNR::CalcPSNRfromSSD, libs/pmbb-ivqm/src/xPSNR.cpp:186-192 */
+static double qo_psnr_from_ssd(double ssd, int64_t area, int32_t bitdepth)
+{
+  const uint64_t maxv = (uint64_t)qo_max_value(bitdepth);
+  const uint64_t MAX  = (uint64_t)area * (maxv * maxv);
+  return ssd > 0 ? 10.0 * log10((double)MAX / ssd) : DBL_MAX;
+}
+
+/* ----------------------------------------------------------------------------------------------- */
+/* a1: raw 4:2:0/4:2:2/4:4:4 -> planar 4:4:4 uint16                                                */
+/* libs/pmbb-core/src/xSeq.cpp:231-290 (xUnpackFrame); replication as xPixelOpsSTD.cpp:30-49,68-87 */
+/* ----------------------------------------------------------------------------------------------- */
+void qo_unpack444(const void* const planes[3], int32_t W, int32_t H, int32_t bitdepth, int32_t chroma_format, uint16_t* dst)
+{
+  const int32_t sx = (chroma_format == 444) ? 0 : 1;
+  const int32_t sy = (chroma_format == 420) ? 1 : 0;
+  for(int32_t c = 0; c < 3; c++)
+  {
+    const int32_t cw = c == 0 ? W : (W >> sx);
+    const int32_t shx = c == 0 ? 0 : sx, shy = c == 0 ? 0 : sy;
+    uint16_t* d = dst + (size_t)c * W * H;
+    for(int32_t y = 0; y < H; y++)
+    {
+      const size_t row = (size_t)(y >> shy) * cw;
+      for(int32_t x = 0; x < W; x++)
+      {
+        const size_t i = row + (x >> shx);
+        d[(size_t)y * W + x] = bitdepth <= 8 ? ((const uint8_t*)planes[c])[i] : ((const uint16_t*)planes[c])[i];
+      }
+    }
+  }
+}
+
+/* ----------------------------------------------------------------------------------------------- */
+/* a3: global colour difference, libs/pmbb-ivqm/src/xGlobClrDiff.cpp:70-103                        */
+/* ----------------------------------------------------------------------------------------------- */
+void qo_gcd(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, const float coef[4], int32_t gcd[4])
+{
+  const int32_t maxv = qo_max_value(bitdepth);
+  const double  area = (double)((int64_t)W * H);
+  int64_t sd[4] = { 0, 0, 0, 0 };
+  for(int32_t c = 0; c < 3; c++)
+  {
+    const uint16_t* t = tst + (size_t)c * W * H;
+    const uint16_t* r = ref + (size_t)c * W * H;
+    for(size_t i = 0; i < (size_t)W * H; i++) { sd[c] += (int32_t)t[i] - (int32_t)r[i]; } /* xDistortionSTD.cpp:12-22 */
+  }
+  for(int32_t c = 0; c < 4; c++)
+  {
+    const int32_t maxdiff = qo_round_f32(coef[c] * (float)maxv);
+    const double  avg     = (double)sd[c] / area;
+    gcd[c] = qo_clampi(qo_round_f64(avg), -maxdiff, maxdiff);
+  }
+}
+
+/* ----------------------------------------------------------------------------------------------- */
+/* a4/a5: corresponding pixel shift, one direction.                                                */
+/* x86 interleaved path: libs/pmbb-ivqm/src/xCorrespPixelShiftSSE.cpp:18-70 (row SSE) and :75-127  */
+/* (shift-compensated picture). Out-of-picture candidates read the edge-replicated margin          */
+/* (margin = roundUp(R,2) >= R, apps/QMIV/src/xAppQMIV.cpp:353, extend() at :899) = clamped index.  */
+/* The test pixel plus GCD is not clipped (xc_CLIP_CURR_TST_RANGE=false, xCommonDefIVQM.h:62).      */
+/* The per-row sums live in 32-bit lanes (_mm_add_epi32) and are sign-extended to 64 bits at the    */
+/* end of the row (:38-40); that is reproduced with uint32 wrap-around and an int32 cast.           */
+/* ----------------------------------------------------------------------------------------------- */
+void qo_cps(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, const int32_t gcd[4],
+            int32_t R, const int32_t cws[4], uint64_t* row_sse, uint16_t* scp)
+{
+  const int32_t  maxv = qo_max_value(bitdepth);
+  const size_t   pl   = (size_t)W * H;
+  for(int32_t y = 0; y < H; y++)
+  {
+    uint32_t rowsum[3] = { 0, 0, 0 };
+    for(int32_t x = 0; x < W; x++)
+    {
+      int32_t s[3];
+      for(int32_t c = 0; c < 3; c++) { s[c] = (int32_t)tst[c * pl + (size_t)y * W + x] + gcd[c]; }
+      int32_t  best_err     = INT32_MAX;
+      uint32_t best_dist[3] = { 0, 0, 0 };
+      int32_t  best_pel[3]  = { 0, 0, 0 };
+      for(int32_t dy = -R; dy <= R; dy++)
+      {
+        const int32_t yy = qo_clampi(y + dy, 0, H - 1);
+        for(int32_t dx = -R; dx <= R; dx++)
+        {
+          const int32_t xx = qo_clampi(x + dx, 0, W - 1);
+          uint32_t dist[3]; int32_t pel[3]; uint32_t err = 0;
+          for(int32_t c = 0; c < 3; c++)
+          {
+            pel[c]  = ref[c * pl + (size_t)yy * W + xx];
+            const uint32_t d = (uint32_t)(s[c] - pel[c]);
+            dist[c] = d * d;                          /* _mm_mullo_epi32, wraps */
+            err    += dist[c] * (uint32_t)cws[c];     /* _mm_mullo_epi32 + horizontal add, wraps */
+          }
+          if((int32_t)err < best_err)                 /* first strict minimum in raster order */
+          {
+            best_err = (int32_t)err;
+            for(int32_t c = 0; c < 3; c++) { best_dist[c] = dist[c]; best_pel[c] = pel[c]; }
+          }
+        }
+      }
+      for(int32_t c = 0; c < 3; c++) { rowsum[c] += best_dist[c]; }
+      if(scp)
+      {
+        for(int32_t c = 0; c < 3; c++)
+        {
+          int32_t v = best_pel[c] - gcd[c];
+          v = v < maxv ? v : maxv;                    /* _mm_min_epi32 */
+          v = v < 0 ? 0 : (v > 65535 ? 65535 : v);    /* _mm_packus_epi32 */
+          scp[c * pl + (size_t)y * W + x] = (uint16_t)v;
+        }
+      }
+    }
+    if(row_sse) { for(int32_t c = 0; c < 3; c++) { row_sse[(size_t)y * 3 + c] = (uint64_t)(int64_t)(int32_t)rowsum[c]; } }
+  }
+}
+
+/* Portable planar path, libs/pmbb-ivqm/src/xCorrespPixelShiftSTD.cpp:19-84: uint64 row accumulation. */
+void qo_cps_rows_std(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, const int32_t gcd[4],
+                     int32_t R, const int32_t cws[4], uint64_t* row_sse)
+{
+  const size_t pl = (size_t)W * H;
+  for(int32_t y = 0; y < H; y++)
+  {
+    uint64_t rowsum[3] = { 0, 0, 0 };
+    for(int32_t x = 0; x < W; x++)
+    {
+      int32_t s[3];
+      for(int32_t c = 0; c < 3; c++) { s[c] = (int32_t)tst[c * pl + (size_t)y * W + x] + gcd[c]; }
+      int32_t best_err = INT32_MAX; int32_t best_pel[3] = { 0, 0, 0 };
+      for(int32_t dy = -R; dy <= R; dy++)
+      {
+        const int32_t yy = qo_clampi(y + dy, 0, H - 1);
+        for(int32_t dx = -R; dx <= R; dx++)
+        {
+          const int32_t xx = qo_clampi(x + dx, 0, W - 1);
+          int32_t err = 0; int32_t pel[3];
+          for(int32_t c = 0; c < 3; c++)
+          {
+            pel[c] = ref[c * pl + (size_t)yy * W + xx];
+            const int32_t d = s[c] - pel[c];
+            err += d * d * cws[c];
+          }
+          if(err < best_err) { best_err = err; for(int32_t c = 0; c < 3; c++) { best_pel[c] = pel[c]; } }
+        }
+      }
+      for(int32_t c = 0; c < 3; c++) { const int32_t d = s[c] - best_pel[c]; rowsum[c] += (uint64_t)(int64_t)(d * d); }
+    }
+    for(int32_t c = 0; c < 3; c++) { row_sse[(size_t)y * 3 + c] = rowsum[c]; }
+  }
+}
+
+/* ----------------------------------------------------------------------------------------------- */
+/* a8: equirectangular weights, libs/pmbb-ivqm/src/xWeightedSpherically.cpp:13-29                   */
+/* ----------------------------------------------------------------------------------------------- */
+void qo_ws_weights(int32_t H, int32_t lat_range, double* w, double* correction)
+{
+  const double pi   = 3.14159265358979323846;              /* xc_Pi, xCommonDefCORE.h:227 */
+  const double heq  = 180.0 * (double)H / (double)lat_range;
+  const double off  = (heq - H) / 2.0;
+  qo_kbns k = { 0.0, 0.0 };
+  for(int32_t h = 0; h < H; h++)
+  {
+    w[h] = cos((h + off - (heq / 2 - 0.5)) * pi / heq);
+    qo_kbns_add(&k, w[h]);
+  }
+  if(correction) { *correction = H / qo_kbns_result(&k); }
+}
+
+/* ----------------------------------------------------------------------------------------------- */
+/* a9/a10: block-averaged SSIM, 8x8 windows at stride 4                                            */
+/* window: libs/pmbb-ivqm/src/xStructSimSTD.cpp:420-461 (AVX-512 CalcBlckAvg8 and                  */
+/*         CalcMultiBlckAvg8S4 give the same per-window value, test-xStructSim.cpp:169-170)         */
+/* loops:  libs/pmbb-ivqm/src/xSSIM.cpp:276-311 (ranges), :328-369 (row and picture KBNS)           */
+/* ERP:    libs/pmbb-ivqm/src/xIVSSIM.cpp:138-173 (row weight w[y + WndSize/2])                     */
+/* ----------------------------------------------------------------------------------------------- */
+static double qo_ssim_window(const uint16_t* t, const uint16_t* r, int32_t stride, double C1, double C2, int32_t calc_l)
+{
+  const double inv = 1.0 / 64.0;
+  int64_t sr = 0, st = 0, srr = 0, stt = 0, srt = 0;
+  for(int32_t y = 0; y < 8; y++)
+  {
+    for(int32_t x = 0; x < 8; x++)
+    {
+      const int32_t R = r[(size_t)y * stride + x], T = t[(size_t)y * stride + x];
+      sr += R; st += T; srr += R * R; stt += T * T; srt += R * T;
+    }
+  }
+  const double avg_r = (double)sr * inv;
+  const double avg_t = (double)st * inv;
+  const double var_r = (double)srr * inv - avg_r * avg_r;
+  const double var_t = (double)stt * inv - avg_t * avg_t;
+  const double cov   = (double)srt * inv - avg_r * avg_t;
+  const double cs    = (2 * cov + C2) / (var_r + var_t + C2);
+  if(!calc_l) { return cs; }
+  const double l = (2 * avg_r * avg_t + C1) / (avg_r * avg_r + avg_t * avg_t + C1);
+  return l * cs;
+}
+
+static int32_t qo_num_windows(int32_t len) { return len < 8 ? 0 : (len - 8) / 4 + 1; } /* xSSIM.cpp:496-519 */
+
+static void qo_ssim_consts(int32_t bitdepth, double* C1, double* C2)
+{
+  const double maxv = (double)qo_max_value(bitdepth);  /* xSSIM.cpp:165-167, K1=0.01, K2=0.03 */
+  const double a = 0.01 * maxv, b = 0.03 * maxv;
+  *C1 = a * a; *C2 = b * b;
+}
+
+void qo_ssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, int32_t calc_l,
+                 const double* ws_weights, double out[3])
+{
+  double C1, C2; qo_ssim_consts(bitdepth, &C1, &C2);
+  const int32_t nx = qo_num_windows(W), ny = qo_num_windows(H);
+  for(int32_t c = 0; c < 3; c++)
+  {
+    const uint16_t* t = tst + (size_t)c * W * H;
+    const uint16_t* r = ref + (size_t)c * W * H;
+    qo_kbns pic = { 0.0, 0.0 }, wacc = { 0.0, 0.0 };
+    for(int32_t j = 0; j < ny; j++)
+    {
+      const int32_t y = 4 * j;
+      qo_kbns row = { 0.0, 0.0 };
+      for(int32_t i = 0; i < nx; i++)
+      {
+        const size_t o = (size_t)y * W + 4 * i;
+        qo_kbns_add(&row, qo_ssim_window(t + o, r + o, W, C1, C2, calc_l));
+      }
+      double rs = qo_kbns_result(&row);
+      if(ws_weights) { const double wt = ws_weights[y + 4]; rs = rs * wt; qo_kbns_add(&wacc, wt); }
+      qo_kbns_add(&pic, rs);
+    }
+    const int64_t active = (int64_t)nx * ny;
+    if(ws_weights)
+    {
+      const double corr = qo_kbns_result(&wacc) / ny;
+      out[c] = qo_kbns_result(&pic) / ((double)active * corr);
+    }
+    else { out[c] = qo_kbns_result(&pic) / (double)active; }
+  }
+}
+
+/* ----------------------------------------------------------------------------------------------- */
+/* a11: MS-SSIM, libs/pmbb-ivqm/src/xSSIM.cpp:230-256, scales :520-532, exponents                  */
+/* libs/pmbb-ivqm/src/xStructSimConsts.h:42-49, downsampling xPixelOpsSTD.cpp:50-67                 */
+/* ----------------------------------------------------------------------------------------------- */
+static const double qo_ms_exponents[5][5] = {
+  { 1.0000, 0.0000, 0.0000, 0.0000, 0.0000 },
+  { 0.1356, 0.8644, 0.0000, 0.0000, 0.0000 },
+  { 0.0711, 0.4530, 0.4760, 0.0000, 0.0000 },
+  { 0.0517, 0.3295, 0.3462, 0.2726, 0.0000 },
+  { 0.0448, 0.2856, 0.3001, 0.2363, 0.1333 },
+};
+
+int32_t qo_num_scales(int32_t W, int32_t H)
+{
+  for(int32_t i = 0; i < 5; i++) { const int32_t lim = 32 << i; if(W < lim || H < lim) { return i; } }
+  return 5;
+}
+
+static void qo_downsample(uint16_t* dst, const uint16_t* src, int32_t W, int32_t H) /* dst (W>>1)x(H>>1) x3 */
+{
+  const int32_t dw = W >> 1, dh = H >> 1;
+  for(int32_t c = 0; c < 3; c++)
+  {
+    const uint16_t* s = src + (size_t)c * W * H;
+    uint16_t*       d = dst + (size_t)c * dw * dh;
+    for(int32_t y = 0; y < dh; y++)
+    {
+      for(int32_t x = 0; x < dw; x++)
+      {
+        const uint16_t* p = s + (size_t)(2 * y) * W + 2 * x;
+        d[(size_t)y * dw + x] = (uint16_t)(((int32_t)p[0] + p[1] + p[W] + p[W + 1] + 2) >> 2);
+      }
+    }
+  }
+}
+
+int qo_msssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, double out[3])
+{
+  const int32_t ns = qo_num_scales(W, H);
+  if(ns < 1) { return -1; }
+  double sub[5][3];
+  qo_ssim_pic(tst, ref, W, H, bitdepth, ns == 1, NULL, sub[0]);
+  uint16_t* bufT = NULL; uint16_t* bufR = NULL;
+  const uint16_t* curT = tst; const uint16_t* curR = ref;
+  int32_t w = W, h = H;
+  for(int32_t i = 1; i < ns; i++)
+  {
+    const int32_t nw = w >> 1, nh = h >> 1;
+    uint16_t* nT = (uint16_t*)malloc((size_t)nw * nh * 3 * sizeof(uint16_t));
+    uint16_t* nR = (uint16_t*)malloc((size_t)nw * nh * 3 * sizeof(uint16_t));
+    qo_downsample(nT, curT, w, h); qo_downsample(nR, curR, w, h);
+    free(bufT); free(bufR); bufT = nT; bufR = nR; curT = nT; curR = nR; w = nw; h = nh;
+    qo_ssim_pic(curT, curR, w, h, bitdepth, i == ns - 1, NULL, sub[i]);
+  }
+  free(bufT); free(bufR);
+  for(int32_t c = 0; c < 3; c++)
+  {
+    double score = 1.0;
+    for(int32_t i = 0; i < ns; i++)
+    {
+      const double v = sub[i][c] < 0 ? 0.0 : sub[i][c];   /* getVecReLU, xVec.h:297 */
+      score *= pow(v, qo_ms_exponents[ns - 1][i]);
+    }
+    out[c] = score;
+  }
+  return 0;
+}
+
+/* ----------------------------------------------------------------------------------------------- */
+/* a6: IV-PSNR of one direction from per-row CPS SSE, libs/pmbb-ivqm/src/xIVPSNR.cpp:163-189        */
+/* ----------------------------------------------------------------------------------------------- */
+static double qo_ivpsnr_quality(const uint64_t* row_sse, int32_t W, int32_t H, int32_t bitdepth, const double* ws, const int32_t cwa[4])
+{
+  double err[3];
+  if(ws)
+  {
+    for(int32_t c = 0; c < 3; c++)
+    {
+      qo_kbns k = { 0.0, 0.0 };
+      for(int32_t y = 0; y < H; y++) { qo_kbns_add(&k, (double)row_sse[(size_t)y * 3 + c] * ws[y]); }
+      err[c] = qo_kbns_result(&k);
+    }
+  }
+  else
+  {
+    for(int32_t c = 0; c < 3; c++)
+    {
+      uint64_t s = 0;
+      for(int32_t y = 0; y < H; y++) { s += row_sse[(size_t)y * 3 + c]; }
+      err[c] = (double)s;
+    }
+  }
+  const int64_t area = (int64_t)W * H;
+  double q[4] = { 0, 0, 0, 0 };
+  for(int32_t c = 0; c < 3; c++) { q[c] = qo_psnr_from_ssd(err[c] > 0 ? err[c] : 1.0, area, bitdepth); }
+  const int32_t wsum = cwa[0] + cwa[1] + cwa[2] + cwa[3];
+  const double  inv  = 1.0 / (double)wsum;
+  return (q[0] * (double)cwa[0] + q[1] * (double)cwa[1] + q[2] * (double)cwa[2] + q[3] * (double)cwa[3]) * inv;
+}
+
+/* ----------------------------------------------------------------------------------------------- */
+/* Full frame pipeline, apps/QMIV/src/xAppQMIV.cpp:761-827 and the calcFrame* functions :927-1108   */
+/* ----------------------------------------------------------------------------------------------- */
+int qo_compute_pair(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,
+                    qo_result* out, uint16_t* scp0, uint16_t* scp1)
+{
+  const int32_t W = p->width, H = p->height, BD = p->bitdepth;
+  const size_t  n = (size_t)W * H * 3;
+  const int64_t area = (int64_t)W * H;
+  memset(out, 0, sizeof(*out));
+
+  uint16_t* P0 = (uint16_t*)malloc(n * sizeof(uint16_t));
+  uint16_t* P1 = (uint16_t*)malloc(n * sizeof(uint16_t));
+  qo_unpack444(planes0, W, H, BD, p->chroma_format, P0);
+  qo_unpack444(planes1, W, H, BD, p->chroma_format, P1);
+
+  int32_t exact[3];
+  for(int32_t c = 0; c < 3; c++) /* equalCmp, xAppQMIV.cpp:894-897 */
+  {
+    exact[c] = memcmp(P0 + (size_t)c * W * H, P1 + (size_t)c * W * H, (size_t)W * H * sizeof(uint16_t)) == 0;
+    out->exact[c] = exact[c];
+  }
+
+  double* ws = NULL; double ws_corr = 1.0;
+  if(p->erp) { ws = (double*)malloc((size_t)H * sizeof(double)); qo_ws_weights(H, p->lat_range, ws, &ws_corr); }
+
+  const double inv_cwa = 1.0 / (double)(p->cwa[0] + p->cwa[1] + p->cwa[2] + p->cwa[3]);
+  #define QO_PER_PIC(v) (((v)[0] * p->cwa[0] + (v)[1] * p->cwa[1] + (v)[2] * p->cwa[2]) * inv_cwa) /* xMetricQMIV.cpp:91-97 */
+  #define QO_PER_PIC4(v) (((v)[0] * (double)p->cwa[0] + (v)[1] * (double)p->cwa[1] + (v)[2] * (double)p->cwa[2] + 0.0 * (double)p->cwa[3]) * inv_cwa) /* xIVSSIM.cpp:51-52 */
+
+  const int need_scp = (mask & (QO_IVSSIM | QO_IVMSSSIM)) || scp0 || scp1;
+  const int need_gcd = (mask & (QO_IVPSNR | QO_IVSSIM | QO_IVMSSSIM)) || need_scp;
+  int32_t gcd[4] = { 0, 0, 0, 0 }, ngcd[4];
+  if(need_gcd) { qo_gcd(P1, P0, W, H, BD, p->unc, gcd); } /* argument swap, xGlobClrDiff.h:41 */
+  for(int32_t c = 0; c < 4; c++) { out->gcd_r2t[c] = gcd[c]; ngcd[c] = -gcd[c]; }
+
+  uint16_t* S0 = NULL; uint16_t* S1 = NULL;
+  if(need_scp) /* xShftCompPic.cpp:219-228 via xAppQMIV.cpp:934-948 */
+  {
+    S0 = (uint16_t*)malloc(n * sizeof(uint16_t));
+    S1 = (uint16_t*)malloc(n * sizeof(uint16_t));
+    qo_cps(P0, P1, W, H, BD, gcd, p->search_range, p->cws, NULL, S1);
+    qo_cps(P1, P0, W, H, BD, ngcd, p->search_range, p->cws, NULL, S0);
+    if(scp0) { memcpy(scp0, S0, n * sizeof(uint16_t)); }
+    if(scp1) { memcpy(scp1, S1, n * sizeof(uint16_t)); }
+  }
+
+  const double fake = qo_psnr_from_ssd(1, area, BD); /* xPSNR.h:55 */
+  if(mask & (QO_PSNR | QO_WSPSNR))
+  {
+    uint64_t ssd[3] = { 0, 0, 0 };
+    for(int32_t c = 0; c < 3; c++)
+    {
+      const uint16_t* a = P0 + (size_t)c * W * H; const uint16_t* b = P1 + (size_t)c * W * H;
+      for(size_t i = 0; i < (size_t)W * H; i++) { const int64_t d = (int64_t)a[i] - b[i]; ssd[c] += (uint64_t)(d * d); }
+    }
+    if(mask & QO_PSNR) /* xPSNR.cpp:146-152, fake values xAppQMIV.cpp:974-981 */
+    {
+      for(int32_t c = 0; c < 3; c++) { out->psnr[c] = exact[c] ? fake : qo_psnr_from_ssd((double)ssd[c], area, BD); }
+      out->psnr_pic = QO_PER_PIC(out->psnr);
+    }
+    if(mask & QO_WSPSNR) /* xWSPSNR.cpp:48-81, :112-138 */
+    {
+      for(int32_t c = 0; c < 3; c++)
+      {
+        double v;
+        if(!ws) { v = qo_psnr_from_ssd((double)ssd[c], area, BD); }
+        else
+        {
+          const uint16_t* a = P0 + (size_t)c * W * H; const uint16_t* b = P1 + (size_t)c * W * H;
+          qo_kbns k = { 0.0, 0.0 };
+          for(int32_t y = 0; y < H; y++)
+          {
+            uint64_t rs = 0;
+            for(int32_t x = 0; x < W; x++) { const int64_t d = (int64_t)a[(size_t)y * W + x] - b[(size_t)y * W + x]; rs += (uint64_t)(d * d); }
+            qo_kbns_add(&k, (double)rs * ws[y]);
+          }
+          const double e = qo_kbns_result(&k) * ws_corr;
+          v = qo_psnr_from_ssd(e, area, BD);
+        }
+        out->wspsnr[c] = exact[c] ? fake : v;
+      }
+      out->wspsnr_pic = QO_PER_PIC(out->wspsnr);
+    }
+  }
+
+  if(mask & QO_IVPSNR) /* xIVPSNR.cpp:109-121 */
+  {
+    uint64_t* rows = (uint64_t*)malloc((size_t)H * 3 * sizeof(uint64_t));
+    qo_cps(P0, P1, W, H, BD, gcd, p->search_range, p->cws, rows, NULL);
+    const double r2t = qo_ivpsnr_quality(rows, W, H, BD, ws, p->cwa);
+    qo_cps(P1, P0, W, H, BD, ngcd, p->search_range, p->cws, rows, NULL);
+    const double t2r = qo_ivpsnr_quality(rows, W, H, BD, ws, p->cwa);
+    free(rows);
+    out->ivpsnr_r2t = r2t; out->ivpsnr_t2r = t2r;
+    out->ivpsnr = t2r < r2t ? t2r : r2t; /* std::min */
+  }
+
+  if(mask & QO_SSIM) /* xSSIM.h:83 -> xSSIM.cpp:315-352, no ERP weighting */
+  {
+    qo_ssim_pic(P0, P1, W, H, BD, 1, NULL, out->ssim);
+    out->ssim_pic = QO_PER_PIC(out->ssim);
+  }
+  int rc = 0;
+  if(mask & QO_MSSSIM)
+  {
+    rc |= qo_msssim_pic(P0, P1, W, H, BD, out->msssim);
+    out->msssim_pic = QO_PER_PIC(out->msssim);
+  }
+  if(mask & QO_IVSSIM) /* xIVSSIM.cpp:31-61 */
+  {
+    double t2r[3], r2t[3];
+    qo_ssim_pic(P0, S1, W, H, BD, 1, ws, t2r);
+    qo_ssim_pic(P1, S0, W, H, BD, 1, ws, r2t);
+    out->ivssim_t2r = QO_PER_PIC4(t2r); out->ivssim_r2t = QO_PER_PIC4(r2t);
+    out->ivssim = out->ivssim_r2t < out->ivssim_t2r ? out->ivssim_r2t : out->ivssim_t2r;
+  }
+  if(mask & QO_IVMSSSIM) /* xIVSSIM.cpp:62-92, no ERP weighting */
+  {
+    double t2r[3], r2t[3];
+    rc |= qo_msssim_pic(P0, S1, W, H, BD, t2r);
+    rc |= qo_msssim_pic(P1, S0, W, H, BD, r2t);
+    out->ivmsssim_t2r = QO_PER_PIC4(t2r); out->ivmsssim_r2t = QO_PER_PIC4(r2t);
+    out->ivmsssim = out->ivmsssim_r2t < out->ivmsssim_t2r ? out->ivmsssim_r2t : out->ivmsssim_t2r;
+  }
+  #undef QO_PER_PIC
+  #undef QO_PER_PIC4
+
+  free(P0); free(P1); free(S0); free(S1); free(ws);
+  return rc;
+}

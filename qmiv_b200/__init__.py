@@ -1,0 +1,277 @@
+"""qmiv_b200 — the QMIV metric hot path (GCD, CPS search, PSNR / WS-PSNR / IV-PSNR, SSIM / MS-SSIM /
+IV-SSIM / IV-MS-SSIM) on B200 GPUs, through the C ABI of libqmiv_b200.so (include/qmiv_gpu.h).
+
+The Python classes mirror the reference's pmbb-ivqm processors:
+
+    reference (libs/pmbb-ivqm/src)                     here
+    xGlobClrDiffProc::CalcGlobalColorDiff(T, R)        Calc.calc_global_color_diff(f0, f1)
+    xShftCompPicProc::GenShftCompPics(...)             Calc.gen_shft_comp_pics(f0, f1)
+    xPSNR::calcPicPSNR / xWSPSNR::calcPicWSPSNR        Calc.calc_pic_psnr / calc_pic_wspsnr
+    xIVPSNR::calcPicIVPSNR(T, R, GCD)                  Calc.calc_pic_ivpsnr(f0, f1)
+    xSSIM::calcPicSSIM / calcPicMSSSIM                 Calc.calc_pic_ssim / calc_pic_msssim
+    xIVSSIM::calcPicIVSSIM / calcPicIVMSSSIM           Calc.calc_pic_ivssim / calc_pic_ivmsssim
+    one frame of xAppQMIV::processAllFrames            Calc.compute(f0, f1, metrics)
+
+A frame is a sequence of three planes (Y, Cb, Cr): numpy arrays (host memory) or CUDA tensors /
+objects exposing __cuda_array_interface__ (device memory), uint8 for bit depth <= 8, else uint16.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (ALL, IVMSSSIM, IVPSNR, IVSSIM, METRIC_BITS, MSSSIM, PSNR, SSIM, WSPSNR, PEL_CNCL, PEL_SKIP,
+                   PEL_STOP, PEL_WARN, QmivError, check)
+
+__all__ = ["Context", "Calc", "Batch", "make_params", "metric_mask", "QmivError", "library",
+           "PSNR", "WSPSNR", "IVPSNR", "SSIM", "MSSSIM", "IVSSIM", "IVMSSSIM", "ALL"]
+
+
+def library():
+    """The loaded libqmiv_b200.so (ctypes.CDLL)."""
+    return _lib.load()
+
+
+def metric_mask(metrics) -> int:
+    if metrics is None:
+        return ALL
+    if isinstance(metrics, int):
+        return metrics
+    if isinstance(metrics, str):
+        metrics = [m.strip() for m in metrics.split(",") if m.strip()]
+    m = 0
+    for name in metrics:
+        key = name.upper().replace("-", "").replace("_", "")
+        if key not in METRIC_BITS:
+            raise ValueError(f"unknown metric {name!r}")
+        m |= METRIC_BITS[key]
+    return m
+
+
+def make_params(search_range=2, cws=(4, 1, 1, 0), cwa=(4, 1, 1, 0), unc=(0.01, 0.01, 0.01, 0.0), erp=False,
+                lon_range=360, lat_range=180, invalid_pel_action=PEL_STOP) -> _lib.QmivParams:
+    p = _lib.QmivParams()
+    library().qmiv_params_default(ctypes.byref(p))
+    p.search_range = search_range
+    p.cws = (ctypes.c_int32 * 4)(*cws)
+    p.cwa = (ctypes.c_int32 * 4)(*cwa)
+    p.unc = (ctypes.c_float * 4)(*unc)
+    p.erp = int(bool(erp))
+    p.lon_range_deg = lon_range
+    p.lat_range_deg = lat_range
+    p.invalid_pel_action = invalid_pel_action
+    return p
+
+
+def _plane_info(plane):
+    """(pointer, pitch in bytes, mem kind, keep-alive object) of one plane."""
+    cai = getattr(plane, "__cuda_array_interface__", None)
+    if cai is not None:
+        shape, strides = cai["shape"], cai.get("strides")
+        itemsize = np.dtype(cai["typestr"]).itemsize
+        if strides is None:
+            pitch = shape[1] * itemsize if len(shape) > 1 else shape[0] * itemsize
+        else:
+            if len(strides) > 1 and strides[1] != itemsize:
+                raise ValueError("device plane rows must be contiguous")
+            pitch = strides[0]
+        return cai["data"][0], pitch, _lib.MEM_DEVICE, plane
+    arr = np.asarray(plane)
+    if arr.ndim != 2:
+        raise ValueError("a plane must be 2-D")
+    if arr.strides[1] != arr.itemsize:
+        arr = np.ascontiguousarray(arr)
+    return arr.ctypes.data, arr.strides[0], _lib.MEM_HOST, arr
+
+
+def make_frame(planes: Sequence) -> tuple[_lib.QmivFrame, list]:
+    if len(planes) != 3:
+        raise ValueError("a frame has three planes (Y, Cb, Cr)")
+    f = _lib.QmivFrame()
+    keep, mems = [], set()
+    for c, pl in enumerate(planes):
+        ptr, pitch, mem, k = _plane_info(pl)
+        f.plane[c] = ptr
+        f.pitch[c] = pitch
+        mems.add(mem)
+        keep.append(k)
+    if len(mems) != 1:
+        raise ValueError("all planes of a frame must live in the same memory")
+    f.mem = mems.pop()
+    return f, keep
+
+
+class Context:
+    """Device + HBM budget (qmiv_ctx_create)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self._lib = library()
+        h = ctypes.c_void_p()
+        check(self._lib.qmiv_ctx_create(device, hbm_budget, ctypes.byref(h)), "qmiv_ctx_create")
+        self.handle = h
+        self.device = device
+
+    def memory(self):
+        used, budget = ctypes.c_uint64(), ctypes.c_uint64()
+        check(self._lib.qmiv_ctx_memory(self.handle, ctypes.byref(used), ctypes.byref(budget)), "qmiv_ctx_memory")
+        return used.value, budget.value
+
+    def close(self):
+        if self.handle:
+            check(self._lib.qmiv_ctx_destroy(self.handle), "qmiv_ctx_destroy")
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Calc:
+    """A metric calculator for one picture shape (qmiv_calc_create)."""
+
+    def __init__(self, ctx: Context, width: int, height: int, bitdepth: int, chroma_format: int = 420, **params):
+        self._lib = library()
+        self.ctx = ctx
+        self.width, self.height, self.bitdepth, self.chroma_format = width, height, bitdepth, chroma_format
+        self.params = make_params(**params)
+        h = ctypes.c_void_p()
+        check(self._lib.qmiv_calc_create(ctx.handle, width, height, bitdepth, chroma_format,
+                                         ctypes.byref(self.params), ctypes.byref(h)), "qmiv_calc_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            check(self._lib.qmiv_calc_destroy(self.handle), "qmiv_calc_destroy")
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- full pipeline -------------------------------------------------------------------------
+    def compute(self, frame0, frame1, metrics=None) -> dict:
+        f0, k0 = make_frame(frame0)
+        f1, k1 = make_frame(frame1)
+        res = _lib.QmivResult()
+        check(self._lib.qmiv_frame_pair_compute(self.handle, ctypes.byref(f0), ctypes.byref(f1),
+                                                metric_mask(metrics), ctypes.byref(res)), "qmiv_frame_pair_compute")
+        return res.as_dict()
+
+    def submit(self, frame0, frame1, metrics=None):
+        f0, k0 = make_frame(frame0)
+        f1, k1 = make_frame(frame1)
+        self._inflight = (k0, k1)
+        check(self._lib.qmiv_frame_pair_submit(self.handle, ctypes.byref(f0), ctypes.byref(f1), metric_mask(metrics)),
+              "qmiv_frame_pair_submit")
+
+    def wait(self, timeout_ms: int = -1) -> dict:
+        res = _lib.QmivResult()
+        check(self._lib.qmiv_frame_pair_wait(self.handle, timeout_ms, ctypes.byref(res)), "qmiv_frame_pair_wait")
+        self._inflight = None
+        return res.as_dict()
+
+    # ---- processor-style calls -----------------------------------------------------------------
+    def calc_global_color_diff(self, frame0, frame1) -> list:
+        f0, k0 = make_frame(frame0)
+        f1, k1 = make_frame(frame1)
+        out = (ctypes.c_int32 * 4)()
+        check(self._lib.qmiv_calc_gcd(self.handle, ctypes.byref(f0), ctypes.byref(f1), out), "qmiv_calc_gcd")
+        return list(out)
+
+    def gen_shft_comp_pics(self, frame0, frame1):
+        """(SCP0, SCP1) as host uint16 arrays of shape (3, H, W)."""
+        f0, k0 = make_frame(frame0)
+        f1, k1 = make_frame(frame1)
+        shp = (3, self.height, self.width)
+        s0, s1 = np.zeros(shp, np.uint16), np.zeros(shp, np.uint16)
+        check(self._lib.qmiv_calc_scp(self.handle, ctypes.byref(f0), ctypes.byref(f1), None,
+                                      s0.ctypes.data_as(ctypes.c_void_p), s1.ctypes.data_as(ctypes.c_void_p),
+                                      _lib.MEM_HOST), "qmiv_calc_scp")
+        return s0, s1
+
+    def cps_rows(self):
+        """Per-row CPS SSE (H, 3) of the last computed pair, (R2T, T2R)."""
+        a = np.zeros((self.height, 3), np.uint64)
+        b = np.zeros((self.height, 3), np.uint64)
+        check(self._lib.qmiv_calc_cps_rows(self.handle, a.ctypes.data_as(ctypes.c_void_p),
+                                           b.ctypes.data_as(ctypes.c_void_p)), "qmiv_calc_cps_rows")
+        return a, b
+
+    def calc_pic_psnr(self, frame0, frame1):
+        r = self.compute(frame0, frame1, PSNR)
+        return r["psnr"][:3]
+
+    def calc_pic_wspsnr(self, frame0, frame1):
+        r = self.compute(frame0, frame1, WSPSNR)
+        return r["wspsnr"][:3]
+
+    def calc_pic_ivpsnr(self, frame0, frame1):
+        return self.compute(frame0, frame1, IVPSNR)["ivpsnr"]
+
+    def calc_pic_ssim(self, frame0, frame1):
+        return self.compute(frame0, frame1, SSIM)["ssim"][:3]
+
+    def calc_pic_msssim(self, frame0, frame1):
+        return self.compute(frame0, frame1, MSSSIM)["msssim"][:3]
+
+    def calc_pic_ivssim(self, frame0, frame1):
+        return self.compute(frame0, frame1, IVSSIM)["ivssim"]
+
+    def calc_pic_ivmsssim(self, frame0, frame1):
+        return self.compute(frame0, frame1, IVMSSSIM)["ivmsssim"]
+
+
+class Batch:
+    """Many frame pairs of uneven shape per call (qmiv_batch_*)."""
+
+    def __init__(self, ctx: Context, max_pairs: int, max_pixels: int, use_graph: bool = True, **params):
+        self._lib = library()
+        self.ctx = ctx
+        self.params = make_params(**params)
+        h = ctypes.c_void_p()
+        check(self._lib.qmiv_batch_create(ctx.handle, max_pairs, max_pixels, ctypes.byref(self.params),
+                                          int(bool(use_graph)), ctypes.byref(h)), "qmiv_batch_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            check(self._lib.qmiv_batch_destroy(self.handle), "qmiv_batch_destroy")
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def compute(self, pairs: Iterable[dict]) -> list[dict]:
+        """pairs: dicts with frame0, frame1, width, height, bitdepth, chroma_format, search_range, metrics."""
+        pairs = list(pairs)
+        descs = (_lib.QmivPairDesc * max(1, len(pairs)))()
+        keep = []
+        for i, p in enumerate(pairs):
+            f0, k0 = make_frame(p["frame0"])
+            f1, k1 = make_frame(p["frame1"])
+            keep += [k0, k1]
+            d = descs[i]
+            d.in0, d.in1 = f0, f1
+            d.width, d.height, d.bitdepth = p["width"], p["height"], p["bitdepth"]
+            d.chroma_format = p.get("chroma_format", 420)
+            d.search_range = p.get("search_range", 2)
+            d.metric_mask = metric_mask(p.get("metrics"))
+        out = (_lib.QmivResult * max(1, len(pairs)))()
+        check(self._lib.qmiv_batch_compute(self.handle, descs, len(pairs), out), "qmiv_batch_compute")
+        return [out[i].as_dict() for i in range(len(pairs))]
+
+    def tuning(self, width, height, bitdepth, search_range):
+        tw, th, p = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.qmiv_batch_tuning(self.handle, width, height, bitdepth, search_range, ctypes.byref(tw),
+                                          ctypes.byref(th), ctypes.byref(p)), "qmiv_batch_tuning")
+        return tw.value, th.value, p.value

@@ -1,0 +1,478 @@
+// Plain form: one frame pair per call (qmiv_calc_* entry points) on top of PairPipeline, the
+// device pipeline of one frame pair that the batched form reuses.
+#include "qmiv_host.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <thread>
+
+namespace qmiv {
+
+// ---------------------------------------------------------------------------------------------
+// shape / parameter validation
+// ---------------------------------------------------------------------------------------------
+qmiv_status Shape::init(int32_t W_, int32_t H_, int32_t bd, int32_t cf)
+{
+  if(W_ <= 0 || H_ <= 0) { return fail(QMIV_ERR_INVALID_ARG, "picture size must be positive"); }
+  if(bd < 1 || bd > 16) { return fail(QMIV_ERR_INVALID_ARG, "bit depth must be in 1..16"); }
+  if(cf != 420 && cf != 422 && cf != 444) { return fail(QMIV_ERR_UNSUPPORTED, "chroma format must be 420, 422 or 444"); }
+  W = W_; H = H_; bitdepth = bd; chroma_format = cf;
+  sx = cf == 444 ? 0 : 1;
+  sy = cf == 420 ? 1 : 0;
+  if((sx && (W & 1)) || (sy && (H & 1))) { return fail(QMIV_ERR_INVALID_ARG, "subsampled chroma needs even picture dimensions"); }
+  cw = W >> sx; ch = H >> sy;
+  esz = bd <= 8 ? 1 : 2;
+  maxv = (1 << bd) - 1;
+  return QMIV_OK;
+}
+
+qmiv_status validate_params(const qmiv_params& p)
+{
+  if(p.search_range < 1 || p.search_range > 5) { return fail(QMIV_ERR_UNSUPPORTED, "search range must be 1..5"); }
+  if(p.cws[3] != 0) { return fail(QMIV_ERR_UNSUPPORTED, "the fourth search weight must be 0"); }
+  for(int c = 0; c < 3; c++) { if(p.cws[c] < 0 || p.cwa[c] < 0) { return fail(QMIV_ERR_INVALID_ARG, "weights must be >= 0"); } }
+  if(p.cwa[0] + p.cwa[1] + p.cwa[2] + p.cwa[3] <= 0) { return fail(QMIV_ERR_INVALID_ARG, "averaging weights sum to 0"); }
+  if(p.ssim_window != 8 || p.ssim_stride != 4) { return fail(QMIV_ERR_UNSUPPORTED, "only BlockAveraged SSIM with 8x8 windows at stride 4 is implemented"); }
+  if(p.erp && (p.lat_range_deg <= 0 || p.lat_range_deg > 180)) { return fail(QMIV_ERR_INVALID_ARG, "lat range must be in 1..180"); }
+  if(p.invalid_pel_action < QMIV_PEL_SKIP || p.invalid_pel_action > QMIV_PEL_CNCL) { return fail(QMIV_ERR_INVALID_ARG, "bad invalid pixel action"); }
+  return QMIV_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// PairPipeline
+// ---------------------------------------------------------------------------------------------
+PairPipeline::~PairPipeline()
+{
+  if(h_out) { cudaFreeHost(h_out); h_out = nullptr; }
+}
+
+qmiv_status PairPipeline::configure(qmiv_ctx_s* ctx, const Shape& shape, const qmiv_params& prm, int32_t search_range)
+{
+  ctx_ = ctx; shape_ = shape; prm_ = prm; R_ = search_range;
+  for(int c = 0; c < 4; c++) { maxdiff_[c] = round_f32_half_away(prm.unc[c] * (float)shape.maxv); }  // xGlobClrDiff.cpp:76
+  fp32_ok_ = cps_fp32_exact(shape.maxv, prm.cws, maxdiff_);
+  ns_ = num_scales(shape.W, shape.H);
+  int32_t w = shape.W, h = shape.H;
+  for(int s = 0; s < 5; s++)
+  {
+    nx_[s] = w >= 8 ? (w - 8) / 4 + 1 : 0;   // xSSIM::xCalcNumBlocks for 8/4
+    ny_[s] = h >= 8 ? (h - 8) / 4 + 1 : 0;
+    w >>= 1; h >>= 1;
+  }
+  nyp_ = (ny_[0] + 31) & ~31;
+  const double maxd = (double)shape.maxv;  // xSSIM.cpp:165-167
+  const double k1 = 0.01 * maxd, k2 = 0.03 * maxd;
+  C1_ = k1 * k1; C2_ = k2 * k2;
+  if(prm.erp) { ws_weights(shape.H, prm.lat_range_deg, ws_host_, ws_corr_); }
+  ws_uploaded_ = false;
+  if(!h_out) { QMIV_CUDA(cudaMallocHost((void**)&h_out, sizeof(PairOut))); }
+  std::memset(h_out, 0, sizeof(PairOut));
+  return QMIV_OK;
+}
+
+qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames)
+{
+  const Shape& S = shape_;
+  const size_t rows_total = (size_t)S.H + 2 * (size_t)S.ch;
+  QMIV_TRY(row_sd_.ensure(ctx_, rows_total * sizeof(int64_t)));
+  QMIV_TRY(row_ssd_.ensure(ctx_, rows_total * sizeof(uint64_t)));
+  QMIV_TRY(out_.ensure(ctx_, sizeof(PairOut)));
+  const bool need_scp = want_scp || (mask & (QMIV_IVSSIM | QMIV_IVMSSSIM));
+  const bool need_search = need_scp || (mask & QMIV_IVPSNR);
+  const bool need_ssim = mask & (QMIV_SSIM | QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM);
+  const bool need_ms = mask & (QMIV_MSSSIM | QMIV_IVMSSSIM);
+  if(need_search) { QMIV_TRY(cps_rows_.ensure(ctx_, (size_t)2 * S.H * 3 * sizeof(uint32_t))); }
+  if(need_scp) { QMIV_TRY(scp_.ensure(ctx_, (size_t)2 * 3 * S.W * S.H * S.esz)); }
+  if(prm_.erp)
+  {
+    QMIV_TRY(ws_.ensure(ctx_, (size_t)S.H * sizeof(double)));
+    if(!ws_uploaded_) { QMIV_CUDA(cudaMemcpy(ws_.p, ws_host_.data(), S.H * sizeof(double), cudaMemcpyHostToDevice)); ws_uploaded_ = true; }
+  }
+  if(need_ssim)
+  {
+    if(nx_[0] < 1 || ny_[0] < 1) { return fail(QMIV_ERR_INVALID_ARG, "picture smaller than one 8x8 SSIM window"); }
+    QMIV_TRY(win_.ensure(ctx_, (size_t)3 * nx_[0] * nyp_ * sizeof(double)));
+    QMIV_TRY(rowsum_.ensure(ctx_, (size_t)kMaxSsimSlots * 3 * ny_[0] * sizeof(double)));
+  }
+  if(need_ms)
+  {
+    if(ns_ < 1) { return fail(QMIV_ERR_INVALID_ARG, "picture too small for MS-SSIM (needs >= 32x32)"); }
+    size_t lv = 0;
+    for(int s = 1; s < ns_; s++) { lv += (size_t)(S.W >> s) * (S.H >> s) * 3; }
+    QMIV_TRY(pyr_.ensure(ctx_, 4 * lv * S.esz));
+  }
+  if(host_frames) { QMIV_TRY(staging_.ensure(ctx_, 2 * S.frame_bytes())); }
+  return QMIV_OK;
+}
+
+qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cudaStream_t s)
+{
+  const Shape& S = shape_;
+  if(!f) { return fail(QMIV_ERR_INVALID_ARG, "frame is null"); }
+  size_t off = (size_t)which * S.frame_bytes();
+  for(int c = 0; c < 3; c++)
+  {
+    if(!f->plane[c]) { return fail(QMIV_ERR_INVALID_ARG, "frame plane is null"); }
+    const size_t row_bytes = S.plane_cols(c) * S.esz;
+    if(f->pitch[c] < (int64_t)row_bytes || (f->pitch[c] % (int64_t)S.esz) != 0) { return fail(QMIV_ERR_INVALID_ARG, "bad plane pitch"); }
+    out.sx[c] = c ? (int8_t)S.sx : 0;
+    out.sy[c] = c ? (int8_t)S.sy : 0;
+    if(f->mem == QMIV_MEM_DEVICE)
+    {
+      out.p[c] = f->plane[c];
+      out.pitch[c] = (int32_t)(f->pitch[c] / (int64_t)S.esz);
+    }
+    else if(f->mem == QMIV_MEM_HOST)
+    {
+      if(!staging_.p) { return fail(QMIV_ERR_INVALID_ARG, "staging not prepared"); }
+      char* dst = staging_.as<char>() + off;
+      QMIV_CUDA(cudaMemcpy2DAsync(dst, row_bytes, f->plane[c], (size_t)f->pitch[c], row_bytes, S.plane_rows(c), cudaMemcpyHostToDevice, s));
+      out.p[c] = dst;
+      out.pitch[c] = (int32_t)S.plane_cols(c);
+      off += row_bytes * S.plane_rows(c);
+    }
+    else { return fail(QMIV_ERR_INVALID_ARG, "frame mem must be QMIV_MEM_HOST or QMIV_MEM_DEVICE"); }
+  }
+  return QMIV_OK;
+}
+
+const void* PairPipeline::scp(int which) const
+{
+  if(!scp_.p) { return nullptr; }
+  return scp_.as<char>() + (size_t)which * 3 * shape_.W * shape_.H * shape_.esz;
+}
+
+FinishInfo PairPipeline::finish_info(uint32_t mask) const
+{
+  FinishInfo fi{};
+  fi.W = shape_.W; fi.H = shape_.H; fi.bitdepth = shape_.bitdepth; fi.mask = mask;
+  fi.erp = prm_.erp; fi.ws_corr = ws_corr_;
+  for(int c = 0; c < 4; c++) { fi.cwa[c] = prm_.cwa[c]; }
+  fi.num_scales = ns_;
+  return fi;
+}
+
+qmiv_status PairPipeline::enqueue(const Img& in0, const Img& in1, uint32_t mask, bool want_scp, bool want_gcd, cudaStream_t s)
+{
+  return shape_.esz == 1 ? enqueue_t<uint8_t>(in0, in1, mask, want_scp, want_gcd, s)
+                         : enqueue_t<uint16_t>(in0, in1, mask, want_scp, want_gcd, s);
+}
+
+static Img img444(const void* base, int32_t W, int32_t H, size_t esz)
+{
+  Img im{};
+  for(int c = 0; c < 3; c++)
+  {
+    im.p[c] = static_cast<const char*>(base) + (size_t)c * W * H * esz;
+    im.pitch[c] = W; im.sx[c] = 0; im.sy[c] = 0;
+  }
+  return im;
+}
+static MutImg mut444(void* base, int32_t W, int32_t H, size_t esz)
+{
+  MutImg im{};
+  for(int c = 0; c < 3; c++) { im.p[c] = static_cast<char*>(base) + (size_t)c * W * H * esz; im.pitch[c] = W; }
+  return im;
+}
+
+template <typename T>
+qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mask, bool want_scp, bool want_gcd, cudaStream_t s)
+{
+  const Shape& S = shape_;
+  const bool need_scp = want_scp || (mask & (QMIV_IVSSIM | QMIV_IVMSSSIM));
+  const bool need_search = need_scp || (mask & QMIV_IVPSNR);
+  const uint32_t clip = prm_.invalid_pel_action == QMIV_PEL_CNCL ? (uint32_t)S.maxv : 0xffffu;
+  PairOut* dout = out_.as<PairOut>();
+
+  QMIV_CUDA(cudaMemsetAsync(dout, 0, sizeof(PairOut), s));
+  if(need_search) { QMIV_CUDA(cudaMemsetAsync(cps_rows_.p, 0, (size_t)2 * S.H * 3 * sizeof(uint32_t), s)); }
+
+  // 1. prepass + reduce (GCD)
+  PrepassArgs pa{};
+  pa.in0 = in0; pa.in1 = in1;
+  for(int c = 0; c < 3; c++) { pa.rows[c] = (int32_t)S.plane_rows(c); pa.cols[c] = (int32_t)S.plane_cols(c); }
+  pa.clip = clip; pa.row_sd = row_sd_.as<int64_t>(); pa.row_ssd = row_ssd_.as<uint64_t>(); pa.out = dout;
+  QMIV_CUDA(launch_prepass<T>(pa, s));
+
+  ReduceArgs ra{};
+  for(int c = 0; c < 3; c++) { ra.rows[c] = pa.rows[c]; ra.mult[c] = c ? (1 << (S.sx + S.sy)) : 1; }
+  ra.area = (int64_t)S.W * S.H; ra.maxv = S.maxv;
+  for(int c = 0; c < 4; c++) { ra.maxdiff[c] = maxdiff_[c]; }
+  ra.need_gcd = need_search || want_gcd; ra.fp32_ok = fp32_ok_; ra.clip_on = prm_.invalid_pel_action == QMIV_PEL_CNCL;
+  ra.row_sd = pa.row_sd; ra.row_ssd = pa.row_ssd; ra.out = dout;
+  QMIV_CUDA(launch_reduce(ra, s));
+
+  // 2. CPS search, both directions, SCP pictures when needed
+  if(need_search)
+  {
+    CpsArgs ca{};
+    ca.in0 = in0; ca.in1 = in1; ca.W = S.W; ca.H = S.H; ca.maxv = S.maxv; ca.clip = clip;
+    for(int c = 0; c < 3; c++) { ca.wi[c] = prm_.cws[c]; ca.wf[c] = (float)prm_.cws[c]; }
+    ca.gcd_src = dout; ca.rows = cps_rows_.as<uint32_t>();
+    ca.scp0 = need_scp ? const_cast<void*>(scp(0)) : nullptr;
+    ca.scp1 = need_scp ? const_cast<void*>(scp(1)) : nullptr;
+    QMIV_CUDA(launch_cps<T>(ca, R_, s));
+  }
+
+  // 3. SSIM family
+  FinalizeArgs fa{};
+  fa.nslots = kMaxSsimSlots;
+  double* rowsum = rowsum_.as<double>();
+  auto run_ssim = [&](const Img& a, const Img& b, int W, int H, int scale, int slot, int calc_l, int use_ws,
+                      const MutImg* down_a, const MutImg* down_b) -> qmiv_status {
+    SsimWinArgs wa{};
+    wa.a = a; wa.b = b; wa.W = W; wa.H = H; wa.nx = nx_[scale]; wa.ny = ny_[scale]; wa.ny_pad = nyp_;
+    wa.clip = clip; wa.C1 = C1_; wa.C2 = C2_; wa.calc_l = calc_l; wa.win = win_.as<double>();
+    if(down_a) { wa.down_a = *down_a; }
+    if(down_b) { wa.down_b = *down_b; }
+    QMIV_CUDA(launch_ssim_win<T>(wa, s));
+    SsimRowArgs rr{};
+    rr.win = wa.win; rr.nx = wa.nx; rr.ny = wa.ny; rr.ny_pad = nyp_;
+    rr.row_sum = rowsum + (size_t)slot * 3 * ny_[0];
+    QMIV_CUDA(launch_ssim_rows(rr, s));
+    fa.slot[slot].row_sum = rr.row_sum; fa.slot[slot].nx = wa.nx; fa.slot[slot].ny = wa.ny; fa.slot[slot].use_ws = use_ws;
+    return QMIV_OK;
+  };
+
+  const Img scp0 = need_scp ? img444(scp(0), S.W, S.H, S.esz) : Img{};
+  const Img scp1 = need_scp ? img444(scp(1), S.W, S.H, S.esz) : Img{};
+  const int use_ws = prm_.erp ? 1 : 0;
+  if(mask & QMIV_SSIM) { QMIV_TRY(run_ssim(in0, in1, S.W, S.H, 0, kSlotSsim, 1, 0, nullptr, nullptr)); }        // xSSIM.h:83
+  if(mask & QMIV_IVSSIM)                                                                                         // xIVSSIM.cpp:46-47
+  {
+    QMIV_TRY(run_ssim(in0, scp1, S.W, S.H, 0, kSlotIvT2R, 1, use_ws, nullptr, nullptr));
+    QMIV_TRY(run_ssim(in1, scp0, S.W, S.H, 0, kSlotIvR2T, 1, use_ws, nullptr, nullptr));
+  }
+  if(mask & (QMIV_MSSSIM | QMIV_IVMSSSIM))                                                                      // xSSIM.cpp:230-256
+  {
+    // pyramid levels 1..ns-1 of In0, In1, SCP0, SCP1
+    size_t lv = 0;
+    for(int s2 = 1; s2 < ns_; s2++) { lv += (size_t)(S.W >> s2) * (S.H >> s2) * 3; }
+    auto level_base = [&](int img, int scale) -> char* {
+      size_t o = (size_t)img * lv;
+      for(int s2 = 1; s2 < scale; s2++) { o += (size_t)(S.W >> s2) * (S.H >> s2) * 3; }
+      return pyr_.as<char>() + o * S.esz;
+    };
+    auto level_img = [&](int img, int scale) -> Img {
+      if(scale == 0) { return img == 0 ? in0 : img == 1 ? in1 : img == 2 ? scp0 : scp1; }
+      return img444(level_base(img, scale), S.W >> scale, S.H >> scale, S.esz);
+    };
+    for(int sc = 0; sc < ns_; sc++)
+    {
+      const int Ws = S.W >> sc, Hs = S.H >> sc;
+      const bool last = sc == ns_ - 1;
+      bool written[4] = { false, false, false, false };
+      auto down = [&](int img, MutImg& m) -> const MutImg* {
+        if(last || written[img]) { return nullptr; }
+        written[img] = true;
+        m = mut444(level_base(img, sc + 1), S.W >> (sc + 1), S.H >> (sc + 1), S.esz);
+        return &m;
+      };
+      MutImg m0, m1, m2, m3, m4, m5;
+      if(mask & QMIV_MSSSIM)
+      {
+        const MutImg* d0 = down(0, m0); const MutImg* d1 = down(1, m1);
+        QMIV_TRY(run_ssim(level_img(0, sc), level_img(1, sc), Ws, Hs, sc, kSlotMs + sc, last ? 1 : 0, 0, d0, d1));
+      }
+      if(mask & QMIV_IVMSSSIM)
+      {
+        const MutImg* d0 = down(0, m2); const MutImg* d3 = down(3, m3);
+        QMIV_TRY(run_ssim(level_img(0, sc), level_img(3, sc), Ws, Hs, sc, kSlotIvmsT2R + sc, last ? 1 : 0, 0, d0, d3));
+        const MutImg* d1 = down(1, m4); const MutImg* d2 = down(2, m5);
+        QMIV_TRY(run_ssim(level_img(1, sc), level_img(2, sc), Ws, Hs, sc, kSlotIvmsR2T + sc, last ? 1 : 0, 0, d1, d2));
+      }
+    }
+  }
+
+  // 4. pooling chains
+  fa.H = S.H;
+  for(int c = 0; c < 3; c++) { fa.rows[c] = (int32_t)S.plane_rows(c); fa.sy[c] = c ? S.sy : 0; fa.mult_row[c] = c ? (1 << S.sx) : 1; }
+  fa.row_ssd = row_ssd_.as<uint64_t>();
+  fa.ws = prm_.erp ? ws_.as<double>() : nullptr;
+  fa.do_wspsnr = (mask & QMIV_WSPSNR) ? 1 : 0;
+  fa.cps_rows = need_search ? cps_rows_.as<uint32_t>() : nullptr;
+  fa.out = dout;
+  QMIV_CUDA(launch_finalize(fa, s));
+  QMIV_CUDA(cudaMemcpyAsync(h_out, dout, sizeof(PairOut), cudaMemcpyDeviceToHost, s));
+  return QMIV_OK;
+}
+
+}  // namespace qmiv
+
+using namespace qmiv;
+
+// =============================================================================================
+// calc entry points
+// =============================================================================================
+static qmiv_status wait_event(cudaEvent_t ev, int32_t timeout_ms)
+{
+  if(timeout_ms < 0) { QMIV_CUDA(cudaEventSynchronize(ev)); return QMIV_OK; }
+  const auto t0 = std::chrono::steady_clock::now();
+  for(;;)
+  {
+    const cudaError_t e = cudaEventQuery(ev);
+    if(e == cudaSuccess) { return QMIV_OK; }
+    if(e != cudaErrorNotReady) { return cuda_fail(e, "cudaEventQuery"); }
+    const auto el = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+    if(el >= timeout_ms) { return fail(QMIV_ERR_TIMEOUT, "result not ready within the timeout"); }
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+static qmiv_status calc_submit(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, uint32_t mask, bool want_scp,
+                               bool want_gcd = false)
+{
+  if(!calc || !in0 || !in1) { return fail(QMIV_ERR_INVALID_ARG, "null argument"); }
+  if(calc->pending) { return fail(QMIV_ERR_BUSY, "a submission is already in flight on this calc"); }
+  if((mask & ~QMIV_ALL) != 0) { return fail(QMIV_ERR_INVALID_ARG, "unknown metric bits"); }
+  QMIV_CUDA(cudaSetDevice(calc->ctx->device));
+  const bool host = in0->mem == QMIV_MEM_HOST || in1->mem == QMIV_MEM_HOST;
+  QMIV_TRY(calc->pipe.prepare(mask, want_scp, host));
+  Img a{}, b{};
+  QMIV_TRY(calc->pipe.resolve(in0, 0, a, calc->stream));
+  QMIV_TRY(calc->pipe.resolve(in1, 1, b, calc->stream));
+  QMIV_TRY(calc->pipe.enqueue(a, b, mask, want_scp, want_gcd, calc->stream));
+  QMIV_CUDA(cudaEventRecord(calc->done, calc->stream));
+  calc->pending = true;
+  calc->pending_mask = mask;
+  return QMIV_OK;
+}
+
+static qmiv_status calc_collect(qmiv_calc calc, int32_t timeout_ms, qmiv_result* out)
+{
+  if(!calc->pending) { return fail(QMIV_ERR_INVALID_ARG, "nothing submitted"); }
+  QMIV_TRY(wait_event(calc->done, timeout_ms));
+  calc->pending = false;
+  calc->has_last = true;
+  const PairOut& o = calc->pipe.host_out();
+  if(out) { finish_result(o, calc->pipe.finish_info(calc->pending_mask), out); }
+  if(calc->prm.invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3))
+  {
+    return fail(QMIV_ERR_INVALID_PIXEL, "input frame contains samples above the bit depth's maximum");
+  }
+  return QMIV_OK;
+}
+
+extern "C" {
+
+qmiv_status qmiv_calc_create(qmiv_ctx ctx, int32_t width, int32_t height, int32_t bitdepth, int32_t chroma_format,
+                             const qmiv_params* params, qmiv_calc* out_calc)
+{
+  if(!ctx || !out_calc) { return fail(QMIV_ERR_INVALID_ARG, "null argument"); }
+  *out_calc = nullptr;
+  qmiv_params prm;
+  if(params) { prm = *params; } else { qmiv_params_default(&prm); }
+  QMIV_TRY(validate_params(prm));
+  Shape shape;
+  QMIV_TRY(shape.init(width, height, bitdepth, chroma_format));
+  QMIV_CUDA(cudaSetDevice(ctx->device));
+  qmiv_calc c = new qmiv_calc_s();
+  c->ctx = ctx; c->shape = shape; c->prm = prm;
+  qmiv_status st = c->pipe.configure(ctx, shape, prm, prm.search_range);
+  if(st == QMIV_OK)
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if(e == cudaSuccess) { e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming); }
+    if(e != cudaSuccess) { st = cuda_fail(e, "stream/event creation"); }
+  }
+  if(st != QMIV_OK) { qmiv_calc_destroy(c); return st; }
+  *out_calc = c;
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_calc_destroy(qmiv_calc calc)
+{
+  if(!calc) { return fail(QMIV_ERR_INVALID_ARG, "calc is null"); }
+  cudaSetDevice(calc->ctx->device);
+  if(calc->stream) { cudaStreamSynchronize(calc->stream); }
+  if(calc->done) { cudaEventDestroy(calc->done); }
+  if(calc->stream) { cudaStreamDestroy(calc->stream); }
+  delete calc;
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_frame_pair_compute(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, uint32_t metric_mask, qmiv_result* out)
+{
+  QMIV_TRY(calc_submit(calc, in0, in1, metric_mask, false));
+  return calc_collect(calc, -1, out);
+}
+
+qmiv_status qmiv_frame_pair_submit(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, uint32_t metric_mask)
+{
+  return calc_submit(calc, in0, in1, metric_mask, false);
+}
+
+qmiv_status qmiv_frame_pair_wait(qmiv_calc calc, int32_t timeout_ms, qmiv_result* out)
+{
+  if(!calc) { return fail(QMIV_ERR_INVALID_ARG, "calc is null"); }
+  return calc_collect(calc, timeout_ms, out);
+}
+
+qmiv_status qmiv_calc_gcd(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, int32_t gcd_r2t[4])
+{
+  if(!gcd_r2t) { return fail(QMIV_ERR_INVALID_ARG, "gcd_r2t is null"); }
+  qmiv_result r;
+  QMIV_TRY(calc_submit(calc, in0, in1, 0, false, true));
+  QMIV_TRY(calc_collect(calc, -1, &r));
+  for(int c = 0; c < 4; c++) { gcd_r2t[c] = r.gcd_r2t[c]; }
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_calc_scp(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, const int32_t* gcd_r2t,
+                          uint16_t* scp0, uint16_t* scp1, int32_t dst_mem)
+{
+  if(dst_mem != QMIV_MEM_HOST && dst_mem != QMIV_MEM_DEVICE) { return fail(QMIV_ERR_INVALID_ARG, "bad dst_mem"); }
+  if(gcd_r2t) { return fail(QMIV_ERR_UNSUPPORTED, "an externally supplied GCD is not supported; pass NULL"); }
+  QMIV_TRY(calc_submit(calc, in0, in1, 0, true));
+  QMIV_TRY(calc_collect(calc, -1, nullptr));
+  const Shape& S = calc->shape;
+  const size_t n = (size_t)3 * S.W * S.H;
+  for(int k = 0; k < 2; k++)
+  {
+    uint16_t* dst = k ? scp1 : scp0;
+    if(!dst) { continue; }
+    const void* src = calc->pipe.scp(k);
+    if(S.esz == 2)
+    {
+      QMIV_CUDA(cudaMemcpy(dst, src, n * 2, dst_mem == QMIV_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+    }
+    else
+    {
+      std::vector<uint8_t> tmp(n);
+      QMIV_CUDA(cudaMemcpy(tmp.data(), src, n, cudaMemcpyDeviceToHost));
+      if(dst_mem == QMIV_MEM_HOST) { for(size_t i = 0; i < n; i++) { dst[i] = tmp[i]; } }
+      else
+      {
+        std::vector<uint16_t> w(tmp.begin(), tmp.end());
+        QMIV_CUDA(cudaMemcpy(dst, w.data(), n * 2, cudaMemcpyHostToDevice));
+      }
+    }
+  }
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_calc_cps_rows(qmiv_calc calc, uint64_t* rows_r2t, uint64_t* rows_t2r)
+{
+  if(!calc) { return fail(QMIV_ERR_INVALID_ARG, "calc is null"); }
+  if(!calc->has_last || !calc->pipe.cps_rows()) { return fail(QMIV_ERR_INVALID_ARG, "no CPS result available"); }
+  const Shape& S = calc->shape;
+  std::vector<uint32_t> tmp((size_t)2 * S.H * 3);
+  QMIV_CUDA(cudaMemcpy(tmp.data(), calc->pipe.cps_rows(), tmp.size() * 4, cudaMemcpyDeviceToHost));
+  for(int d = 0; d < 2; d++)
+  {
+    uint64_t* dst = d ? rows_t2r : rows_r2t;
+    if(!dst) { continue; }
+    for(size_t i = 0; i < (size_t)S.H * 3; i++) { dst[i] = (uint64_t)(int64_t)(int32_t)tmp[(size_t)d * S.H * 3 + i]; }
+  }
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_calc_stream(qmiv_calc calc, void** cuda_stream)
+{
+  if(!calc || !cuda_stream) { return fail(QMIV_ERR_INVALID_ARG, "null argument"); }
+  *cuda_stream = (void*)calc->stream;
+  return QMIV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// Host-side internals of the QMIV B200 library (not part of the public ABI).
+#pragma once
+#include "qmiv_gpu.h"
+#include "qmiv_kernels.cuh"
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+struct qmiv_ctx_s
+{
+  int32_t    device = 0;
+  uint64_t   budget = 0;  // 0 = unlimited
+  uint64_t   used   = 0;
+  std::mutex mu;
+  bool reserve(size_t n);
+  void unreserve(size_t n);
+};
+
+namespace qmiv {
+
+extern thread_local std::string g_last_error;
+qmiv_status fail(qmiv_status st, const std::string& msg);
+qmiv_status cuda_fail(cudaError_t e, const char* what);
+
+#define QMIV_CUDA(call)                                           \
+  do {                                                            \
+    const cudaError_t qmiv_e_ = (call);                           \
+    if(qmiv_e_ != cudaSuccess) { return cuda_fail(qmiv_e_, #call); } \
+  } while(0)
+
+#define QMIV_TRY(call)                                            \
+  do {                                                            \
+    const qmiv_status qmiv_s_ = (call);                           \
+    if(qmiv_s_ != QMIV_OK) { return qmiv_s_; }                    \
+  } while(0)
+
+// Device allocation counted against the owning context's HBM budget.
+struct DevMem
+{
+  void*       p     = nullptr;
+  size_t      bytes = 0;
+  qmiv_ctx_s* ctx   = nullptr;
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem() { release(); }
+  qmiv_status alloc(qmiv_ctx_s* c, size_t n);
+  qmiv_status ensure(qmiv_ctx_s* c, size_t n);
+  void        release();
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// SSIM result slots of PairOut::ssim
+constexpr int kSlotSsim = 0, kSlotIvT2R = 1, kSlotIvR2T = 2, kSlotMs = 3, kSlotIvmsT2R = 8, kSlotIvmsR2T = 13;
+
+struct FinishInfo
+{
+  int32_t  W, H, bitdepth;
+  uint32_t mask;
+  int32_t  erp;
+  double   ws_corr;
+  int32_t  cwa[4];
+  int32_t  num_scales;
+};
+
+double  psnr_from_ssd(double ssd, int64_t area, int32_t bitdepth);
+int32_t num_scales(int32_t W, int32_t H);
+int32_t round_f32_half_away(float f);
+void    ws_weights(int32_t H, int32_t lat_range, std::vector<double>& w, double& correction);
+void    finish_result(const PairOut& o, const FinishInfo& fi, qmiv_result* r);
+
+// Geometry of one frame-pair shape.
+struct Shape
+{
+  int32_t W = 0, H = 0, bitdepth = 0, chroma_format = 0;
+  int32_t sx = 0, sy = 0;        // chroma subsampling shifts
+  int32_t cw = 0, ch = 0;        // chroma plane size
+  size_t  esz = 0;               // bytes per sample (1 or 2)
+  int32_t maxv = 0;
+  qmiv_status init(int32_t W, int32_t H, int32_t bitdepth, int32_t chroma_format);
+  size_t  plane_cols(int c) const { return c == 0 ? (size_t)W : (size_t)cw; }
+  size_t  plane_rows(int c) const { return c == 0 ? (size_t)H : (size_t)ch; }
+  size_t  frame_bytes() const { return esz * ((size_t)W * H + 2 * (size_t)cw * ch); }
+};
+
+qmiv_status validate_params(const qmiv_params& p);
+
+// The device pipeline of one frame pair of a fixed shape, with its scratch buffers.
+class PairPipeline
+{
+public:
+  qmiv_status configure(qmiv_ctx_s* ctx, const Shape& shape, const qmiv_params& prm, int32_t search_range);
+  // Reserve every buffer the metrics in `mask` need (lazily grows).
+  qmiv_status prepare(uint32_t mask, bool want_scp, bool host_frames);
+  // Resolve a frame: device frames are used in place, host frames are copied to staging.
+  qmiv_status resolve(const qmiv_frame* f, int which, Img& out, cudaStream_t s);
+  // Enqueue the full pipeline; results land in the pinned host PairOut after the stream syncs.
+  qmiv_status enqueue(const Img& in0, const Img& in1, uint32_t mask, bool want_scp, bool want_gcd, cudaStream_t s);
+  const PairOut& host_out() const { return *h_out; }
+  FinishInfo finish_info(uint32_t mask) const;
+  // SCP planes (T samples, planar 3 x W*H) of the last run, or null
+  const void* scp(int which) const;
+  const uint32_t* cps_rows() const { return cps_rows_.as<uint32_t>(); }
+  const Shape& shape() const { return shape_; }
+  int32_t search_range() const { return R_; }
+  ~PairPipeline();
+
+private:
+  template <typename T> qmiv_status enqueue_t(const Img& in0, const Img& in1, uint32_t mask, bool want_scp, bool want_gcd, cudaStream_t s);
+
+  qmiv_ctx_s*  ctx_ = nullptr;
+  Shape        shape_;
+  qmiv_params  prm_{};
+  int32_t      R_ = 2;
+  int32_t      maxdiff_[4] = { 0, 0, 0, 0 };
+  bool         fp32_ok_ = true;
+  int32_t      ns_ = 0;
+  int32_t      nx_[5] = {}, ny_[5] = {}, nyp_ = 0;
+  std::vector<double> ws_host_;
+  double       ws_corr_ = 1.0;
+  double       C1_ = 0, C2_ = 0;
+
+  DevMem row_sd_, row_ssd_, cps_rows_, out_, ws_, scp_, pyr_, win_, rowsum_, staging_;
+  PairOut* h_out = nullptr;
+  bool ws_uploaded_ = false;
+};
+
+}  // namespace qmiv
+
+struct qmiv_calc_s
+{
+  qmiv_ctx_s*          ctx = nullptr;
+  qmiv::Shape          shape;
+  qmiv_params          prm{};
+  qmiv::PairPipeline   pipe;
+  cudaStream_t         stream = nullptr;
+  cudaEvent_t          done = nullptr;
+  bool                 pending = false;
+  uint32_t             pending_mask = 0;
+  bool                 has_last = false;
+};

@@ -1,0 +1,642 @@
+// QMIV metric kernels for B200 (sm_100a).
+//
+// Pipeline of one frame pair (the reference runs the same steps per frame on the CPU,
+// apps/QMIV/src/xAppQMIV.cpp:761-827):
+//   k_prepass   per raw row: SD(In1-In0), SSD, max sample        (HBM bound, reads both frames once)
+//   k_reduce    totals, GCD, exactness of the fp32 search path   (one CTA)
+//   k_cps       corresponding-pixel-shift search, both directions in one pass; per-row SSE into
+//               32-bit lanes and, when an IV-SSIM metric needs them, the shift-compensated pictures
+//   k_ssim_win  8x8/stride-4 block SSIM per window from exact integer moments, FP64 formula,
+//               fused 2x2 downsampling for the next MS-SSIM scale
+//   k_ssim_rows per window row, compensated sum of the windows in x order
+//   k_finalize  every order-dependent FP64 pooling chain of the pair (one thread per chain)
+#include "qmiv_kernels.cuh"
+
+#include <cstdio>
+
+namespace qmiv {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// =============================================================================================
+// prepass
+// =============================================================================================
+template <typename T>
+__global__ void __launch_bounds__(256) k_prepass(const __grid_constant__ PrepassArgs a)
+{
+  const int warp  = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane  = threadIdx.x & 31;
+  const int total = a.rows[0] + a.rows[1] + a.rows[2];
+  if(warp >= total) { return; }
+  int c = 0, r = warp;
+  if(r >= a.rows[0]) { r -= a.rows[0]; c = 1; if(r >= a.rows[1]) { r -= a.rows[1]; c = 2; } }
+  const T* p0 = static_cast<const T*>(a.in0.p[c]) + (size_t)r * a.in0.pitch[c];
+  const T* p1 = static_cast<const T*>(a.in1.p[c]) + (size_t)r * a.in1.pitch[c];
+  const int n = a.cols[c];
+
+  int64_t  sd  = 0;
+  uint64_t ssd = 0;
+  uint32_t m0 = 0, m1 = 0;
+  for(int x = lane; x < n; x += 32)
+  {
+    uint32_t v0 = __ldg(p0 + x), v1 = __ldg(p1 + x);
+    m0 = max(m0, v0); m1 = max(m1, v1);
+    v0 = min(v0, a.clip); v1 = min(v1, a.clip);
+    const int32_t d = (int32_t)v1 - (int32_t)v0;
+    sd  += d;
+    ssd += (uint64_t)((int64_t)d * d);
+  }
+  #pragma unroll
+  for(int o = 16; o > 0; o >>= 1)
+  {
+    sd  += __shfl_xor_sync(kFull, sd, o);
+    ssd += __shfl_xor_sync(kFull, ssd, o);
+  }
+  m0 = __reduce_max_sync(kFull, m0);
+  m1 = __reduce_max_sync(kFull, m1);
+  if(lane == 0)
+  {
+    a.row_sd[warp]  = sd;
+    a.row_ssd[warp] = ssd;
+    atomicMax(&a.out->max_sample[0], m0);
+    atomicMax(&a.out->max_sample[1], m1);
+  }
+}
+
+template <typename T>
+cudaError_t launch_prepass(const PrepassArgs& a, cudaStream_t s)
+{
+  const int total  = a.rows[0] + a.rows[1] + a.rows[2];
+  const int blocks = (total + 7) / 8;
+  k_prepass<T><<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+template cudaError_t launch_prepass<uint8_t>(const PrepassArgs&, cudaStream_t);
+template cudaError_t launch_prepass<uint16_t>(const PrepassArgs&, cudaStream_t);
+
+// =============================================================================================
+// reduce: totals and GCD (libs/pmbb-ivqm/src/xGlobClrDiff.cpp:70-103)
+// =============================================================================================
+__global__ void __launch_bounds__(1024) k_reduce(const __grid_constant__ ReduceArgs a)
+{
+  __shared__ int64_t  s_sd[3][32];
+  __shared__ uint64_t s_ssd[3][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int off = 0;
+  for(int c = 0; c < 3; c++)
+  {
+    int64_t sd = 0; uint64_t ssd = 0;
+    for(int r = threadIdx.x; r < a.rows[c]; r += blockDim.x) { sd += a.row_sd[off + r]; ssd += a.row_ssd[off + r]; }
+    #pragma unroll
+    for(int o = 16; o > 0; o >>= 1) { sd += __shfl_xor_sync(kFull, sd, o); ssd += __shfl_xor_sync(kFull, ssd, o); }
+    if(lane == 0) { s_sd[c][wid] = sd; s_ssd[c][wid] = ssd; }
+    off += a.rows[c];
+  }
+  __syncthreads();
+  if(threadIdx.x == 0)
+  {
+    PairOut* o = a.out;
+    const int nw = blockDim.x >> 5;
+    for(int c = 0; c < 3; c++)
+    {
+      int64_t sd = 0; uint64_t ssd = 0;
+      for(int w = 0; w < nw; w++) { sd += s_sd[c][w]; ssd += s_ssd[c][w]; }
+      o->sd[c]  = sd * a.mult[c];
+      o->ssd[c] = ssd * (uint64_t)a.mult[c];
+    }
+    const double area = (double)a.area;
+    for(int c = 0; c < 4; c++)
+    {
+      int32_t g = 0;
+      if(a.need_gcd)
+      {
+        const double avg = ddiv(c < 3 ? (double)o->sd[c] : 0.0, area);
+        g = clampi(round_half_away(avg), -a.maxdiff[c], a.maxdiff[c]);
+      }
+      o->gcd[c] = g;
+    }
+    const int inv0 = o->max_sample[0] > (uint32_t)a.maxv;
+    const int inv1 = o->max_sample[1] > (uint32_t)a.maxv;
+    const int int_path = !a.fp32_ok || ((inv0 || inv1) && !a.clip_on);
+    o->flags = inv0 | (inv1 << 1) | (int_path << 2);
+  }
+}
+
+cudaError_t launch_reduce(const ReduceArgs& a, cudaStream_t s)
+{
+  k_reduce<<<1, 1024, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// =============================================================================================
+// CPS search (libs/pmbb-ivqm/src/xCorrespPixelShiftSSE.cpp:18-127)
+//
+// Both pictures of a tile (plus an R-pixel halo, clamped) are staged in shared memory as
+// float4 (Y, Cb, Cr, q + 2^23) with q = sum_c w_c * ref_c^2. For a test pixel s (test + GCD,
+// unclipped) the weighted error of candidate r is e = sum_c w_c (s_c - r_c)^2, and
+//     e - sum_c w_c s_c^2 + 2^23 = (q(r) + 2^23) + sum_c (-2 w_c s_c) r_c
+// is three FFMAs. When every partial sum is an integer below 2^24 in magnitude (checked on the host
+// from bit depth, weights and the GCD clip range) the FFMAs are exact, so the ordering of candidates
+// and all ties are those of the reference's int32 error. The result lies in [2^20, 2^24), where the
+// IEEE bit pattern grows with the value, so
+//     key = ((bits - bits(2^20)) << 7) + k,   k = (dy+R)(2R+1) + (dx+R)  (raster index, < 128)
+// orders candidates exactly as the reference's "first strict minimum in raster order" does, and the
+// search is one unsigned min per candidate. Each thread owns P vertically adjacent pixels, so every
+// staged reference pixel is reused by up to 2R+1 of them from registers.
+//
+// When the fp32 path is not exact (bit depth > 10, large weights, out-of-range samples) the same
+// kernel runs an int32 search that mirrors the SSE path's wrap-around arithmetic literally.
+// =============================================================================================
+constexpr float    kBias    = 8388608.0f;   // 2^23
+constexpr uint32_t kKeyBase = 0x49800000u;  // bit pattern of 2^20f
+
+bool cps_fp32_exact(int32_t maxv, const int32_t w[3], const int32_t maxdiff[3])
+{
+  const int64_t bias = 1LL << 23;
+  int64_t e = 0, q = 0, up = 0, lo = 0;
+  for(int c = 0; c < 3; c++)
+  {
+    const int64_t g = maxdiff[c] < 0 ? -(int64_t)maxdiff[c] : maxdiff[c];
+    if(w[c] < 0) { return false; }
+    e  += (int64_t)w[c] * (maxv + g) * (maxv + g);   // max of sum_c w_c (s_c - r_c)^2 and of sum_c w_c s_c^2
+    q  += (int64_t)w[c] * maxv * maxv;
+    up += 2 * (int64_t)w[c] * g * maxv;              // largest positive -2 w s r (s negative)
+    lo += 2 * (int64_t)w[c] * (maxv + g) * maxv;     // largest negative -2 w s r
+  }
+  const int64_t lim = 1LL << 24;
+  if(bias - e < (1LL << 20)) { return false; }       // key base
+  if(bias + e >= lim) { return false; }
+  if(bias + q + up >= lim) { return false; }         // partial sums of the FFMA chain
+  if(bias - lo <= -lim) { return false; }
+  return true;
+}
+
+template <int R, int P, typename T>
+__global__ void __launch_bounds__(128) k_cps(const __grid_constant__ CpsArgs a)
+{
+  constexpr int D  = 2 * R + 1;
+  constexpr int TX = 32, TY = 4;
+  constexpr int TW = TX, TH = TY * P;
+  constexpr int SW = TW + 2 * R, SH = TH + 2 * R;
+  extern __shared__ float4 sm[];
+  float4* const tile0 = sm;
+  float4* const tile1 = sm + SH * SW;
+
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  const int W = a.W, H = a.H;
+  const int g0 = a.gcd_src->gcd[0], g1 = a.gcd_src->gcd[1], g2 = a.gcd_src->gcd[2];
+  const bool int_path = (a.gcd_src->flags & 4) != 0;
+
+  for(int i = threadIdx.x; i < SH * SW; i += TX * TY)
+  {
+    const int ly = i / SW, lx = i - ly * SW;
+    const int gx = clampi(x0 + lx - R, 0, W - 1), gy = clampi(y0 + ly - R, 0, H - 1);
+    #pragma unroll
+    for(int f = 0; f < 2; f++)
+    {
+      const Img& im = f ? a.in1 : a.in0;
+      const float v0 = (float)min((uint32_t)fetch<T>(im, 0, gx, gy), a.clip);
+      const float v1 = (float)min((uint32_t)fetch<T>(im, 1, gx, gy), a.clip);
+      const float v2 = (float)min((uint32_t)fetch<T>(im, 2, gx, gy), a.clip);
+      const float q  = fmaf(a.wf[2], v2 * v2, fmaf(a.wf[1], v1 * v1, fmaf(a.wf[0], v0 * v0, kBias)));
+      (f ? tile1 : tile0)[i] = make_float4(v0, v1, v2, q);
+    }
+  }
+  __syncthreads();
+
+  #pragma unroll 1
+  for(int dir = 0; dir < 2; dir++)
+  {
+    // dir 0 (R2T): test = In0 + GCD searched in In1 -> rows[0], SCP1 = clip(In1[best] - GCD)
+    // dir 1 (T2R): test = In1 - GCD searched in In0 -> rows[1], SCP0 = clip(In0[best] + GCD)
+    const float4* tst = dir ? tile1 : tile0;
+    const float4* ref = dir ? tile0 : tile1;
+    const int sg = dir ? -1 : 1;
+    const int ga = sg * g0, gb = sg * g1, gc = sg * g2;
+
+    uint32_t idx[P];
+    if(!int_path)
+    {
+      float    c0[P], c1[P], c2[P];
+      uint32_t best[P];
+      #pragma unroll
+      for(int i = 0; i < P; i++)
+      {
+        const float4 t = tst[(ty * P + i + R) * SW + tx + R];
+        c0[i] = -2.0f * a.wf[0] * (t.x + (float)ga);
+        c1[i] = -2.0f * a.wf[1] * (t.y + (float)gb);
+        c2[i] = -2.0f * a.wf[2] * (t.z + (float)gc);
+        best[i] = 0xffffffffu;
+      }
+      #pragma unroll
+      for(int dxi = 0; dxi < D; dxi++)
+      {
+        #pragma unroll
+        for(int ry = 0; ry < P + 2 * R; ry++)
+        {
+          const float4 r = ref[(ty * P + ry) * SW + tx + dxi];
+          #pragma unroll
+          for(int i = 0; i < P; i++)
+          {
+            const int dyi = ry - i;
+            if(dyi >= 0 && dyi < D)
+            {
+              const float    e   = fmaf(c2[i], r.z, fmaf(c1[i], r.y, fmaf(c0[i], r.x, r.w)));
+              const uint32_t key = (__float_as_uint(e) << 7) + (uint32_t)(dyi * D + dxi) - (kKeyBase << 7);
+              best[i] = min(best[i], key);
+            }
+          }
+        }
+      }
+      #pragma unroll
+      for(int i = 0; i < P; i++) { idx[i] = best[i] & 127u; }
+    }
+    else
+    {
+      #pragma unroll 1
+      for(int i = 0; i < P; i++)
+      {
+        const float4 t = tst[(ty * P + i + R) * SW + tx + R];
+        const int s0 = (int)t.x + ga, s1 = (int)t.y + gb, s2 = (int)t.z + gc;
+        int32_t  best_err = 0x7fffffff;
+        uint32_t bi = 0;
+        for(int dyi = 0; dyi < D; dyi++)
+        {
+          for(int dxi = 0; dxi < D; dxi++)
+          {
+            const float4   r  = ref[(ty * P + i + dyi) * SW + tx + dxi];
+            const uint32_t d0 = (uint32_t)(s0 - (int)r.x), d1 = (uint32_t)(s1 - (int)r.y), d2 = (uint32_t)(s2 - (int)r.z);
+            const uint32_t err = d0 * d0 * (uint32_t)a.wi[0] + d1 * d1 * (uint32_t)a.wi[1] + d2 * d2 * (uint32_t)a.wi[2];
+            if((int32_t)err < best_err) { best_err = (int32_t)err; bi = (uint32_t)(dyi * D + dxi); }
+          }
+        }
+        idx[i] = bi;
+      }
+    }
+
+    // epilogue: winner's per-component squared difference into the row sums, SCP store
+    uint32_t* rows = a.rows + (size_t)dir * H * 3;
+    T* scp = static_cast<T*>(dir ? a.scp0 : a.scp1);
+    const size_t plane = (size_t)W * H;
+    const int x = x0 + tx;
+    #pragma unroll
+    for(int i = 0; i < P; i++)
+    {
+      const int y = y0 + ty * P + i;
+      const bool valid = (x < W) && (y < H);
+      const int dyi = (int)(idx[i] / D), dxi = (int)(idx[i] - dyi * D);
+      const float4 r = ref[(ty * P + i + dyi) * SW + tx + dxi];
+      const float4 t = tst[(ty * P + i + R) * SW + tx + R];
+      const int r0 = (int)r.x, r1 = (int)r.y, r2 = (int)r.z;
+      const uint32_t e0 = (uint32_t)((int)t.x + ga - r0), e1 = (uint32_t)((int)t.y + gb - r1), e2 = (uint32_t)((int)t.z + gc - r2);
+      const uint32_t s0 = __reduce_add_sync(kFull, valid ? e0 * e0 : 0u);
+      const uint32_t s1 = __reduce_add_sync(kFull, valid ? e1 * e1 : 0u);
+      const uint32_t s2 = __reduce_add_sync(kFull, valid ? e2 * e2 : 0u);
+      if(tx == 0 && y < H)
+      {
+        atomicAdd(rows + (size_t)y * 3 + 0, s0);
+        atomicAdd(rows + (size_t)y * 3 + 1, s1);
+        atomicAdd(rows + (size_t)y * 3 + 2, s2);
+      }
+      if(scp != nullptr && valid)
+      {
+        const size_t o = (size_t)y * W + x;
+        scp[o]             = (T)clampi(r0 - ga, 0, a.maxv);
+        scp[plane + o]     = (T)clampi(r1 - gb, 0, a.maxv);
+        scp[2 * plane + o] = (T)clampi(r2 - gc, 0, a.maxv);
+      }
+    }
+  }
+}
+
+template <int R, typename T>
+static cudaError_t launch_cps_r(const CpsArgs& a, cudaStream_t s)
+{
+  constexpr int P = 8, TW = 32, TH = 4 * P;
+  constexpr size_t smem = 2 * sizeof(float4) * (TW + 2 * R) * (TH + 2 * R);
+  static bool configured = false;
+  if(!configured)
+  {
+    const cudaError_t e = cudaFuncSetAttribute(k_cps<R, P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if(e != cudaSuccess) { return e; }
+    configured = true;
+  }
+  const dim3 grid((a.W + TW - 1) / TW, (a.H + TH - 1) / TH);
+  k_cps<R, P, T><<<grid, 128, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_cps(const CpsArgs& a, int R, cudaStream_t s)
+{
+  switch(R)
+  {
+  case 1: return launch_cps_r<1, T>(a, s);
+  case 2: return launch_cps_r<2, T>(a, s);
+  case 3: return launch_cps_r<3, T>(a, s);
+  case 4: return launch_cps_r<4, T>(a, s);
+  case 5: return launch_cps_r<5, T>(a, s);
+  default: return cudaErrorInvalidValue;
+  }
+}
+template cudaError_t launch_cps<uint8_t>(const CpsArgs&, int, cudaStream_t);
+template cudaError_t launch_cps<uint16_t>(const CpsArgs&, int, cudaStream_t);
+
+// =============================================================================================
+// block SSIM windows (libs/pmbb-ivqm/src/xStructSimSTD.cpp:420-461; loop ranges xSSIM.cpp:276-311)
+//
+// A CTA owns 32x8 windows (origins 4i, 4j), i.e. a 132x36 pixel region of both pictures. 4x4
+// sub-block moments are formed once and every window adds four of them, so all sums are exact
+// integers; the SSIM formula is then evaluated in FP64 with the reference's operation order.
+// The CTA grid covers the whole picture so that the fused 2x2 mean (xPixelOpsSTD.cpp:50-67) of
+// each owned 128x32 region can be written for the next MS-SSIM scale.
+// =============================================================================================
+constexpr int kSwX = 32, kSwY = 8;                      // windows per CTA
+constexpr int kSpX = kSwX * 4 + 4, kSpY = kSwY * 4 + 4; // pixel region 132 x 36
+constexpr int kSbX = kSwX + 1, kSbY = kSwY + 1;         // sub-blocks 33 x 9
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_ssim_win(const __grid_constant__ SsimWinArgs a)
+{
+  __shared__ uint16_t pa[kSpY][kSpX];
+  __shared__ uint16_t pb[kSpY][kSpX];
+  __shared__ uint32_t sa[kSbY][kSbX], sb[kSbY][kSbX];
+  __shared__ uint64_t saa[kSbY][kSbX], sbb[kSbY][kSbX], sab[kSbY][kSbX];
+
+  const int c   = blockIdx.z;
+  const int px0 = blockIdx.x * (kSwX * 4), py0 = blockIdx.y * (kSwY * 4);
+  const int W = a.W, H = a.H;
+
+  for(int i = threadIdx.x; i < kSpX * kSpY; i += blockDim.x)
+  {
+    const int ly = i / kSpX, lx = i - ly * kSpX;
+    const int gx = min(px0 + lx, W - 1), gy = min(py0 + ly, H - 1);
+    pa[ly][lx] = (uint16_t)min((uint32_t)fetch<T>(a.a, c, gx, gy), a.clip);
+    pb[ly][lx] = (uint16_t)min((uint32_t)fetch<T>(a.b, c, gx, gy), a.clip);
+  }
+  __syncthreads();
+
+  for(int i = threadIdx.x; i < kSbX * kSbY; i += blockDim.x)
+  {
+    const int by = i / kSbX, bx = i - by * kSbX;
+    uint32_t s_a = 0, s_b = 0;
+    uint64_t s_aa = 0, s_bb = 0, s_ab = 0;
+    #pragma unroll
+    for(int y = 0; y < 4; y++)
+    {
+      #pragma unroll
+      for(int x = 0; x < 4; x++)
+      {
+        const uint32_t va = pa[by * 4 + y][bx * 4 + x], vb = pb[by * 4 + y][bx * 4 + x];
+        s_a += va; s_b += vb;
+        s_aa += va * va; s_bb += vb * vb; s_ab += va * vb;
+      }
+    }
+    sa[by][bx] = s_a; sb[by][bx] = s_b; saa[by][bx] = s_aa; sbb[by][bx] = s_bb; sab[by][bx] = s_ab;
+  }
+  __syncthreads();
+
+  {
+    const int wx = threadIdx.x & 31, wy = threadIdx.x >> 5;
+    const int i = blockIdx.x * kSwX + wx, j = blockIdx.y * kSwY + wy;
+    if(i < a.nx && j < a.ny)
+    {
+      const uint32_t sr  = sb[wy][wx] + sb[wy][wx + 1] + sb[wy + 1][wx] + sb[wy + 1][wx + 1];
+      const uint32_t st  = sa[wy][wx] + sa[wy][wx + 1] + sa[wy + 1][wx] + sa[wy + 1][wx + 1];
+      const uint64_t srr = sbb[wy][wx] + sbb[wy][wx + 1] + sbb[wy + 1][wx] + sbb[wy + 1][wx + 1];
+      const uint64_t stt = saa[wy][wx] + saa[wy][wx + 1] + saa[wy + 1][wx] + saa[wy + 1][wx + 1];
+      const uint64_t srt = sab[wy][wx] + sab[wy][wx + 1] + sab[wy + 1][wx] + sab[wy + 1][wx + 1];
+      const double inv   = 0.015625;  // 1/64, exact
+      const double avg_r = dmul((double)sr, inv);
+      const double avg_t = dmul((double)st, inv);
+      const double var_r = dsub(dmul((double)srr, inv), dmul(avg_r, avg_r));
+      const double var_t = dsub(dmul((double)stt, inv), dmul(avg_t, avg_t));
+      const double cov   = dsub(dmul((double)srt, inv), dmul(avg_r, avg_t));
+      const double cs    = ddiv(dadd(dmul(2.0, cov), a.C2), dadd(dadd(var_r, var_t), a.C2));
+      double v = cs;
+      if(a.calc_l)
+      {
+        const double l = ddiv(dadd(dmul(dmul(2.0, avg_r), avg_t), a.C1), dadd(dadd(dmul(avg_r, avg_r), dmul(avg_t, avg_t)), a.C1));
+        v = dmul(l, cs);
+      }
+      a.win[((size_t)c * a.nx + i) * a.ny_pad + j] = v;
+    }
+  }
+
+  // fused 2x2 downsampling of the owned 128x32 region for the next MS-SSIM scale
+  const int dw = W >> 1, dh = H >> 1;
+  const int dx0 = px0 >> 1, dy0 = py0 >> 1;
+  if(a.down_a.p[c] != nullptr || a.down_b.p[c] != nullptr)
+  {
+    for(int i = threadIdx.x; i < (kSwX * 2) * (kSwY * 2); i += blockDim.x)
+    {
+      const int ly = i / (kSwX * 2), lx = i - ly * (kSwX * 2);
+      const int dx = dx0 + lx, dy = dy0 + ly;
+      if(dx >= dw || dy >= dh) { continue; }
+      if(a.down_a.p[c] != nullptr)
+      {
+        const uint32_t v = ((uint32_t)pa[2 * ly][2 * lx] + pa[2 * ly][2 * lx + 1] + pa[2 * ly + 1][2 * lx] + pa[2 * ly + 1][2 * lx + 1] + 2) >> 2;
+        static_cast<T*>(a.down_a.p[c])[(size_t)dy * a.down_a.pitch[c] + dx] = (T)v;
+      }
+      if(a.down_b.p[c] != nullptr)
+      {
+        const uint32_t v = ((uint32_t)pb[2 * ly][2 * lx] + pb[2 * ly][2 * lx + 1] + pb[2 * ly + 1][2 * lx] + pb[2 * ly + 1][2 * lx + 1] + 2) >> 2;
+        static_cast<T*>(a.down_b.p[c])[(size_t)dy * a.down_b.pitch[c] + dx] = (T)v;
+      }
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_ssim_win(const SsimWinArgs& a, cudaStream_t s)
+{
+  const dim3 grid((a.W + kSwX * 4 - 1) / (kSwX * 4), (a.H + kSwY * 4 - 1) / (kSwY * 4), 3);
+  k_ssim_win<T><<<grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+template cudaError_t launch_ssim_win<uint8_t>(const SsimWinArgs&, cudaStream_t);
+template cudaError_t launch_ssim_win<uint16_t>(const SsimWinArgs&, cudaStream_t);
+
+// =============================================================================================
+// per window row: compensated sum of the windows in x order (xSSIM.cpp:353-369)
+// =============================================================================================
+__global__ void __launch_bounds__(128) k_ssim_rows(const __grid_constant__ SsimRowArgs a)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if(t >= 3 * a.ny) { return; }
+  const int c = t / a.ny, j = t - c * a.ny;
+  const double* col = a.win + (size_t)c * a.nx * a.ny_pad + j;
+  Kbns k;
+  constexpr int B = 8;
+  int i = 0;
+  for(; i + B <= a.nx; i += B)
+  {
+    double v[B];
+    #pragma unroll
+    for(int u = 0; u < B; u++) { v[u] = col[(size_t)(i + u) * a.ny_pad]; }
+    #pragma unroll
+    for(int u = 0; u < B; u++) { k.add(v[u]); }
+  }
+  for(; i < a.nx; i++) { k.add(col[(size_t)i * a.ny_pad]); }
+  a.row_sum[(size_t)c * a.ny + j] = k.result();
+}
+
+cudaError_t launch_ssim_rows(const SsimRowArgs& a, cudaStream_t s)
+{
+  const int n = 3 * a.ny;
+  k_ssim_rows<<<(n + 127) / 128, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// =============================================================================================
+// finalize: the order-dependent FP64 pooling chains of one pair, one thread per chain.
+// Inputs are staged chunk by chunk into shared memory by all threads so that each chain only
+// waits on its own floating-point dependency.
+//   WS-PSNR   KBNS over rows of rowSSD * w[y]            (xWSPSNR.cpp:123-132)
+//   IV-PSNR   KBNS over rows of rowSSE * w[y] (ERP)       (xIVPSNR.cpp:171-175) + exact uint64 sums
+//   SSIM      KBNS over window rows (ERP: row * w[y + 4], weights KBNS) (xSSIM.cpp:348-351,
+//             xIVSSIM.cpp:148-172)
+// =============================================================================================
+constexpr int kChunk = 128;
+
+struct Chain
+{
+  int kind;  // 0 = WS-PSNR, 1 = IV-PSNR (ERP), 2 = SSIM, 3 = SSIM ERP weight sum
+  int a, b;  // component / direction / slot
+};
+
+__global__ void __launch_bounds__(256) k_finalize(const __grid_constant__ FinalizeArgs a)
+{
+  extern __shared__ double stage[];   // [nchains][kChunk + 1]
+  __shared__ Chain chains[3 + 6 + 3 * kMaxSsimSlots + 1];
+  __shared__ int nch;
+  __shared__ int ws_ny;
+  __shared__ double s_wsum;
+  __shared__ unsigned long long cps_acc[2][3];
+  PairOut* o = a.out;
+
+  if(threadIdx.x == 0)
+  {
+    int n = 0, wny = 0;
+    if(a.do_wspsnr && a.ws) { for(int c = 0; c < 3; c++) { chains[n++] = { 0, c, 0 }; } }
+    if(a.cps_rows && a.ws) { for(int d = 0; d < 2; d++) { for(int c = 0; c < 3; c++) { chains[n++] = { 1, d, c }; } } }
+    for(int s = 0; s < a.nslots; s++)
+    {
+      if(a.slot[s].row_sum == nullptr || a.slot[s].ny <= 0) { continue; }
+      for(int c = 0; c < 3; c++) { chains[n++] = { 2, s, c }; }
+      if(a.slot[s].use_ws) { wny = a.slot[s].ny; }   // ERP-weighted slots are all at full resolution
+    }
+    if(wny > 0 && a.ws) { chains[n++] = { 3, 0, 0 }; }
+    nch = n; ws_ny = wny; s_wsum = 0.0;
+  }
+  if(threadIdx.x < 6) { cps_acc[threadIdx.x / 3][threadIdx.x % 3] = 0ull; }
+  __syncthreads();
+  const int n = nch;
+
+  // exact uint64 totals of the sign-extended 32-bit row sums (order independent)
+  if(a.cps_rows)
+  {
+    unsigned long long loc[6] = { 0, 0, 0, 0, 0, 0 };
+    for(int y = threadIdx.x; y < a.H; y += blockDim.x)
+    {
+      for(int d = 0; d < 2; d++)
+      {
+        for(int c = 0; c < 3; c++)
+        {
+          loc[d * 3 + c] += (unsigned long long)(long long)(int32_t)a.cps_rows[((size_t)d * a.H + y) * 3 + c];
+        }
+      }
+    }
+    for(int k = 0; k < 6; k++) { atomicAdd(&cps_acc[k / 3][k % 3], loc[k]); }
+  }
+
+  auto chain_len = [&](const Chain& ch) { return ch.kind == 2 ? a.slot[ch.a].ny : (ch.kind == 3 ? ws_ny : a.H); };
+  int maxlen = 0;
+  for(int k = 0; k < n; k++) { maxlen = max(maxlen, chain_len(chains[k])); }
+
+  Kbns sum;
+  for(int base = 0; base < maxlen; base += kChunk)
+  {
+    __syncthreads();
+    for(int e = threadIdx.x; e < n * kChunk; e += blockDim.x)
+    {
+      const int k = e / kChunk, u = e - k * kChunk, y = base + u;
+      const Chain ch = chains[k];
+      double v = 0.0;
+      if(y < chain_len(ch))
+      {
+        if(ch.kind == 0)
+        {
+          int off = 0; for(int q = 0; q < ch.a; q++) { off += a.rows[q]; }
+          const uint64_t r = a.row_ssd[off + (y >> a.sy[ch.a])] * (uint64_t)a.mult_row[ch.a];
+          v = dmul((double)r, a.ws[y]);
+        }
+        else if(ch.kind == 1)
+        {
+          const uint64_t r = (uint64_t)(int64_t)(int32_t)a.cps_rows[((size_t)ch.a * a.H + y) * 3 + ch.b];
+          v = dmul((double)r, a.ws[y]);
+        }
+        else if(ch.kind == 2)
+        {
+          const SsimSlot& sl = a.slot[ch.a];
+          v = sl.row_sum[(size_t)ch.b * sl.ny + y];
+          if(sl.use_ws) { v = dmul(v, a.ws[4 * y + 4]); }
+        }
+        else { v = a.ws[4 * y + 4]; }
+      }
+      stage[k * (kChunk + 1) + u] = v;
+    }
+    __syncthreads();
+    if(threadIdx.x < n)
+    {
+      const int cnt = min(kChunk, chain_len(chains[threadIdx.x]) - base);
+      const double* src = stage + threadIdx.x * (kChunk + 1);
+      for(int u = 0; u < cnt; u++) { sum.add(src[u]); }
+    }
+  }
+  __syncthreads();
+  if(threadIdx.x < n && chains[threadIdx.x].kind == 3) { s_wsum = sum.result(); }
+  __syncthreads();
+
+  if(threadIdx.x < n)
+  {
+    const Chain ch = chains[threadIdx.x];
+    if(ch.kind == 0) { o->ws_ssd[ch.a] = sum.result(); }
+    else if(ch.kind == 1) { o->cps_ws[ch.a][ch.b] = sum.result(); }
+    else if(ch.kind == 2)
+    {
+      const SsimSlot& sl = a.slot[ch.a];
+      const double active = (double)((int64_t)sl.nx * sl.ny);
+      double r;
+      if(sl.use_ws)
+      {
+        const double corr = ddiv(s_wsum, (double)sl.ny);
+        r = ddiv(sum.result(), dmul(active, corr));
+      }
+      else { r = ddiv(sum.result(), active); }
+      o->ssim[ch.a][ch.b] = r;
+    }
+  }
+  if(a.cps_rows && threadIdx.x < 6) { o->cps_sum[threadIdx.x / 3][threadIdx.x % 3] = cps_acc[threadIdx.x / 3][threadIdx.x % 3]; }
+}
+
+cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s)
+{
+  int active = 0;
+  for(int s = 0; s < a.nslots; s++) { active += (a.slot[s].row_sum != nullptr && a.slot[s].ny > 0) ? 1 : 0; }
+  const int nch = (a.do_wspsnr && a.ws ? 3 : 0) + (a.cps_rows && a.ws ? 6 : 0) + 3 * active + 1;
+  const size_t smem = (size_t)max(nch, 1) * (kChunk + 1) * sizeof(double);
+  static bool configured = false;
+  if(!configured)
+  {
+    const cudaError_t e = cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)((3 + 6 + 3 * kMaxSsimSlots + 1) * (kChunk + 1) * sizeof(double)));
+    if(e != cudaSuccess) { return e; }
+    configured = true;
+  }
+  k_finalize<<<1, 256, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace qmiv

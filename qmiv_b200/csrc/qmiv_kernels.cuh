@@ -1,0 +1,113 @@
+// Kernel argument blocks and host-side launch wrappers of the QMIV metric kernels.
+#pragma once
+#include "qmiv_device.cuh"
+
+namespace qmiv {
+
+// ---------------------------------------------------------------------------------------------
+// prepass: per raw row of every plane, SD (In1 - In0) and SSD, plus the largest sample per frame
+// ---------------------------------------------------------------------------------------------
+struct PrepassArgs
+{
+  Img       in0, in1;
+  int32_t   rows[3];       // raw rows per plane
+  int32_t   cols[3];       // raw samples per row per plane
+  uint32_t  clip;          // conceal: samples above are clipped (65535 = no clipping)
+  int64_t*  row_sd;        // [rows[0] + rows[1] + rows[2]]
+  uint64_t* row_ssd;       // same indexing
+  PairOut*  out;           // max_sample (atomicMax)
+};
+
+// ---------------------------------------------------------------------------------------------
+// reduce: totals, GCD, path flags
+// ---------------------------------------------------------------------------------------------
+struct ReduceArgs
+{
+  int32_t         rows[3];
+  int32_t         mult[3];     // 4:4:4 multiplicity of a raw chroma sample (1 << (sx + sy))
+  int64_t         area;
+  int32_t         maxv;
+  int32_t         maxdiff[4];  // round(unc * Max) per component, computed on the host in float
+  int32_t         need_gcd;
+  int32_t         fp32_ok;     // fp32 exact-key CPS path is valid for in-range samples
+  int32_t         clip_on;     // conceal active
+  const int64_t*  row_sd;
+  const uint64_t* row_ssd;
+  PairOut*        out;
+};
+
+// ---------------------------------------------------------------------------------------------
+// CPS search, both directions in one pass
+// ---------------------------------------------------------------------------------------------
+struct CpsArgs
+{
+  Img            in0, in1;
+  int32_t        W, H;
+  int32_t        maxv;
+  uint32_t       clip;
+  int32_t        wi[3];        // search weights
+  float          wf[3];
+  const PairOut* gcd_src;      // gcd + flags
+  uint32_t*      rows;         // [2][H][3], zeroed, 32-bit wrap-around sums
+  void*          scp0;         // In0 resampled (T2R search result), planar 3 x W*H, may be null
+  void*          scp1;         // In1 resampled (R2T search result)
+};
+
+// ---------------------------------------------------------------------------------------------
+// block SSIM: per-window values (+ fused 2x2 downsampling of the inputs)
+// ---------------------------------------------------------------------------------------------
+struct SsimWinArgs
+{
+  Img     a, b;                // a = "Tst" picture, b = "Ref" picture of xSSIM::xCalcPicSSIM
+  int32_t W, H;
+  int32_t nx, ny, ny_pad;      // windows per row / column, column stride of win
+  uint32_t clip;
+  double  C1, C2;
+  int32_t calc_l;
+  double* win;                 // [3][nx][ny_pad]
+  MutImg  down_a, down_b;      // outputs ((W>>1) x (H>>1), 4:4:4) or null planes
+};
+
+struct SsimRowArgs
+{
+  const double* win;           // [3][nx][ny_pad]
+  int32_t       nx, ny, ny_pad;
+  double*       row_sum;       // [3][ny]
+};
+
+// ---------------------------------------------------------------------------------------------
+// finalize: every serial KBNS chain of one frame pair, one thread per chain
+// ---------------------------------------------------------------------------------------------
+struct SsimSlot
+{
+  const double* row_sum;       // [3][ny]
+  int32_t       nx, ny;
+  int32_t       use_ws;        // ERP row weights w[4j + 4] (xIVSSIM.cpp:148-165)
+};
+
+struct FinalizeArgs
+{
+  int32_t         H;
+  int32_t         rows[3];
+  int32_t         sy[3], mult_row[3];   // 4:4:4 row y of plane c = raw row (y >> sy) times mult_row
+  const uint64_t* row_ssd;              // prepass rows
+  const double*   ws;                   // [H] equirectangular weights or null
+  int32_t         do_wspsnr;
+  const uint32_t* cps_rows;             // [2][H][3] or null
+  int32_t         nslots;
+  SsimSlot        slot[kMaxSsimSlots];
+  PairOut*        out;
+};
+
+// launch wrappers (return cudaError_t of the launch)
+template <typename T> cudaError_t launch_prepass(const PrepassArgs& a, cudaStream_t s);
+cudaError_t launch_reduce(const ReduceArgs& a, cudaStream_t s);
+template <typename T> cudaError_t launch_cps(const CpsArgs& a, int R, cudaStream_t s);
+template <typename T> cudaError_t launch_ssim_win(const SsimWinArgs& a, cudaStream_t s);
+cudaError_t launch_ssim_rows(const SsimRowArgs& a, cudaStream_t s);
+cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
+
+// Exactness check of the fp32 key path for a given bit depth, weights and GCD clip range.
+bool cps_fp32_exact(int32_t maxv, const int32_t w[3], const int32_t maxdiff[3]);
+
+}  // namespace qmiv
