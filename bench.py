@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Throughput of the QMIV metric hot path on B200: IV-PSNR + WS-PSNR + IV-SSIM frame pairs per second
+on 4096x2048 10-bit 4:2:0 equirectangular pairs (the reference's workload, synthetic frames).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qmiv|reference]
+
+One step = one pass of the metric pipeline over a batch of 8 frame pairs per GPU. N > 1 runs one
+process per GPU (torchrun); pairs are independent, so every rank processes its own 8 pairs (weak
+scaling, no collective on the data path) and rank 0 prints one JSON line.
+
+`--impl reference` times the reference's own multithreaded CPU implementation (the QMIV app built
+from its sources into oracle/_ref by oracle/Makefile) on the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, BD, CF = 4096, 2048, 10, 420
+PAIRS_PER_STEP = 8
+METRIC_NAME = "IV-PSNR frame-pairs/s @4096x2048 10b"
+METRICS = ("IVPSNR", "WSPSNR", "IVSSIM")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------------------------
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, local):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------------------------
+def make_workload(rank, n=PAIRS_PER_STEP):
+    from qmiv_b200 import synth
+    t0 = time.time()
+    pairs = [synth.make_pair(W, H, BD, seed=1000 * rank + i) for i in range(n)]
+    log(f"[rank {rank}] generated {n} synthetic {W}x{H} {BD}-bit pairs in {time.time() - t0:.1f}s")
+    return pairs
+
+
+def frame_bytes(frame):
+    return int(sum(p.nbytes for p in frame))
+
+
+def cps_candidates(R=2):
+    return 2 * W * H * (2 * R + 1) ** 2
+
+
+def run_qmiv(args, world, rank, local):
+    import torch
+    import qmiv_b200
+    from qmiv_b200 import _lib
+
+    torch.cuda.set_device(local)
+    pairs = make_workload(rank)
+    mask = qmiv_b200.metric_mask(METRICS)
+    dev_pairs = [tuple(tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in fr) for fr in pr) for pr in pairs]
+    host_pairs = [tuple(tuple(torch.from_numpy(np.ascontiguousarray(p)).pin_memory() for p in fr) for fr in pr)
+                  for pr in pairs]
+    host_np = [tuple(tuple(t.numpy() for t in fr) for fr in pr) for pr in host_pairs]
+
+    def descs(src):
+        return [dict(frame0=a, frame1=b, width=W, height=H, bitdepth=BD, chroma_format=CF, search_range=2,
+                     metrics=mask) for a, b in src]
+
+    ctx = qmiv_b200.Context(local)
+    batch = qmiv_b200.Batch(ctx, max_pairs=PAIRS_PER_STEP, max_pixels=PAIRS_PER_STEP * W * H, erp=True)
+    stream = torch.cuda.ExternalStream(batch.stream(), device=f"cuda:{local}")
+    dev_desc, host_desc = descs(dev_pairs), descs(host_np)
+
+    for _ in range(args.warmup):
+        batch.compute(dev_desc)
+    torch.cuda.synchronize()
+
+    # ---- device-resident inputs (value) ----
+    ctx.stage_times(reset=True)
+    ctx.set_profiling(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        results = None
+        for _ in range(args.steps):
+            results = batch.compute(dev_desc)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    ctx.set_profiling(False)
+    ms = ev0.elapsed_time(ev1)
+    stage = ctx.stage_times(reset=True)
+    ms_max = max_over_ranks(ms, world, local)
+
+    # ---- end to end through the public API, pinned host frames (e2e) ----
+    for _ in range(max(1, args.warmup // 2)):
+        batch.compute(host_desc)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        host_results = batch.compute(host_desc)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, local)
+    assert host_results == results, "host-frame and device-frame results differ"
+
+    # ---- probes for the search kernel's roofline denominator ----
+    lib = qmiv_b200.library()
+    int_peak = __import__("ctypes").c_double()
+    _lib.check(lib.qmiv_probe_int32_peak(local, 4096, __import__("ctypes").byref(int_peak)), "probe")
+
+    batch.close()
+    ctx.close()
+
+    units = world * PAIRS_PER_STEP * args.steps
+    value = units / (ms_max / 1e3)
+    e2e_value = units / (e2e_ms / 1e3)
+    cps_ms, cps_n = stage["cps"]
+    cps_avg_ms = cps_ms / max(cps_n, 1)
+    ops_per_launch = 8.0 * cps_candidates()
+    achieved = ops_per_launch / (cps_avg_ms * 1e-3) / 1e12
+    h2d = sum(frame_bytes(a) + frame_bytes(b) for a, b in pairs)
+    d2h = PAIRS_PER_STEP * 632  # sizeof(PairOut), the device result block read back per pair
+    return dict(value=value, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
+                achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
+                sample=results[0])
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU side: the reference app on the host cores
+# ---------------------------------------------------------------------------------------------
+def reference_app():
+    import oracle
+    path = os.path.join(oracle.reference_dir(), "QMIV")
+    return path if os.path.exists(path) else None
+
+
+def run_reference_app(n_frames, threads, seed=0):
+    app = reference_app()
+    if app is None:
+        return None
+    from qmiv_b200 import synth
+    tmp = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    files = [os.path.join(tmp, "in0.yuv"), os.path.join(tmp, "in1.yuv")]
+    try:
+        with open(files[0], "wb") as f0, open(files[1], "wb") as f1:
+            for i in range(n_frames):
+                a, b = synth.make_pair(W, H, BD, seed=seed + i)
+                for p in a:
+                    f0.write(np.ascontiguousarray(p).tobytes())
+                for p in b:
+                    f1.write(np.ascontiguousarray(p).tobytes())
+        cmd = [app, "-i0", files[0], "-i1", files[1], "-ps", f"{W}x{H}", "-bd", str(BD), "-cf", str(CF), "-erp",
+               "-ml", ", ".join(METRICS), "-nth", str(threads), "-v", "3"]
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=900).stdout
+    finally:
+        for f in files:
+            if os.path.exists(f):
+                os.remove(f)
+        os.rmdir(tmp)
+    m = re.search(r"TotalProcessingTime\s*=\s*([0-9.]+)\s*s", out)
+    if not m:
+        raise RuntimeError("could not parse the reference app's output:\n" + out[-2000:])
+    secs = float(m.group(1))
+    ivpsnr = re.search(r"Average\s+IVPSNR\s+([0-9.]+)", out)
+    return dict(value=n_frames / secs, secs=secs, frames=n_frames, threads=threads,
+                ivpsnr=float(ivpsnr.group(1)) if ivpsnr else None)
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["qmiv", "reference"], default="qmiv")
+    ap.add_argument("--cpu-frames", type=int, default=4, help="frames of the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warm-up raised to 3 steps")
+        args.warmup = 3
+
+    world, rank, local = dist_setup(args.gpus)
+    cfg = {"workload": "IV-PSNR + WS-PSNR + IV-SSIM, 8 frame pairs per GPU per step, 4096x2048 10-bit 4:2:0 ERP",
+           "width": W, "height": H, "bitdepth": BD, "chroma_format": CF, "search_range": 2,
+           "pairs_per_step_per_gpu": PAIRS_PER_STEP, "metrics": list(METRICS),
+           "l2": "inputs 8 pairs x 50 MB per GPU exceed the 126 MB L2; no flush needed",
+           "parallelism": f"replicas{world}"}
+
+    if args.impl == "reference":
+        if rank == 0:
+            threads = host_threads()
+            # each step: one bounded sample of the workload through the reference app
+            vals = []
+            for s in range(args.warmup + args.steps):
+                r = run_reference_app(max(1, args.cpu_frames // 2), threads, seed=s * 100)
+                if r is None:
+                    print(json.dumps({"impl": "reference", "unavailable": "reference app not built (oracle/_ref missing)"}))
+                    return
+                if s >= args.warmup:
+                    vals.append(r)
+            secs = sum(v["secs"] for v in vals)
+            frames = sum(v["frames"] for v in vals)
+            value = frames / secs
+            out = {"metric": METRIC_NAME, "value": value, "unit": "frame-pairs/s", "n_gpus": args.gpus,
+                   "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(vals),
+                   "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32+f64",
+                   "data": "synthetic", "config": cfg, "impl": "reference",
+                   "cpu_baseline": {"value": value, "unit": "frame-pairs/s", "cores": threads, "kind": "reference",
+                                    "sample": f"{vals[0]['frames']} frame pairs per step through the QMIV app "
+                                              f"(oracle/_ref) with -nth {threads}"},
+                   "e2e": {"value": value, "unit": "frame-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(out))
+        barrier(world)
+        return
+
+    r = run_qmiv(args, world, rank, local)
+    if rank != 0:
+        barrier(world)
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            c = run_reference_app(args.cpu_frames, host_threads())
+            if c:
+                cpu = {"value": c["value"], "unit": "frame-pairs/s", "cores": c["threads"], "kind": "reference",
+                       "sample": f"{c['frames']} frame pairs of the same workload through the QMIV app "
+                                 f"(oracle/_ref) with -nth {c['threads']}, {c['secs']:.2f} s"}
+        except Exception as e:  # the GPU number stands without the CPU baseline
+            log("cpu baseline failed:", e)
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        with open(pk) as f:
+            peaks = json.load(f)
+    out = {"metric": METRIC_NAME, "value": r["value"], "unit": "frame-pairs/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "int32+f64", "data": "synthetic", "config": cfg,
+           "e2e": {"value": r["e2e"], "unit": "frame-pairs/s", "h2d_bytes_per_step": r["h2d"],
+                   "d2h_bytes_per_step": r["d2h"]},
+           "gpu_launches": None,
+           "roofline": {"kernel": "k_cps (CPS search, both directions)", "bound": "int32",
+                        "achieved": r["achieved"], "peak": r["int_peak"], "unit": "TOP/s",
+                        "frac": r["achieved"] / r["int_peak"] if r["int_peak"] else None,
+                        "traffic": None,
+                        "accounting": "8 int32 ops per candidate, 2*W*H*25 candidates per launch; peak measured "
+                                      "by qmiv_probe_int32_peak on this GPU",
+                        "avg_launch_ms": r["cps_avg_ms"]},
+           "stage_ms_per_pair": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
+           "clocks": r["clocks"],
+           "cpu_baseline": cpu,
+           "sample_result": {k: r["sample"][k] for k in ("gcd_r2t", "ivpsnr", "wspsnr_pic", "ivssim")},
+           "hbm_peak_gbs": peaks.get("hbm_gbs")}
+    launches = sum(v[1] for k, v in r["stage"].items() if k not in ("h2d", "d2h"))
+    out["gpu_launches"] = launches
+    print(json.dumps(out))
+    barrier(world)
+
+
+if __name__ == "__main__":
+    main()

@@ -145,6 +145,26 @@ QMIV_API qmiv_status qmiv_ctx_create(int32_t device, uint64_t hbm_budget_bytes, 
 QMIV_API qmiv_status qmiv_ctx_destroy(qmiv_ctx ctx);
 QMIV_API qmiv_status qmiv_ctx_memory(qmiv_ctx ctx, uint64_t* used_bytes, uint64_t* budget_bytes);
 
+/* Per-stage device timing, the counterpart of the reference's per-stage tick accounting at
+   VerboseLevel >= 3 (apps/QMIV/src/xAppQMIV.cpp:763-826, AvgTime table :1151-1219). When enabled,
+   every calc/batch of the context brackets each stage's launches with CUDA events on the stream
+   they run on; qmiv_ctx_stage_times returns the accumulated milliseconds and launch counts per
+   stage (indices QMIV_STAGE_*) and, if reset != 0, clears them. */
+enum
+{
+  QMIV_STAGE_H2D = 0,        /* host frame upload */
+  QMIV_STAGE_PREPASS = 1,    /* per-row SD/SSD */
+  QMIV_STAGE_REDUCE = 2,     /* totals + GCD */
+  QMIV_STAGE_CPS = 3,        /* corresponding-pixel-shift search, both directions */
+  QMIV_STAGE_SSIM_WIN = 4,   /* SSIM windows (+ pyramid downsampling) */
+  QMIV_STAGE_SSIM_ROWS = 5,  /* per-row SSIM sums */
+  QMIV_STAGE_FINALIZE = 6,   /* FP64 pooling chains */
+  QMIV_STAGE_D2H = 7,        /* result read-back */
+  QMIV_NUM_STAGES = 8
+};
+QMIV_API qmiv_status qmiv_ctx_set_profiling(qmiv_ctx ctx, int32_t enable);
+QMIV_API qmiv_status qmiv_ctx_stage_times(qmiv_ctx ctx, double ms[8], uint64_t launches[8], int32_t reset);
+
 /* ---- plain form: one frame pair per call -------------------------------------------------- */
 QMIV_API qmiv_status qmiv_calc_create(qmiv_ctx ctx, int32_t width, int32_t height, int32_t bitdepth, int32_t chroma_format,
                              const qmiv_params* params, qmiv_calc* out_calc);
@@ -170,6 +190,11 @@ QMIV_API qmiv_status qmiv_calc_gcd(qmiv_calc calc, const qmiv_frame* in0, const 
 QMIV_API qmiv_status qmiv_calc_scp(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, const int32_t* gcd_r2t,
                           uint16_t* scp0, uint16_t* scp1, int32_t dst_mem);
 
+/* Use a caller-supplied GCD (R2T convention) instead of computing it, for the reference's
+   calcPicIVPSNR(Tst, Ref, GlobalColorDiffRef2Tst) (xIVPSNR.h:36) and GenShftCompPics(..., GCD)
+   (xShftCompPic.h:44-47) forms. NULL restores the computed GCD. Applies to later calls. */
+QMIV_API qmiv_status qmiv_calc_set_gcd(qmiv_calc calc, const int32_t* gcd_r2t);
+
 /* Per-row CPS SSE of the last computed pair: rows_r2t/rows_t2r receive H*3 uint64 values
    (row-major, component fastest) with the reference's 32-bit-lane accumulation semantics
    (xCorrespPixelShiftSSE.cpp:29-40). Either pointer may be NULL. */
@@ -194,6 +219,8 @@ QMIV_API qmiv_status qmiv_batch_create(qmiv_ctx ctx, int32_t max_pairs, int64_t 
                               int32_t use_graph, qmiv_batch* out_batch);
 QMIV_API qmiv_status qmiv_batch_destroy(qmiv_batch batch);
 QMIV_API qmiv_status qmiv_batch_compute(qmiv_batch batch, const qmiv_pair_desc* pairs, int32_t num_pairs, qmiv_result* out);
+/* Device stream (cudaStream_t) the batch enqueues on. */
+QMIV_API qmiv_status qmiv_batch_stream(qmiv_batch batch, void** cuda_stream);
 /* Tile shapes picked by the autotuner for (width, height, bitdepth, R): for inspection and tests. */
 QMIV_API qmiv_status qmiv_batch_tuning(qmiv_batch batch, int32_t width, int32_t height, int32_t bitdepth, int32_t search_range,
                               int32_t* cps_tile_w, int32_t* cps_tile_h, int32_t* cps_rows_per_thread);

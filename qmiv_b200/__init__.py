@@ -119,6 +119,15 @@ class Context:
         check(self._lib.qmiv_ctx_memory(self.handle, ctypes.byref(used), ctypes.byref(budget)), "qmiv_ctx_memory")
         return used.value, budget.value
 
+    def set_profiling(self, enable: bool = True):
+        check(self._lib.qmiv_ctx_set_profiling(self.handle, int(bool(enable))), "qmiv_ctx_set_profiling")
+
+    def stage_times(self, reset: bool = False) -> dict:
+        """{stage: (milliseconds, launches)} accumulated while profiling was on."""
+        ms, n = (ctypes.c_double * 8)(), (ctypes.c_uint64 * 8)()
+        check(self._lib.qmiv_ctx_stage_times(self.handle, ms, n, int(bool(reset))), "qmiv_ctx_stage_times")
+        return {name: (ms[i], n[i]) for i, name in enumerate(_lib.STAGES)}
+
     def close(self):
         if self.handle:
             check(self._lib.qmiv_ctx_destroy(self.handle), "qmiv_ctx_destroy")
@@ -196,6 +205,11 @@ class Calc:
                                       _lib.MEM_HOST), "qmiv_calc_scp")
         return s0, s1
 
+    def set_gcd(self, gcd_r2t=None):
+        """Use a given GCD (R2T convention) for later calls, as calcPicIVPSNR(Tst, Ref, GCD); None clears."""
+        arg = None if gcd_r2t is None else (ctypes.c_int32 * 4)(*gcd_r2t)
+        check(self._lib.qmiv_calc_set_gcd(self.handle, arg), "qmiv_calc_set_gcd")
+
     def cps_rows(self):
         """Per-row CPS SSE (H, 3) of the last computed pair, (R2T, T2R)."""
         a = np.zeros((self.height, 3), np.uint64)
@@ -269,6 +283,12 @@ class Batch:
         out = (_lib.QmivResult * max(1, len(pairs)))()
         check(self._lib.qmiv_batch_compute(self.handle, descs, len(pairs), out), "qmiv_batch_compute")
         return [out[i].as_dict() for i in range(len(pairs))]
+
+    def stream(self) -> int:
+        """cudaStream_t of the batch, as an integer (for torch.cuda.ExternalStream)."""
+        p = ctypes.c_void_p()
+        check(self._lib.qmiv_batch_stream(self.handle, ctypes.byref(p)), "qmiv_batch_stream")
+        return p.value or 0
 
     def tuning(self, width, height, bitdepth, search_range):
         tw, th, p = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()

@@ -21,6 +21,7 @@ METRIC_BITS = {"PSNR": PSNR, "WSPSNR": WSPSNR, "IVPSNR": IVPSNR, "SSIM": SSIM, "
                "IVSSIM": IVSSIM, "IVMSSSIM": IVMSSSIM}
 
 MEM_HOST, MEM_DEVICE = 0, 1
+STAGES = ["h2d", "prepass", "reduce", "cps", "ssim_win", "ssim_rows", "finalize", "d2h"]
 PEL_SKIP, PEL_WARN, PEL_STOP, PEL_CNCL = 0, 1, 2, 3
 
 
@@ -75,6 +76,8 @@ SIGNATURES = {
     "qmiv_ctx_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, _PP]),
     "qmiv_ctx_destroy": (ctypes.c_int, [_P]),
     "qmiv_ctx_memory": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "qmiv_ctx_set_profiling": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "qmiv_ctx_stage_times": (ctypes.c_int, [_P, ctypes.c_double * 8, ctypes.c_uint64 * 8, ctypes.c_int32]),
     "qmiv_calc_create": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.POINTER(QmivParams), _PP]),
     "qmiv_calc_destroy": (ctypes.c_int, [_P]),
@@ -85,11 +88,15 @@ SIGNATURES = {
     "qmiv_calc_gcd": (ctypes.c_int, [_P, ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame), ctypes.c_int32 * 4]),
     "qmiv_calc_scp": (ctypes.c_int, [_P, ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame),
                                      ctypes.POINTER(ctypes.c_int32), _P, _P, ctypes.c_int32]),
+    "qmiv_calc_set_gcd": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "qmiv_calc_cps_rows": (ctypes.c_int, [_P, _P, _P]),
     "qmiv_calc_stream": (ctypes.c_int, [_P, _PP]),
     "qmiv_batch_create": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(QmivParams),
                                          ctypes.c_int32, _PP]),
+    "qmiv_probe_int32_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
+    "qmiv_probe_fp32_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "qmiv_batch_destroy": (ctypes.c_int, [_P]),
+    "qmiv_batch_stream": (ctypes.c_int, [_P, _PP]),
     "qmiv_batch_compute": (ctypes.c_int, [_P, ctypes.POINTER(QmivPairDesc), ctypes.c_int32, ctypes.POINTER(QmivResult)]),
     "qmiv_batch_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),

@@ -86,11 +86,19 @@ qmiv_status qmiv_batch_compute(qmiv_batch b, const qmiv_pair_desc* pairs, int32_
   qmiv_status st = QMIV_OK;
   for(int i = 0; i < n; i++)
   {
+    b->pipes[i]->harvest_profile();
     const PairOut& o = b->pipes[i]->host_out();
     finish_result(o, b->pipes[i]->finish_info(pairs[i].metric_mask), &out[i]);
     if(b->prm.invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3)) { st = fail(QMIV_ERR_INVALID_PIXEL, "invalid pixel in a batched pair"); }
   }
   return st;
+}
+
+qmiv_status qmiv_batch_stream(qmiv_batch b, void** cuda_stream)
+{
+  if(!b || !cuda_stream) { return fail(QMIV_ERR_INVALID_ARG, "null argument"); }
+  *cuda_stream = (void*)b->stream;
+  return QMIV_OK;
 }
 
 qmiv_status qmiv_batch_tuning(qmiv_batch b, int32_t width, int32_t height, int32_t bitdepth, int32_t search_range,

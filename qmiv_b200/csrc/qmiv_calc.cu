@@ -45,6 +45,40 @@ qmiv_status validate_params(const qmiv_params& p)
 PairPipeline::~PairPipeline()
 {
   if(h_out) { cudaFreeHost(h_out); h_out = nullptr; }
+  for(cudaEvent_t e : ev_pool_) { cudaEventDestroy(e); }
+}
+
+int PairPipeline::prof_begin(cudaStream_t s)
+{
+  if(!ctx_ || !ctx_->profiling) { return -1; }
+  while(ev_pool_.size() < ev_used_ + 2)
+  {
+    cudaEvent_t e;
+    if(cudaEventCreate(&e) != cudaSuccess) { return -1; }
+    ev_pool_.push_back(e);
+  }
+  const int tok = (int)ev_used_;
+  ev_used_ += 2;
+  cudaEventRecord(ev_pool_[tok], s);
+  return tok;
+}
+
+void PairPipeline::prof_end(cudaStream_t s, int stage, int tok)
+{
+  if(tok < 0) { return; }
+  cudaEventRecord(ev_pool_[tok + 1], s);
+  ev_pending_.emplace_back(stage, tok);
+}
+
+void PairPipeline::harvest_profile()
+{
+  for(const auto& p : ev_pending_)
+  {
+    float ms = 0.f;
+    if(cudaEventElapsedTime(&ms, ev_pool_[p.second], ev_pool_[p.second + 1]) == cudaSuccess) { ctx_->add_stage(p.first, ms); }
+  }
+  ev_pending_.clear();
+  ev_used_ = 0;
 }
 
 qmiv_status PairPipeline::configure(qmiv_ctx_s* ctx, const Shape& shape, const qmiv_params& prm, int32_t search_range)
@@ -111,6 +145,7 @@ qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cuda
   const Shape& S = shape_;
   if(!f) { return fail(QMIV_ERR_INVALID_ARG, "frame is null"); }
   size_t off = (size_t)which * S.frame_bytes();
+  const int tok = f->mem == QMIV_MEM_HOST ? prof_begin(s) : -1;
   for(int c = 0; c < 3; c++)
   {
     if(!f->plane[c]) { return fail(QMIV_ERR_INVALID_ARG, "frame plane is null"); }
@@ -134,6 +169,7 @@ qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cuda
     }
     else { return fail(QMIV_ERR_INVALID_ARG, "frame mem must be QMIV_MEM_HOST or QMIV_MEM_DEVICE"); }
   }
+  prof_end(s, QMIV_STAGE_H2D, tok);
   return QMIV_OK;
 }
 
@@ -193,15 +229,22 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
   pa.in0 = in0; pa.in1 = in1;
   for(int c = 0; c < 3; c++) { pa.rows[c] = (int32_t)S.plane_rows(c); pa.cols[c] = (int32_t)S.plane_cols(c); }
   pa.clip = clip; pa.row_sd = row_sd_.as<int64_t>(); pa.row_ssd = row_ssd_.as<uint64_t>(); pa.out = dout;
-  QMIV_CUDA(launch_prepass<T>(pa, s));
+  { const int t = prof_begin(s); QMIV_CUDA(launch_prepass<T>(pa, s)); prof_end(s, QMIV_STAGE_PREPASS, t); }
 
   ReduceArgs ra{};
   for(int c = 0; c < 3; c++) { ra.rows[c] = pa.rows[c]; ra.mult[c] = c ? (1 << (S.sx + S.sy)) : 1; }
   ra.area = (int64_t)S.W * S.H; ra.maxv = S.maxv;
   for(int c = 0; c < 4; c++) { ra.maxdiff[c] = maxdiff_[c]; }
   ra.need_gcd = need_search || want_gcd; ra.fp32_ok = fp32_ok_; ra.clip_on = prm_.invalid_pel_action == QMIV_PEL_CNCL;
+  if(gcd_override_on_)
+  {
+    int32_t mag[4];
+    for(int c = 0; c < 4; c++) { ra.gcd_override[c] = gcd_override_[c]; mag[c] = gcd_override_[c] < 0 ? -gcd_override_[c] : gcd_override_[c]; }
+    ra.gcd_override_on = 1;
+    ra.fp32_ok = cps_fp32_exact(S.maxv, prm_.cws, mag);
+  }
   ra.row_sd = pa.row_sd; ra.row_ssd = pa.row_ssd; ra.out = dout;
-  QMIV_CUDA(launch_reduce(ra, s));
+  { const int t = prof_begin(s); QMIV_CUDA(launch_reduce(ra, s)); prof_end(s, QMIV_STAGE_REDUCE, t); }
 
   // 2. CPS search, both directions, SCP pictures when needed
   if(need_search)
@@ -212,7 +255,9 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
     ca.gcd_src = dout; ca.rows = cps_rows_.as<uint32_t>();
     ca.scp0 = need_scp ? const_cast<void*>(scp(0)) : nullptr;
     ca.scp1 = need_scp ? const_cast<void*>(scp(1)) : nullptr;
+    const int t = prof_begin(s);
     QMIV_CUDA(launch_cps<T>(ca, R_, s));
+    prof_end(s, QMIV_STAGE_CPS, t);
   }
 
   // 3. SSIM family
@@ -226,11 +271,11 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
     wa.clip = clip; wa.C1 = C1_; wa.C2 = C2_; wa.calc_l = calc_l; wa.win = win_.as<double>();
     if(down_a) { wa.down_a = *down_a; }
     if(down_b) { wa.down_b = *down_b; }
-    QMIV_CUDA(launch_ssim_win<T>(wa, s));
+    { const int t = prof_begin(s); QMIV_CUDA(launch_ssim_win<T>(wa, s)); prof_end(s, QMIV_STAGE_SSIM_WIN, t); }
     SsimRowArgs rr{};
     rr.win = wa.win; rr.nx = wa.nx; rr.ny = wa.ny; rr.ny_pad = nyp_;
     rr.row_sum = rowsum + (size_t)slot * 3 * ny_[0];
-    QMIV_CUDA(launch_ssim_rows(rr, s));
+    { const int t = prof_begin(s); QMIV_CUDA(launch_ssim_rows(rr, s)); prof_end(s, QMIV_STAGE_SSIM_ROWS, t); }
     fa.slot[slot].row_sum = rr.row_sum; fa.slot[slot].nx = wa.nx; fa.slot[slot].ny = wa.ny; fa.slot[slot].use_ws = use_ws;
     return QMIV_OK;
   };
@@ -293,8 +338,8 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
   fa.do_wspsnr = (mask & QMIV_WSPSNR) ? 1 : 0;
   fa.cps_rows = need_search ? cps_rows_.as<uint32_t>() : nullptr;
   fa.out = dout;
-  QMIV_CUDA(launch_finalize(fa, s));
-  QMIV_CUDA(cudaMemcpyAsync(h_out, dout, sizeof(PairOut), cudaMemcpyDeviceToHost, s));
+  { const int t = prof_begin(s); QMIV_CUDA(launch_finalize(fa, s)); prof_end(s, QMIV_STAGE_FINALIZE, t); }
+  { const int t = prof_begin(s); QMIV_CUDA(cudaMemcpyAsync(h_out, dout, sizeof(PairOut), cudaMemcpyDeviceToHost, s)); prof_end(s, QMIV_STAGE_D2H, t); }
   return QMIV_OK;
 }
 
@@ -345,6 +390,7 @@ static qmiv_status calc_collect(qmiv_calc calc, int32_t timeout_ms, qmiv_result*
   QMIV_TRY(wait_event(calc->done, timeout_ms));
   calc->pending = false;
   calc->has_last = true;
+  calc->pipe.harvest_profile();
   const PairOut& o = calc->pipe.host_out();
   if(out) { finish_result(o, calc->pipe.finish_info(calc->pending_mask), out); }
   if(calc->prm.invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3))
@@ -423,9 +469,14 @@ qmiv_status qmiv_calc_scp(qmiv_calc calc, const qmiv_frame* in0, const qmiv_fram
                           uint16_t* scp0, uint16_t* scp1, int32_t dst_mem)
 {
   if(dst_mem != QMIV_MEM_HOST && dst_mem != QMIV_MEM_DEVICE) { return fail(QMIV_ERR_INVALID_ARG, "bad dst_mem"); }
-  if(gcd_r2t) { return fail(QMIV_ERR_UNSUPPORTED, "an externally supplied GCD is not supported; pass NULL"); }
-  QMIV_TRY(calc_submit(calc, in0, in1, 0, true));
-  QMIV_TRY(calc_collect(calc, -1, nullptr));
+  if(!calc) { return fail(QMIV_ERR_INVALID_ARG, "calc is null"); }
+  int32_t saved[4];
+  const bool had = calc->pipe.get_gcd_override(saved);
+  if(gcd_r2t) { calc->pipe.set_gcd_override(gcd_r2t); }
+  qmiv_status st = calc_submit(calc, in0, in1, 0, true);
+  if(st == QMIV_OK) { st = calc_collect(calc, -1, nullptr); }
+  calc->pipe.set_gcd_override(had ? saved : nullptr);
+  QMIV_TRY(st);
   const Shape& S = calc->shape;
   const size_t n = (size_t)3 * S.W * S.H;
   for(int k = 0; k < 2; k++)
@@ -465,6 +516,14 @@ qmiv_status qmiv_calc_cps_rows(qmiv_calc calc, uint64_t* rows_r2t, uint64_t* row
     if(!dst) { continue; }
     for(size_t i = 0; i < (size_t)S.H * 3; i++) { dst[i] = (uint64_t)(int64_t)(int32_t)tmp[(size_t)d * S.H * 3 + i]; }
   }
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_calc_set_gcd(qmiv_calc calc, const int32_t* gcd_r2t)
+{
+  if(!calc) { return fail(QMIV_ERR_INVALID_ARG, "calc is null"); }
+  if(calc->pending) { return fail(QMIV_ERR_BUSY, "a submission is in flight on this calc"); }
+  calc->pipe.set_gcd_override(gcd_r2t);
   return QMIV_OK;
 }
 

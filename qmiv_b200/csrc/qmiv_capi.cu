@@ -288,6 +288,27 @@ qmiv_status qmiv_ctx_destroy(qmiv_ctx ctx)
   return QMIV_OK;
 }
 
+qmiv_status qmiv_ctx_set_profiling(qmiv_ctx ctx, int32_t enable)
+{
+  if(!ctx) { return fail(QMIV_ERR_INVALID_ARG, "ctx is null"); }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->profiling = enable != 0;
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_ctx_stage_times(qmiv_ctx ctx, double ms[8], uint64_t launches[8], int32_t reset)
+{
+  if(!ctx) { return fail(QMIV_ERR_INVALID_ARG, "ctx is null"); }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  for(int i = 0; i < QMIV_NUM_STAGES; i++)
+  {
+    if(ms) { ms[i] = ctx->stage_ms[i]; }
+    if(launches) { launches[i] = ctx->stage_n[i]; }
+    if(reset) { ctx->stage_ms[i] = 0.0; ctx->stage_n[i] = 0; }
+  }
+  return QMIV_OK;
+}
+
 qmiv_status qmiv_ctx_memory(qmiv_ctx ctx, uint64_t* used_bytes, uint64_t* budget_bytes)
 {
   if(!ctx) { return fail(QMIV_ERR_INVALID_ARG, "ctx is null"); }

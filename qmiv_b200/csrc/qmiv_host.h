@@ -16,6 +16,16 @@ struct qmiv_ctx_s
   std::mutex mu;
   bool reserve(size_t n);
   void unreserve(size_t n);
+  // per-stage timing (QMIV_STAGE_*)
+  bool     profiling = false;
+  double   stage_ms[QMIV_NUM_STAGES] = {};
+  uint64_t stage_n[QMIV_NUM_STAGES] = {};
+  void add_stage(int stage, double ms)
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    stage_ms[stage] += ms;
+    stage_n[stage] += 1;
+  }
 };
 
 namespace qmiv {
@@ -105,6 +115,20 @@ public:
   const uint32_t* cps_rows() const { return cps_rows_.as<uint32_t>(); }
   const Shape& shape() const { return shape_; }
   int32_t search_range() const { return R_; }
+  void set_gcd_override(const int32_t* g)
+  {
+    gcd_override_on_ = g != nullptr;
+    for(int c = 0; c < 4; c++) { gcd_override_[c] = g ? g[c] : 0; }
+  }
+  bool get_gcd_override(int32_t g[4]) const
+  {
+    for(int c = 0; c < 4; c++) { g[c] = gcd_override_[c]; }
+    return gcd_override_on_;
+  }
+  // stage timing: events recorded on the launching stream, harvested after the stream synced
+  int  prof_begin(cudaStream_t s);
+  void prof_end(cudaStream_t s, int stage, int token);
+  void harvest_profile();
   ~PairPipeline();
 
 private:
@@ -125,6 +149,11 @@ private:
   DevMem row_sd_, row_ssd_, cps_rows_, out_, ws_, scp_, pyr_, win_, rowsum_, staging_;
   PairOut* h_out = nullptr;
   bool ws_uploaded_ = false;
+  bool gcd_override_on_ = false;
+  int32_t gcd_override_[4] = { 0, 0, 0, 0 };
+  std::vector<cudaEvent_t> ev_pool_;
+  size_t ev_used_ = 0;
+  std::vector<std::pair<int, int>> ev_pending_;  // (stage, index of the begin event)
 };
 
 }  // namespace qmiv

@@ -108,7 +108,8 @@ __global__ void __launch_bounds__(1024) k_reduce(const __grid_constant__ ReduceA
     for(int c = 0; c < 4; c++)
     {
       int32_t g = 0;
-      if(a.need_gcd)
+      if(a.gcd_override_on) { g = a.gcd_override[c]; }
+      else if(a.need_gcd)
       {
         const double avg = ddiv(c < 3 ? (double)o->sd[c] : 0.0, area);
         g = clampi(round_half_away(avg), -a.maxdiff[c], a.maxdiff[c]);

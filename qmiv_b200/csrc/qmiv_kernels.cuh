@@ -29,6 +29,8 @@ struct ReduceArgs
   int32_t         maxv;
   int32_t         maxdiff[4];  // round(unc * Max) per component, computed on the host in float
   int32_t         need_gcd;
+  int32_t         gcd_override_on;  // use gcd_override instead of the computed GCD
+  int32_t         gcd_override[4];
   int32_t         fp32_ok;     // fp32 exact-key CPS path is valid for in-range samples
   int32_t         clip_on;     // conceal active
   const int64_t*  row_sd;

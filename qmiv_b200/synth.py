@@ -21,9 +21,9 @@ import numpy as np
 def _gradient_texture(rng, h, w, maxv, tex_sigma):
     yy = np.linspace(0.0, 1.0, h, dtype=np.float32)[:, None]
     xx = np.linspace(0.0, 1.0, w, dtype=np.float32)[None, :]
-    a, b = rng.uniform(0.15, 0.35, 2)
+    a, b = rng.uniform(0.12, 0.28, 2)
     fx, fy, ph = rng.uniform(0.5, 3.0), rng.uniform(0.5, 3.0), rng.uniform(0, 2 * math.pi)
-    base = maxv * (0.2 + a * xx + b * yy + 0.1 * np.sin(2 * math.pi * (fx * xx + fy * yy) + ph))
+    base = maxv * (0.16 + a * xx + b * yy + 0.06 * np.sin(2 * math.pi * (fx * xx + fy * yy) + ph))
     return base.astype(np.float32) + rng.normal(0.0, tex_sigma, (h, w)).astype(np.float32)
 
 

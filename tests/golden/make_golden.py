@@ -1,0 +1,180 @@
+"""Generates the golden fixtures in tests/golden/ by running the QMIV reference itself.
+
+The reference is compiled from its own sources by oracle/Makefile into oracle/_ref/<arch>/; this
+script only runs where that build exists (the development container). The GPU box never runs it:
+tests read the committed JSON / npz files.
+
+The x86-64-v3 (AVX2) build is used: the x86-64-v4 (AVX-512) build of the reference mis-converts
+8-bit 4:2:0 chroma when the picture width is 64 modulo 128 (xPixelOpsAVX512.cpp CvtUpsampleHV builds
+a store mask with a 64-bit shift by 64), which the portable and AVX2 builds do not.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+import oracle  # noqa: E402
+from detgen import det_pair, hash32, to444  # noqa: E402
+
+ARCH = "x86-64-v3"
+
+# (width, height, bitdepth, chroma_format, R, erp, seed, extra params)
+PIPELINE_CASES = [
+    (64, 64, 8, 420, 2, False, 1, {}),
+    (96, 64, 10, 420, 2, True, 2, {}),
+    (128, 96, 8, 444, 2, False, 3, {}),
+    (130, 66, 10, 422, 4, True, 4, {}),
+    (256, 128, 10, 420, 2, True, 5, {}),
+    (200, 100, 8, 420, 3, False, 6, {}),
+    (320, 192, 10, 420, 5, True, 7, {}),
+    (66, 34, 8, 420, 1, False, 8, {}),
+    (512, 256, 10, 420, 2, True, 9, {}),
+    (1024, 512, 8, 420, 4, False, 10, {}),
+    (1920, 1080, 8, 420, 2, False, 11, {}),
+    (96, 96, 14, 444, 2, False, 12, {}),
+    (128, 64, 12, 420, 2, True, 13, {}),
+    (64, 64, 10, 420, 2, False, 14, {"cws": (2, 1, 1, 0), "cwa": (6, 1, 1, 0)}),
+    (128, 128, 10, 420, 3, True, 15, {"unc": (0.02, 0.02, 0.02, 0.0)}),
+    (192, 64, 8, 420, 2, False, 16, {"lat_range": 120}),
+    (96, 64, 10, 420, 2, True, 17, {"variant": "exact_chroma"}),
+    (64, 48, 8, 420, 2, False, 18, {"variant": "identical"}),
+]
+
+CPS_SIZES = [(64, 64)]
+CPS_BITDEPTHS = [8, 10, 14]
+CPS_GCDS = [(0, 0, 0, 0), (1, 1, 1, 0), (-1, -1, -1, 0), (-1, 1, 1, 0)]
+
+
+def fhex(v):
+    return float(v).hex()
+
+
+def case_frames(W, H, bd, cf, seed, variant=None):
+    f0, f1 = det_pair(W, H, bd, seed, cf)
+    if variant == "exact_chroma":
+        f1 = (f1[0], f0[1].copy(), f0[2].copy())
+    elif variant == "identical":
+        f1 = tuple(p.copy() for p in f0)
+    return f0, f1
+
+
+def make_pipeline(ref):
+    out = []
+    for (W, H, bd, cf, R, erp, seed, extra) in PIPELINE_CASES:
+        extra = dict(extra)
+        variant = extra.pop("variant", None)
+        kw = dict(search_range=R, erp=erp, num_threads=8)
+        kw.update({k: v for k, v in extra.items() if k in ("cws", "cwa", "unc", "lat_range")})
+        p = oracle.make_params(W, H, bd, cf, **kw)
+        f0, f1 = case_frames(W, H, bd, cf, seed, variant)
+        mask = oracle.ALL
+        if oracle.Oracle().num_scales(W, H) < 1:
+            mask &= ~(oracle.MSSSIM | oracle.IVMSSSIM)
+        r = ref.compute_pair(p, f0, f1, mask, want_scp=True)
+        t0, t1 = to444(f0, cf), to444(f1, cf)
+        g = r["gcd_r2t"]
+        rows_r2t, _ = ref.cps_rows(t0, t1, bd, g, R, kw.get("cws", (4, 1, 1, 0)))
+        rows_t2r, _ = ref.cps_rows(t1, t0, bd, [-x for x in g], R, kw.get("cws", (4, 1, 1, 0)))
+        exp = {}
+        for k, v in r.items():
+            if k.startswith("scp"):
+                exp[k + "_sha256"] = hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest()
+            elif isinstance(v, list):
+                exp[k] = [fhex(x) if isinstance(x, float) else int(x) for x in v]
+            else:
+                exp[k] = fhex(v) if isinstance(v, float) else int(v)
+        out.append(dict(width=W, height=H, bitdepth=bd, chroma_format=cf, search_range=R, erp=erp, seed=seed,
+                        variant=variant, params={k: list(v) if isinstance(v, tuple) else v
+                                                 for k, v in kw.items() if k != "num_threads"},
+                        mask=mask, expected=exp,
+                        cps_rows_r2t=rows_r2t.astype(np.int64).tolist(),
+                        cps_rows_t2r=rows_t2r.astype(np.int64).tolist()))
+        print("pipeline", W, H, bd, cf, R, erp, variant, r["ivpsnr"])
+    return out
+
+
+def make_cps(ref):
+    """Fixtures in the manner of libs/pmbb-ivqm/test/test-xCorrespPixelShift.cpp: Perlin-noise originals
+    (xPerlinNoise::fillPerlinNoiseI), block-noise modifications (xTestUtilsIVQM::addBlockNoise) on all
+    three components, margin 8 edge-replicated, R = 2, weights 4:1:1, GCD in {0, +1, -1, (-1,+1,+1)}."""
+    state = 666  # xTestUtils::c_XorShiftSeed
+    arrays, cases = {}, []
+    margin = 8
+    for (W, H) in CPS_SIZES:
+        for bd in CPS_BITDEPTHS:
+            org = np.zeros((3, H, W), np.uint16)
+            for c in range(3):
+                org[c] = ref.fill_perlin(H, W, bd, 8, state)
+                state = ref.xorshift32(state)
+            mod = np.zeros_like(org)
+            for c in range(3):
+                pad = np.pad(org[c], margin, mode="edge")
+                mod[c], state = ref.add_block_noise(pad, margin, W, H, bd, state)
+            key = f"{W}x{H}_{bd}"
+            arrays[key + "_org"], arrays[key + "_mod"] = org, mod
+            for g in CPS_GCDS:
+                a, b = ref.cps_rows(mod, org, bd, g, 2, (4, 1, 1, 0))
+                cases.append(dict(key=key, width=W, height=H, bitdepth=bd, gcd=list(g),
+                                  rows_interleaved=a.astype(np.int64).tolist(), rows_planar=b.astype(np.int64).tolist()))
+            print("cps", key, int(org.max()), int(mod.max()))
+    np.savez_compressed(os.path.join(HERE, "cps_fixtures.npz"), **arrays)
+    return cases
+
+
+def make_gcd(ref):
+    """xGlobClrDiff::CalcGlobalColorDiff on deterministic pictures, default and unit coefficients."""
+    cases = []
+    for (W, H, bd, seed) in [(128, 128, 8, 1), (256, 128, 10, 2), (128, 256, 12, 3), (256, 256, 14, 4)]:
+        f0, f1 = det_pair(W, H, bd, seed, 444, offset=(5, -7, 1))
+        t0, t1 = to444(f0, 444), to444(f1, 444)
+        for coef in [(0.01, 0.01, 0.01, 0.0), (1.0, 1.0, 1.0, 1.0), (0.003, 0.02, 0.5, 0.0)]:
+            cases.append(dict(width=W, height=H, bitdepth=bd, seed=seed, coef=list(coef),
+                              gcd_10=ref.gcd(t1, t0, bd, coef), gcd_01=ref.gcd(t0, t1, bd, coef)))
+    return cases
+
+
+def make_ssim_windows(ref):
+    """xStructSim::CalcBlckAvg (dispatched) and xStructSimSTD::CalcBlckAvg on 8x8 windows."""
+    import ctypes
+    cases = []
+    for bd in (8, 10, 12, 14):
+        maxv = (1 << bd) - 1
+        for k in range(8):
+            h = hash32(np.arange(128, dtype=np.uint32) + np.uint32(bd * 1000 + k * 7919))
+            t = (h[:64] % (maxv + 1)).astype(np.uint16).reshape(8, 8)
+            r = (h[64:] % (maxv + 1)).astype(np.uint16).reshape(8, 8)
+            if k % 2:
+                r = np.clip(t.astype(np.int64) + (h[64:].reshape(8, 8) % 21).astype(np.int64) - 10, 0, maxv).astype(np.uint16)
+            tt, rr = np.ascontiguousarray(t), np.ascontiguousarray(r)
+            vals = {}
+            for calc_l in (0, 1):
+                for std in (0, 1):
+                    v = ref.lib.ref_ssim_block(tt.ctypes.data_as(ctypes.c_void_p), rr.ctypes.data_as(ctypes.c_void_p),
+                                               8, 8, bd, calc_l, std)
+                    vals[f"l{calc_l}_std{std}"] = fhex(v)
+            cases.append(dict(bitdepth=bd, k=k, tst=t.tolist(), ref=r.tolist(), values=vals))
+    return cases
+
+
+def main():
+    ref = oracle.Reference(ARCH)
+    data = dict(generator="tests/golden/make_golden.py", reference_build=ARCH,
+                pipeline=make_pipeline(ref), cps=make_cps(ref), gcd=make_gcd(ref), ssim_windows=make_ssim_windows(ref))
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(data, f, separators=(",", ":"))
+    print("wrote", os.path.join(HERE, "golden.json"))
+
+
+if __name__ == "__main__":
+    main()

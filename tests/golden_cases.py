@@ -1,0 +1,64 @@
+"""Helpers shared by the tests: rebuild the golden cases' frames and compare result dicts."""
+import hashlib
+
+import numpy as np
+
+from detgen import det_pair
+
+RESULT_FLOAT_KEYS = ["psnr", "psnr_pic", "wspsnr", "wspsnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r", "ssim",
+                     "ssim_pic", "msssim", "msssim_pic", "ivssim", "ivssim_r2t", "ivssim_t2r", "ivmsssim",
+                     "ivmsssim_r2t", "ivmsssim_t2r"]
+METRIC_OF_KEY = {"psnr": 1, "wspsnr": 2, "ivpsnr": 4, "ssim": 8, "msssim": 16, "ivssim": 32, "ivmsssim": 64}
+
+
+def case_frames(case):
+    f0, f1 = det_pair(case["width"], case["height"], case["bitdepth"], case["seed"], case["chroma_format"])
+    if case.get("variant") == "exact_chroma":
+        f1 = (f1[0], f0[1].copy(), f0[2].copy())
+    elif case.get("variant") == "identical":
+        f1 = tuple(p.copy() for p in f0)
+    return f0, f1
+
+
+def case_params(case):
+    p = dict(case["params"])
+    for k in ("cws", "cwa", "unc"):
+        if k in p:
+            p[k] = tuple(p[k])
+    return p
+
+
+def unhex(v):
+    if isinstance(v, list):
+        return [float.fromhex(x) if isinstance(x, str) else x for x in v]
+    return float.fromhex(v) if isinstance(v, str) else v
+
+
+def metric_enabled(key, mask):
+    base = key.split("_")[0]
+    return bool(METRIC_OF_KEY.get(base, 0) & mask)
+
+
+def compare_result(got, expected, mask, ignore=()):
+    """Bit-exact comparison of a result dict against a golden 'expected' block. Returns mismatches."""
+    bad = []
+    for k in ["gcd_r2t", "exact"]:
+        if k in ignore:
+            continue
+        if list(got[k][:3]) != list(expected[k][:3]):
+            bad.append((k, got[k], expected[k]))
+    for k in RESULT_FLOAT_KEYS:
+        if k in ignore or not metric_enabled(k, mask):
+            continue
+        e = unhex(expected[k])
+        g = got[k]
+        if isinstance(e, list):
+            if [float(x) for x in g[:3]] != [float(x) for x in e[:3]]:
+                bad.append((k, g[:3], e[:3]))
+        elif float(g) != float(e):
+            bad.append((k, g, e))
+    return bad
+
+
+def sha256(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()

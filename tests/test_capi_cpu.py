@@ -1,0 +1,72 @@
+"""The C ABI library without a GPU: it loads, exports every symbol include/*.h declares, and its
+host-only entry points behave."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, cuda_available
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        with open(h) as f:
+            text = f.read()
+        names |= set(re.findall(r"QMIV_API\s+[\w\s\*]+?\b(qmiv_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    for n in ["qmiv_ctx_create", "qmiv_calc_create", "qmiv_frame_pair_compute", "qmiv_calc_scp", "qmiv_batch_compute"]:
+        assert n in names
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    import qmiv_b200
+    from qmiv_b200 import _lib
+    lib = qmiv_b200.library()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_status_strings_and_version():
+    import qmiv_b200
+    lib = qmiv_b200.library()
+    assert lib.qmiv_api_version() == 1
+    assert lib.qmiv_status_string(0) == b"ok"
+    assert lib.qmiv_status_string(6) == b"HBM budget exceeded"
+    assert lib.qmiv_status_string(99) == b"unknown status"
+
+
+def test_params_default_match_reference_defaults():
+    """xCorrespPixelShiftPrms.h:22-24, xGlobClrDiff.h:20, xSSIM.h:35-37."""
+    import qmiv_b200
+    p = qmiv_b200.make_params()
+    assert p.search_range == 2
+    assert list(p.cws) == [4, 1, 1, 0] and list(p.cwa) == [4, 1, 1, 0]
+    assert [round(x, 6) for x in p.unc] == [0.01, 0.01, 0.01, 0.0]
+    assert (p.ssim_window, p.ssim_stride) == (8, 4)
+    assert p.invalid_pel_action == qmiv_b200.PEL_STOP
+
+
+@pytest.mark.skipif(cuda_available(), reason="checks the no-GPU error path")
+def test_ctx_create_without_gpu_fails_cleanly():
+    import qmiv_b200
+    with pytest.raises(qmiv_b200.QmivError) as ei:
+        qmiv_b200.Context(0)
+    assert ei.value.status in (1, 3)
+
+
+def test_null_arguments_are_rejected():
+    import qmiv_b200
+    lib = qmiv_b200.library()
+    assert lib.qmiv_ctx_create(0, 0, None) == 1
+    assert lib.qmiv_calc_create(None, 64, 64, 8, 420, None, None) == 1
+    assert lib.qmiv_frame_pair_compute(None, None, None, 0, None) == 1
+    assert lib.qmiv_calc_destroy(None) == 1
+    assert lib.qmiv_batch_destroy(None) == 1

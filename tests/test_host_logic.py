@@ -1,0 +1,98 @@
+"""Host-side logic that needs no GPU: metric selection, frame descriptors, synthetic workloads, the
+deterministic fixture generator, and the fp32 exactness bound of the CPS search keys."""
+import numpy as np
+import pytest
+
+import qmiv_b200
+from qmiv_b200 import synth
+from detgen import det_pair, hash32
+
+
+def test_metric_mask_parsing():
+    assert qmiv_b200.metric_mask(None) == qmiv_b200.ALL
+    assert qmiv_b200.metric_mask("IVPSNR, WS-PSNR") == qmiv_b200.IVPSNR | qmiv_b200.WSPSNR
+    assert qmiv_b200.metric_mask(["psnr", "IV_SSIM"]) == qmiv_b200.PSNR | qmiv_b200.IVSSIM
+    with pytest.raises(ValueError):
+        qmiv_b200.metric_mask("VMAF")
+
+
+def test_make_frame_host_planes():
+    f0, _ = synth.make_pair(64, 32, 10, seed=1)
+    fr, keep = qmiv_b200.make_frame(f0)
+    assert fr.mem == 0
+    assert [fr.pitch[c] for c in range(3)] == [128, 64, 64]
+    with pytest.raises(ValueError):
+        qmiv_b200.make_frame(f0[:2])
+
+
+@pytest.mark.parametrize("cf", [420, 422, 444])
+def test_synth_shapes_and_ranges(cf):
+    f0, f1 = synth.make_pair(128, 64, 10, seed=3, chroma_format=cf)
+    cw = 128 if cf == 444 else 64
+    ch = 32 if cf == 420 else 64
+    assert f0[0].shape == (64, 128) and f0[1].shape == (ch, cw) and f1[2].shape == (ch, cw)
+    assert all(p.dtype == np.uint16 and p.max() <= 1023 for p in f0 + f1)
+    g0, g1 = synth.make_pair(512, 256, 8, seed=3)
+    assert g0[0].dtype == np.uint8
+    # the distorted frame carries the global offset (+3, -2, +2 in 8-bit units)
+    d = [float(g1[c].astype(float).mean() - g0[c].astype(float).mean()) for c in range(3)]
+    assert d[0] > 2.0 and d[1] < -1.0 and d[2] > 1.0
+
+
+def test_config_specs():
+    specs = synth.config3_specs(64, seed=3)
+    assert len(specs) == 64
+    assert {(s["width"], s["height"]) for s in specs} <= set(synth.CONFIG3_RESOLUTIONS)
+    assert {s["bitdepth"] for s in specs} <= {8, 10} and {s["search_range"] for s in specs} <= {2, 4}
+    reqs = synth.config4_requests(duration_s=0.5, rate=200.0, seed=4)
+    assert 60 <= len(reqs) <= 140
+    assert all(1 <= len(r.specs) <= 32 for r in reqs)
+    assert all(b.arrival_s > a.arrival_s for a, b in zip(reqs, reqs[1:]))
+
+
+def test_detgen_is_deterministic():
+    assert hash32(np.array([0, 1, 2], np.uint32)).tolist() == [0, 1753845952, 3507691905]
+    a = det_pair(64, 32, 10, 5)
+    b = det_pair(64, 32, 10, 5)
+    assert all(np.array_equal(x, y) for x, y in zip(a[0] + a[1], b[0] + b[1]))
+
+
+def cps_fp32_exact(maxv, w, maxdiff):
+    """Python statement of the kernel's exactness test (qmiv_kernels.cu, cps_fp32_exact)."""
+    bias, lim = 1 << 23, 1 << 24
+    e = sum(w[c] * (maxv + maxdiff[c]) ** 2 for c in range(3))
+    q = sum(w[c] * maxv * maxv for c in range(3))
+    up = sum(2 * w[c] * maxdiff[c] * maxv for c in range(3))
+    lo = sum(2 * w[c] * (maxv + maxdiff[c]) * maxv for c in range(3))
+    return bias - e >= (1 << 20) and bias + e < lim and bias + q + up < lim and bias - lo > -lim
+
+
+def test_fp32_key_bound_covers_default_8_and_10_bit():
+    assert cps_fp32_exact(255, (4, 1, 1), (3, 3, 3))
+    assert cps_fp32_exact(1023, (4, 1, 1), (10, 10, 10))
+    assert not cps_fp32_exact(4095, (4, 1, 1), (41, 41, 41))
+
+
+@pytest.mark.parametrize("bd,w,g", [(8, (4, 1, 1), (3, 3, 3)), (10, (4, 1, 1), (10, 10, 10)), (10, (2, 1, 1), (10, 10, 10))])
+def test_fp32_keys_order_like_int32_errors(bd, w, g):
+    """Within the bound, the three-FFMA biased error is exact and its key orders candidates exactly as
+    (int32 error, raster index) -- checked exhaustively over random candidates in float32 numpy."""
+    rng = np.random.default_rng(bd)
+    maxv = (1 << bd) - 1
+    n = 20000
+    s = rng.integers(-g[0], maxv + g[0] + 1, (n, 3)).astype(np.int64)
+    r = rng.integers(0, maxv + 1, (n, 25, 3)).astype(np.int64)
+    r[:, 7] = r[:, 3]  # force ties
+    wi = np.array(w, np.int64)
+    err = ((s[:, None, :] - r) ** 2 * wi).sum(-1)
+    best_ref = np.argmin(err, axis=1)  # first minimum in index order
+    f32 = np.float32
+    q = (wi[0] * r[..., 0] ** 2 + wi[1] * r[..., 1] ** 2 + wi[2] * r[..., 2] ** 2 + (1 << 23)).astype(f32)
+    a = (-2 * wi * s).astype(f32)
+    e = q
+    for c in range(3):
+        e = (a[:, None, c] * r[..., c].astype(f32) + e).astype(f32)
+    assert np.array_equal(e.astype(np.int64), err - (wi * s * s).sum(-1)[:, None] + (1 << 23))
+    bits = e.view(np.uint32).astype(np.uint64)
+    key = ((bits - 0x49800000) << 7) + np.arange(25, dtype=np.uint64)[None, :]
+    assert np.array_equal(np.argmin(key, axis=1), best_ref)

@@ -1,0 +1,114 @@
+"""Pins the C restatement (oracle/qmiv_oracle.c) to the golden fixtures produced by the compiled QMIV
+reference (tests/golden/make_golden.py). Everything here runs on the CPU."""
+import numpy as np
+import pytest
+
+import oracle
+from golden_cases import case_frames, case_params, compare_result, sha256, unhex
+
+
+def _pipeline_ids(golden_json=None):
+    import json, os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")) as f:
+        g = json.load(f)
+    return [f"{c['width']}x{c['height']}_{c['bitdepth']}b_{c['chroma_format']}_R{c['search_range']}"
+            f"{'_erp' if c['erp'] else ''}{'_' + c['variant'] if c.get('variant') else ''}" for c in g["pipeline"]]
+
+
+@pytest.mark.parametrize("idx", range(len(_pipeline_ids())), ids=_pipeline_ids())
+def test_pipeline_matches_reference(idx, golden, oracle_lib):
+    case = golden["pipeline"][idx]
+    f0, f1 = case_frames(case)
+    p = oracle.make_params(case["width"], case["height"], case["bitdepth"], case["chroma_format"], **case_params(case))
+    got = oracle_lib.compute_pair(p, f0, f1, case["mask"], want_scp=True)
+    exp = case["expected"]
+    assert compare_result(got, exp, case["mask"]) == []
+    assert sha256(got["scp0"]) == exp["scp0_sha256"]
+    assert sha256(got["scp1"]) == exp["scp1_sha256"]
+
+
+@pytest.mark.parametrize("idx", range(len(_pipeline_ids())), ids=_pipeline_ids())
+def test_cps_rows_match_reference(idx, golden, oracle_lib):
+    case = golden["pipeline"][idx]
+    f0, f1 = case_frames(case)
+    cf, bd, R = case["chroma_format"], case["bitdepth"], case["search_range"]
+    t0 = oracle_lib.unpack444(f0, case["width"], case["height"], bd, cf)
+    t1 = oracle_lib.unpack444(f1, case["width"], case["height"], bd, cf)
+    g = unhex(case["expected"]["gcd_r2t"])
+    cws = tuple(case["params"].get("cws", (4, 1, 1, 0)))
+    r2t, _ = oracle_lib.cps(t0, t1, bd, g, R, cws, want_scp=False)
+    t2r, _ = oracle_lib.cps(t1, t0, bd, [-x for x in g], R, cws, want_scp=False)
+    assert r2t.astype(np.int64).tolist() == case["cps_rows_r2t"]
+    assert t2r.astype(np.int64).tolist() == case["cps_rows_t2r"]
+
+
+def test_cps_unit_fixtures(golden, cps_arrays, oracle_lib):
+    """libs/pmbb-ivqm/test/test-xCorrespPixelShift.cpp style: Perlin originals, block noise, 4 GCDs."""
+    for case in golden["cps"]:
+        org, mod = cps_arrays[case["key"] + "_org"], cps_arrays[case["key"] + "_mod"]
+        rows, scp = oracle_lib.cps(mod, org, case["bitdepth"], case["gcd"], 2, (4, 1, 1, 0), want_scp=True)
+        assert rows.astype(np.int64).tolist() == case["rows_interleaved"]
+        std = oracle_lib.cps_rows_std(mod, org, case["gcd"], 2, (4, 1, 1, 0))
+        assert std.astype(np.int64).tolist() == case["rows_planar"]
+        # SSD(Tst, SCP) == CPS SSE when no clipping happens (test-xCorrespPixelShift.cpp:155-179)
+        g = np.array(case["gcd"][:3], np.int64)[:, None, None]
+        d = mod.astype(np.int64) + g - (scp.astype(np.int64) + g)
+        maxv = (1 << case["bitdepth"]) - 1
+        unclipped = (scp.astype(np.int64) > 0) & (scp.astype(np.int64) < maxv)
+        if unclipped.all():
+            assert (d ** 2).reshape(3, -1).sum(axis=1).tolist() == rows.sum(axis=0).tolist()
+
+
+def test_gcd_matches_reference(golden, oracle_lib):
+    from detgen import det_pair, to444
+    for case in golden["gcd"]:
+        f0, f1 = det_pair(case["width"], case["height"], case["bitdepth"], case["seed"], 444, offset=(5, -7, 1))
+        t0, t1 = to444(f0, 444), to444(f1, 444)
+        assert oracle_lib.gcd(t1, t0, case["bitdepth"], case["coef"]) == case["gcd_10"]
+        assert oracle_lib.gcd(t0, t1, case["bitdepth"], case["coef"]) == case["gcd_01"]
+
+
+@pytest.mark.parametrize("bd", [8, 10, 12, 14])
+@pytest.mark.parametrize("size", [(128, 128), (256, 128), (128, 256), (256, 256)])
+def test_gcd_known_answers(bd, size, oracle_lib):
+    """libs/pmbb-ivqm/test/test-xGlobClrDiff.cpp:45-87 with coefficient 1.0."""
+    W, H = size
+    maxv = (1 << bd) - 1
+    one = (1.0, 1.0, 1.0, 1.0)
+    ref = np.zeros((3, H, W), np.uint16)
+    for fill, expect in [(0, 0), (1, 1), (maxv, maxv)]:
+        mod = np.full((3, H, W), fill, np.uint16)
+        assert oracle_lib.gcd(mod, ref, bd, one)[:3] == [expect] * 3
+        assert oracle_lib.gcd(ref, mod, bd, one)[:3] == [-expect] * 3
+    rng = np.random.default_rng(bd * 7 + W)
+    ref = rng.integers(0, maxv - 8, (3, H, W)).astype(np.uint16)
+    mod = ref + np.array([4, 3, 2], np.uint16)[:, None, None]
+    assert oracle_lib.gcd(mod, ref, bd, one)[:3] == [4, 3, 2]
+    assert oracle_lib.gcd(ref, mod, bd, one)[:3] == [-4, -3, -2]
+    assert oracle_lib.gcd(ref, ref, bd, one)[:3] == [0, 0, 0]
+
+
+def test_ssim_windows_match_reference(golden, oracle_lib):
+    for case in golden["ssim_windows"]:
+        t = np.array(case["tst"], np.uint16)
+        r = np.array(case["ref"], np.uint16)
+        vals = case["values"]
+        # the dispatched (SIMD) and portable reference windows agree (test-xStructSim.cpp:169-170)
+        assert vals["l0_std0"] == vals["l0_std1"] and vals["l1_std0"] == vals["l1_std1"]
+        for calc_l in (0, 1):
+            got = oracle_lib.ssim_pic(np.stack([t] * 3), np.stack([r] * 3), case["bitdepth"], calc_l)
+            assert got == [float.fromhex(vals[f"l{calc_l}_std1"])] * 3
+
+
+def test_window_counts():
+    """xSSIM::xCalcNumBlocks against brute force, as libs/pmbb-ivqm/test/test-xSSIM.cpp:29-51."""
+    for length in range(100, 4097, 27):
+        cnt = len(range(0, length - 8 + 1, 4))
+        assert cnt == (length - 8) // 4 + 1
+
+
+def test_num_scales(oracle_lib):
+    assert oracle_lib.num_scales(2048, 2048) == 5
+    assert oracle_lib.num_scales(256, 128) == 3
+    assert oracle_lib.num_scales(31, 500) == 0
+    assert oracle_lib.num_scales(4096, 2048) == 5
