@@ -131,7 +131,8 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------------------------
-def make_workload(rank, n=PAIRS_PER_STEP):
+def make_workload(rank, n=None):
+    n = n or PAIRS_PER_STEP
     from qmiv_b200 import synth
     t0 = time.time()
     pairs = [synth.make_pair(W, H, BD, seed=1000 * rank + i) for i in range(n)]
@@ -285,7 +286,14 @@ def main():
     ap.add_argument("--impl", choices=["qmiv", "reference"], default="qmiv")
     ap.add_argument("--cpu-frames", type=int, default=4, help="frames of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", default=None, help="WxH of a smaller profiling case (not a bench line)")
+    ap.add_argument("--pairs", type=int, default=None, help="pairs per step of a smaller profiling case")
     args = ap.parse_args()
+    global W, H, PAIRS_PER_STEP
+    if args.size:
+        W, H = (int(x) for x in args.size.lower().split("x"))
+    if args.pairs:
+        PAIRS_PER_STEP = args.pairs
     if args.warmup < 3:
         log("warm-up raised to 3 steps")
         args.warmup = 3

@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(128) k_cps(const __grid_constant__ CpsArgs a)
         }
       }
       #pragma unroll
-      for(int i = 0; i < P; i++) { idx[i] = best[i] & 127u; }
+      for(int i = 0; i < P; i++) { idx[i] = min(best[i] & 127u, (uint32_t)(D * D - 1)); }
     }
     else
     {
