@@ -14,11 +14,16 @@ struct qmiv_batch_s
   int32_t      max_pairs = 0;
   int64_t      max_pixels = 0;
   int32_t      use_graph = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;           // the batch's stream: a call starts and ends on it
+  std::vector<cudaStream_t> lanes;         // worker streams the pairs are spread over
+  std::vector<cudaEvent_t>  lane_done;
+  cudaEvent_t               start = nullptr;
   // one pipeline per (pair index) so that every pair of a call has its own scratch
   std::vector<std::unique_ptr<PairPipeline>> pipes;
   std::vector<std::tuple<int32_t, int32_t, int32_t, int32_t, int32_t>> keys;
 };
+
+static constexpr int kBatchLanes = 4;
 
 extern "C" {
 
@@ -33,8 +38,16 @@ qmiv_status qmiv_batch_create(qmiv_ctx ctx, int32_t max_pairs, int64_t max_pixel
   QMIV_CUDA(cudaSetDevice(ctx->device));
   qmiv_batch b = new qmiv_batch_s();
   b->ctx = ctx; b->prm = prm; b->max_pairs = max_pairs; b->max_pixels = max_pixels; b->use_graph = use_graph;
-  const cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
-  if(e != cudaSuccess) { delete b; return cuda_fail(e, "cudaStreamCreateWithFlags"); }
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if(e == cudaSuccess) { e = cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming); }
+  for(int k = 0; k < kBatchLanes && e == cudaSuccess; k++)
+  {
+    cudaStream_t s; cudaEvent_t d;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if(e == cudaSuccess) { b->lanes.push_back(s); e = cudaEventCreateWithFlags(&d, cudaEventDisableTiming); }
+    if(e == cudaSuccess) { b->lane_done.push_back(d); }
+  }
+  if(e != cudaSuccess) { qmiv_batch_destroy(b); return cuda_fail(e, "batch stream/event creation"); }
   b->pipes.resize(max_pairs);
   b->keys.resize(max_pairs);
   *out_batch = b;
@@ -45,9 +58,12 @@ qmiv_status qmiv_batch_destroy(qmiv_batch b)
 {
   if(!b) { return fail(QMIV_ERR_INVALID_ARG, "batch is null"); }
   cudaSetDevice(b->ctx->device);
-  cudaStreamSynchronize(b->stream);
+  if(b->stream) { cudaStreamSynchronize(b->stream); }
+  for(cudaStream_t s : b->lanes) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+  for(cudaEvent_t d : b->lane_done) { cudaEventDestroy(d); }
+  if(b->start) { cudaEventDestroy(b->start); }
   b->pipes.clear();
-  cudaStreamDestroy(b->stream);
+  if(b->stream) { cudaStreamDestroy(b->stream); }
   delete b;
   return QMIV_OK;
 }
@@ -60,8 +76,12 @@ qmiv_status qmiv_batch_compute(qmiv_batch b, const qmiv_pair_desc* pairs, int32_
   for(int i = 0; i < n; i++) { px += (int64_t)pairs[i].width * pairs[i].height; }
   if(px > b->max_pixels) { return fail(QMIV_ERR_INVALID_ARG, "more pixels than max_pixels"); }
   QMIV_CUDA(cudaSetDevice(b->ctx->device));
+  // fork: every lane starts after the work already queued on the batch's stream
+  QMIV_CUDA(cudaEventRecord(b->start, b->stream));
+  for(cudaStream_t s : b->lanes) { QMIV_CUDA(cudaStreamWaitEvent(s, b->start, 0)); }
   for(int i = 0; i < n; i++)
   {
+    cudaStream_t lane = b->lanes[i % b->lanes.size()];
     const qmiv_pair_desc& d = pairs[i];
     const auto key = std::make_tuple(d.width, d.height, d.bitdepth, d.chroma_format, d.search_range);
     if(!b->pipes[i] || b->keys[i] != key)
@@ -78,9 +98,15 @@ qmiv_status qmiv_batch_compute(qmiv_batch b, const qmiv_pair_desc* pairs, int32_
     const bool host = d.in0.mem == QMIV_MEM_HOST || d.in1.mem == QMIV_MEM_HOST;
     QMIV_TRY(p.prepare(d.metric_mask, false, host));
     Img a{}, c{};
-    QMIV_TRY(p.resolve(&d.in0, 0, a, b->stream));
-    QMIV_TRY(p.resolve(&d.in1, 1, c, b->stream));
-    QMIV_TRY(p.enqueue(a, c, d.metric_mask, false, false, b->stream));
+    QMIV_TRY(p.resolve(&d.in0, 0, a, lane));
+    QMIV_TRY(p.resolve(&d.in1, 1, c, lane));
+    QMIV_TRY(p.enqueue(a, c, d.metric_mask, false, false, lane));
+  }
+  // join: the batch's stream waits for every lane
+  for(size_t k = 0; k < b->lanes.size(); k++)
+  {
+    QMIV_CUDA(cudaEventRecord(b->lane_done[k], b->lanes[k]));
+    QMIV_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
   }
   QMIV_CUDA(cudaStreamSynchronize(b->stream));
   qmiv_status st = QMIV_OK;

@@ -94,7 +94,7 @@ qmiv_status PairPipeline::configure(qmiv_ctx_s* ctx, const Shape& shape, const q
     ny_[s] = h >= 8 ? (h - 8) / 4 + 1 : 0;
     w >>= 1; h >>= 1;
   }
-  nyp_ = (ny_[0] + 31) & ~31;
+  nxp_ = (nx_[0] + 31) & ~31;
   const double maxd = (double)shape.maxv;  // xSSIM.cpp:165-167
   const double k1 = 0.01 * maxd, k2 = 0.03 * maxd;
   C1_ = k1 * k1; C2_ = k2 * k2;
@@ -126,7 +126,7 @@ qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames
   if(need_ssim)
   {
     if(nx_[0] < 1 || ny_[0] < 1) { return fail(QMIV_ERR_INVALID_ARG, "picture smaller than one 8x8 SSIM window"); }
-    QMIV_TRY(win_.ensure(ctx_, (size_t)3 * nx_[0] * nyp_ * sizeof(double)));
+    QMIV_TRY(win_.ensure(ctx_, (size_t)3 * ny_[0] * nxp_ * sizeof(double)));
     QMIV_TRY(rowsum_.ensure(ctx_, (size_t)kMaxSsimSlots * 3 * ny_[0] * sizeof(double)));
   }
   if(need_ms)
@@ -267,13 +267,13 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
   auto run_ssim = [&](const Img& a, const Img& b, int W, int H, int scale, int slot, int calc_l, int use_ws,
                       const MutImg* down_a, const MutImg* down_b) -> qmiv_status {
     SsimWinArgs wa{};
-    wa.a = a; wa.b = b; wa.W = W; wa.H = H; wa.nx = nx_[scale]; wa.ny = ny_[scale]; wa.ny_pad = nyp_;
+    wa.a = a; wa.b = b; wa.W = W; wa.H = H; wa.nx = nx_[scale]; wa.ny = ny_[scale]; wa.nx_pad = nxp_;
     wa.clip = clip; wa.C1 = C1_; wa.C2 = C2_; wa.calc_l = calc_l; wa.win = win_.as<double>();
     if(down_a) { wa.down_a = *down_a; }
     if(down_b) { wa.down_b = *down_b; }
     { const int t = prof_begin(s); QMIV_CUDA(launch_ssim_win<T>(wa, s)); prof_end(s, QMIV_STAGE_SSIM_WIN, t); }
     SsimRowArgs rr{};
-    rr.win = wa.win; rr.nx = wa.nx; rr.ny = wa.ny; rr.ny_pad = nyp_;
+    rr.win = wa.win; rr.nx = wa.nx; rr.ny = wa.ny; rr.nx_pad = nxp_;
     rr.row_sum = rowsum + (size_t)slot * 3 * ny_[0];
     { const int t = prof_begin(s); QMIV_CUDA(launch_ssim_rows(rr, s)); prof_end(s, QMIV_STAGE_SSIM_ROWS, t); }
     fa.slot[slot].row_sum = rr.row_sum; fa.slot[slot].nx = wa.nx; fa.slot[slot].ny = wa.ny; fa.slot[slot].use_ws = use_ws;

@@ -141,7 +141,7 @@ private:
   int32_t      maxdiff_[4] = { 0, 0, 0, 0 };
   bool         fp32_ok_ = true;
   int32_t      ns_ = 0;
-  int32_t      nx_[5] = {}, ny_[5] = {}, nyp_ = 0;
+  int32_t      nx_[5] = {}, ny_[5] = {}, nxp_ = 0;
   std::vector<double> ws_host_;
   double       ws_corr_ = 1.0;
   double       C1_ = 0, C2_ = 0;

@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(256) k_ssim_win(const __grid_constant__ SsimWi
         const double l = ddiv(dadd(dmul(dmul(2.0, avg_r), avg_t), a.C1), dadd(dadd(dmul(avg_r, avg_r), dmul(avg_t, avg_t)), a.C1));
         v = dmul(l, cs);
       }
-      a.win[((size_t)c * a.nx + i) * a.ny_pad + j] = v;
+      a.win[((size_t)c * a.ny + j) * a.nx_pad + i] = v;
     }
   }
 
@@ -462,31 +462,49 @@ template cudaError_t launch_ssim_win<uint16_t>(const SsimWinArgs&, cudaStream_t)
 // =============================================================================================
 // per window row: compensated sum of the windows in x order (xSSIM.cpp:353-369)
 // =============================================================================================
-__global__ void __launch_bounds__(128) k_ssim_rows(const __grid_constant__ SsimRowArgs a)
+// One warp per window row: the row is staged into shared memory with coalesced loads (all lanes,
+// independent), then lane 0 runs the order-dependent sum from shared memory.
+__global__ void __launch_bounds__(256) k_ssim_rows(const __grid_constant__ SsimRowArgs a)
 {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if(t >= 3 * a.ny) { return; }
-  const int c = t / a.ny, j = t - c * a.ny;
-  const double* col = a.win + (size_t)c * a.nx * a.ny_pad + j;
-  Kbns k;
-  constexpr int B = 8;
-  int i = 0;
-  for(; i + B <= a.nx; i += B)
+  extern __shared__ double rowbuf[];  // [warps per block][nx_pad]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int row = blockIdx.x * (blockDim.x >> 5) + w;
+  if(row >= 3 * a.ny) { return; }
+  const double* src = a.win + (size_t)row * a.nx_pad;
+  double* buf = rowbuf + (size_t)w * a.nx_pad;
+  for(int i = lane; i < a.nx; i += 32) { buf[i] = src[i]; }
+  __syncwarp();
+  if(lane == 0)
   {
-    double v[B];
-    #pragma unroll
-    for(int u = 0; u < B; u++) { v[u] = col[(size_t)(i + u) * a.ny_pad]; }
-    #pragma unroll
-    for(int u = 0; u < B; u++) { k.add(v[u]); }
+    Kbns k;
+    int i = 0;
+    for(; i + 8 <= a.nx; i += 8)
+    {
+      double v[8];
+      #pragma unroll
+      for(int u = 0; u < 8; u++) { v[u] = buf[i + u]; }
+      #pragma unroll
+      for(int u = 0; u < 8; u++) { k.add(v[u]); }
+    }
+    for(; i < a.nx; i++) { k.add(buf[i]); }
+    a.row_sum[row] = k.result();  // row = c * ny + j
   }
-  for(; i < a.nx; i++) { k.add(col[(size_t)i * a.ny_pad]); }
-  a.row_sum[(size_t)c * a.ny + j] = k.result();
 }
 
 cudaError_t launch_ssim_rows(const SsimRowArgs& a, cudaStream_t s)
 {
+  const size_t per_warp = (size_t)a.nx_pad * sizeof(double);
+  int warps = (int)min((size_t)8, (size_t)(200 * 1024) / per_warp);
+  warps = max(warps, 1);
+  static bool configured = false;
+  if(!configured)
+  {
+    const cudaError_t e = cudaFuncSetAttribute(k_ssim_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 8192);
+    if(e != cudaSuccess) { return e; }
+    configured = true;
+  }
   const int n = 3 * a.ny;
-  k_ssim_rows<<<(n + 127) / 128, 128, 0, s>>>(a);
+  k_ssim_rows<<<(n + warps - 1) / warps, 32 * warps, per_warp * warps, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -499,144 +517,115 @@ cudaError_t launch_ssim_rows(const SsimRowArgs& a, cudaStream_t s)
 //   SSIM      KBNS over window rows (ERP: row * w[y + 4], weights KBNS) (xSSIM.cpp:348-351,
 //             xIVSSIM.cpp:148-172)
 // =============================================================================================
-constexpr int kChunk = 128;
-
-struct Chain
+// One CTA per chain: all threads stage the chain's inputs (independent loads) into shared memory,
+// then thread 0 runs the ordered compensated sum. Chains of one pair run on different SMs.
+__device__ __forceinline__ double chain_value(const FinalizeArgs& a, const FinChain& ch, int y)
 {
-  int kind;  // 0 = WS-PSNR, 1 = IV-PSNR (ERP), 2 = SSIM, 3 = SSIM ERP weight sum
-  int a, b;  // component / direction / slot
-};
+  if(ch.kind == kChainWsPsnr)
+  {
+    int off = 0;
+    for(int q = 0; q < ch.a; q++) { off += a.rows[q]; }
+    const uint64_t r = a.row_ssd[off + (y >> a.sy[ch.a])] * (uint64_t)a.mult_row[ch.a];
+    return dmul((double)r, a.ws[y]);
+  }
+  if(ch.kind == kChainIvPsnr)
+  {
+    const uint64_t r = (uint64_t)(int64_t)(int32_t)a.cps_rows[((size_t)ch.a * a.H + y) * 3 + ch.b];
+    return dmul((double)r, a.ws[y]);
+  }
+  const SsimSlot& sl = a.slot[ch.a];
+  const double v = sl.row_sum[(size_t)ch.b * sl.ny + y];
+  return sl.use_ws ? dmul(v, a.ws[4 * y + 4]) : v;
+}
 
 __global__ void __launch_bounds__(256) k_finalize(const __grid_constant__ FinalizeArgs a)
 {
-  extern __shared__ double stage[];   // [nchains][kChunk + 1]
-  __shared__ Chain chains[3 + 6 + 3 * kMaxSsimSlots + 1];
-  __shared__ int nch;
-  __shared__ int ws_ny;
-  __shared__ double s_wsum;
-  __shared__ unsigned long long cps_acc[2][3];
+  extern __shared__ double stage[];  // [len] values, then [len] ERP weights for weighted SSIM chains
   PairOut* o = a.out;
-
-  if(threadIdx.x == 0)
+  if(blockIdx.x == (unsigned)a.nchains)
   {
-    int n = 0, wny = 0;
-    if(a.do_wspsnr && a.ws) { for(int c = 0; c < 3; c++) { chains[n++] = { 0, c, 0 }; } }
-    if(a.cps_rows && a.ws) { for(int d = 0; d < 2; d++) { for(int c = 0; c < 3; c++) { chains[n++] = { 1, d, c }; } } }
-    for(int s = 0; s < a.nslots; s++)
-    {
-      if(a.slot[s].row_sum == nullptr || a.slot[s].ny <= 0) { continue; }
-      for(int c = 0; c < 3; c++) { chains[n++] = { 2, s, c }; }
-      if(a.slot[s].use_ws) { wny = a.slot[s].ny; }   // ERP-weighted slots are all at full resolution
-    }
-    if(wny > 0 && a.ws) { chains[n++] = { 3, 0, 0 }; }
-    nch = n; ws_ny = wny; s_wsum = 0.0;
-  }
-  if(threadIdx.x < 6) { cps_acc[threadIdx.x / 3][threadIdx.x % 3] = 0ull; }
-  __syncthreads();
-  const int n = nch;
-
-  // exact uint64 totals of the sign-extended 32-bit row sums (order independent)
-  if(a.cps_rows)
-  {
+    // exact uint64 totals of the sign-extended 32-bit CPS row sums (order independent)
+    __shared__ unsigned long long acc[6];
+    if(threadIdx.x < 6) { acc[threadIdx.x] = 0ull; }
+    __syncthreads();
     unsigned long long loc[6] = { 0, 0, 0, 0, 0, 0 };
     for(int y = threadIdx.x; y < a.H; y += blockDim.x)
     {
-      for(int d = 0; d < 2; d++)
+      #pragma unroll
+      for(int k = 0; k < 6; k++)
       {
-        for(int c = 0; c < 3; c++)
-        {
-          loc[d * 3 + c] += (unsigned long long)(long long)(int32_t)a.cps_rows[((size_t)d * a.H + y) * 3 + c];
-        }
+        loc[k] += (unsigned long long)(long long)(int32_t)a.cps_rows[((size_t)(k / 3) * a.H + y) * 3 + (k % 3)];
       }
     }
-    for(int k = 0; k < 6; k++) { atomicAdd(&cps_acc[k / 3][k % 3], loc[k]); }
+    #pragma unroll
+    for(int k = 0; k < 6; k++) { atomicAdd(&acc[k], loc[k]); }
+    __syncthreads();
+    if(threadIdx.x < 6) { o->cps_sum[threadIdx.x / 3][threadIdx.x % 3] = acc[threadIdx.x]; }
+    return;
   }
-
-  auto chain_len = [&](const Chain& ch) { return ch.kind == 2 ? a.slot[ch.a].ny : (ch.kind == 3 ? ws_ny : a.H); };
-  int maxlen = 0;
-  for(int k = 0; k < n; k++) { maxlen = max(maxlen, chain_len(chains[k])); }
-
-  Kbns sum;
-  for(int base = 0; base < maxlen; base += kChunk)
+  const FinChain ch = a.chain[blockIdx.x];
+  const bool wsum = ch.kind == kChainSsim && a.slot[ch.a].use_ws;
+  const int len = ch.kind == kChainSsim ? a.slot[ch.a].ny : a.H;
+  double* vals = stage;
+  double* wts = stage + len;
+  for(int y = threadIdx.x; y < len; y += blockDim.x)
   {
-    __syncthreads();
-    for(int e = threadIdx.x; e < n * kChunk; e += blockDim.x)
-    {
-      const int k = e / kChunk, u = e - k * kChunk, y = base + u;
-      const Chain ch = chains[k];
-      double v = 0.0;
-      if(y < chain_len(ch))
-      {
-        if(ch.kind == 0)
-        {
-          int off = 0; for(int q = 0; q < ch.a; q++) { off += a.rows[q]; }
-          const uint64_t r = a.row_ssd[off + (y >> a.sy[ch.a])] * (uint64_t)a.mult_row[ch.a];
-          v = dmul((double)r, a.ws[y]);
-        }
-        else if(ch.kind == 1)
-        {
-          const uint64_t r = (uint64_t)(int64_t)(int32_t)a.cps_rows[((size_t)ch.a * a.H + y) * 3 + ch.b];
-          v = dmul((double)r, a.ws[y]);
-        }
-        else if(ch.kind == 2)
-        {
-          const SsimSlot& sl = a.slot[ch.a];
-          v = sl.row_sum[(size_t)ch.b * sl.ny + y];
-          if(sl.use_ws) { v = dmul(v, a.ws[4 * y + 4]); }
-        }
-        else { v = a.ws[4 * y + 4]; }
-      }
-      stage[k * (kChunk + 1) + u] = v;
-    }
-    __syncthreads();
-    if(threadIdx.x < n)
-    {
-      const int cnt = min(kChunk, chain_len(chains[threadIdx.x]) - base);
-      const double* src = stage + threadIdx.x * (kChunk + 1);
-      for(int u = 0; u < cnt; u++) { sum.add(src[u]); }
-    }
+    vals[y] = chain_value(a, ch, y);
+    if(wsum) { wts[y] = a.ws[4 * y + 4]; }
   }
   __syncthreads();
-  if(threadIdx.x < n && chains[threadIdx.x].kind == 3) { s_wsum = sum.result(); }
-  __syncthreads();
-
-  if(threadIdx.x < n)
+  if(threadIdx.x != 0) { return; }
+  Kbns sum, wk;
+  int y = 0;
+  for(; y + 8 <= len; y += 8)
   {
-    const Chain ch = chains[threadIdx.x];
-    if(ch.kind == 0) { o->ws_ssd[ch.a] = sum.result(); }
-    else if(ch.kind == 1) { o->cps_ws[ch.a][ch.b] = sum.result(); }
-    else if(ch.kind == 2)
-    {
-      const SsimSlot& sl = a.slot[ch.a];
-      const double active = (double)((int64_t)sl.nx * sl.ny);
-      double r;
-      if(sl.use_ws)
-      {
-        const double corr = ddiv(s_wsum, (double)sl.ny);
-        r = ddiv(sum.result(), dmul(active, corr));
-      }
-      else { r = ddiv(sum.result(), active); }
-      o->ssim[ch.a][ch.b] = r;
-    }
+    double v[8], w[8];
+    #pragma unroll
+    for(int u = 0; u < 8; u++) { v[u] = vals[y + u]; w[u] = wsum ? wts[y + u] : 0.0; }
+    #pragma unroll
+    for(int u = 0; u < 8; u++) { sum.add(v[u]); if(wsum) { wk.add(w[u]); } }
   }
-  if(a.cps_rows && threadIdx.x < 6) { o->cps_sum[threadIdx.x / 3][threadIdx.x % 3] = cps_acc[threadIdx.x / 3][threadIdx.x % 3]; }
+  for(; y < len; y++) { sum.add(vals[y]); if(wsum) { wk.add(wts[y]); } }
+  if(ch.kind == kChainWsPsnr) { o->ws_ssd[ch.a] = sum.result(); }
+  else if(ch.kind == kChainIvPsnr) { o->cps_ws[ch.a][ch.b] = sum.result(); }
+  else
+  {
+    const SsimSlot& sl = a.slot[ch.a];
+    const double active = (double)((int64_t)sl.nx * sl.ny);
+    double r;
+    if(wsum)
+    {
+      const double corr = ddiv(wk.result(), (double)sl.ny);
+      r = ddiv(sum.result(), dmul(active, corr));
+    }
+    else { r = ddiv(sum.result(), active); }
+    o->ssim[ch.a][ch.b] = r;
+  }
 }
 
-cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s)
+cudaError_t launch_finalize(const FinalizeArgs& a_in, cudaStream_t s)
 {
-  int active = 0;
-  for(int s = 0; s < a.nslots; s++) { active += (a.slot[s].row_sum != nullptr && a.slot[s].ny > 0) ? 1 : 0; }
-  const int nch = (a.do_wspsnr && a.ws ? 3 : 0) + (a.cps_rows && a.ws ? 6 : 0) + 3 * active + 1;
-  const size_t smem = (size_t)max(nch, 1) * (kChunk + 1) * sizeof(double);
+  FinalizeArgs a = a_in;
+  a.nchains = 0;
+  if(a.do_wspsnr && a.ws) { for(int c = 0; c < 3; c++) { a.chain[a.nchains++] = { kChainWsPsnr, c, 0 }; } }
+  if(a.cps_rows && a.ws) { for(int d = 0; d < 2; d++) { for(int c = 0; c < 3; c++) { a.chain[a.nchains++] = { kChainIvPsnr, d, c }; } } }
+  for(int sl = 0; sl < a.nslots; sl++)
+  {
+    if(a.slot[sl].row_sum == nullptr || a.slot[sl].ny <= 0) { continue; }
+    for(int c = 0; c < 3; c++) { a.chain[a.nchains++] = { kChainSsim, sl, c }; }
+  }
+  const int blocks = a.nchains + (a.cps_rows ? 1 : 0);
+  if(blocks == 0) { return cudaSuccess; }
+  const size_t smem = (size_t)2 * max(a.H, 1) * sizeof(double);
   static bool configured = false;
   if(!configured)
   {
-    const cudaError_t e = cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)((3 + 6 + 3 * kMaxSsimSlots + 1) * (kChunk + 1) * sizeof(double)));
+    const cudaError_t e = cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if(e != cudaSuccess) { return e; }
     configured = true;
   }
-  k_finalize<<<1, 256, smem, s>>>(a);
+  if(smem > 200 * 1024) { return cudaErrorInvalidValue; }
+  k_finalize<<<blocks, 256, smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -62,18 +62,18 @@ struct SsimWinArgs
 {
   Img     a, b;                // a = "Tst" picture, b = "Ref" picture of xSSIM::xCalcPicSSIM
   int32_t W, H;
-  int32_t nx, ny, ny_pad;      // windows per row / column, column stride of win
+  int32_t nx, ny, nx_pad;      // windows per row / column, row stride of win
   uint32_t clip;
   double  C1, C2;
   int32_t calc_l;
-  double* win;                 // [3][nx][ny_pad]
+  double* win;                 // [3][ny][nx_pad]
   MutImg  down_a, down_b;      // outputs ((W>>1) x (H>>1), 4:4:4) or null planes
 };
 
 struct SsimRowArgs
 {
-  const double* win;           // [3][nx][ny_pad]
-  int32_t       nx, ny, ny_pad;
+  const double* win;           // [3][ny][nx_pad]
+  int32_t       nx, ny, nx_pad;
   double*       row_sum;       // [3][ny]
 };
 
@@ -87,6 +87,13 @@ struct SsimSlot
   int32_t       use_ws;        // ERP row weights w[4j + 4] (xIVSSIM.cpp:148-165)
 };
 
+enum { kChainWsPsnr = 0, kChainIvPsnr = 1, kChainSsim = 2 };
+struct FinChain
+{
+  int32_t kind;  // kChain*
+  int32_t a, b;  // component / direction / slot
+};
+
 struct FinalizeArgs
 {
   int32_t         H;
@@ -98,6 +105,8 @@ struct FinalizeArgs
   const uint32_t* cps_rows;             // [2][H][3] or null
   int32_t         nslots;
   SsimSlot        slot[kMaxSsimSlots];
+  int32_t         nchains;              // filled by launch_finalize
+  FinChain        chain[3 + 6 + 3 * kMaxSsimSlots];
   PairOut*        out;
 };
 
