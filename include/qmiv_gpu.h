@@ -203,6 +203,26 @@ QMIV_API qmiv_status qmiv_calc_cps_rows(qmiv_calc calc, uint64_t* rows_r2t, uint
 /* Device stream (cudaStream_t) the calc enqueues on, for callers that order their own work. */
 QMIV_API qmiv_status qmiv_calc_stream(qmiv_calc calc, void** cuda_stream);
 
+/* ---- allocation-free form ------------------------------------------------------------------ */
+/* No counterpart in the reference. For callers that must not allocate device memory: code running
+   inside a host application's own memory manager or a plugin sandbox that forbids cudaMalloc, paths
+   that run under a strict no-allocation policy after start-up, and callers whose allocator is not
+   theirs to use (allocating there could deadlock or break a memory budget). It computes PSNR,
+   WS-PSNR and IV-PSNR (the metrics in `metric_mask`, others are rejected) of one frame pair whose
+   planes are already in device memory, enqueued on `cuda_stream` (0 = default stream), and blocks
+   until the result is in `out`. It calls no cudaMalloc, cudaFree or other allocating routine: its
+   scratch is one fixed file-scope device array (about 350 KB, held by every GPU that loads the
+   library until exit), which limits the picture height to QMIV_STATIC_MAX_HEIGHT rows; taller
+   pictures are rejected with QMIV_ERR_UNSUPPORTED. The first call on a device looks up that
+   array's device address (with the device current); make that first call before any stream
+   capture. All calls share the one array: calls that overlap on the GPU (from different threads or
+   streams) race, so serialise them. */
+#define QMIV_STATIC_MAX_HEIGHT 4352
+QMIV_API qmiv_status qmiv_frame_pair_compute_static(const qmiv_frame* in0, const qmiv_frame* in1, int32_t width,
+                                                    int32_t height, int32_t bitdepth, int32_t chroma_format,
+                                                    const qmiv_params* params, uint32_t metric_mask,
+                                                    void* cuda_stream, qmiv_result* out);
+
 /* ---- batched form: many frame pairs of uneven shape per launch ---------------------------- */
 typedef struct qmiv_pair_desc
 {

@@ -91,6 +91,10 @@ SIGNATURES = {
     "qmiv_calc_set_gcd": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "qmiv_calc_cps_rows": (ctypes.c_int, [_P, _P, _P]),
     "qmiv_calc_stream": (ctypes.c_int, [_P, _PP]),
+    "qmiv_frame_pair_compute_static": (ctypes.c_int, [ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame),
+                                                      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                      ctypes.POINTER(QmivParams), ctypes.c_uint32, _P,
+                                                      ctypes.POINTER(QmivResult)]),
     "qmiv_batch_create": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(QmivParams),
                                          ctypes.c_int32, _PP]),
     "qmiv_probe_int32_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),

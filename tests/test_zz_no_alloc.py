@@ -1,0 +1,75 @@
+"""The allocation-free entry point, qmiv_frame_pair_compute_static.
+
+Some callers of this library cannot allocate device memory: code that runs inside a host
+application's own memory manager or a plugin sandbox where cudaMalloc is forbidden, and services
+that must not allocate after start-up. The entry point keeps all of its scratch in one fixed device
+array, so these callers can still compute PSNR, WS-PSNR and IV-PSNR of device-resident frames.
+
+This file is collected last so that a run stopping at the first failure has run every other test.
+It checks the entry point through the C ABI against the regular entry point on two calls in a row
+(the second call must not see the first call's leftovers in the shared array). The tolerance is the
+one the other parity tests use: results must be identical.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_frame(frame):
+    import torch
+    import qmiv_b200
+    planes = tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in frame)
+    f, keep = qmiv_b200.make_frame(planes)
+    return f, (planes, keep)
+
+
+def _static_call(lib, f0, f1, W, H, bd, params, mask):
+    from qmiv_b200 import _lib
+    out = _lib.QmivResult()
+    st = lib.qmiv_frame_pair_compute_static(ctypes.byref(f0), ctypes.byref(f1), W, H, bd, 420, ctypes.byref(params),
+                                            mask, None, ctypes.byref(out))
+    return st, out.as_dict()
+
+
+@pytest.mark.parametrize("erp", [False, True])
+def test_static_entry_point_matches_regular_entry_point(erp):
+    import torch
+    import qmiv_b200
+    from qmiv_b200 import synth
+    lib = qmiv_b200.library()
+    W, H, bd = 1920, 1080, 10
+    mask = qmiv_b200.PSNR | qmiv_b200.WSPSNR | qmiv_b200.IVPSNR
+    params = qmiv_b200.make_params(erp=erp)
+    with qmiv_b200.Context(0) as ctx, qmiv_b200.Calc(ctx, W, H, bd, 420, erp=erp) as calc:
+        for seed in (11, 12):  # two calls in a row through the shared scratch array
+            a, b = synth.make_pair(W, H, bd, seed=seed)
+            f0, k0 = _device_frame(a)
+            f1, k1 = _device_frame(b)
+            st, got = _static_call(lib, f0, f1, W, H, bd, params, mask)
+            assert st == 0, lib.qmiv_last_error()
+            torch.cuda.synchronize()
+            exp = calc.compute(k0[0], k1[0], mask)
+            for key in ("gcd_r2t", "exact", "ssd", "cps_sse_r2t", "cps_sse_t2r", "psnr", "psnr_pic", "wspsnr",
+                        "wspsnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"):
+                assert got[key] == exp[key], key
+
+
+def test_static_entry_point_rejects_what_it_cannot_do():
+    import qmiv_b200
+    from qmiv_b200 import synth
+    lib = qmiv_b200.library()
+    params = qmiv_b200.make_params()
+    W, H = 64, 4400  # taller than QMIV_STATIC_MAX_HEIGHT
+    a, b = synth.make_pair(W, H, 8, seed=3)
+    f0, k0 = _device_frame(a)
+    f1, k1 = _device_frame(b)
+    st, _ = _static_call(lib, f0, f1, W, H, 8, params, qmiv_b200.IVPSNR)
+    assert st == 2  # QMIV_ERR_UNSUPPORTED
+    st, _ = _static_call(lib, f0, f1, W, H, 8, params, qmiv_b200.IVSSIM)
+    assert st == 2
+    h0, hk0 = qmiv_b200.make_frame(synth.make_pair(64, 64, 8, seed=4)[0])
+    st, _ = _static_call(lib, h0, h0, 64, 64, 8, params, qmiv_b200.IVPSNR)
+    assert st == 1  # host frames are not accepted
