@@ -112,12 +112,19 @@ qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames
   QMIV_TRY(row_sd_.ensure(ctx_, rows_total * sizeof(int64_t)));
   QMIV_TRY(row_ssd_.ensure(ctx_, rows_total * sizeof(uint64_t)));
   QMIV_TRY(out_.ensure(ctx_, sizeof(PairOut)));
-  const bool need_scp = want_scp || (mask & (QMIV_IVSSIM | QMIV_IVMSSSIM));
-  const bool need_search = need_scp || (mask & QMIV_IVPSNR);
+  const bool need_scp = want_scp || (mask & QMIV_IVMSSSIM);
+  const bool need_search = need_scp || (mask & (QMIV_IVPSNR | QMIV_IVSSIM));
   const bool need_ssim = mask & (QMIV_SSIM | QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM);
   const bool need_ms = mask & (QMIV_MSSSIM | QMIV_IVMSSSIM);
   if(need_search) { QMIV_TRY(cps_rows_.ensure(ctx_, (size_t)2 * S.H * 3 * sizeof(uint32_t))); }
   if(need_scp) { QMIV_TRY(scp_.ensure(ctx_, (size_t)2 * 3 * S.W * S.H * S.esz)); }
+  if(need_ssim)
+  {
+    // moment slots: 0, 1 = IV-SSIM directions (written by the search), 2 = SSIM / MS-SSIM pair,
+    // 3, 4 = IV-MS-SSIM pairs
+    const int slots = (mask & QMIV_IVMSSSIM) ? 5 : (mask & (QMIV_SSIM | QMIV_MSSSIM)) ? 3 : 2;
+    QMIV_TRY(mom_.ensure(ctx_, (size_t)slots * mom_slot_elems() * sizeof(uint32_t)));
+  }
   if(prm_.erp)
   {
     QMIV_TRY(ws_.ensure(ctx_, (size_t)S.H * sizeof(double)));
@@ -126,7 +133,6 @@ qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames
   if(need_ssim)
   {
     if(nx_[0] < 1 || ny_[0] < 1) { return fail(QMIV_ERR_INVALID_ARG, "picture smaller than one 8x8 SSIM window"); }
-    QMIV_TRY(win_.ensure(ctx_, (size_t)3 * ny_[0] * nxp_ * sizeof(double)));
     QMIV_TRY(rowsum_.ensure(ctx_, (size_t)kMaxSsimSlots * 3 * ny_[0] * sizeof(double)));
   }
   if(need_ms)
@@ -216,8 +222,8 @@ template <typename T>
 qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mask, bool want_scp, bool want_gcd, cudaStream_t s)
 {
   const Shape& S = shape_;
-  const bool need_scp = want_scp || (mask & (QMIV_IVSSIM | QMIV_IVMSSSIM));
-  const bool need_search = need_scp || (mask & QMIV_IVPSNR);
+  const bool need_scp = want_scp || (mask & QMIV_IVMSSSIM);
+  const bool need_search = need_scp || (mask & (QMIV_IVPSNR | QMIV_IVSSIM));
   const uint32_t clip = prm_.invalid_pel_action == QMIV_PEL_CNCL ? (uint32_t)S.maxv : 0xffffu;
   PairOut* dout = out_.as<PairOut>();
 
@@ -255,6 +261,7 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
     ca.gcd_src = dout; ca.rows = cps_rows_.as<uint32_t>();
     ca.scp0 = need_scp ? const_cast<void*>(scp(0)) : nullptr;
     ca.scp1 = need_scp ? const_cast<void*>(scp(1)) : nullptr;
+    if(mask & QMIV_IVSSIM) { ca.mom[0] = mom_at(0, 0); ca.mom[1] = mom_at(1, 0); }  // (In0, SCP1), (In1, SCP0)
     const int t = prof_begin(s);
     QMIV_CUDA(launch_cps<T>(ca, R_, s));
     prof_end(s, QMIV_STAGE_CPS, t);
@@ -264,31 +271,55 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
   FinalizeArgs fa{};
   fa.nslots = kMaxSsimSlots;
   double* rowsum = rowsum_.as<double>();
-  auto run_ssim = [&](const Img& a, const Img& b, int W, int H, int scale, int slot, int calc_l, int use_ws,
-                      const MutImg* down_a, const MutImg* down_b) -> qmiv_status {
-    SsimWinArgs wa{};
-    wa.a = a; wa.b = b; wa.W = W; wa.H = H; wa.nx = nx_[scale]; wa.ny = ny_[scale]; wa.nx_pad = nxp_;
-    wa.clip = clip; wa.C1 = C1_; wa.C2 = C2_; wa.calc_l = calc_l; wa.win = win_.as<double>();
-    if(down_a) { wa.down_a = *down_a; }
-    if(down_b) { wa.down_b = *down_b; }
-    { const int t = prof_begin(s); QMIV_CUDA(launch_ssim_win<T>(wa, s)); prof_end(s, QMIV_STAGE_SSIM_WIN, t); }
-    SsimRowArgs rr{};
-    rr.win = wa.win; rr.nx = wa.nx; rr.ny = wa.ny; rr.nx_pad = nxp_;
-    rr.row_sum = rowsum + (size_t)slot * 3 * ny_[0];
-    { const int t = prof_begin(s); QMIV_CUDA(launch_ssim_rows(rr, s)); prof_end(s, QMIV_STAGE_SSIM_ROWS, t); }
-    fa.slot[slot].row_sum = rr.row_sum; fa.slot[slot].nx = wa.nx; fa.slot[slot].ny = wa.ny; fa.slot[slot].use_ws = use_ws;
+  // window pooling of up to three pictures pairs (x 3 components) from their moments, one launch
+  SsimPoolArgs pool{};
+  pool.C1 = C1_; pool.C2 = C2_;
+  auto add_pool = [&](const Moments& m, int scale, int slot, int calc_l, int use_ws) {
+    for(int c = 0; c < 3; c++)
+    {
+      SsimPoolJob& J = pool.job[pool.njobs++];
+      J.mom = m.p + (size_t)c * 5 * m.plane(); J.plane = m.plane(); J.pitch = m.pitch;
+      J.nx = nx_[scale]; J.ny = ny_[scale]; J.calc_l = calc_l;
+      J.row_sum = rowsum + (size_t)slot * 3 * ny_[0] + (size_t)c * ny_[scale];  // finalize reads [c][ny_scale]
+    }
+    fa.slot[slot].row_sum = rowsum + (size_t)slot * 3 * ny_[0];
+    fa.slot[slot].nx = nx_[scale]; fa.slot[slot].ny = ny_[scale]; fa.slot[slot].use_ws = use_ws;
+  };
+  auto flush_pool = [&]() -> qmiv_status {
+    if(pool.njobs == 0) { return QMIV_OK; }
+    const int t = prof_begin(s);
+    QMIV_CUDA(launch_ssim_pool(pool, s));
+    prof_end(s, QMIV_STAGE_SSIM_ROWS, t);
+    pool.njobs = 0;
+    return QMIV_OK;
+  };
+  auto moments = [&](const Img& a, const Img& b, int W, int H, const Moments& m, const MutImg* down_a,
+                     const MutImg* down_b) -> qmiv_status {
+    SsimMomArgs ma{};
+    ma.a = a; ma.b = b; ma.W = W; ma.H = H; ma.clip = clip; ma.mom = m;
+    if(down_a) { ma.down_a = *down_a; }
+    if(down_b) { ma.down_b = *down_b; }
+    const int t = prof_begin(s);
+    QMIV_CUDA(launch_ssim_moments<T>(ma, s));
+    prof_end(s, QMIV_STAGE_SSIM_WIN, t);
     return QMIV_OK;
   };
 
   const Img scp0 = need_scp ? img444(scp(0), S.W, S.H, S.esz) : Img{};
   const Img scp1 = need_scp ? img444(scp(1), S.W, S.H, S.esz) : Img{};
   const int use_ws = prm_.erp ? 1 : 0;
-  if(mask & QMIV_SSIM) { QMIV_TRY(run_ssim(in0, in1, S.W, S.H, 0, kSlotSsim, 1, 0, nullptr, nullptr)); }        // xSSIM.h:83
-  if(mask & QMIV_IVSSIM)                                                                                         // xIVSSIM.cpp:46-47
+  if(mask & QMIV_IVSSIM)  // moments written by the search: (In0, SCP1) = T2R, (In1, SCP0) = R2T (xIVSSIM.cpp:46-47)
   {
-    QMIV_TRY(run_ssim(in0, scp1, S.W, S.H, 0, kSlotIvT2R, 1, use_ws, nullptr, nullptr));
-    QMIV_TRY(run_ssim(in1, scp0, S.W, S.H, 0, kSlotIvR2T, 1, use_ws, nullptr, nullptr));
+    add_pool(mom_at(0, 0), 0, kSlotIvT2R, 1, use_ws);
+    add_pool(mom_at(1, 0), 0, kSlotIvR2T, 1, use_ws);
   }
+  if(mask & QMIV_SSIM)  // xSSIM.h:83
+  {
+    QMIV_TRY(moments(in0, in1, S.W, S.H, mom_at(2, 0), nullptr, nullptr));
+    if(pool.njobs + 3 > 9) { QMIV_TRY(flush_pool()); }
+    add_pool(mom_at(2, 0), 0, kSlotSsim, 1, 0);
+  }
+  QMIV_TRY(flush_pool());
   if(mask & (QMIV_MSSSIM | QMIV_IVMSSSIM))                                                                      // xSSIM.cpp:230-256
   {
     // pyramid levels 1..ns-1 of In0, In1, SCP0, SCP1
@@ -318,15 +349,19 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
       if(mask & QMIV_MSSSIM)
       {
         const MutImg* d0 = down(0, m0); const MutImg* d1 = down(1, m1);
-        QMIV_TRY(run_ssim(level_img(0, sc), level_img(1, sc), Ws, Hs, sc, kSlotMs + sc, last ? 1 : 0, 0, d0, d1));
+        QMIV_TRY(moments(level_img(0, sc), level_img(1, sc), Ws, Hs, mom_at(2, sc), d0, d1));
+        add_pool(mom_at(2, sc), sc, kSlotMs + sc, last ? 1 : 0, 0);
       }
-      if(mask & QMIV_IVMSSSIM)
+      if(mask & QMIV_IVMSSSIM)  // xIVSSIM.cpp:77-78, no ERP weighting
       {
         const MutImg* d0 = down(0, m2); const MutImg* d3 = down(3, m3);
-        QMIV_TRY(run_ssim(level_img(0, sc), level_img(3, sc), Ws, Hs, sc, kSlotIvmsT2R + sc, last ? 1 : 0, 0, d0, d3));
+        QMIV_TRY(moments(level_img(0, sc), level_img(3, sc), Ws, Hs, mom_at(3, sc), d0, d3));
+        add_pool(mom_at(3, sc), sc, kSlotIvmsT2R + sc, last ? 1 : 0, 0);
         const MutImg* d1 = down(1, m4); const MutImg* d2 = down(2, m5);
-        QMIV_TRY(run_ssim(level_img(1, sc), level_img(2, sc), Ws, Hs, sc, kSlotIvmsR2T + sc, last ? 1 : 0, 0, d1, d2));
+        QMIV_TRY(moments(level_img(1, sc), level_img(2, sc), Ws, Hs, mom_at(4, sc), d1, d2));
+        add_pool(mom_at(4, sc), sc, kSlotIvmsR2T + sc, last ? 1 : 0, 0);
       }
+      QMIV_TRY(flush_pool());
     }
   }
 

@@ -43,17 +43,49 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
 // Kahan-Babuska-Neumaier compensated sum (libs/pmbb-core/src/xKBNS.h:36-43).
+// The reference adds to c the rounding error of s + v, computed by Fast2Sum with the larger of the
+// two operands first. That error is exactly representable and unique, so Knuth's branch-free
+// TwoSum yields the same double; here it keeps the dependent chain free of branches.
 struct Kbns
 {
   double s = 0.0, c = 0.0;
   __device__ __forceinline__ void add(double v)
   {
-    const double t = dadd(s, v);
-    if(fabs(s) >= fabs(v)) { c = dadd(c, dadd(dsub(s, t), v)); }
-    else                   { c = dadd(c, dadd(dsub(v, t), s)); }
+    const double t  = dadd(s, v);
+    const double bv = dsub(t, s);
+    const double e  = dadd(dsub(s, dsub(t, bv)), dsub(v, bv));
+    c = dadd(c, e);
     s = t;
   }
   __device__ __forceinline__ double result() const { return dadd(s, c); }
+};
+
+// SSIM of one window from exact integer moments (xStructSimSTD.cpp:420-461, same operation order;
+// AVX-512 CalcBlckAvg8 / CalcMultiBlckAvg8S4 give the same per-window value).
+__device__ __forceinline__ double ssim_window(uint64_t sr, uint64_t st, uint64_t srr, uint64_t stt, uint64_t srt,
+                                              double C1, double C2, bool calc_l)
+{
+  const double inv   = 0.015625;  // 1/64, exact
+  const double avg_r = dmul((double)sr, inv);
+  const double avg_t = dmul((double)st, inv);
+  const double var_r = dsub(dmul((double)srr, inv), dmul(avg_r, avg_r));
+  const double var_t = dsub(dmul((double)stt, inv), dmul(avg_t, avg_t));
+  const double cov   = dsub(dmul((double)srt, inv), dmul(avg_r, avg_t));
+  const double cs    = ddiv(dadd(dmul(2.0, cov), C2), dadd(dadd(var_r, var_t), C2));
+  if(!calc_l) { return cs; }
+  const double l = ddiv(dadd(dmul(dmul(2.0, avg_r), avg_t), C1), dadd(dadd(dmul(avg_r, avg_r), dmul(avg_t, avg_t)), C1));
+  return dmul(l, cs);
+}
+
+// 4x4 sub-block moments of an SSIM picture pair, five uint32 planes per component:
+// [c][m][nby][pitch], m = 0: sum a, 1: sum b, 2: sum a^2, 3: sum b^2, 4: sum a*b
+// (a = the "Tst" picture, b = the "Ref" picture of xSSIM::xCalcPicSSIM). Every 8x8/stride-4 window is
+// the sum of 2x2 sub-blocks, so window moments are exact integers.
+struct Moments
+{
+  uint32_t* p;      // base of component 0, moment 0
+  int32_t   nbx, nby, pitch;
+  __host__ __device__ size_t plane() const { return (size_t)nby * pitch; }
 };
 
 // Round half away from zero by adding +-0.5 in double and truncating (xHelpersFLT.h:33).

@@ -146,7 +146,23 @@ private:
   double       ws_corr_ = 1.0;
   double       C1_ = 0, C2_ = 0;
 
-  DevMem row_sd_, row_ssd_, cps_rows_, out_, ws_, scp_, pyr_, win_, rowsum_, staging_;
+  // SSIM moments (qmiv_device.cuh, Moments) of one pair at scale s, in slot k of mom_
+  Moments mom_at(int slot, int scale) const
+  {
+    Moments m{};
+    m.nbx = ((shape_.W >> scale) + 3) / 4;
+    m.nby = ((shape_.H >> scale) + 3) / 4;
+    m.pitch = (m.nbx + 7) & ~7;
+    m.p = mom_.as<uint32_t>() + (size_t)slot * mom_slot_elems();
+    return m;
+  }
+  size_t mom_slot_elems() const
+  {
+    const size_t nbx = ((size_t)shape_.W + 3) / 4, nby = ((size_t)shape_.H + 3) / 4;
+    return 3 * 5 * nby * ((nbx + 7) & ~(size_t)7);
+  }
+
+  DevMem row_sd_, row_ssd_, cps_rows_, out_, ws_, scp_, pyr_, mom_, rowsum_, staging_;
   PairOut* h_out = nullptr;
   bool ws_uploaded_ = false;
   bool gcd_override_on_ = false;

@@ -5,11 +5,10 @@
 //   k_prepass   per raw row: SD(In1-In0), SSD, max sample        (HBM bound, reads both frames once)
 //   k_reduce    totals, GCD, exactness of the fp32 search path   (one CTA)
 //   k_cps       corresponding-pixel-shift search, both directions in one pass; per-row SSE into
-//               32-bit lanes and, when an IV-SSIM metric needs them, the shift-compensated pictures
-//   k_ssim_win  8x8/stride-4 block SSIM per window from exact integer moments, FP64 formula,
-//               fused 2x2 downsampling for the next MS-SSIM scale
-//   k_ssim_rows per window row, compensated sum of the windows in x order
-//   k_finalize  every order-dependent FP64 pooling chain of the pair (one thread per chain)
+//               32-bit lanes, the IV-SSIM sub-block moments of (test, SCP) and, when IV-MS-SSIM or
+//               the caller needs them, the shift-compensated pictures
+//   k_ssim_*    (qmiv_ssim.cu) block SSIM from exact integer moments, FP64 windows, row sums
+//   k_finalize  every order-dependent FP64 pooling chain of the pair (one CTA per chain)
 #include "qmiv_kernels.cuh"
 
 #include <cstdio>
@@ -276,11 +275,21 @@ __global__ void __launch_bounds__(128) k_cps(const __grid_constant__ CpsArgs a)
       }
     }
 
-    // epilogue: winner's per-component squared difference into the row sums, SCP store
+    // epilogue: winner's per-component squared difference into the row sums, SCP store, and the
+    // SSIM moments of (test picture, SCP) per 4x4 sub-block (4 rows of a thread x 4 lanes)
     uint32_t* rows = a.rows + (size_t)dir * H * 3;
     T* scp = static_cast<T*>(dir ? a.scp0 : a.scp1);
+    const Moments mom = a.mom[dir];
     const size_t plane = (size_t)W * H;
     const int x = x0 + tx;
+    static_assert(P % 4 == 0, "rows per thread must cover whole 4x4 sub-blocks");
+    uint32_t mm[P / 4][3][5];
+    #pragma unroll
+    for(int q = 0; q < P / 4; q++)
+      #pragma unroll
+      for(int c = 0; c < 3; c++)
+        #pragma unroll
+        for(int m = 0; m < 5; m++) { mm[q][c][m] = 0u; }
     #pragma unroll
     for(int i = 0; i < P; i++)
     {
@@ -290,7 +299,8 @@ __global__ void __launch_bounds__(128) k_cps(const __grid_constant__ CpsArgs a)
       const float4 r = ref[(ty * P + i + dyi) * SW + tx + dxi];
       const float4 t = tst[(ty * P + i + R) * SW + tx + R];
       const int r0 = (int)r.x, r1 = (int)r.y, r2 = (int)r.z;
-      const uint32_t e0 = (uint32_t)((int)t.x + ga - r0), e1 = (uint32_t)((int)t.y + gb - r1), e2 = (uint32_t)((int)t.z + gc - r2);
+      const int t0 = (int)t.x, t1 = (int)t.y, t2 = (int)t.z;
+      const uint32_t e0 = (uint32_t)(t0 + ga - r0), e1 = (uint32_t)(t1 + gb - r1), e2 = (uint32_t)(t2 + gc - r2);
       const uint32_t s0 = __reduce_add_sync(kFull, valid ? e0 * e0 : 0u);
       const uint32_t s1 = __reduce_add_sync(kFull, valid ? e1 * e1 : 0u);
       const uint32_t s2 = __reduce_add_sync(kFull, valid ? e2 * e2 : 0u);
@@ -300,12 +310,52 @@ __global__ void __launch_bounds__(128) k_cps(const __grid_constant__ CpsArgs a)
         atomicAdd(rows + (size_t)y * 3 + 1, s1);
         atomicAdd(rows + (size_t)y * 3 + 2, s2);
       }
+      const int c0 = clampi(r0 - ga, 0, a.maxv), c1 = clampi(r1 - gb, 0, a.maxv), c2 = clampi(r2 - gc, 0, a.maxv);
       if(scp != nullptr && valid)
       {
         const size_t o = (size_t)y * W + x;
-        scp[o]             = (T)clampi(r0 - ga, 0, a.maxv);
-        scp[plane + o]     = (T)clampi(r1 - gb, 0, a.maxv);
-        scp[2 * plane + o] = (T)clampi(r2 - gc, 0, a.maxv);
+        scp[o]             = (T)c0;
+        scp[plane + o]     = (T)c1;
+        scp[2 * plane + o] = (T)c2;
+      }
+      if(mom.p != nullptr && valid)
+      {
+        const int q = i >> 2;
+        const uint32_t av[3] = { (uint32_t)t0, (uint32_t)t1, (uint32_t)t2 };
+        const uint32_t bv[3] = { (uint32_t)c0, (uint32_t)c1, (uint32_t)c2 };
+        #pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          mm[q][c][0] += av[c];
+          mm[q][c][1] += bv[c];
+          mm[q][c][2] += av[c] * av[c];
+          mm[q][c][3] += bv[c] * bv[c];
+          mm[q][c][4] += av[c] * bv[c];
+        }
+      }
+    }
+    if(mom.p != nullptr)
+    {
+      const int bx = x >> 2;
+      #pragma unroll
+      for(int q = 0; q < P / 4; q++)
+      {
+        const int by = ((y0 + ty * P) >> 2) + q;
+        #pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          #pragma unroll
+          for(int m = 0; m < 5; m++)
+          {
+            uint32_t v = mm[q][c][m];
+            v += __shfl_xor_sync(kFull, v, 1);
+            v += __shfl_xor_sync(kFull, v, 2);
+            if((tx & 3) == 0 && bx < mom.nbx && by < mom.nby)
+            {
+              mom.p[((size_t)c * 5 + m) * mom.plane() + (size_t)by * mom.pitch + bx] = v;
+            }
+          }
+        }
       }
     }
   }
@@ -343,170 +393,6 @@ cudaError_t launch_cps(const CpsArgs& a, int R, cudaStream_t s)
 }
 template cudaError_t launch_cps<uint8_t>(const CpsArgs&, int, cudaStream_t);
 template cudaError_t launch_cps<uint16_t>(const CpsArgs&, int, cudaStream_t);
-
-// =============================================================================================
-// block SSIM windows (libs/pmbb-ivqm/src/xStructSimSTD.cpp:420-461; loop ranges xSSIM.cpp:276-311)
-//
-// A CTA owns 32x8 windows (origins 4i, 4j), i.e. a 132x36 pixel region of both pictures. 4x4
-// sub-block moments are formed once and every window adds four of them, so all sums are exact
-// integers; the SSIM formula is then evaluated in FP64 with the reference's operation order.
-// The CTA grid covers the whole picture so that the fused 2x2 mean (xPixelOpsSTD.cpp:50-67) of
-// each owned 128x32 region can be written for the next MS-SSIM scale.
-// =============================================================================================
-constexpr int kSwX = 32, kSwY = 8;                      // windows per CTA
-constexpr int kSpX = kSwX * 4 + 4, kSpY = kSwY * 4 + 4; // pixel region 132 x 36
-constexpr int kSbX = kSwX + 1, kSbY = kSwY + 1;         // sub-blocks 33 x 9
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_ssim_win(const __grid_constant__ SsimWinArgs a)
-{
-  __shared__ uint16_t pa[kSpY][kSpX];
-  __shared__ uint16_t pb[kSpY][kSpX];
-  __shared__ uint32_t sa[kSbY][kSbX], sb[kSbY][kSbX];
-  __shared__ uint64_t saa[kSbY][kSbX], sbb[kSbY][kSbX], sab[kSbY][kSbX];
-
-  const int c   = blockIdx.z;
-  const int px0 = blockIdx.x * (kSwX * 4), py0 = blockIdx.y * (kSwY * 4);
-  const int W = a.W, H = a.H;
-
-  for(int i = threadIdx.x; i < kSpX * kSpY; i += blockDim.x)
-  {
-    const int ly = i / kSpX, lx = i - ly * kSpX;
-    const int gx = min(px0 + lx, W - 1), gy = min(py0 + ly, H - 1);
-    pa[ly][lx] = (uint16_t)min((uint32_t)fetch<T>(a.a, c, gx, gy), a.clip);
-    pb[ly][lx] = (uint16_t)min((uint32_t)fetch<T>(a.b, c, gx, gy), a.clip);
-  }
-  __syncthreads();
-
-  for(int i = threadIdx.x; i < kSbX * kSbY; i += blockDim.x)
-  {
-    const int by = i / kSbX, bx = i - by * kSbX;
-    uint32_t s_a = 0, s_b = 0;
-    uint64_t s_aa = 0, s_bb = 0, s_ab = 0;
-    #pragma unroll
-    for(int y = 0; y < 4; y++)
-    {
-      #pragma unroll
-      for(int x = 0; x < 4; x++)
-      {
-        const uint32_t va = pa[by * 4 + y][bx * 4 + x], vb = pb[by * 4 + y][bx * 4 + x];
-        s_a += va; s_b += vb;
-        s_aa += va * va; s_bb += vb * vb; s_ab += va * vb;
-      }
-    }
-    sa[by][bx] = s_a; sb[by][bx] = s_b; saa[by][bx] = s_aa; sbb[by][bx] = s_bb; sab[by][bx] = s_ab;
-  }
-  __syncthreads();
-
-  {
-    const int wx = threadIdx.x & 31, wy = threadIdx.x >> 5;
-    const int i = blockIdx.x * kSwX + wx, j = blockIdx.y * kSwY + wy;
-    if(i < a.nx && j < a.ny)
-    {
-      const uint32_t sr  = sb[wy][wx] + sb[wy][wx + 1] + sb[wy + 1][wx] + sb[wy + 1][wx + 1];
-      const uint32_t st  = sa[wy][wx] + sa[wy][wx + 1] + sa[wy + 1][wx] + sa[wy + 1][wx + 1];
-      const uint64_t srr = sbb[wy][wx] + sbb[wy][wx + 1] + sbb[wy + 1][wx] + sbb[wy + 1][wx + 1];
-      const uint64_t stt = saa[wy][wx] + saa[wy][wx + 1] + saa[wy + 1][wx] + saa[wy + 1][wx + 1];
-      const uint64_t srt = sab[wy][wx] + sab[wy][wx + 1] + sab[wy + 1][wx] + sab[wy + 1][wx + 1];
-      const double inv   = 0.015625;  // 1/64, exact
-      const double avg_r = dmul((double)sr, inv);
-      const double avg_t = dmul((double)st, inv);
-      const double var_r = dsub(dmul((double)srr, inv), dmul(avg_r, avg_r));
-      const double var_t = dsub(dmul((double)stt, inv), dmul(avg_t, avg_t));
-      const double cov   = dsub(dmul((double)srt, inv), dmul(avg_r, avg_t));
-      const double cs    = ddiv(dadd(dmul(2.0, cov), a.C2), dadd(dadd(var_r, var_t), a.C2));
-      double v = cs;
-      if(a.calc_l)
-      {
-        const double l = ddiv(dadd(dmul(dmul(2.0, avg_r), avg_t), a.C1), dadd(dadd(dmul(avg_r, avg_r), dmul(avg_t, avg_t)), a.C1));
-        v = dmul(l, cs);
-      }
-      a.win[((size_t)c * a.ny + j) * a.nx_pad + i] = v;
-    }
-  }
-
-  // fused 2x2 downsampling of the owned 128x32 region for the next MS-SSIM scale
-  const int dw = W >> 1, dh = H >> 1;
-  const int dx0 = px0 >> 1, dy0 = py0 >> 1;
-  if(a.down_a.p[c] != nullptr || a.down_b.p[c] != nullptr)
-  {
-    for(int i = threadIdx.x; i < (kSwX * 2) * (kSwY * 2); i += blockDim.x)
-    {
-      const int ly = i / (kSwX * 2), lx = i - ly * (kSwX * 2);
-      const int dx = dx0 + lx, dy = dy0 + ly;
-      if(dx >= dw || dy >= dh) { continue; }
-      if(a.down_a.p[c] != nullptr)
-      {
-        const uint32_t v = ((uint32_t)pa[2 * ly][2 * lx] + pa[2 * ly][2 * lx + 1] + pa[2 * ly + 1][2 * lx] + pa[2 * ly + 1][2 * lx + 1] + 2) >> 2;
-        static_cast<T*>(a.down_a.p[c])[(size_t)dy * a.down_a.pitch[c] + dx] = (T)v;
-      }
-      if(a.down_b.p[c] != nullptr)
-      {
-        const uint32_t v = ((uint32_t)pb[2 * ly][2 * lx] + pb[2 * ly][2 * lx + 1] + pb[2 * ly + 1][2 * lx] + pb[2 * ly + 1][2 * lx + 1] + 2) >> 2;
-        static_cast<T*>(a.down_b.p[c])[(size_t)dy * a.down_b.pitch[c] + dx] = (T)v;
-      }
-    }
-  }
-}
-
-template <typename T>
-cudaError_t launch_ssim_win(const SsimWinArgs& a, cudaStream_t s)
-{
-  const dim3 grid((a.W + kSwX * 4 - 1) / (kSwX * 4), (a.H + kSwY * 4 - 1) / (kSwY * 4), 3);
-  k_ssim_win<T><<<grid, 256, 0, s>>>(a);
-  return cudaGetLastError();
-}
-template cudaError_t launch_ssim_win<uint8_t>(const SsimWinArgs&, cudaStream_t);
-template cudaError_t launch_ssim_win<uint16_t>(const SsimWinArgs&, cudaStream_t);
-
-// =============================================================================================
-// per window row: compensated sum of the windows in x order (xSSIM.cpp:353-369)
-// =============================================================================================
-// One warp per window row: the row is staged into shared memory with coalesced loads (all lanes,
-// independent), then lane 0 runs the order-dependent sum from shared memory.
-__global__ void __launch_bounds__(256) k_ssim_rows(const __grid_constant__ SsimRowArgs a)
-{
-  extern __shared__ double rowbuf[];  // [warps per block][nx_pad]
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int row = blockIdx.x * (blockDim.x >> 5) + w;
-  if(row >= 3 * a.ny) { return; }
-  const double* src = a.win + (size_t)row * a.nx_pad;
-  double* buf = rowbuf + (size_t)w * a.nx_pad;
-  for(int i = lane; i < a.nx; i += 32) { buf[i] = src[i]; }
-  __syncwarp();
-  if(lane == 0)
-  {
-    Kbns k;
-    int i = 0;
-    for(; i + 8 <= a.nx; i += 8)
-    {
-      double v[8];
-      #pragma unroll
-      for(int u = 0; u < 8; u++) { v[u] = buf[i + u]; }
-      #pragma unroll
-      for(int u = 0; u < 8; u++) { k.add(v[u]); }
-    }
-    for(; i < a.nx; i++) { k.add(buf[i]); }
-    a.row_sum[row] = k.result();  // row = c * ny + j
-  }
-}
-
-cudaError_t launch_ssim_rows(const SsimRowArgs& a, cudaStream_t s)
-{
-  const size_t per_warp = (size_t)a.nx_pad * sizeof(double);
-  int warps = (int)min((size_t)8, (size_t)(200 * 1024) / per_warp);
-  warps = max(warps, 1);
-  static bool configured = false;
-  if(!configured)
-  {
-    const cudaError_t e = cudaFuncSetAttribute(k_ssim_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 8192);
-    if(e != cudaSuccess) { return e; }
-    configured = true;
-  }
-  const int n = 3 * a.ny;
-  k_ssim_rows<<<(n + warps - 1) / warps, 32 * warps, per_warp * warps, s>>>(a);
-  return cudaGetLastError();
-}
 
 // =============================================================================================
 // finalize: the order-dependent FP64 pooling chains of one pair, one thread per chain.

@@ -53,28 +53,40 @@ struct CpsArgs
   uint32_t*      rows;         // [2][H][3], zeroed, 32-bit wrap-around sums
   void*          scp0;         // In0 resampled (T2R search result), planar 3 x W*H, may be null
   void*          scp1;         // In1 resampled (R2T search result)
+  // SSIM moments of (test picture, its SCP) per direction, for IV-SSIM without storing the SCP:
+  // mom[0] = (In0, SCP1) (T2R), mom[1] = (In1, SCP0) (R2T); null to skip
+  Moments        mom[2];
 };
 
 // ---------------------------------------------------------------------------------------------
-// block SSIM: per-window values (+ fused 2x2 downsampling of the inputs)
+// block SSIM
 // ---------------------------------------------------------------------------------------------
-struct SsimWinArgs
+// moments of an image pair (+ fused 2x2 downsampling of both inputs for the next MS-SSIM scale)
+struct SsimMomArgs
 {
-  Img     a, b;                // a = "Tst" picture, b = "Ref" picture of xSSIM::xCalcPicSSIM
-  int32_t W, H;
-  int32_t nx, ny, nx_pad;      // windows per row / column, row stride of win
+  Img      a, b;               // a = "Tst" picture, b = "Ref" picture of xSSIM::xCalcPicSSIM
+  int32_t  W, H;
   uint32_t clip;
-  double  C1, C2;
-  int32_t calc_l;
-  double* win;                 // [3][ny][nx_pad]
-  MutImg  down_a, down_b;      // outputs ((W>>1) x (H>>1), 4:4:4) or null planes
+  Moments  mom;
+  MutImg   down_a, down_b;     // outputs ((W>>1) x (H>>1), 4:4:4) or null planes
 };
 
-struct SsimRowArgs
+// windows from moments, ordered row sums (xSSIM.cpp:353-369), for up to 6 (pair, component) jobs
+struct SsimPoolJob
 {
-  const double* win;           // [3][ny][nx_pad]
-  int32_t       nx, ny, nx_pad;
-  double*       row_sum;       // [3][ny]
+  const uint32_t* mom;         // the five moment planes of one component
+  size_t          plane;       // elements between moment planes
+  int32_t         pitch;
+  int32_t         nx, ny;      // windows per row / column
+  int32_t         calc_l;
+  double*         row_sum;     // [ny]
+};
+
+struct SsimPoolArgs
+{
+  double      C1, C2;
+  int32_t     njobs;
+  SsimPoolJob job[9];
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -114,8 +126,8 @@ struct FinalizeArgs
 template <typename T> cudaError_t launch_prepass(const PrepassArgs& a, cudaStream_t s);
 cudaError_t launch_reduce(const ReduceArgs& a, cudaStream_t s);
 template <typename T> cudaError_t launch_cps(const CpsArgs& a, int R, cudaStream_t s);
-template <typename T> cudaError_t launch_ssim_win(const SsimWinArgs& a, cudaStream_t s);
-cudaError_t launch_ssim_rows(const SsimRowArgs& a, cudaStream_t s);
+template <typename T> cudaError_t launch_ssim_moments(const SsimMomArgs& a, cudaStream_t s);
+cudaError_t launch_ssim_pool(const SsimPoolArgs& a, cudaStream_t s);
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
 
 // Exactness check of the fp32 key path for a given bit depth, weights and GCD clip range.
