@@ -175,8 +175,6 @@ def run_qmiv(args, world, rank, local):
     torch.cuda.synchronize()
 
     # ---- device-resident inputs (value) ----
-    ctx.stage_times(reset=True)
-    ctx.set_profiling(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         barrier(world)
@@ -188,10 +186,24 @@ def run_qmiv(args, world, rank, local):
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
-    ctx.set_profiling(False)
     ms = ev0.elapsed_time(ev1)
-    stage = ctx.stage_times(reset=True)
     ms_max = max_over_ranks(ms, world, local)
+
+    # ---- isolated per-kernel times: the same steps with the pairs run one after another on one
+    # stream, every stage bracketed by CUDA events on that stream (the library's stage timers) ----
+    sbatch = qmiv_b200.Batch(ctx, max_pairs=PAIRS_PER_STEP, max_pixels=PAIRS_PER_STEP * W * H, erp=True, serial=True)
+    sbatch.compute(dev_desc)
+    torch.cuda.synchronize()
+    ctx.stage_times(reset=True)
+    ctx.set_profiling(True)
+    prof_steps = max(3, args.steps // 4)
+    for _ in range(prof_steps):
+        assert sbatch.compute(dev_desc) == results, "serial and concurrent batches differ"
+    torch.cuda.synchronize()
+    ctx.set_profiling(False)
+    stage = ctx.stage_times(reset=True)
+    sbatch.close()
+    launches_per_step = sum(v[1] for k, v in stage.items() if k not in ("h2d", "d2h")) / prof_steps
 
     # ---- end to end through the public API, pinned host frames (e2e) ----
     for _ in range(max(1, args.warmup // 2)):
@@ -227,7 +239,7 @@ def run_qmiv(args, world, rank, local):
     d2h = PAIRS_PER_STEP * 632  # sizeof(PairOut), the device result block read back per pair
     return dict(value=value, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
                 achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
-                sample=results[0])
+                sample=results[0], launches=int(round(launches_per_step * args.steps)))
 
 
 # ---------------------------------------------------------------------------------------------
@@ -364,13 +376,12 @@ def main():
                         "accounting": "8 int32 ops per candidate, 2*W*H*25 candidates per launch; peak measured "
                                       "by qmiv_probe_int32_peak on this GPU",
                         "avg_launch_ms": r["cps_avg_ms"]},
-           "stage_ms_per_pair": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
+           "stage_ms_per_launch_isolated": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
            "clocks": r["clocks"],
            "cpu_baseline": cpu,
            "sample_result": {k: r["sample"][k] for k in ("gcd_r2t", "ivpsnr", "wspsnr_pic", "ivssim")},
            "hbm_peak_gbs": peaks.get("hbm_gbs")}
-    launches = sum(v[1] for k, v in r["stage"].items() if k not in ("h2d", "d2h"))
-    out["gpu_launches"] = launches
+    out["gpu_launches"] = r["launches"]
     print(json.dumps(out))
     barrier(world)
 

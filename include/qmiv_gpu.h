@@ -233,10 +233,14 @@ typedef struct qmiv_pair_desc
 } qmiv_pair_desc;
 
 /* max_pairs: pairs per qmiv_batch_compute call; max_pixels: sum of W*H over one call's pairs.
-   params: shared weights/coefficients (search_range is taken per pair). use_graph: capture the
-   launch sequence in CUDA graphs keyed by the batch's shape signature. */
+   params: shared weights/coefficients (search_range is taken per pair). flags: QMIV_BATCH_*. */
+enum
+{
+  QMIV_BATCH_GRAPH  = 1,  /* replay the launch sequence from CUDA graphs keyed by the call's shape signature */
+  QMIV_BATCH_SERIAL = 2   /* run the pairs one after another on one stream (isolated per-kernel timing) */
+};
 QMIV_API qmiv_status qmiv_batch_create(qmiv_ctx ctx, int32_t max_pairs, int64_t max_pixels, const qmiv_params* params,
-                              int32_t use_graph, qmiv_batch* out_batch);
+                              int32_t flags, qmiv_batch* out_batch);
 QMIV_API qmiv_status qmiv_batch_destroy(qmiv_batch batch);
 QMIV_API qmiv_status qmiv_batch_compute(qmiv_batch batch, const qmiv_pair_desc* pairs, int32_t num_pairs, qmiv_result* out);
 /* Device stream (cudaStream_t) the batch enqueues on. */

@@ -245,13 +245,17 @@ class Calc:
 class Batch:
     """Many frame pairs of uneven shape per call (qmiv_batch_*)."""
 
-    def __init__(self, ctx: Context, max_pairs: int, max_pixels: int, use_graph: bool = True, **params):
+    GRAPH, SERIAL = 1, 2
+
+    def __init__(self, ctx: Context, max_pairs: int, max_pixels: int, graph: bool = False, serial: bool = False,
+                 **params):
         self._lib = library()
         self.ctx = ctx
         self.params = make_params(**params)
+        flags = (self.GRAPH if graph else 0) | (self.SERIAL if serial else 0)
         h = ctypes.c_void_p()
         check(self._lib.qmiv_batch_create(ctx.handle, max_pairs, max_pixels, ctypes.byref(self.params),
-                                          int(bool(use_graph)), ctypes.byref(h)), "qmiv_batch_create")
+                                          flags, ctypes.byref(h)), "qmiv_batch_create")
         self.handle = h
 
     def close(self):

@@ -13,7 +13,7 @@ struct qmiv_batch_s
   qmiv_params  prm{};
   int32_t      max_pairs = 0;
   int64_t      max_pixels = 0;
-  int32_t      use_graph = 0;
+  int32_t      flags = 0;
   cudaStream_t stream = nullptr;           // the batch's stream: a call starts and ends on it
   std::vector<cudaStream_t> lanes;         // worker streams the pairs are spread over
   std::vector<cudaEvent_t>  lane_done;
@@ -28,7 +28,7 @@ static constexpr int kBatchLanes = 4;
 extern "C" {
 
 qmiv_status qmiv_batch_create(qmiv_ctx ctx, int32_t max_pairs, int64_t max_pixels, const qmiv_params* params,
-                              int32_t use_graph, qmiv_batch* out_batch)
+                              int32_t flags, qmiv_batch* out_batch)
 {
   if(!ctx || !out_batch || max_pairs <= 0 || max_pixels <= 0) { return fail(QMIV_ERR_INVALID_ARG, "bad batch arguments"); }
   *out_batch = nullptr;
@@ -37,10 +37,11 @@ qmiv_status qmiv_batch_create(qmiv_ctx ctx, int32_t max_pairs, int64_t max_pixel
   QMIV_TRY(validate_params(prm));
   QMIV_CUDA(cudaSetDevice(ctx->device));
   qmiv_batch b = new qmiv_batch_s();
-  b->ctx = ctx; b->prm = prm; b->max_pairs = max_pairs; b->max_pixels = max_pixels; b->use_graph = use_graph;
+  b->ctx = ctx; b->prm = prm; b->max_pairs = max_pairs; b->max_pixels = max_pixels; b->flags = flags;
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if(e == cudaSuccess) { e = cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming); }
-  for(int k = 0; k < kBatchLanes && e == cudaSuccess; k++)
+  const int lanes = (flags & QMIV_BATCH_SERIAL) ? 1 : kBatchLanes;
+  for(int k = 0; k < lanes && e == cudaSuccess; k++)
   {
     cudaStream_t s; cudaEvent_t d;
     e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);

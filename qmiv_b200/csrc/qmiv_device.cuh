@@ -35,6 +35,11 @@ __device__ __forceinline__ int32_t fetch(const Img& im, int c, int32_t x, int32_
 
 __device__ __forceinline__ int32_t clampi(int32_t v, int32_t lo, int32_t hi) { return min(max(v, lo), hi); }
 
+// Exact conversions between integers in [0, 2^23) and floats without the (quarter-rate) conversion
+// pipe: a float in [2^23, 2^24) has a unit ulp, so its low mantissa bits are the integer.
+__device__ __forceinline__ float u2f_exact(uint32_t v) { return __uint_as_float(v | 0x4B000000u) - 8388608.0f; }
+__device__ __forceinline__ int32_t f2i_exact(float f) { return (int32_t)(__float_as_uint(f + 8388608.0f) - 0x4B000000u); }
+
 // Exact IEEE double operations, never contracted into FMA, so device results equal the host
 // reference's separately rounded operations bit for bit.
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }

@@ -188,19 +188,26 @@ __global__ void __launch_bounds__(128) k_cps(const __grid_constant__ CpsArgs a)
   const int g0 = a.gcd_src->gcd[0], g1 = a.gcd_src->gcd[1], g2 = a.gcd_src->gcd[2];
   const bool int_path = (a.gcd_src->flags & 4) != 0;
 
-  for(int i = threadIdx.x; i < SH * SW; i += TX * TY)
   {
-    const int ly = i / SW, lx = i - ly * SW;
-    const int gx = clampi(x0 + lx - R, 0, W - 1), gy = clampi(y0 + ly - R, 0, H - 1);
-    #pragma unroll
-    for(int f = 0; f < 2; f++)
+    const T* p0[2] = { static_cast<const T*>(a.in0.p[0]), static_cast<const T*>(a.in1.p[0]) };
+    const T* p1[2] = { static_cast<const T*>(a.in0.p[1]), static_cast<const T*>(a.in1.p[1]) };
+    const T* p2[2] = { static_cast<const T*>(a.in0.p[2]), static_cast<const T*>(a.in1.p[2]) };
+    const int sx = a.in0.sx[1], sy = a.in0.sy[1];
+    for(int i = threadIdx.x; i < SH * SW; i += TX * TY)
     {
-      const Img& im = f ? a.in1 : a.in0;
-      const float v0 = (float)min((uint32_t)fetch<T>(im, 0, gx, gy), a.clip);
-      const float v1 = (float)min((uint32_t)fetch<T>(im, 1, gx, gy), a.clip);
-      const float v2 = (float)min((uint32_t)fetch<T>(im, 2, gx, gy), a.clip);
-      const float q  = fmaf(a.wf[2], v2 * v2, fmaf(a.wf[1], v1 * v1, fmaf(a.wf[0], v0 * v0, kBias)));
-      (f ? tile1 : tile0)[i] = make_float4(v0, v1, v2, q);
+      const int ly = i / SW, lx = i - ly * SW;
+      const int gx = clampi(x0 + lx - R, 0, W - 1), gy = clampi(y0 + ly - R, 0, H - 1);
+      const int cx = gx >> sx, cy = gy >> sy;
+      #pragma unroll
+      for(int f = 0; f < 2; f++)
+      {
+        const Img& im = f ? a.in1 : a.in0;
+        const float v0 = u2f_exact(min((uint32_t)__ldg(p0[f] + gy * im.pitch[0] + gx), a.clip));
+        const float v1 = u2f_exact(min((uint32_t)__ldg(p1[f] + cy * im.pitch[1] + cx), a.clip));
+        const float v2 = u2f_exact(min((uint32_t)__ldg(p2[f] + cy * im.pitch[2] + cx), a.clip));
+        const float q  = fmaf(a.wf[2], v2 * v2, fmaf(a.wf[1], v1 * v1, fmaf(a.wf[0], v0 * v0, kBias)));
+        (f ? tile1 : tile0)[i] = make_float4(v0, v1, v2, q);
+      }
     }
   }
   __syncthreads();
@@ -298,8 +305,8 @@ __global__ void __launch_bounds__(128) k_cps(const __grid_constant__ CpsArgs a)
       const int dyi = (int)(idx[i] / D), dxi = (int)(idx[i] - dyi * D);
       const float4 r = ref[(ty * P + i + dyi) * SW + tx + dxi];
       const float4 t = tst[(ty * P + i + R) * SW + tx + R];
-      const int r0 = (int)r.x, r1 = (int)r.y, r2 = (int)r.z;
-      const int t0 = (int)t.x, t1 = (int)t.y, t2 = (int)t.z;
+      const int r0 = f2i_exact(r.x), r1 = f2i_exact(r.y), r2 = f2i_exact(r.z);
+      const int t0 = f2i_exact(t.x), t1 = f2i_exact(t.y), t2 = f2i_exact(t.z);
       const uint32_t e0 = (uint32_t)(t0 + ga - r0), e1 = (uint32_t)(t1 + gb - r1), e2 = (uint32_t)(t2 + gc - r2);
       const uint32_t s0 = __reduce_add_sync(kFull, valid ? e0 * e0 : 0u);
       const uint32_t s1 = __reduce_add_sync(kFull, valid ? e1 * e1 : 0u);
