@@ -116,7 +116,8 @@ qmiv_status qmiv_batch_compute(qmiv_batch b, const qmiv_pair_desc* pairs, int32_
     b->pipes[i]->harvest_profile();
     const PairOut& o = b->pipes[i]->host_out();
     finish_result(o, b->pipes[i]->finish_info(pairs[i].metric_mask), &out[i]);
-    if(b->prm.invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3)) { st = fail(QMIV_ERR_INVALID_PIXEL, "invalid pixel in a batched pair"); }
+    const qmiv_status ps = pair_status(o, b->prm.invalid_pel_action);
+    if(ps != QMIV_OK && st == QMIV_OK) { st = ps; }
   }
   return st;
 }

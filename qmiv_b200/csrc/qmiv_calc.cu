@@ -142,7 +142,7 @@ qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames
     for(int s = 1; s < ns_; s++) { lv += (size_t)(S.W >> s) * (S.H >> s) * 3; }
     QMIV_TRY(pyr_.ensure(ctx_, 4 * lv * S.esz));
   }
-  if(host_frames) { QMIV_TRY(staging_.ensure(ctx_, 2 * S.frame_bytes())); }
+  if(host_frames) { QMIV_TRY(staging_.ensure(ctx_, 2 * S.staged_frame_bytes())); }
   return QMIV_OK;
 }
 
@@ -150,7 +150,7 @@ qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cuda
 {
   const Shape& S = shape_;
   if(!f) { return fail(QMIV_ERR_INVALID_ARG, "frame is null"); }
-  size_t off = (size_t)which * S.frame_bytes();
+  size_t off = (size_t)which * S.staged_frame_bytes();
   const int tok = f->mem == QMIV_MEM_HOST ? prof_begin(s) : -1;
   for(int c = 0; c < 3; c++)
   {
@@ -168,10 +168,11 @@ qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cuda
     {
       if(!staging_.p) { return fail(QMIV_ERR_INVALID_ARG, "staging not prepared"); }
       char* dst = staging_.as<char>() + off;
-      QMIV_CUDA(cudaMemcpy2DAsync(dst, row_bytes, f->plane[c], (size_t)f->pitch[c], row_bytes, S.plane_rows(c), cudaMemcpyHostToDevice, s));
+      QMIV_CUDA(cudaMemcpy2DAsync(dst, S.staged_pitch(c), f->plane[c], (size_t)f->pitch[c], row_bytes, S.plane_rows(c),
+                                  cudaMemcpyHostToDevice, s));
       out.p[c] = dst;
-      out.pitch[c] = (int32_t)S.plane_cols(c);
-      off += row_bytes * S.plane_rows(c);
+      out.pitch[c] = (int32_t)(S.staged_pitch(c) / S.esz);
+      off += S.staged_plane_bytes(c);
     }
     else { return fail(QMIV_ERR_INVALID_ARG, "frame mem must be QMIV_MEM_HOST or QMIV_MEM_DEVICE"); }
   }
@@ -428,11 +429,7 @@ static qmiv_status calc_collect(qmiv_calc calc, int32_t timeout_ms, qmiv_result*
   calc->pipe.harvest_profile();
   const PairOut& o = calc->pipe.host_out();
   if(out) { finish_result(o, calc->pipe.finish_info(calc->pending_mask), out); }
-  if(calc->prm.invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3))
-  {
-    return fail(QMIV_ERR_INVALID_PIXEL, "input frame contains samples above the bit depth's maximum");
-  }
-  return QMIV_OK;
+  return pair_status(o, calc->prm.invalid_pel_action);
 }
 
 extern "C" {

@@ -117,6 +117,16 @@ static double per_pic4(const double v[4], const int32_t w[4])
   return (v[0] * (double)w[0] + v[1] * (double)w[1] + v[2] * (double)w[2] + v[3] * (double)w[3]) * inv;
 }
 
+qmiv_status pair_status(const PairOut& o, int32_t invalid_pel_action)
+{
+  if(o.flags & 8) { return fail(QMIV_ERR_TIMEOUT, "a CPS tile load did not complete within its wait bound"); }
+  if(invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3))
+  {
+    return fail(QMIV_ERR_INVALID_PIXEL, "input frame contains samples above the bit depth's maximum");
+  }
+  return QMIV_OK;
+}
+
 void finish_result(const PairOut& o, const FinishInfo& fi, qmiv_result* r)
 {
   std::memset(r, 0, sizeof(*r));

@@ -1,0 +1,797 @@
+// Corresponding-pixel-shift search (libs/pmbb-ivqm/src/xCorrespPixelShiftSSE.cpp:18-127) for
+// sm_100a: persistent CTAs, TMA tile loads, 4 x 2 pixels per thread.
+//
+// Per tile of 128 x TH output pixels (TH = 32, or 16 when shared memory is short) a CTA of
+// 2 x TH / 4 warps
+//   1. receives both pictures' raw samples of the tile plus an R-pixel halo (luma box and the
+//      two chroma boxes of each picture) through TMA into shared memory; the copies of tile n+1
+//      are issued as soon as tile n's raw samples are converted, so they land during its search;
+//   2. converts them into two float4 tiles (Y, Cb, Cr, q + 2^23), q = sum_c w_c * ref_c^2,
+//      reading every sample at its clamped picture coordinate (the reference's edge-replicated
+//      margin, apps/QMIV/src/xAppQMIV.cpp:353 and :899) and the chroma of 4:2:0 / 4:2:2 at
+//      (x >> sx, y >> sy) (the nearest upsampling of libs/pmbb-core/src/xPixelOpsSTD.cpp:30-87);
+//   3. searches both directions. A thread owns 4 rows x 2 columns of output pixels, so each
+//      staged reference pixel is loaded once per thread for up to 8 of its pixels; two lanes
+//      together hold one 4x4 SSIM sub-block.
+//
+// Exact fp32 keys: for a test pixel s (test + GCD, unclipped) and candidate r,
+//     e - sum_c w_c s_c^2 + 2^23 = (q(r) + 2^23) + sum_c (-2 w_c s_c) r_c
+// is three FFMAs. When every partial sum is an integer below 2^24 in magnitude (checked on the
+// host from bit depth, weights and the GCD range) they are exact, so the order of candidates and
+// all ties are those of the reference's int32 error. The value lies in [2^20, 2^24), where the IEEE
+// bit pattern grows with the value, so
+//     key = ((bits - bits(2^20)) << 7) + k,   k = (dy+R)(2R+1) + (dx+R)  (raster index, < 128)
+// orders candidates as "first strict minimum in raster order" does (xCorrespPixelShiftSSE.cpp:
+// 60-79), and the search is one unsigned min per candidate.
+// When the fp32 path is not exact the same kernel runs an int32 search mirroring the SSE path's
+// wrap-around arithmetic literally.
+//
+// Shared-memory float tiles are de-interleaved by column parity: element (y, x) sits at
+// y * RP + (x & 1) * Q + (x >> 1). A warp reading column 2 * lane + rx for fixed rx touches 32
+// consecutive float4 (no bank conflict), and with Q = 4 (mod 8) the conversion's stores of 32
+// consecutive columns are conflict-free as well.
+#include "qmiv_kernels.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <mutex>
+
+namespace qmiv {
+
+namespace {
+
+constexpr float    kBias     = 8388608.0f;   // 2^23
+constexpr uint32_t kKeyBase  = 0x49800000u;  // bit pattern of 2^20f
+constexpr uint32_t kBiasBits = 0x4B000000u;  // bit pattern of 2^23f
+constexpr unsigned kFull     = 0xffffffffu;
+constexpr long long kWaitCycles = 1LL << 31; // bound of one tile-load wait (about a second)
+
+template <int R, int WY>
+struct Geo
+{
+  static constexpr int D  = 2 * R + 1;
+  static constexpr int NT = 64 * WY;                  // two warps across, WY warps down
+  static constexpr int TW = 128, TH = 4 * WY;
+  static constexpr int SW = TW + 2 * R, SH = TH + 2 * R;
+  static constexpr int Q0 = (SW + 1) / 2;
+  static constexpr int Q  = Q0 + (12 - Q0 % 8) % 8;   // smallest >= Q0 with Q % 8 == 4
+  static constexpr int RP = 2 * Q;                    // row pitch in float4
+  static constexpr uint32_t kTileBytes = (uint32_t)SH * RP * 16u;
+};
+
+struct CpsGeomArgs
+{
+  int32_t  ntx, ntiles;
+  int32_t  use_tma;
+  int32_t  ax;                 // 16 bytes in samples: TMA boxes start this far left of the tile
+  int32_t  bwl, bhl, bwc, bhc; // raw box sizes in samples (luma, chroma)
+  int32_t  sx, sy;             // chroma subsampling shifts
+  uint32_t off[2][3];          // byte offsets of the raw boxes in shared memory
+  uint32_t raw_bytes;          // raw region, multiple of 128
+  uint32_t tx_bytes;           // bytes the six copies of one tile deliver
+  int32_t* status;             // PairOut::flags: bit 3 = a tile load did not complete
+};
+
+struct alignas(64) CpsKernelArgs
+{
+  CUtensorMap map[2][3];       // [picture][plane]
+  CpsArgs     a;
+  CpsGeomArgs g;
+};
+
+// ---- TMA / mbarrier ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+    "{\n\t.reg .pred p;\n\t"
+    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+    "selp.u32 %0, 1, 0, p;\n\t}"
+    : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Waits for the phase with the given parity; gives up (false) after about `limit` cycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit)
+{
+  if(mbar_try_wait(bar, parity)) { return true; }
+  const long long t0 = clock64();
+  do
+  {
+    if(mbar_try_wait(bar, parity)) { return true; }
+  } while(clock64() - t0 <= limit);
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
+{
+  asm volatile(
+    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+    ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)) : "memory");
+}
+
+// ---- tile loads ---------------------------------------------------------------------------------
+template <int R, int WY>
+__device__ __forceinline__ void issue_tile(const CpsKernelArgs& k, unsigned char* raw, uint64_t* bar, int t)
+{
+  using G = Geo<R, WY>;
+  const int x0 = (t % k.g.ntx) * G::TW, y0 = (t / k.g.ntx) * G::TH;
+  const int xl = x0 - k.g.ax, yl = y0 - R;
+  const int xc = (x0 >> k.g.sx) - k.g.ax, yc = (y0 - R) >> k.g.sy;
+  mbar_expect_tx(bar, k.g.tx_bytes);
+  #pragma unroll
+  for(int f = 0; f < 2; f++)
+  {
+    tma_load_2d(raw + k.g.off[f][0], &k.map[f][0], xl, yl, bar);
+    tma_load_2d(raw + k.g.off[f][1], &k.map[f][1], xc, yc, bar);
+    tma_load_2d(raw + k.g.off[f][2], &k.map[f][2], xc, yc, bar);
+  }
+}
+
+// Same boxes with plain loads, for frames whose address or pitch TMA cannot take. Samples outside
+// the picture are left unwritten: the conversion only reads clamped in-picture coordinates.
+template <typename T, int R, int WY>
+__device__ void load_plain(const CpsKernelArgs& k, unsigned char* raw, int x0, int y0)
+{
+  constexpr int NW = Geo<R, WY>::NT / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  #pragma unroll 1
+  for(int f = 0; f < 2; f++)
+  {
+    const Img& im = f ? k.a.in1 : k.a.in0;
+    #pragma unroll 1
+    for(int c = 0; c < 3; c++)
+    {
+      const int pw = c ? (k.a.W >> k.g.sx) : k.a.W, ph = c ? (k.a.H >> k.g.sy) : k.a.H;
+      const int bw = c ? k.g.bwc : k.g.bwl, bh = c ? k.g.bhc : k.g.bhl;
+      const int xs = c ? (x0 >> k.g.sx) - k.g.ax : x0 - k.g.ax, ys = c ? (y0 - R) >> k.g.sy : y0 - R;
+      T* dst = reinterpret_cast<T*>(raw + k.g.off[f][c]);
+      const T* src = static_cast<const T*>(im.p[c]);
+      for(int r = warp; r < bh; r += NW)
+      {
+        const int gy = ys + r;
+        if(gy < 0 || gy >= ph) { continue; }
+        for(int col = lane; col < bw; col += 32)
+        {
+          const int gx = xs + col;
+          if(gx >= 0 && gx < pw) { dst[r * bw + col] = __ldg(src + (size_t)gy * im.pitch[c] + gx); }
+        }
+      }
+    }
+  }
+}
+
+// raw boxes -> float4 tiles F0 (In0) and F1 (In1). The 2 * SH tile rows of both pictures are dealt
+// to the warps round-robin; lane L converts columns L + 32 * kk of a row. Column offsets into the
+// raw boxes (clamped to the picture) are per lane and computed once.
+template <typename T, int R, int WY, bool CLIP>
+__device__ void convert(const CpsKernelArgs& k, const unsigned char* raw, float4* F0, float4* F1, int x0, int y0)
+{
+  using G = Geo<R, WY>;
+  constexpr int NW = G::NT / 32, NK = (G::SW + 31) / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int W = k.a.W, H = k.a.H, sx = k.g.sx, sy = k.g.sy;
+  const int xl = x0 - k.g.ax, yl = y0 - R, xc = (x0 >> sx) - k.g.ax, yc = (y0 - R) >> sy;
+  const float w0 = k.a.wf[0], w1 = k.a.wf[1], w2 = k.a.wf[2];
+  const uint32_t clip = k.a.clip;
+  int colL[NK], colC[NK];
+  #pragma unroll
+  for(int kk = 0; kk < NK; kk++)
+  {
+    const int gx = clampi(x0 - R + lane + 32 * kk, 0, W - 1);
+    colL[kk] = gx - xl;
+    colC[kk] = (gx >> sx) - xc;
+  }
+  #pragma unroll 1
+  for(int row = warp; row < 2 * G::SH; row += NW)
+  {
+    const int f  = row >= G::SH ? 1 : 0;
+    const int ly = row - f * G::SH;
+    const int gy = clampi(y0 - R + ly, 0, H - 1);
+    const T* rl = reinterpret_cast<const T*>(raw + k.g.off[f][0]) + (gy - yl) * k.g.bwl;
+    const T* ru = reinterpret_cast<const T*>(raw + k.g.off[f][1]) + ((gy >> sy) - yc) * k.g.bwc;
+    const T* rv = reinterpret_cast<const T*>(raw + k.g.off[f][2]) + ((gy >> sy) - yc) * k.g.bwc;
+    float4* frow = (f ? F1 : F0) + ly * G::RP + (lane & 1) * G::Q + (lane >> 1);
+    #pragma unroll
+    for(int kk = 0; kk < NK; kk++)
+    {
+      if(kk < NK - 1 || lane + 32 * kk < G::SW)
+      {
+        uint32_t v0 = rl[colL[kk]], v1 = ru[colC[kk]], v2 = rv[colC[kk]];
+        if(CLIP) { v0 = min(v0, clip); v1 = min(v1, clip); v2 = min(v2, clip); }
+        const float y = __uint2float_rn(v0), u = __uint2float_rn(v1), v = __uint2float_rn(v2);
+        frow[16 * kk] = make_float4(y, u, v, fmaf(w2, v * v, fmaf(w1, u * u, fmaf(w0, y * y, kBias))));
+      }
+    }
+  }
+}
+
+// ---- search ---------------------------------------------------------------------------------
+// Thread (warp w, lane L) owns rows 4 * (w >> 1) + i (i < 4) of columns 64 * (w & 1) + 2L + j
+// (j < 2); p = 2 * i + j indexes its eight pixels.
+struct Thr
+{
+  int y0;     // first tile row of the thread's pixels
+  int hx;     // (first column) >> 1 = 32 * (w & 1) + L
+  int lane;
+  __device__ __forceinline__ Thr()
+  {
+    const int w = threadIdx.x >> 5;
+    lane = threadIdx.x & 31;
+    y0 = 4 * (w >> 1);
+    hx = 32 * (w & 1) + lane;
+  }
+};
+
+// Code of candidate (dy + R, dx + R) in the low 7 bits of a key: increasing in raster order and,
+// for 2R + 1 <= 8, two bit fields.
+template <int R>
+struct Code
+{
+  static constexpr int D  = 2 * R + 1;
+  static constexpr int KS = D <= 8 ? 8 : D;
+  static constexpr uint32_t kMax = (uint32_t)((D - 1) * KS + (D - 1));
+  static_assert(kMax < 128, "candidate code must fit 7 bits");
+  __device__ static __forceinline__ int dy(uint32_t k) { return KS == 8 ? (int)(k >> 3) : (int)(k / D); }
+  __device__ static __forceinline__ int dx(uint32_t k) { return KS == 8 ? (int)(k & 7) : (int)(k - (k / D) * D); }
+  __host__ __device__ static constexpr uint32_t of(int dyi, int dxi) { return (uint32_t)(dyi * KS + dxi); }
+};
+
+// float4 of tile pixel (row y, column 2 * hx + dx) for a compile-time dx >= 0
+template <int R, int WY>
+__device__ __forceinline__ int at_hx(int y, int hx, int dx)
+{
+  using G = Geo<R, WY>;
+  return y * G::RP + (dx & 1) * G::Q + hx + (dx >> 1);
+}
+
+template <int R, int WY>
+__device__ __forceinline__ void search_fp32(const Thr& th, const float4* tst, const float4* ref, const float wf[3],
+                                            float ga, float gb, float gc, uint32_t idx[8])
+{
+  using G = Geo<R, WY>;
+  using C = Code<R>;
+  constexpr int D = G::D;
+  float c0[8], c1[8], c2[8];
+  uint32_t best[8];
+  #pragma unroll
+  for(int p = 0; p < 8; p++)
+  {
+    const float4 t = tst[at_hx<R, WY>(th.y0 + (p >> 1) + R, th.hx, (p & 1) + R)];
+    c0[p] = -2.0f * wf[0] * (t.x + ga);
+    c1[p] = -2.0f * wf[1] * (t.y + gb);
+    c2[p] = -2.0f * wf[2] * (t.z + gc);
+    best[p] = 0xffffffffu;
+  }
+  const float4* rb = ref + at_hx<R, WY>(th.y0, th.hx, 0);
+  #pragma unroll
+  for(int ry = 0; ry < 4 + 2 * R; ry++)
+  {
+    #pragma unroll
+    for(int rx = 0; rx < 2 + 2 * R; rx++)
+    {
+      const float4 r = rb[ry * G::RP + (rx & 1) * G::Q + (rx >> 1)];
+      #pragma unroll
+      for(int i = 0; i < 4; i++)
+      {
+        const int dyi = ry - i;
+        if(dyi < 0 || dyi >= D) { continue; }
+        #pragma unroll
+        for(int j = 0; j < 2; j++)
+        {
+          const int dxi = rx - j;
+          if(dxi < 0 || dxi >= D) { continue; }
+          const int p = 2 * i + j;
+          const float e = fmaf(c2[p], r.z, fmaf(c1[p], r.y, fmaf(c0[p], r.x, r.w)));
+          const uint32_t key = (__float_as_uint(e) << 7) + C::of(dyi, dxi) - (kKeyBase << 7);
+          best[p] = min(best[p], key);
+        }
+      }
+    }
+  }
+  #pragma unroll
+  for(int p = 0; p < 8; p++) { idx[p] = min(best[p] & 127u, C::kMax); }
+}
+
+template <int R, int WY>
+__device__ __forceinline__ void search_int(const Thr& th, const float4* tst, const float4* ref, const int32_t wi[3],
+                                           int ga, int gb, int gc, uint32_t idx[8])
+{
+  using G = Geo<R, WY>;
+  constexpr int D = G::D;
+  const uint32_t w0 = (uint32_t)wi[0], w1 = (uint32_t)wi[1], w2 = (uint32_t)wi[2];
+  #pragma unroll
+  for(int p = 0; p < 8; p++)
+  {
+    const int i = p >> 1, j = p & 1;
+    const float4 t = tst[at_hx<R, WY>(th.y0 + i + R, th.hx, j + R)];
+    const int s0 = f2i_exact(t.x) + ga, s1 = f2i_exact(t.y) + gb, s2 = f2i_exact(t.z) + gc;
+    int32_t  best_err = 0x7fffffff;
+    uint32_t bi = 0;
+    #pragma unroll 1
+    for(int dyi = 0; dyi < D; dyi++)
+    {
+      #pragma unroll 1
+      for(int dxi = 0; dxi < D; dxi++)
+      {
+        const int dx = j + dxi;
+        const float4   r  = ref[(th.y0 + i + dyi) * G::RP + (dx & 1) * G::Q + th.hx + (dx >> 1)];
+        const uint32_t d0 = (uint32_t)(s0 - f2i_exact(r.x)), d1 = (uint32_t)(s1 - f2i_exact(r.y)),
+                       d2 = (uint32_t)(s2 - f2i_exact(r.z));
+        const uint32_t err = d0 * d0 * w0 + d1 * d1 * w1 + d2 * d2 * w2;
+        if((int32_t)err < best_err) { best_err = (int32_t)err; bi = Code<R>::of(dyi, dxi); }
+      }
+    }
+    idx[p] = bi;
+  }
+}
+
+// ---- epilogue ---------------------------------------------------------------------------------
+// Winner of every pixel: per-component squared difference into the 32-bit row sums, SCP store,
+// and the SSIM moments of (test picture, SCP) of the 4x4 block the thread shares with its lane
+// neighbour.
+//
+// fp32 path: all values are integers below 2^24 (path condition), so float arithmetic is exact.
+// Tiles that reach past the picture (EDGE) weight every pixel by 1 (inside) or 0 (outside).
+template <int R, int WY, typename T, bool EDGE, bool MOM, bool SCP>
+__device__ __forceinline__ void epilogue_fp(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref,
+                                            const uint32_t idx[8], int dir, int x0, int y0, int ga, int gb, int gc)
+{
+  using G = Geo<R, WY>;
+  using C = Code<R>;
+  uint32_t* rows = a.rows + (size_t)dir * a.H * 3;
+  T* scp = static_cast<T*>(dir ? a.scp0 : a.scp1);
+  const size_t plane = (size_t)a.W * a.H;
+  const int xb = x0 + 2 * th.hx, yb = y0 + th.y0;
+  const float fg[3] = { (float)ga, (float)gb, (float)gc };
+  const float fmax = (float)a.maxv;
+  const float4* rrow = ref + th.y0 * G::RP + th.hx;
+  const float4* trow = tst + (th.y0 + R) * G::RP + th.hx;
+  float cm[2] = { 1.f, 1.f };
+  if(EDGE) { cm[0] = xb < a.W ? 1.f : 0.f; cm[1] = xb + 1 < a.W ? 1.f : 0.f; }
+  float mm[3][5];
+  #pragma unroll
+  for(int c = 0; c < 3; c++)
+  {
+    #pragma unroll
+    for(int m = 0; m < 5; m++) { mm[c][m] = 0.f; }
+  }
+  #pragma unroll
+  for(int i = 0; i < 4; i++)
+  {
+    const int y = yb + i;
+    const float rmask = (!EDGE || y < a.H) ? 1.f : 0.f;
+    float frs[3] = { 0.f, 0.f, 0.f };
+    #pragma unroll
+    for(int j = 0; j < 2; j++)
+    {
+      const uint32_t k = idx[2 * i + j];
+      const int dyi = C::dy(k), dx = j + C::dx(k);
+      const float4 r = rrow[(i + dyi) * G::RP + (dx & 1) * G::Q + (dx >> 1)];
+      const float4 t = trow[i * G::RP + ((j + R) & 1) * G::Q + ((j + R) >> 1)];
+      const float m = EDGE ? rmask * cm[j] : 1.f;
+      const float rv[3] = { r.x, r.y, r.z }, tv[3] = { t.x, t.y, t.z };
+      #pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const float d = (tv[c] + fg[c]) - rv[c];
+        const float b = fminf(fmaxf(rv[c] - fg[c], 0.f), fmax);
+        frs[c] = fmaf(EDGE ? d * m : d, d, frs[c]);
+        if(MOM)
+        {
+          const float tm = EDGE ? tv[c] * m : tv[c], bm = EDGE ? b * m : b;
+          mm[c][0] += tm;
+          mm[c][1] += bm;
+          mm[c][2] = fmaf(tm, tv[c], mm[c][2]);
+          mm[c][3] = fmaf(bm, b, mm[c][3]);
+          mm[c][4] = fmaf(tm, b, mm[c][4]);
+        }
+        if(SCP && (!EDGE || m != 0.f)) { scp[(size_t)c * plane + (size_t)y * a.W + xb + j] = (T)f2i_exact(b); }
+      }
+    }
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      // 2^23 + (a sum below 2^23) has the sum in its low bits; 32 lanes add 32 x 0x4B000000
+      const uint32_t s = __reduce_add_sync(kFull, __float_as_uint(frs[c] + kBias)) - 32u * kBiasBits;
+      if(th.lane == 0 && (!EDGE || y < a.H)) { atomicAdd(rows + (size_t)y * 3 + c, s); }
+    }
+  }
+  if(MOM)
+  {
+    // lanes 2m and 2m + 1 hold the two column halves of block bx
+    const Moments mom = a.mom[dir];
+    const int bx = xb >> 2, by = yb >> 2;
+    const bool store = (th.lane & 1) == 0 && bx < mom.nbx && by < mom.nby;
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      #pragma unroll
+      for(int m = 0; m < 5; m++)
+      {
+        const float f = mm[c][m] + __shfl_xor_sync(kFull, mm[c][m], 1);   // exact: integers below 2^24
+        if(store) { mom.p[((size_t)c * 5 + m) * mom.plane() + (size_t)by * mom.pitch + bx] = __float2uint_rn(f); }
+      }
+    }
+  }
+}
+
+// int32 path: the SSE path's wrap-around arithmetic
+template <int R, int WY, typename T>
+__device__ __noinline__ void epilogue_int(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref,
+                                          const uint32_t idx[8], int dir, int x0, int y0, int ga, int gb, int gc)
+{
+  using G = Geo<R, WY>;
+  using C = Code<R>;
+  uint32_t* rows = a.rows + (size_t)dir * a.H * 3;
+  T* scp = static_cast<T*>(dir ? a.scp0 : a.scp1);
+  const Moments mom = a.mom[dir];
+  const size_t plane = (size_t)a.W * a.H;
+  const int xb = x0 + 2 * th.hx, yb = y0 + th.y0;
+  const int ig[3] = { ga, gb, gc };
+  uint32_t mm[3][5];
+  #pragma unroll
+  for(int c = 0; c < 3; c++)
+  {
+    #pragma unroll
+    for(int m = 0; m < 5; m++) { mm[c][m] = 0u; }
+  }
+  #pragma unroll
+  for(int i = 0; i < 4; i++)
+  {
+    const int  y  = yb + i;
+    const bool yv = y < a.H;
+    uint32_t irs[3] = { 0u, 0u, 0u };
+    #pragma unroll
+    for(int j = 0; j < 2; j++)
+    {
+      const int  x     = xb + j;
+      const bool valid = yv && x < a.W;
+      const uint32_t k = idx[2 * i + j];
+      const int dyi = C::dy(k), dx = j + C::dx(k);
+      const float4 r = ref[(th.y0 + i + dyi) * G::RP + (dx & 1) * G::Q + th.hx + (dx >> 1)];
+      const float4 t = tst[at_hx<R, WY>(th.y0 + i + R, th.hx, j + R)];
+      const float rv[3] = { r.x, r.y, r.z }, tv[3] = { t.x, t.y, t.z };
+      #pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const int ti = f2i_exact(tv[c]), ri = f2i_exact(rv[c]);
+        const uint32_t e = (uint32_t)(ti + ig[c] - ri);
+        const uint32_t b = (uint32_t)clampi(ri - ig[c], 0, a.maxv);
+        if(valid)
+        {
+          irs[c] += e * e;
+          if(scp != nullptr) { scp[(size_t)c * plane + (size_t)y * a.W + x] = (T)b; }
+          mm[c][0] += (uint32_t)ti;
+          mm[c][1] += b;
+          mm[c][2] += (uint32_t)ti * (uint32_t)ti;
+          mm[c][3] += b * b;
+          mm[c][4] += (uint32_t)ti * b;
+        }
+      }
+    }
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      const uint32_t s = __reduce_add_sync(kFull, irs[c]);
+      if(th.lane == 0 && yv) { atomicAdd(rows + (size_t)y * 3 + c, s); }
+    }
+  }
+  if(mom.p != nullptr)
+  {
+    const int bx = xb >> 2, by = yb >> 2;
+    const bool store = (th.lane & 1) == 0 && bx < mom.nbx && by < mom.nby;
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      #pragma unroll
+      for(int m = 0; m < 5; m++)
+      {
+        const uint32_t v = mm[c][m] + __shfl_xor_sync(kFull, mm[c][m], 1);
+        if(store) { mom.p[((size_t)c * 5 + m) * mom.plane() + (size_t)by * mom.pitch + bx] = v; }
+      }
+    }
+  }
+}
+
+template <int R, int WY, typename T>
+__device__ __forceinline__ void epilogue_dispatch(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref,
+                                                  const uint32_t idx[8], int dir, int x0, int y0, int ga, int gb, int gc)
+{
+  using G = Geo<R, WY>;
+  const int sel = ((x0 + G::TW > a.W || y0 + G::TH > a.H) ? 4 : 0) | (a.mom[dir].p != nullptr ? 2 : 0) |
+                  ((dir ? a.scp0 : a.scp1) != nullptr ? 1 : 0);
+  switch(sel)
+  {
+  case 0: epilogue_fp<R, WY, T, false, false, false>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  case 1: epilogue_fp<R, WY, T, false, false, true>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  case 2: epilogue_fp<R, WY, T, false, true, false>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  case 3: epilogue_fp<R, WY, T, false, true, true>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  case 4: epilogue_fp<R, WY, T, true, false, false>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  case 5: epilogue_fp<R, WY, T, true, false, true>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  case 6: epilogue_fp<R, WY, T, true, true, false>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  default: epilogue_fp<R, WY, T, true, true, true>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  }
+}
+
+// ---- kernel -------------------------------------------------------------------------------------
+template <int R, int WY, typename T>
+__global__ void __launch_bounds__(64 * WY, 1) k_cps(const __grid_constant__ CpsKernelArgs k)
+{
+  using G = Geo<R, WY>;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  unsigned char* base = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);   // TMA boxes: 128-byte aligned
+  float4* F0 = reinterpret_cast<float4*>(base);
+  float4* F1 = F0 + G::SH * G::RP;
+  unsigned char* raw = base + 2 * G::kTileBytes;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(raw + k.g.raw_bytes);
+  const CpsArgs& a = k.a;
+  const int  ntiles = k.g.ntiles;
+  const bool tma = k.g.use_tma != 0;
+  const bool clip = a.clip < (sizeof(T) == 1 ? 0xffu : 0xffffu);
+  const Thr th;
+
+  if(tma && threadIdx.x == 0) { mbar_init(bar, 1); fence_barrier_init(); }
+  __syncthreads();
+  int t = blockIdx.x;
+  if(tma && threadIdx.x == 0 && t < ntiles) { issue_tile<R, WY>(k, raw, bar, t); }
+
+  const int g0 = a.gcd_src->gcd[0], g1 = a.gcd_src->gcd[1], g2 = a.gcd_src->gcd[2];
+  const bool int_path = (a.gcd_src->flags & 4) != 0;
+  uint32_t parity = 0;
+  for(; t < ntiles; t += gridDim.x)
+  {
+    const int x0 = (t % k.g.ntx) * G::TW, y0 = (t / k.g.ntx) * G::TH;
+    if(tma)
+    {
+      const bool ok = mbar_wait(bar, parity, kWaitCycles);
+      parity ^= 1u;
+      if(__syncthreads_or(!ok))
+      {
+        // the copies did not complete: report, give them one more bounded wait, stop
+        if(threadIdx.x == 0) { atomicOr(k.g.status, 8); mbar_wait(bar, parity ^ 1u, kWaitCycles); }
+        return;
+      }
+    }
+    else
+    {
+      load_plain<T, R, WY>(k, raw, x0, y0);
+      __syncthreads();
+    }
+    if(clip) { convert<T, R, WY, true>(k, raw, F0, F1, x0, y0); }
+    else { convert<T, R, WY, false>(k, raw, F0, F1, x0, y0); }
+    __syncthreads();
+    // the raw boxes are free again: the next tile's copies overlap this tile's search
+    if(tma && threadIdx.x == 0 && t + (int)gridDim.x < ntiles)
+    {
+      fence_proxy_async();
+      issue_tile<R, WY>(k, raw, bar, t + gridDim.x);
+    }
+    #pragma unroll 1
+    for(int dir = 0; dir < 2; dir++)
+    {
+      // dir 0 (R2T): test = In0 + GCD searched in In1 -> rows[0], SCP1 = clip(In1[best] - GCD)
+      // dir 1 (T2R): test = In1 - GCD searched in In0 -> rows[1], SCP0 = clip(In0[best] + GCD)
+      const float4* tst = dir ? F1 : F0;
+      const float4* ref = dir ? F0 : F1;
+      const int sg = dir ? -1 : 1;
+      const int ga = sg * g0, gb = sg * g1, gc = sg * g2;
+      uint32_t idx[8];
+      if(!int_path)
+      {
+        search_fp32<R, WY>(th, tst, ref, a.wf, (float)ga, (float)gb, (float)gc, idx);
+        epilogue_dispatch<R, WY, T>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc);
+      }
+      else
+      {
+        search_int<R, WY>(th, tst, ref, a.wi, ga, gb, gc, idx);
+        epilogue_int<R, WY, T>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- host -------------------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+       q == cudaDriverEntryPointSuccess)
+    {
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+  });
+  return fn;
+}
+
+// One 2D tensor map per plane. Returns false when TMA cannot take the plane (alignment, pitch).
+bool encode_plane(CUtensorMap* m, const void* p, int32_t w, int32_t h, int64_t pitch_elems, int esz, int bw, int bh)
+{
+  const uint64_t pitch = (uint64_t)pitch_elems * (uint64_t)esz;
+  if(((uintptr_t)p & 15) != 0 || (pitch & 15) != 0 || pitch >= (1ULL << 40) || w <= 0 || h <= 0) { return false; }
+  PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+  if(fn == nullptr) { return false; }
+  const cuuint64_t dims[2] = { (cuuint64_t)w, (cuuint64_t)h };
+  const cuuint64_t strides[1] = { (cuuint64_t)pitch };
+  const cuuint32_t box[2] = { (cuuint32_t)bw, (cuuint32_t)bh };
+  const cuuint32_t estr[2] = { 1, 1 };
+  const CUresult r = fn(m, esz == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(p),
+                        dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+struct DevInfo
+{
+  int sms = 0, smem_optin = 0;
+};
+DevInfo dev_info(int dev)
+{
+  static std::mutex mu;
+  static DevInfo cache[64];
+  std::lock_guard<std::mutex> lk(mu);
+  if(dev < 0 || dev >= 64) { return DevInfo{ 1, 48 * 1024 }; }
+  if(cache[dev].sms == 0)
+  {
+    cudaDeviceGetAttribute(&cache[dev].sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&cache[dev].smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if(cache[dev].sms <= 0) { cache[dev].sms = 1; }
+  }
+  return cache[dev];
+}
+
+constexpr int kAlign = 128;
+inline uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
+
+// Geometry for one (R, WY, sample size, subsampling); returns the dynamic shared memory size.
+template <int R, int WY>
+size_t plan(CpsGeomArgs& g, int esz, int sx, int sy)
+{
+  using G = Geo<R, WY>;
+  g.ax = 16 / esz;
+  g.sx = sx; g.sy = sy;
+  g.bwl = (int)align_up((uint32_t)(g.ax + G::TW + R), (uint32_t)g.ax);
+  g.bhl = G::SH;
+  const int chi = (G::TW - 1 + R) >> sx;                          // last chroma column, relative to x0 >> sx
+  g.bwc = (int)align_up((uint32_t)(g.ax + chi + 1), (uint32_t)g.ax);
+  g.bhc = ((G::TH - 1 + R) >> sy) - ((-R) >> sy) + 1;
+  uint32_t cur = 0;
+  for(int f = 0; f < 2; f++)
+  {
+    g.off[f][0] = cur; cur += align_up((uint32_t)(g.bwl * g.bhl * esz), kAlign);
+    g.off[f][1] = cur; cur += align_up((uint32_t)(g.bwc * g.bhc * esz), kAlign);
+    g.off[f][2] = cur; cur += align_up((uint32_t)(g.bwc * g.bhc * esz), kAlign);
+  }
+  g.raw_bytes = cur;
+  g.tx_bytes = (uint32_t)(2 * (g.bwl * g.bhl + 2 * g.bwc * g.bhc) * esz);
+  return kAlign + 2 * (size_t)G::kTileBytes + cur + 16;
+}
+
+template <int R, int WY, typename T>
+cudaError_t launch_inst(CpsKernelArgs& k, size_t smem, int dev, cudaStream_t s)
+{
+  using G = Geo<R, WY>;
+  static std::atomic<uint64_t> configured{ 0 };
+  const uint64_t bit = 1ULL << (dev & 63);
+  if(!(configured.load() & bit))
+  {
+    const DevInfo di = dev_info(dev);
+    const cudaError_t e = cudaFuncSetAttribute(k_cps<R, WY, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, di.smem_optin);
+    if(e != cudaSuccess) { return e; }
+    configured.fetch_or(bit);
+  }
+  const int nty = (k.a.H + G::TH - 1) / G::TH;
+  k.g.ntx = (k.a.W + G::TW - 1) / G::TW;
+  k.g.ntiles = k.g.ntx * nty;
+  int occ = 1;
+  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cps<R, WY, T>, G::NT, smem) != cudaSuccess || occ < 1) { occ = 1; }
+  const int grid = std::min(k.g.ntiles, dev_info(dev).sms * occ);
+  k_cps<R, WY, T><<<grid, G::NT, smem, s>>>(k);
+  return cudaGetLastError();
+}
+
+template <int R, typename T>
+cudaError_t launch_r(CpsKernelArgs& k, cudaStream_t s)
+{
+  // 16 warps (128 x 32 tiles) for R <= 3, where both float tiles and the raw boxes of any chroma
+  // format fit in shared memory; 8 warps (128 x 16 tiles) for R = 5; R = 4 takes the tall tiles
+  // unless 4:4:4 boxes do not fit.
+  constexpr bool kTall = R <= 4, kShort = R >= 4;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess) { return e; }
+  const DevInfo di = dev_info(dev);
+  const int esz = (int)sizeof(T);
+  const int sx = k.a.in0.sx[1], sy = k.a.in0.sy[1];
+  CpsGeomArgs gt = k.g, gs = k.g;
+  size_t st = 0, ss = 0;
+  if constexpr(kTall) { st = plan<R, 8>(gt, esz, sx, sy); }
+  if constexpr(kShort) { ss = plan<R, 4>(gs, esz, sx, sy); }
+  const bool tall = kTall && st <= (size_t)di.smem_optin;
+  if(!tall && !(kShort && ss <= (size_t)di.smem_optin)) { return cudaErrorInvalidConfiguration; }
+  k.g = tall ? gt : gs;
+  // tensor maps of the six planes; any plane TMA cannot take switches the launch to plain loads
+  const int cw = k.a.W >> sx, ch = k.a.H >> sy;
+  bool ok = true;
+  for(int f = 0; f < 2 && ok; f++)
+  {
+    const Img& im = f ? k.a.in1 : k.a.in0;
+    ok = ok && encode_plane(&k.map[f][0], im.p[0], k.a.W, k.a.H, im.pitch[0], esz, k.g.bwl, k.g.bhl);
+    ok = ok && encode_plane(&k.map[f][1], im.p[1], cw, ch, im.pitch[1], esz, k.g.bwc, k.g.bhc);
+    ok = ok && encode_plane(&k.map[f][2], im.p[2], cw, ch, im.pitch[2], esz, k.g.bwc, k.g.bhc);
+  }
+  k.g.use_tma = ok ? 1 : 0;
+  if constexpr(kTall)
+  {
+    if(tall) { return launch_inst<R, 8, T>(k, st, dev, s); }
+  }
+  if constexpr(kShort) { return launch_inst<R, 4, T>(k, ss, dev, s); }
+  return cudaErrorInvalidConfiguration;
+}
+
+}  // namespace
+
+bool cps_fp32_exact(int32_t maxv, const int32_t w[3], const int32_t maxdiff[3])
+{
+  const int64_t bias = 1LL << 23;
+  int64_t e = 0, q = 0, up = 0, lo = 0;
+  for(int c = 0; c < 3; c++)
+  {
+    const int64_t g = maxdiff[c] < 0 ? -(int64_t)maxdiff[c] : maxdiff[c];
+    if(w[c] < 0) { return false; }
+    e  += (int64_t)w[c] * (maxv + g) * (maxv + g);   // max of sum_c w_c (s_c - r_c)^2 and of sum_c w_c s_c^2
+    q  += (int64_t)w[c] * maxv * maxv;
+    up += 2 * (int64_t)w[c] * g * maxv;              // largest positive -2 w s r (s negative)
+    lo += 2 * (int64_t)w[c] * (maxv + g) * maxv;     // largest negative -2 w s r
+    // epilogue: four squared differences of a row (maxv + g)^2 add below 2^23
+    if(4 * (maxv + g) * (maxv + g) >= bias) { return false; }
+  }
+  const int64_t lim = 1LL << 24;
+  if(bias - e < (1LL << 20)) { return false; }       // key base
+  if(bias + e >= lim) { return false; }
+  if(bias + q + up >= lim) { return false; }         // partial sums of the FFMA chain
+  if(bias - lo <= -lim) { return false; }
+  if(16LL * maxv * maxv >= lim) { return false; }    // float SSIM moments of a 4x4 block
+  return true;
+}
+
+template <typename T>
+cudaError_t launch_cps(const CpsArgs& a, int R, cudaStream_t s)
+{
+  CpsKernelArgs k;
+  std::memset(&k, 0, sizeof(k));
+  k.a = a;
+  k.g.status = const_cast<int32_t*>(&a.gcd_src->flags);
+  switch(R)
+  {
+  case 1: return launch_r<1, T>(k, s);
+  case 2: return launch_r<2, T>(k, s);
+  case 3: return launch_r<3, T>(k, s);
+  case 4: return launch_r<4, T>(k, s);
+  case 5: return launch_r<5, T>(k, s);
+  default: return cudaErrorInvalidValue;
+  }
+}
+template cudaError_t launch_cps<uint8_t>(const CpsArgs&, int, cudaStream_t);
+template cudaError_t launch_cps<uint16_t>(const CpsArgs&, int, cudaStream_t);
+
+}  // namespace qmiv

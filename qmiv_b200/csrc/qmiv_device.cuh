@@ -106,7 +106,8 @@ constexpr int kMaxSsimSlots = 18;   // SSIM 1 + IV-SSIM 2 + MS-SSIM 5 + IV-MS-SS
 struct PairOut
 {
   int32_t  gcd[4];
-  int32_t  flags;            // bit0: frame0 invalid, bit1: frame1 invalid, bit2: integer CPS path
+  int32_t  flags;            // bit0: frame0 invalid, bit1: frame1 invalid, bit2: integer CPS path,
+                             // bit3: a CPS tile load did not complete (bounded wait ran out)
   uint32_t max_sample[2];
   int64_t  sd[3];            // 4:4:4 totals of In1 - In0
   uint64_t ssd[3];           // 4:4:4 totals

@@ -80,6 +80,9 @@ int32_t num_scales(int32_t W, int32_t H);
 int32_t round_f32_half_away(float f);
 void    ws_weights(int32_t H, int32_t lat_range, std::vector<double>& w, double& correction);
 void    finish_result(const PairOut& o, const FinishInfo& fi, qmiv_result* r);
+// Status of a finished pair from its device flags: a CPS tile load that did not complete, then
+// invalid samples under QMIV_PEL_STOP.
+qmiv_status pair_status(const PairOut& o, int32_t invalid_pel_action);
 
 // Geometry of one frame-pair shape.
 struct Shape
@@ -93,6 +96,11 @@ struct Shape
   size_t  plane_cols(int c) const { return c == 0 ? (size_t)W : (size_t)cw; }
   size_t  plane_rows(int c) const { return c == 0 ? (size_t)H : (size_t)ch; }
   size_t  frame_bytes() const { return esz * ((size_t)W * H + 2 * (size_t)cw * ch); }
+  // device copy of a host frame: rows padded to 16 bytes and planes to 256 bytes, so that TMA can
+  // load the planes directly
+  size_t  staged_pitch(int c) const { return (plane_cols(c) * esz + 15) & ~(size_t)15; }
+  size_t  staged_plane_bytes(int c) const { return (staged_pitch(c) * plane_rows(c) + 255) & ~(size_t)255; }
+  size_t  staged_frame_bytes() const { return staged_plane_bytes(0) + staged_plane_bytes(1) + staged_plane_bytes(2); }
 };
 
 qmiv_status validate_params(const qmiv_params& p);

@@ -187,9 +187,5 @@ extern "C" qmiv_status qmiv_frame_pair_compute_static(const qmiv_frame* in0, con
   for(int c = 0; c < 4; c++) { fi.cwa[c] = prm.cwa[c]; }
   fi.num_scales = num_scales(S.W, S.H);
   finish_result(host, fi, out);
-  if(prm.invalid_pel_action == QMIV_PEL_STOP && (host.flags & 3))
-  {
-    return fail(QMIV_ERR_INVALID_PIXEL, "input frame contains samples above the bit depth's maximum");
-  }
-  return QMIV_OK;
+  return pair_status(host, prm.invalid_pel_action);
 }

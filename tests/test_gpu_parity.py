@@ -170,3 +170,32 @@ def test_full_size_properties(qctx):
         assert b["ivpsnr_r2t"] == a["ivpsnr_t2r"] and b["ivpsnr_t2r"] == a["ivpsnr_r2t"]
         assert b["ivssim_r2t"] == a["ivssim_t2r"] and b["ivssim_t2r"] == a["ivssim_r2t"]
         assert a["psnr"] == b["psnr"] and a["ssim"] == b["ssim"]
+
+
+def test_cps_tma_and_plain_tile_loads_agree(qctx, oracle_lib):
+    """Device planes with 16-byte row pitches reach the search through TMA tile loads, planes with an
+    odd pitch through plain loads; host frames are staged with aligned pitches. All equal the oracle."""
+    import torch
+    import qmiv_b200
+    from qmiv_b200 import synth
+    W, H, bd = 640, 360, 10
+    f0, f1 = synth.make_pair(W, H, bd, seed=99)
+    mask = qmiv_b200.IVPSNR | qmiv_b200.IVSSIM | qmiv_b200.PSNR | qmiv_b200.WSPSNR
+    exp = oracle_lib.compute_pair(oracle.make_params(W, H, bd, 420, erp=True), f0, f1, mask)
+
+    def strided(frame, extra):
+        views = []
+        for pl in frame:
+            h, w = pl.shape
+            big = np.zeros((h, w + extra), dtype=pl.dtype)
+            big[:, :w] = pl
+            views.append(torch.from_numpy(big).cuda()[:, :w])
+        return tuple(views)
+
+    keys = ["gcd_r2t", "psnr", "wspsnr", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r", "ivssim", "ivssim_r2t", "ivssim_t2r"]
+    with qmiv_b200.Calc(qctx, W, H, bd, 420, erp=True) as calc:
+        for a, b in [(f0, f1), (_device(f0), _device(f1)), (strided(f0, 3), strided(f1, 3)),
+                     (strided(f0, 8), strided(f1, 5))]:
+            got = calc.compute(a, b, mask)
+            for k in keys:
+                assert got[k] == exp[k], k
