@@ -213,7 +213,7 @@ __device__ void convert(const CpsKernelArgs& k, const unsigned char* raw, float4
       {
         uint32_t v0 = rl[colL[kk]], v1 = ru[colC[kk]], v2 = rv[colC[kk]];
         if(CLIP) { v0 = min(v0, clip); v1 = min(v1, clip); v2 = min(v2, clip); }
-        const float y = __uint2float_rn(v0), u = __uint2float_rn(v1), v = __uint2float_rn(v2);
+        const float y = u2f_exact(v0), u = u2f_exact(v1), v = u2f_exact(v2);
         frow[16 * kk] = make_float4(y, u, v, fmaf(w2, v * v, fmaf(w1, u * u, fmaf(w0, y * y, kBias))));
       }
     }
@@ -268,13 +268,16 @@ __device__ __forceinline__ void search_fp32(const Thr& th, const float4* tst, co
   constexpr int D = G::D;
   float c0[8], c1[8], c2[8];
   uint32_t best[8];
+  // c = -2 w (t + g) = (-2 w) t + (-2 w g): integers below 2^24, exact in one FFMA
+  const float m0 = -2.0f * wf[0], m1 = -2.0f * wf[1], m2 = -2.0f * wf[2];
+  const float o0 = m0 * ga, o1 = m1 * gb, o2 = m2 * gc;
   #pragma unroll
   for(int p = 0; p < 8; p++)
   {
     const float4 t = tst[at_hx<R, WY>(th.y0 + (p >> 1) + R, th.hx, (p & 1) + R)];
-    c0[p] = -2.0f * wf[0] * (t.x + ga);
-    c1[p] = -2.0f * wf[1] * (t.y + gb);
-    c2[p] = -2.0f * wf[2] * (t.z + gc);
+    c0[p] = fmaf(m0, t.x, o0);
+    c1[p] = fmaf(m1, t.y, o1);
+    c2[p] = fmaf(m2, t.z, o2);
     best[p] = 0xffffffffu;
   }
   const float4* rb = ref + at_hx<R, WY>(th.y0, th.hx, 0);
@@ -388,8 +391,9 @@ __device__ __forceinline__ void epilogue_fp(const Thr& th, const CpsArgs& a, con
       #pragma unroll
       for(int c = 0; c < 3; c++)
       {
-        const float d = (tv[c] + fg[c]) - rv[c];
-        const float b = fminf(fmaxf(rv[c] - fg[c], 0.f), fmax);
+        const float rg = rv[c] - fg[c];
+        const float d = tv[c] - rg;
+        const float b = fminf(fmaxf(rg, 0.f), fmax);
         frs[c] = fmaf(EDGE ? d * m : d, d, frs[c]);
         if(MOM)
         {
@@ -432,7 +436,7 @@ __device__ __forceinline__ void epilogue_fp(const Thr& th, const CpsArgs& a, con
 
 // int32 path: the SSE path's wrap-around arithmetic
 template <int R, int WY, typename T>
-__device__ __noinline__ void epilogue_int(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref,
+__device__ __forceinline__ void epilogue_int(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref,
                                           const uint32_t idx[8], int dir, int x0, int y0, int ga, int gb, int gc)
 {
   using G = Geo<R, WY>;
@@ -506,6 +510,15 @@ __device__ __noinline__ void epilogue_int(const Thr& th, const CpsArgs& a, const
       }
     }
   }
+}
+
+template <int R, int WY, typename T>
+__device__ __noinline__ void direction_int(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref, int dir,
+                                           int x0, int y0, int ga, int gb, int gc)
+{
+  uint32_t idx[8];
+  search_int<R, WY>(th, tst, ref, a.wi, ga, gb, gc, idx);
+  epilogue_int<R, WY, T>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc);
 }
 
 template <int R, int WY, typename T>
@@ -590,17 +603,13 @@ __global__ void __launch_bounds__(64 * WY, 1) k_cps(const __grid_constant__ CpsK
       const float4* ref = dir ? F0 : F1;
       const int sg = dir ? -1 : 1;
       const int ga = sg * g0, gb = sg * g1, gc = sg * g2;
-      uint32_t idx[8];
       if(!int_path)
       {
+        uint32_t idx[8];
         search_fp32<R, WY>(th, tst, ref, a.wf, (float)ga, (float)gb, (float)gc, idx);
         epilogue_dispatch<R, WY, T>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc);
       }
-      else
-      {
-        search_int<R, WY>(th, tst, ref, a.wi, ga, gb, gc, idx);
-        epilogue_int<R, WY, T>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc);
-      }
+      else { direction_int<R, WY, T>(th, a, tst, ref, dir, x0, y0, ga, gb, gc); }
     }
     __syncthreads();
   }
