@@ -274,12 +274,12 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
   double* rowsum = rowsum_.as<double>();
   // window pooling of up to three pictures pairs (x 3 components) from their moments, one launch
   SsimPoolArgs pool{};
-  pool.C1 = C1_; pool.C2 = C2_;
   auto add_pool = [&](const Moments& m, int scale, int slot, int calc_l, int use_ws) {
     for(int c = 0; c < 3; c++)
     {
       SsimPoolJob& J = pool.job[pool.njobs++];
       J.mom = m.p + (size_t)c * 5 * m.plane(); J.plane = m.plane(); J.pitch = m.pitch;
+      J.C1 = C1_; J.C2 = C2_;
       J.nx = nx_[scale]; J.ny = ny_[scale]; J.calc_l = calc_l;
       J.row_sum = rowsum + (size_t)slot * 3 * ny_[0] + (size_t)c * ny_[scale];  // finalize reads [c][ny_scale]
     }

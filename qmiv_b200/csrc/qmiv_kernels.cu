@@ -12,6 +12,7 @@
 #include "qmiv_kernels.cuh"
 
 #include <cstdio>
+#include <mutex>
 
 namespace qmiv {
 
@@ -21,9 +22,8 @@ constexpr unsigned kFull = 0xffffffffu;
 // prepass
 // =============================================================================================
 template <typename T>
-__global__ void __launch_bounds__(256) k_prepass(const __grid_constant__ PrepassArgs a)
+__device__ __forceinline__ void prepass_body(const PrepassArgs& a, int warp)
 {
-  const int warp  = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane  = threadIdx.x & 31;
   const int total = a.rows[0] + a.rows[1] + a.rows[2];
   if(warp >= total) { return; }
@@ -63,6 +63,19 @@ __global__ void __launch_bounds__(256) k_prepass(const __grid_constant__ Prepass
 }
 
 template <typename T>
+__global__ void __launch_bounds__(256) k_prepass(const __grid_constant__ PrepassArgs a)
+{
+  prepass_body<T>(a, (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5));
+}
+
+// one job (frame pair) per blockIdx.y
+template <typename T>
+__global__ void __launch_bounds__(256) k_prepass_multi(const PrepassArgs* __restrict__ jobs)
+{
+  prepass_body<T>(jobs[blockIdx.y], (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5));
+}
+
+template <typename T>
 cudaError_t launch_prepass(const PrepassArgs& a, cudaStream_t s)
 {
   const int total  = a.rows[0] + a.rows[1] + a.rows[2];
@@ -73,10 +86,20 @@ cudaError_t launch_prepass(const PrepassArgs& a, cudaStream_t s)
 template cudaError_t launch_prepass<uint8_t>(const PrepassArgs&, cudaStream_t);
 template cudaError_t launch_prepass<uint16_t>(const PrepassArgs&, cudaStream_t);
 
+template <typename T>
+cudaError_t launch_prepass_multi(const PrepassArgs* d_jobs, int njobs, int max_rows, cudaStream_t s)
+{
+  if(njobs <= 0) { return cudaSuccess; }
+  k_prepass_multi<T><<<dim3((max_rows + 7) / 8, njobs), 256, 0, s>>>(d_jobs);
+  return cudaGetLastError();
+}
+template cudaError_t launch_prepass_multi<uint8_t>(const PrepassArgs*, int, int, cudaStream_t);
+template cudaError_t launch_prepass_multi<uint16_t>(const PrepassArgs*, int, int, cudaStream_t);
+
 // =============================================================================================
 // reduce: totals and GCD (libs/pmbb-ivqm/src/xGlobClrDiff.cpp:70-103)
 // =============================================================================================
-__global__ void __launch_bounds__(1024) k_reduce(const __grid_constant__ ReduceArgs a)
+__device__ __forceinline__ void reduce_body(const ReduceArgs& a)
 {
   __shared__ int64_t  s_sd[3][32];
   __shared__ uint64_t s_ssd[3][32];
@@ -122,9 +145,21 @@ __global__ void __launch_bounds__(1024) k_reduce(const __grid_constant__ ReduceA
   }
 }
 
+__global__ void __launch_bounds__(1024) k_reduce(const __grid_constant__ ReduceArgs a) { reduce_body(a); }
+
+// one job (frame pair) per CTA
+__global__ void __launch_bounds__(1024) k_reduce_multi(const ReduceArgs* __restrict__ jobs) { reduce_body(jobs[blockIdx.x]); }
+
 cudaError_t launch_reduce(const ReduceArgs& a, cudaStream_t s)
 {
   k_reduce<<<1, 1024, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_multi(const ReduceArgs* d_jobs, int njobs, cudaStream_t s)
+{
+  if(njobs <= 0) { return cudaSuccess; }
+  k_reduce_multi<<<njobs, 1024, 0, s>>>(d_jobs);
   return cudaGetLastError();
 }
 
@@ -160,11 +195,10 @@ __device__ __forceinline__ double chain_value(const FinalizeArgs& a, const FinCh
   return sl.use_ws ? dmul(v, a.ws[4 * y + 4]) : v;
 }
 
-__global__ void __launch_bounds__(256) k_finalize(const __grid_constant__ FinalizeArgs a)
+__device__ __forceinline__ void finalize_body(const FinalizeArgs& a, int chain, double* stage)
 {
-  extern __shared__ double stage[];  // [len] values, then [len] ERP weights for weighted SSIM chains
   PairOut* o = a.out;
-  if(blockIdx.x == (unsigned)a.nchains)
+  if(chain == a.nchains)
   {
     // exact uint64 totals of the sign-extended 32-bit CPS row sums (order independent)
     __shared__ unsigned long long acc[6];
@@ -185,7 +219,7 @@ __global__ void __launch_bounds__(256) k_finalize(const __grid_constant__ Finali
     if(threadIdx.x < 6) { o->cps_sum[threadIdx.x / 3][threadIdx.x % 3] = acc[threadIdx.x]; }
     return;
   }
-  const FinChain ch = a.chain[blockIdx.x];
+  const FinChain ch = a.chain[chain];
   const bool wsum = ch.kind == kChainSsim && a.slot[ch.a].use_ws;
   const int len = ch.kind == kChainSsim ? a.slot[ch.a].ny : a.H;
   double* vals = stage;
@@ -225,9 +259,22 @@ __global__ void __launch_bounds__(256) k_finalize(const __grid_constant__ Finali
   }
 }
 
-cudaError_t launch_finalize(const FinalizeArgs& a_in, cudaStream_t s)
+__global__ void __launch_bounds__(256) k_finalize(const __grid_constant__ FinalizeArgs a)
 {
-  FinalizeArgs a = a_in;
+  extern __shared__ double stage[];  // [len] values, then [len] ERP weights for weighted SSIM chains
+  finalize_body(a, blockIdx.x, stage);
+}
+
+// one (pair, chain) job per CTA
+__global__ void __launch_bounds__(256) k_finalize_multi(const FinalizeArgs* __restrict__ pairs, const FinJob* __restrict__ jobs)
+{
+  extern __shared__ double stage[];
+  const FinJob j = jobs[blockIdx.x];
+  finalize_body(pairs[j.pair], j.chain, stage);
+}
+
+int finalize_plan(FinalizeArgs& a)
+{
   a.nchains = 0;
   if(a.do_wspsnr && a.ws) { for(int c = 0; c < 3; c++) { a.chain[a.nchains++] = { kChainWsPsnr, c, 0 }; } }
   if(a.cps_rows && a.ws) { for(int d = 0; d < 2; d++) { for(int c = 0; c < 3; c++) { a.chain[a.nchains++] = { kChainIvPsnr, d, c }; } } }
@@ -236,18 +283,47 @@ cudaError_t launch_finalize(const FinalizeArgs& a_in, cudaStream_t s)
     if(a.slot[sl].row_sum == nullptr || a.slot[sl].ny <= 0) { continue; }
     for(int c = 0; c < 3; c++) { a.chain[a.nchains++] = { kChainSsim, sl, c }; }
   }
-  const int blocks = a.nchains + (a.cps_rows ? 1 : 0);
+  return a.nchains + (a.cps_rows ? 1 : 0);
+}
+
+size_t finalize_smem(const FinalizeArgs& a) { return (size_t)2 * max(a.H, 1) * sizeof(double); }
+
+static cudaError_t finalize_configure()
+{
+  static std::mutex mu;
+  static uint64_t done = 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess) { return e; }
+  const uint64_t bit = 1ULL << (dev & 63);
+  std::lock_guard<std::mutex> lk(mu);
+  if(done & bit) { return cudaSuccess; }
+  e = cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, kFinalizeMaxSmem);
+  if(e == cudaSuccess) { e = cudaFuncSetAttribute(k_finalize_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, kFinalizeMaxSmem); }
+  if(e == cudaSuccess) { done |= bit; }
+  return e;
+}
+
+cudaError_t launch_finalize(const FinalizeArgs& a_in, cudaStream_t s)
+{
+  FinalizeArgs a = a_in;
+  const int blocks = finalize_plan(a);
   if(blocks == 0) { return cudaSuccess; }
-  const size_t smem = (size_t)2 * max(a.H, 1) * sizeof(double);
-  static bool configured = false;
-  if(!configured)
-  {
-    const cudaError_t e = cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    if(e != cudaSuccess) { return e; }
-    configured = true;
-  }
-  if(smem > 200 * 1024) { return cudaErrorInvalidValue; }
+  const size_t smem = finalize_smem(a);
+  if(smem > kFinalizeMaxSmem) { return cudaErrorInvalidValue; }
+  cudaError_t e = finalize_configure();
+  if(e != cudaSuccess) { return e; }
   k_finalize<<<blocks, 256, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_multi(const FinalizeArgs* d_pairs, const FinJob* d_jobs, int njobs, size_t smem, cudaStream_t s)
+{
+  if(njobs <= 0) { return cudaSuccess; }
+  if(smem > kFinalizeMaxSmem) { return cudaErrorInvalidValue; }
+  cudaError_t e = finalize_configure();
+  if(e != cudaSuccess) { return e; }
+  k_finalize_multi<<<njobs, 256, smem, s>>>(d_pairs, d_jobs);
   return cudaGetLastError();
 }
 

@@ -74,6 +74,7 @@ struct SsimMomArgs
 // windows from moments, ordered row sums (xSSIM.cpp:353-369), for up to 6 (pair, component) jobs
 struct SsimPoolJob
 {
+  double          C1, C2;      // (0.01 Max)^2, (0.03 Max)^2 of the pair's bit depth
   const uint32_t* mom;         // the five moment planes of one component
   size_t          plane;       // elements between moment planes
   int32_t         pitch;
@@ -84,7 +85,6 @@ struct SsimPoolJob
 
 struct SsimPoolArgs
 {
-  double      C1, C2;
   int32_t     njobs;
   SsimPoolJob job[9];
 };
@@ -122,6 +122,13 @@ struct FinalizeArgs
   PairOut*        out;
 };
 
+// one (pair, chain) CTA of the multi-pair finalize; chain == nchains of the pair is its exact CPS sums
+struct FinJob
+{
+  int32_t pair, chain;
+};
+constexpr size_t kFinalizeMaxSmem = 200 * 1024;
+
 // launch wrappers (return cudaError_t of the launch)
 template <typename T> cudaError_t launch_prepass(const PrepassArgs& a, cudaStream_t s);
 cudaError_t launch_reduce(const ReduceArgs& a, cudaStream_t s);
@@ -129,6 +136,16 @@ template <typename T> cudaError_t launch_cps(const CpsArgs& a, int R, cudaStream
 template <typename T> cudaError_t launch_ssim_moments(const SsimMomArgs& a, cudaStream_t s);
 cudaError_t launch_ssim_pool(const SsimPoolArgs& a, cudaStream_t s);
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
+int         finalize_plan(FinalizeArgs& a);          // fills a.chain / a.nchains, returns the CTA count
+size_t      finalize_smem(const FinalizeArgs& a);
+
+// multi-pair forms: argument blocks in device memory, one launch for every pair of a batch
+template <typename T> cudaError_t launch_prepass_multi(const PrepassArgs* d_jobs, int njobs, int max_rows, cudaStream_t s);
+cudaError_t launch_reduce_multi(const ReduceArgs* d_jobs, int njobs, cudaStream_t s);
+template <typename T>
+cudaError_t launch_ssim_moments_multi(const SsimMomArgs* d_jobs, int njobs, int max_nbx, int max_nby, cudaStream_t s);
+cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_ny, cudaStream_t s);
+cudaError_t launch_finalize_multi(const FinalizeArgs* d_pairs, const FinJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
 
 // Exactness check of the fp32 key path for a given bit depth, weights and GCD clip range.
 bool cps_fp32_exact(int32_t maxv, const int32_t w[3], const int32_t maxdiff[3]);

@@ -14,9 +14,8 @@ namespace qmiv {
 // moments of an image pair, one thread per 4x4 sub-block
 // =============================================================================================
 template <typename T>
-__global__ void __launch_bounds__(256) k_ssim_moments(const __grid_constant__ SsimMomArgs a)
+__device__ __forceinline__ void ssim_moments_body(const SsimMomArgs& a, int c)
 {
-  const int c  = blockIdx.z;
   const int bx = blockIdx.x * 32 + (threadIdx.x & 31);
   const int by = blockIdx.y * 8 + (threadIdx.x >> 5);
   const Moments& M = a.mom;
@@ -74,6 +73,30 @@ __global__ void __launch_bounds__(256) k_ssim_moments(const __grid_constant__ Ss
 }
 
 template <typename T>
+__global__ void __launch_bounds__(256) k_ssim_moments(const __grid_constant__ SsimMomArgs a)
+{
+  ssim_moments_body<T>(a, blockIdx.z);
+}
+
+// blockIdx.z = 3 * job + component
+template <typename T>
+__global__ void __launch_bounds__(256) k_ssim_moments_multi(const SsimMomArgs* __restrict__ jobs)
+{
+  ssim_moments_body<T>(jobs[blockIdx.z / 3], blockIdx.z % 3);
+}
+
+template <typename T>
+cudaError_t launch_ssim_moments_multi(const SsimMomArgs* d_jobs, int njobs, int max_nbx, int max_nby, cudaStream_t s)
+{
+  if(njobs <= 0) { return cudaSuccess; }
+  const dim3 grid((max_nbx + 31) / 32, (max_nby + 7) / 8, 3 * njobs);
+  k_ssim_moments_multi<T><<<grid, 256, 0, s>>>(d_jobs);
+  return cudaGetLastError();
+}
+template cudaError_t launch_ssim_moments_multi<uint8_t>(const SsimMomArgs*, int, int, int, cudaStream_t);
+template cudaError_t launch_ssim_moments_multi<uint16_t>(const SsimMomArgs*, int, int, int, cudaStream_t);
+
+template <typename T>
 cudaError_t launch_ssim_moments(const SsimMomArgs& a, cudaStream_t s)
 {
   const dim3 grid((a.mom.nbx + 31) / 32, (a.mom.nby + 7) / 8, 3);
@@ -95,11 +118,10 @@ constexpr int kSubR = kBandJ + 1, kSubC = kChunkI + 1;
 constexpr int kStageN = 5 * kSubR * kSubC;      // staged moment values per chunk
 constexpr int kStagePerThread = (kStageN + 255) / 256;
 
-__global__ void __launch_bounds__(256) k_ssim_pool(const __grid_constant__ SsimPoolArgs a)
+__device__ __forceinline__ void ssim_pool_body(const SsimPoolJob& J)
 {
   __shared__ uint32_t st[2][5][kSubR][kSubC];
   __shared__ double vals[kBandJ][kChunkI + 1];
-  const SsimPoolJob& J = a.job[blockIdx.y];
   const int j0 = blockIdx.x * kBandJ;
   if(j0 >= J.ny) { return; }
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -152,7 +174,7 @@ __global__ void __launch_bounds__(256) k_ssim_pool(const __grid_constant__ SsimP
           sm[m] = (uint64_t)st[buf][m][ty][tx] + st[buf][m][ty][tx + 1] + st[buf][m][ty + 1][tx] + st[buf][m][ty + 1][tx + 1];
         }
         // moment 0/2 = "Tst" picture, 1/3 = "Ref" picture
-        v = ssim_window(sm[1], sm[0], sm[3], sm[2], sm[4], a.C1, a.C2, J.calc_l != 0);
+        v = ssim_window(sm[1], sm[0], sm[3], sm[2], sm[4], J.C1, J.C2, J.calc_l != 0);
       }
       vals[ty][tx] = v;
     }
@@ -166,6 +188,17 @@ __global__ void __launch_bounds__(256) k_ssim_pool(const __grid_constant__ SsimP
     __syncthreads();
   }
   if(ty == 0 && tx < kBandJ && j0 + tx < J.ny) { J.row_sum[j0 + tx] = row.result(); }
+}
+
+__global__ void __launch_bounds__(256) k_ssim_pool(const __grid_constant__ SsimPoolArgs a) { ssim_pool_body(a.job[blockIdx.y]); }
+
+__global__ void __launch_bounds__(256) k_ssim_pool_multi(const SsimPoolJob* __restrict__ jobs) { ssim_pool_body(jobs[blockIdx.y]); }
+
+cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_ny, cudaStream_t s)
+{
+  if(njobs <= 0) { return cudaSuccess; }
+  k_ssim_pool_multi<<<dim3((max_ny + kBandJ - 1) / kBandJ, njobs), 256, 0, s>>>(d_jobs);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_ssim_pool(const SsimPoolArgs& a, cudaStream_t s)

@@ -67,8 +67,8 @@ def make_pair(width, height, bitdepth=8, seed=0, chroma_format=420, shift_range=
             d = _block_shift(r, shy >> sy if sy else shy, shx >> sx if sx else shx, block >> max(sx, sy))
         d = d + offset[c] * scale + rng.normal(0.0, noise_sigma * scale, (h, w)).astype(np.float32)
         d = _blur(d, blur_sigma)
-        ref.append(r.astype(dtype))
-        dist.append(np.clip(np.rint(d), 0, maxv).astype(dtype))
+        ref.append(np.ascontiguousarray(r, dtype=dtype))
+        dist.append(np.ascontiguousarray(np.clip(np.rint(d), 0, maxv), dtype=dtype))
     return tuple(ref), tuple(dist)
 
 
