@@ -38,6 +38,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 namespace qmiv {
@@ -125,13 +126,28 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 }
 
 // ---- tile loads ---------------------------------------------------------------------------------
-template <int R, int WY>
+// Tensor maps written to global memory by a host copy are made visible to the TMA unit
+__device__ __forceinline__ void fence_tensormap_acquire(const CUtensorMap* map)
+{
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+template <int R, int WY, bool GMAPS>
 __device__ __forceinline__ void issue_tile(const CpsKernelArgs& k, unsigned char* raw, uint64_t* bar, int t)
 {
   using G = Geo<R, WY>;
   const int x0 = (t % k.g.ntx) * G::TW, y0 = (t / k.g.ntx) * G::TH;
   const int xl = x0 - k.g.ax, yl = y0 - R;
   const int xc = (x0 >> k.g.sx) - k.g.ax, yc = (y0 - R) >> k.g.sy;
+  if(GMAPS)
+  {
+    #pragma unroll
+    for(int f = 0; f < 2; f++)
+    {
+      #pragma unroll
+      for(int c = 0; c < 3; c++) { fence_tensormap_acquire(&k.map[f][c]); }
+    }
+  }
   mbar_expect_tx(bar, k.g.tx_bytes);
   #pragma unroll
   for(int f = 0; f < 2; f++)
@@ -145,21 +161,21 @@ __device__ __forceinline__ void issue_tile(const CpsKernelArgs& k, unsigned char
 // Same boxes with plain loads, for frames whose address or pitch TMA cannot take. Samples outside
 // the picture are left unwritten: the conversion only reads clamped in-picture coordinates.
 template <typename T, int R, int WY>
-__device__ void load_plain(const CpsKernelArgs& k, unsigned char* raw, int x0, int y0)
+__device__ void load_plain(const CpsArgs& a, const CpsGeomArgs& g, unsigned char* raw, int x0, int y0)
 {
   constexpr int NW = Geo<R, WY>::NT / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   #pragma unroll 1
   for(int f = 0; f < 2; f++)
   {
-    const Img& im = f ? k.a.in1 : k.a.in0;
+    const Img& im = f ? a.in1 : a.in0;
     #pragma unroll 1
     for(int c = 0; c < 3; c++)
     {
-      const int pw = c ? (k.a.W >> k.g.sx) : k.a.W, ph = c ? (k.a.H >> k.g.sy) : k.a.H;
-      const int bw = c ? k.g.bwc : k.g.bwl, bh = c ? k.g.bhc : k.g.bhl;
-      const int xs = c ? (x0 >> k.g.sx) - k.g.ax : x0 - k.g.ax, ys = c ? (y0 - R) >> k.g.sy : y0 - R;
-      T* dst = reinterpret_cast<T*>(raw + k.g.off[f][c]);
+      const int pw = c ? (a.W >> g.sx) : a.W, ph = c ? (a.H >> g.sy) : a.H;
+      const int bw = c ? g.bwc : g.bwl, bh = c ? g.bhc : g.bhl;
+      const int xs = c ? (x0 >> g.sx) - g.ax : x0 - g.ax, ys = c ? (y0 - R) >> g.sy : y0 - R;
+      T* dst = reinterpret_cast<T*>(raw + g.off[f][c]);
       const T* src = static_cast<const T*>(im.p[c]);
       for(int r = warp; r < bh; r += NW)
       {
@@ -179,15 +195,16 @@ __device__ void load_plain(const CpsKernelArgs& k, unsigned char* raw, int x0, i
 // to the warps round-robin; lane L converts columns L + 32 * kk of a row. Column offsets into the
 // raw boxes (clamped to the picture) are per lane and computed once.
 template <typename T, int R, int WY, bool CLIP>
-__device__ void convert(const CpsKernelArgs& k, const unsigned char* raw, float4* F0, float4* F1, int x0, int y0)
+__device__ void convert(const CpsArgs& a, const CpsGeomArgs& g, const unsigned char* raw, float4* F0, float4* F1,
+                        int x0, int y0)
 {
   using G = Geo<R, WY>;
   constexpr int NW = G::NT / 32, NK = (G::SW + 31) / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int W = k.a.W, H = k.a.H, sx = k.g.sx, sy = k.g.sy;
-  const int xl = x0 - k.g.ax, yl = y0 - R, xc = (x0 >> sx) - k.g.ax, yc = (y0 - R) >> sy;
-  const float w0 = k.a.wf[0], w1 = k.a.wf[1], w2 = k.a.wf[2];
-  const uint32_t clip = k.a.clip;
+  const int W = a.W, H = a.H, sx = g.sx, sy = g.sy;
+  const int xl = x0 - g.ax, yl = y0 - R, xc = (x0 >> sx) - g.ax, yc = (y0 - R) >> sy;
+  const float w0 = a.wf[0], w1 = a.wf[1], w2 = a.wf[2];
+  const uint32_t clip = a.clip;
   int colL[NK], colC[NK];
   #pragma unroll
   for(int kk = 0; kk < NK; kk++)
@@ -202,9 +219,9 @@ __device__ void convert(const CpsKernelArgs& k, const unsigned char* raw, float4
     const int f  = row >= G::SH ? 1 : 0;
     const int ly = row - f * G::SH;
     const int gy = clampi(y0 - R + ly, 0, H - 1);
-    const T* rl = reinterpret_cast<const T*>(raw + k.g.off[f][0]) + (gy - yl) * k.g.bwl;
-    const T* ru = reinterpret_cast<const T*>(raw + k.g.off[f][1]) + ((gy >> sy) - yc) * k.g.bwc;
-    const T* rv = reinterpret_cast<const T*>(raw + k.g.off[f][2]) + ((gy >> sy) - yc) * k.g.bwc;
+    const T* rl = reinterpret_cast<const T*>(raw + g.off[f][0]) + (gy - yl) * g.bwl;
+    const T* ru = reinterpret_cast<const T*>(raw + g.off[f][1]) + ((gy >> sy) - yc) * g.bwc;
+    const T* rv = reinterpret_cast<const T*>(raw + g.off[f][2]) + ((gy >> sy) - yc) * g.bwc;
     float4* frow = (f ? F1 : F0) + ly * G::RP + (lane & 1) * G::Q + (lane >> 1);
     #pragma unroll
     for(int kk = 0; kk < NK; kk++)
@@ -542,8 +559,16 @@ __device__ __forceinline__ void epilogue_dispatch(const Thr& th, const CpsArgs& 
 }
 
 // ---- kernel -------------------------------------------------------------------------------------
-template <int R, int WY, typename T>
-__global__ void __launch_bounds__(64 * WY, 1) k_cps(const __grid_constant__ CpsKernelArgs k)
+struct TileRef
+{
+  const CpsKernelArgs* k;     // the frame pair's arguments
+  int                  tile;  // tile index within the pair
+};
+
+// Persistent tile loop. `locate` maps a work-list index to (pair, tile); GMAPS: the pairs' tensor
+// maps live in global memory. raw_cap: bytes of the raw-box region (the same for every pair).
+template <int R, int WY, typename T, bool GMAPS, typename Locate>
+__device__ __forceinline__ void cps_loop(int ntiles, const Locate& locate, uint32_t raw_cap)
 {
   using G = Geo<R, WY>;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
@@ -551,49 +576,70 @@ __global__ void __launch_bounds__(64 * WY, 1) k_cps(const __grid_constant__ CpsK
   float4* F0 = reinterpret_cast<float4*>(base);
   float4* F1 = F0 + G::SH * G::RP;
   unsigned char* raw = base + 2 * G::kTileBytes;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(raw + k.g.raw_bytes);
-  const CpsArgs& a = k.a;
-  const int  ntiles = k.g.ntiles;
-  const bool tma = k.g.use_tma != 0;
-  const bool clip = a.clip < (sizeof(T) == 1 ? 0xffu : 0xffffu);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(raw + raw_cap);
   const Thr th;
+  // the current pair's arguments, copied to shared memory whenever the work list enters a new pair
+  __shared__ __align__(16) CpsArgs s_a;
+  __shared__ __align__(16) CpsGeomArgs s_g;
+  static_assert(sizeof(CpsArgs) % 4 == 0 && sizeof(CpsGeomArgs) % 4 == 0, "word copies");
 
-  if(tma && threadIdx.x == 0) { mbar_init(bar, 1); fence_barrier_init(); }
+  if(threadIdx.x == 0) { mbar_init(bar, 1); fence_barrier_init(); }
   __syncthreads();
   int t = blockIdx.x;
-  if(tma && threadIdx.x == 0 && t < ntiles) { issue_tile<R, WY>(k, raw, bar, t); }
-
-  const int g0 = a.gcd_src->gcd[0], g1 = a.gcd_src->gcd[1], g2 = a.gcd_src->gcd[2];
-  const bool int_path = (a.gcd_src->flags & 4) != 0;
+  if(t < ntiles && threadIdx.x == 0)
+  {
+    const TileRef L = locate(t);
+    if(L.k->g.use_tma) { issue_tile<R, WY, GMAPS>(*L.k, raw, bar, L.tile); }
+  }
   uint32_t parity = 0;
+  const CpsKernelArgs* cur = nullptr;
   for(; t < ntiles; t += gridDim.x)
   {
-    const int x0 = (t % k.g.ntx) * G::TW, y0 = (t / k.g.ntx) * G::TH;
-    if(tma)
+    const TileRef L = locate(t);
+    if(L.k != cur)
+    {
+      const uint32_t* sa = reinterpret_cast<const uint32_t*>(&L.k->a);
+      const uint32_t* sg = reinterpret_cast<const uint32_t*>(&L.k->g);
+      for(int w = threadIdx.x; w < (int)(sizeof(CpsArgs) / 4); w += G::NT) { reinterpret_cast<uint32_t*>(&s_a)[w] = sa[w]; }
+      for(int w = threadIdx.x; w < (int)(sizeof(CpsGeomArgs) / 4); w += G::NT) { reinterpret_cast<uint32_t*>(&s_g)[w] = sg[w]; }
+      __syncthreads();
+      cur = L.k;
+    }
+    const CpsArgs& a = s_a;
+    const CpsGeomArgs& g = s_g;
+    const int x0 = (L.tile % g.ntx) * G::TW, y0 = (L.tile / g.ntx) * G::TH;
+    if(g.use_tma)
     {
       const bool ok = mbar_wait(bar, parity, kWaitCycles);
       parity ^= 1u;
       if(__syncthreads_or(!ok))
       {
         // the copies did not complete: report, give them one more bounded wait, stop
-        if(threadIdx.x == 0) { atomicOr(k.g.status, 8); mbar_wait(bar, parity ^ 1u, kWaitCycles); }
+        if(threadIdx.x == 0) { atomicOr(g.status, 8); mbar_wait(bar, parity ^ 1u, kWaitCycles); }
         return;
       }
     }
     else
     {
-      load_plain<T, R, WY>(k, raw, x0, y0);
+      load_plain<T, R, WY>(a, g, raw, x0, y0);
       __syncthreads();
     }
-    if(clip) { convert<T, R, WY, true>(k, raw, F0, F1, x0, y0); }
-    else { convert<T, R, WY, false>(k, raw, F0, F1, x0, y0); }
+    if(a.clip < (sizeof(T) == 1 ? 0xffu : 0xffffu)) { convert<T, R, WY, true>(a, g, raw, F0, F1, x0, y0); }
+    else { convert<T, R, WY, false>(a, g, raw, F0, F1, x0, y0); }
     __syncthreads();
     // the raw boxes are free again: the next tile's copies overlap this tile's search
-    if(tma && threadIdx.x == 0 && t + (int)gridDim.x < ntiles)
+    const int tn = t + (int)gridDim.x;
+    if(tn < ntiles && threadIdx.x == 0)
     {
-      fence_proxy_async();
-      issue_tile<R, WY>(k, raw, bar, t + gridDim.x);
+      const TileRef N = locate(tn);
+      if(N.k->g.use_tma)
+      {
+        fence_proxy_async();
+        issue_tile<R, WY, GMAPS>(*N.k, raw, bar, N.tile);
+      }
     }
+    const int g0 = a.gcd_src->gcd[0], g1 = a.gcd_src->gcd[1], g2 = a.gcd_src->gcd[2];
+    const bool int_path = (a.gcd_src->flags & 4) != 0;
     #pragma unroll 1
     for(int dir = 0; dir < 2; dir++)
     {
@@ -613,6 +659,30 @@ __global__ void __launch_bounds__(64 * WY, 1) k_cps(const __grid_constant__ CpsK
     }
     __syncthreads();
   }
+}
+
+// one frame pair, arguments in parameter space
+template <int R, int WY, typename T>
+__global__ void __launch_bounds__(64 * WY, 1) k_cps(const __grid_constant__ CpsKernelArgs k)
+{
+  cps_loop<R, WY, T, false>(k.g.ntiles, [&](int t) { return TileRef{ &k, t }; }, k.g.raw_bytes);
+}
+
+// work list over the tiles of many frame pairs: pair p owns tiles [prefix[p], prefix[p + 1])
+template <int R, int WY, typename T>
+__global__ void __launch_bounds__(64 * WY, 1) k_cps_multi(const CpsKernelArgs* __restrict__ descs,
+                                                          const int32_t* __restrict__ prefix, int npairs, int ntiles,
+                                                          uint32_t raw_cap)
+{
+  cps_loop<R, WY, T, true>(ntiles, [&](int t) {
+    int lo = 0, hi = npairs - 1;
+    while(lo < hi)
+    {
+      const int mid = (lo + hi + 1) >> 1;
+      if(prefix[mid] <= t) { lo = mid; } else { hi = mid - 1; }
+    }
+    return TileRef{ &descs[lo], t - prefix[lo] };
+  }, raw_cap);
 }
 
 // ---- host -------------------------------------------------------------------------------------
@@ -669,6 +739,7 @@ DevInfo dev_info(int dev)
 }
 
 constexpr int kAlign = 128;
+constexpr size_t kStaticSmem = 1024;   // the kernel's static shared memory (argument copy), rounded up
 inline uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
 // Geometry for one (R, WY, sample size, subsampling); returns the dynamic shared memory size.
@@ -695,69 +766,188 @@ size_t plan(CpsGeomArgs& g, int esz, int sx, int sy)
   return kAlign + 2 * (size_t)G::kTileBytes + cur + 16;
 }
 
-template <int R, int WY, typename T>
-cudaError_t launch_inst(CpsKernelArgs& k, size_t smem, int dev, cudaStream_t s)
+template <int R, int WY>
+void plan_pair(CpsGeomArgs& g, size_t& smem, int esz, int sx, int sy, int W, int H)
 {
   using G = Geo<R, WY>;
-  static std::atomic<uint64_t> configured{ 0 };
-  const uint64_t bit = 1ULL << (dev & 63);
-  if(!(configured.load() & bit))
+  smem = plan<R, WY>(g, esz, sx, sy);
+  g.ntx = (W + G::TW - 1) / G::TW;
+  g.ntiles = g.ntx * ((H + G::TH - 1) / G::TH);
+}
+
+// runtime (R, WY) -> plan_pair; false for combinations that are never instantiated (R = 5 with
+// 128 x 32 tiles never fits shared memory)
+bool plan_any(int R, int wy, CpsGeomArgs& g, size_t& smem, int esz, int sx, int sy, int W, int H)
+{
+  switch(R * 16 + wy)
   {
-    const DevInfo di = dev_info(dev);
-    const cudaError_t e = cudaFuncSetAttribute(k_cps<R, WY, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, di.smem_optin);
-    if(e != cudaSuccess) { return e; }
-    configured.fetch_or(bit);
+  case 1 * 16 + 8: plan_pair<1, 8>(g, smem, esz, sx, sy, W, H); return true;
+  case 2 * 16 + 8: plan_pair<2, 8>(g, smem, esz, sx, sy, W, H); return true;
+  case 3 * 16 + 8: plan_pair<3, 8>(g, smem, esz, sx, sy, W, H); return true;
+  case 4 * 16 + 8: plan_pair<4, 8>(g, smem, esz, sx, sy, W, H); return true;
+  case 1 * 16 + 4: plan_pair<1, 4>(g, smem, esz, sx, sy, W, H); return true;
+  case 2 * 16 + 4: plan_pair<2, 4>(g, smem, esz, sx, sy, W, H); return true;
+  case 3 * 16 + 4: plan_pair<3, 4>(g, smem, esz, sx, sy, W, H); return true;
+  case 4 * 16 + 4: plan_pair<4, 4>(g, smem, esz, sx, sy, W, H); return true;
+  case 5 * 16 + 4: plan_pair<5, 4>(g, smem, esz, sx, sy, W, H); return true;
+  default: return false;
   }
-  const int nty = (k.a.H + G::TH - 1) / G::TH;
-  k.g.ntx = (k.a.W + G::TW - 1) / G::TW;
-  k.g.ntiles = k.g.ntx * nty;
+}
+
+// Tensor maps of the six planes; false when TMA cannot take one of them (plain loads then).
+bool encode_maps(CpsKernelArgs& k, int esz)
+{
+  const int cw = k.a.W >> k.g.sx, ch = k.a.H >> k.g.sy;
+  for(int f = 0; f < 2; f++)
+  {
+    const Img& im = f ? k.a.in1 : k.a.in0;
+    if(!encode_plane(&k.map[f][0], im.p[0], k.a.W, k.a.H, im.pitch[0], esz, k.g.bwl, k.g.bhl)) { return false; }
+    if(!encode_plane(&k.map[f][1], im.p[1], cw, ch, im.pitch[1], esz, k.g.bwc, k.g.bhc)) { return false; }
+    if(!encode_plane(&k.map[f][2], im.p[2], cw, ch, im.pitch[2], esz, k.g.bwc, k.g.bhc)) { return false; }
+  }
+  return true;
+}
+
+// Raises the kernel's dynamic shared memory limit once per (kernel, device). The opt-in limit
+// covers the kernel's static shared memory (the argument copy) and the dynamic part together.
+template <typename F>
+cudaError_t configure_once(F* fn, int dev)
+{
+  static std::mutex mu;
+  static std::map<const void*, uint64_t> done;
+  const uint64_t bit = 1ULL << (dev & 63);
+  std::lock_guard<std::mutex> lk(mu);
+  uint64_t& m = done[reinterpret_cast<const void*>(fn)];
+  if(m & bit) { return cudaSuccess; }
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if(e != cudaSuccess) { return e; }
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_info(dev).smem_optin - (int)fa.sharedSizeBytes);
+  if(e == cudaSuccess) { m |= bit; }
+  return e;
+}
+
+template <typename F>
+int grid_for(F* fn, int threads, size_t smem, int ntiles, int dev)
+{
   int occ = 1;
-  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cps<R, WY, T>, G::NT, smem) != cudaSuccess || occ < 1) { occ = 1; }
-  const int grid = std::min(k.g.ntiles, dev_info(dev).sms * occ);
-  k_cps<R, WY, T><<<grid, G::NT, smem, s>>>(k);
+  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess || occ < 1) { occ = 1; }
+  return std::max(1, std::min(ntiles, dev_info(dev).sms * occ));
+}
+
+template <int R, int WY, typename T>
+cudaError_t launch_inst(const CpsKernelArgs& k, size_t smem, int dev, cudaStream_t s)
+{
+  using G = Geo<R, WY>;
+  cudaError_t e = configure_once(k_cps<R, WY, T>, dev);
+  if(e != cudaSuccess) { return e; }
+  k_cps<R, WY, T><<<grid_for(k_cps<R, WY, T>, G::NT, smem, k.g.ntiles, dev), G::NT, smem, s>>>(k);
+  return cudaGetLastError();
+}
+
+template <int R, int WY, typename T>
+cudaError_t launch_multi_inst(const CpsKernelArgs* d, const int32_t* prefix, int npairs, int ntiles, uint32_t raw_cap,
+                              size_t smem, int dev, cudaStream_t s)
+{
+  using G = Geo<R, WY>;
+  cudaError_t e = configure_once(k_cps_multi<R, WY, T>, dev);
+  if(e != cudaSuccess) { return e; }
+  const int grid = grid_for(k_cps_multi<R, WY, T>, G::NT, smem, ntiles, dev);
+  k_cps_multi<R, WY, T><<<grid, G::NT, smem, s>>>(d, prefix, npairs, ntiles, raw_cap);
   return cudaGetLastError();
 }
 
 template <int R, typename T>
 cudaError_t launch_r(CpsKernelArgs& k, cudaStream_t s)
 {
-  // 16 warps (128 x 32 tiles) for R <= 3, where both float tiles and the raw boxes of any chroma
-  // format fit in shared memory; 8 warps (128 x 16 tiles) for R = 5; R = 4 takes the tall tiles
-  // unless 4:4:4 boxes do not fit.
-  constexpr bool kTall = R <= 4, kShort = R >= 4;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if(e != cudaSuccess) { return e; }
-  const DevInfo di = dev_info(dev);
   const int esz = (int)sizeof(T);
-  const int sx = k.a.in0.sx[1], sy = k.a.in0.sy[1];
-  CpsGeomArgs gt = k.g, gs = k.g;
-  size_t st = 0, ss = 0;
-  if constexpr(kTall) { st = plan<R, 8>(gt, esz, sx, sy); }
-  if constexpr(kShort) { ss = plan<R, 4>(gs, esz, sx, sy); }
-  const bool tall = kTall && st <= (size_t)di.smem_optin;
-  if(!tall && !(kShort && ss <= (size_t)di.smem_optin)) { return cudaErrorInvalidConfiguration; }
-  k.g = tall ? gt : gs;
-  // tensor maps of the six planes; any plane TMA cannot take switches the launch to plain loads
-  const int cw = k.a.W >> sx, ch = k.a.H >> sy;
-  bool ok = true;
-  for(int f = 0; f < 2 && ok; f++)
+  const int wy = cps_pick_wy(R, esz, k.a.in0.sx[1], k.a.in0.sy[1]);
+  if(wy == 0) { return cudaErrorInvalidConfiguration; }
+  size_t smem = 0;
+  plan_any(R, wy, k.g, smem, esz, k.a.in0.sx[1], k.a.in0.sy[1], k.a.W, k.a.H);
+  k.g.use_tma = encode_maps(k, esz) ? 1 : 0;
+  if constexpr(R <= 4)
   {
-    const Img& im = f ? k.a.in1 : k.a.in0;
-    ok = ok && encode_plane(&k.map[f][0], im.p[0], k.a.W, k.a.H, im.pitch[0], esz, k.g.bwl, k.g.bhl);
-    ok = ok && encode_plane(&k.map[f][1], im.p[1], cw, ch, im.pitch[1], esz, k.g.bwc, k.g.bhc);
-    ok = ok && encode_plane(&k.map[f][2], im.p[2], cw, ch, im.pitch[2], esz, k.g.bwc, k.g.bhc);
+    if(wy == 8) { return launch_inst<R, 8, T>(k, smem, dev, s); }
   }
-  k.g.use_tma = ok ? 1 : 0;
-  if constexpr(kTall)
+  if constexpr(R >= 4) { return launch_inst<R, 4, T>(k, smem, dev, s); }
+  return cudaErrorInvalidConfiguration;
+}
+
+template <int R, typename T>
+cudaError_t launch_multi_r(const CpsKernelArgs* d, const int32_t* prefix, int npairs, int ntiles, int wy,
+                           uint32_t raw_cap, size_t smem, int dev, cudaStream_t s)
+{
+  if constexpr(R <= 4)
   {
-    if(tall) { return launch_inst<R, 8, T>(k, st, dev, s); }
+    if(wy == 8) { return launch_multi_inst<R, 8, T>(d, prefix, npairs, ntiles, raw_cap, smem, dev, s); }
   }
-  if constexpr(kShort) { return launch_inst<R, 4, T>(k, ss, dev, s); }
+  if(wy == 4) { return launch_multi_inst<R, 4, T>(d, prefix, npairs, ntiles, raw_cap, smem, dev, s); }
   return cudaErrorInvalidConfiguration;
 }
 
 }  // namespace
+
+// 16 warps (128 x 32 tiles) where both float tiles and the raw boxes fit in shared memory: always
+// for R <= 3, for R = 4 unless 4:4:4 boxes do not fit; 8 warps (128 x 16 tiles) otherwise.
+int cps_pick_wy(int R, int esz, int sx, int sy)
+{
+  if(R <= 4 && cps_tile_fits(R, 8, esz, sx, sy)) { return 8; }
+  if(cps_tile_fits(R, 4, esz, sx, sy)) { return 4; }
+  return 0;
+}
+
+bool cps_tile_fits(int R, int wy, int esz, int sx, int sy)
+{
+  int dev = 0;
+  if(cudaGetDevice(&dev) != cudaSuccess) { return false; }
+  CpsGeomArgs g{};
+  size_t smem = 0;
+  return plan_any(R, wy, g, smem, esz, sx, sy, 1, 1) && smem + kStaticSmem <= (size_t)dev_info(dev).smem_optin;
+}
+
+size_t cps_desc_bytes() { return sizeof(CpsKernelArgs); }
+
+cudaError_t cps_describe(void* desc, const CpsArgs& a, int R, int esz, int wy, CpsPairPlan* plan)
+{
+  CpsKernelArgs& k = *static_cast<CpsKernelArgs*>(desc);
+  std::memset(&k, 0, sizeof(k));
+  k.a = a;
+  k.g.status = const_cast<int32_t*>(&a.gcd_src->flags);
+  size_t smem = 0;
+  if(!plan_any(R, wy, k.g, smem, esz, a.in0.sx[1], a.in0.sy[1], a.W, a.H)) { return cudaErrorInvalidConfiguration; }
+  k.g.use_tma = encode_maps(k, esz) ? 1 : 0;
+  plan->ntiles = k.g.ntiles;
+  plan->raw_bytes = k.g.raw_bytes;
+  plan->smem = smem;
+  return cudaSuccess;
+}
+
+cudaError_t launch_cps_multi(const void* d_descs, const int32_t* d_prefix, int npairs, int ntiles, int R, int wy,
+                             int esz, uint32_t raw_cap, size_t smem, cudaStream_t s)
+{
+  if(npairs <= 0 || ntiles <= 0) { return cudaSuccess; }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess) { return e; }
+  const CpsKernelArgs* d = static_cast<const CpsKernelArgs*>(d_descs);
+  auto go = [&](auto tag) -> cudaError_t {
+    using T = decltype(tag);
+    switch(R)
+    {
+    case 1: return launch_multi_r<1, T>(d, d_prefix, npairs, ntiles, wy, raw_cap, smem, dev, s);
+    case 2: return launch_multi_r<2, T>(d, d_prefix, npairs, ntiles, wy, raw_cap, smem, dev, s);
+    case 3: return launch_multi_r<3, T>(d, d_prefix, npairs, ntiles, wy, raw_cap, smem, dev, s);
+    case 4: return launch_multi_r<4, T>(d, d_prefix, npairs, ntiles, wy, raw_cap, smem, dev, s);
+    case 5: return launch_multi_r<5, T>(d, d_prefix, npairs, ntiles, wy, raw_cap, smem, dev, s);
+    default: return cudaErrorInvalidValue;
+    }
+  };
+  return esz == 1 ? go(uint8_t{}) : go(uint16_t{});
+}
 
 bool cps_fp32_exact(int32_t maxv, const int32_t w[3], const int32_t maxdiff[3])
 {

@@ -147,6 +147,22 @@ cudaError_t launch_ssim_moments_multi(const SsimMomArgs* d_jobs, int njobs, int 
 cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_ny, cudaStream_t s);
 cudaError_t launch_finalize_multi(const FinalizeArgs* d_pairs, const FinJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
 
+// CPS work-list form: one 64-byte aligned descriptor (tensor maps + tile geometry) per frame pair,
+// pairs grouped by (search range, sample size, tile height); pair p owns work-list tiles
+// [prefix[p], prefix[p + 1]).
+struct CpsPairPlan
+{
+  int32_t  ntiles;
+  uint32_t raw_bytes;   // raw-box region of the pair
+  size_t   smem;        // dynamic shared memory of the pair alone
+};
+size_t      cps_desc_bytes();
+int         cps_pick_wy(int R, int esz, int sx, int sy);   // warps per tile column: 8 (128x32) or 4 (128x16), 0 = none
+bool        cps_tile_fits(int R, int wy, int esz, int sx, int sy);
+cudaError_t cps_describe(void* desc, const CpsArgs& a, int R, int esz, int wy, CpsPairPlan* plan);
+cudaError_t launch_cps_multi(const void* d_descs, const int32_t* d_prefix, int npairs, int ntiles, int R, int wy,
+                             int esz, uint32_t raw_cap, size_t smem, cudaStream_t s);
+
 // Exactness check of the fp32 key path for a given bit depth, weights and GCD clip range.
 bool cps_fp32_exact(int32_t maxv, const int32_t w[3], const int32_t maxdiff[3]);
 
