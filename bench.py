@@ -21,6 +21,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import time
 import threading
 import time
 
@@ -166,7 +167,8 @@ def run_qmiv(args, world, rank, local):
                      metrics=mask) for a, b in src]
 
     ctx = qmiv_b200.Context(local)
-    batch = qmiv_b200.Batch(ctx, max_pairs=PAIRS_PER_STEP, max_pixels=PAIRS_PER_STEP * W * H, erp=True)
+    batch = qmiv_b200.Batch(ctx, max_pairs=PAIRS_PER_STEP, max_pixels=PAIRS_PER_STEP * W * H, erp=True, graph=True,
+                            autotune=True)
     stream = torch.cuda.ExternalStream(batch.stream(), device=f"cuda:{local}")
     dev_desc, host_desc = descs(dev_pairs), descs(host_np)
 
@@ -189,21 +191,31 @@ def run_qmiv(args, world, rank, local):
     ms = ev0.elapsed_time(ev1)
     ms_max = max_over_ranks(ms, world, local)
 
-    # ---- isolated per-kernel times: the same steps with the pairs run one after another on one
-    # stream, every stage bracketed by CUDA events on that stream (the library's stage timers) ----
-    sbatch = qmiv_b200.Batch(ctx, max_pairs=PAIRS_PER_STEP, max_pixels=PAIRS_PER_STEP * W * H, erp=True, serial=True)
-    sbatch.compute(dev_desc)
-    torch.cuda.synchronize()
+    # ---- per-stage kernel times: the same steps with the library's stage timers (CUDA events on the
+    # batch stream around every stage's launch; graphs are not replayed while the timers are on) ----
     ctx.stage_times(reset=True)
     ctx.set_profiling(True)
     prof_steps = max(3, args.steps // 4)
     for _ in range(prof_steps):
-        assert sbatch.compute(dev_desc) == results, "serial and concurrent batches differ"
+        assert batch.compute(dev_desc) == results, "timed and replayed batches differ"
     torch.cuda.synchronize()
     ctx.set_profiling(False)
     stage = ctx.stage_times(reset=True)
-    sbatch.close()
     launches_per_step = sum(v[1] for k, v in stage.items() if k not in ("h2d", "d2h")) / prof_steps
+
+    # ---- the plain one-pair-per-call form on the same pairs ----
+    calc = qmiv_b200.Calc(ctx, W, H, BD, CF, search_range=2, erp=True)
+    for a, b in dev_pairs[:2]:
+        calc.compute(a, b, mask)
+    torch.cuda.synchronize()
+    p0 = time.perf_counter()
+    plain_steps = max(1, args.steps // 4)
+    for _ in range(plain_steps):
+        for i, (a, b) in enumerate(dev_pairs):
+            assert calc.compute(a, b, mask) == results[i], "plain and batched forms differ"
+    torch.cuda.synchronize()
+    plain_value = plain_steps * len(dev_pairs) / (time.perf_counter() - p0)
+    calc.close()
 
     # ---- end to end through the public API, pinned host frames (e2e) ----
     for _ in range(max(1, args.warmup // 2)):
@@ -220,6 +232,8 @@ def run_qmiv(args, world, rank, local):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, local)
     assert host_results == results, "host-frame and device-frame results differ"
 
+    cps_tile = batch.tuning(W, H, BD, 2)
+
     # ---- probes for the search kernel's roofline denominator ----
     lib = qmiv_b200.library()
     int_peak = __import__("ctypes").c_double()
@@ -233,13 +247,14 @@ def run_qmiv(args, world, rank, local):
     e2e_value = units / (e2e_ms / 1e3)
     cps_ms, cps_n = stage["cps"]
     cps_avg_ms = cps_ms / max(cps_n, 1)
-    ops_per_launch = 8.0 * cps_candidates()
+    ops_per_launch = 8.0 * cps_candidates() * PAIRS_PER_STEP  # one work-list launch covers the step's pairs
     achieved = ops_per_launch / (cps_avg_ms * 1e-3) / 1e12
     h2d = sum(frame_bytes(a) + frame_bytes(b) for a, b in pairs)
     d2h = PAIRS_PER_STEP * 632  # sizeof(PairOut), the device result block read back per pair
     return dict(value=value, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
                 achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
-                sample=results[0], launches=int(round(launches_per_step * args.steps)))
+                sample=results[0], launches=int(round(launches_per_step * args.steps)), plain=plain_value,
+                cps_tile=cps_tile)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -369,14 +384,20 @@ def main():
            "e2e": {"value": r["e2e"], "unit": "frame-pairs/s", "h2d_bytes_per_step": r["h2d"],
                    "d2h_bytes_per_step": r["d2h"]},
            "gpu_launches": None,
-           "roofline": {"kernel": "k_cps (CPS search, both directions)", "bound": "int32",
+           "roofline": {"kernel": "k_cps_multi (CPS search, both directions, work list of the step's pairs)",
+                        "bound": "int32",
                         "achieved": r["achieved"], "peak": r["int_peak"], "unit": "TOP/s",
                         "frac": r["achieved"] / r["int_peak"] if r["int_peak"] else None,
                         "traffic": None,
-                        "accounting": "8 int32 ops per candidate, 2*W*H*25 candidates per launch; peak measured "
-                                      "by qmiv_probe_int32_peak on this GPU",
-                        "avg_launch_ms": r["cps_avg_ms"]},
-           "stage_ms_per_launch_isolated": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
+                        "accounting": "8 int32 ops per candidate, 2*W*H*25 candidates per pair, "
+                                      f"{PAIRS_PER_STEP} pairs per launch; peak measured by qmiv_probe_int32_peak on "
+                                      "this GPU",
+                        "avg_launch_ms": r["cps_avg_ms"],
+                        "tile": {"w": r["cps_tile"][0], "h": r["cps_tile"][1], "pixels_per_thread": 8,
+                                 "picked_by": "autotuner (qmiv_batch_tuning)"}},
+           "plain_form": {"value": r["plain"], "unit": "frame-pairs/s",
+                          "what": "the same pairs, one qmiv_frame_pair_compute call per pair (device frames)"},
+           "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
            "clocks": r["clocks"],
            "cpu_baseline": cpu,
            "sample_result": {k: r["sample"][k] for k in ("gcd_r2t", "ivpsnr", "wspsnr_pic", "ivssim")},

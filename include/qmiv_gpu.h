@@ -236,8 +236,8 @@ typedef struct qmiv_pair_desc
    params: shared weights/coefficients (search_range is taken per pair). flags: QMIV_BATCH_*. */
 enum
 {
-  QMIV_BATCH_GRAPH  = 1,  /* replay the launch sequence from CUDA graphs keyed by the call's shape signature */
-  QMIV_BATCH_SERIAL = 2   /* run the pairs one after another on one stream (isolated per-kernel timing) */
+  QMIV_BATCH_GRAPH    = 1,  /* replay the launch sequence from CUDA graphs keyed by the call's shape signature */
+  QMIV_BATCH_AUTOTUNE = 4   /* time the CPS tile shapes on the first pair of every (W, H, bit depth, R) and keep the faster */
 };
 QMIV_API qmiv_status qmiv_batch_create(qmiv_ctx ctx, int32_t max_pairs, int64_t max_pixels, const qmiv_params* params,
                               int32_t flags, qmiv_batch* out_batch);

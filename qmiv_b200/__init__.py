@@ -245,14 +245,14 @@ class Calc:
 class Batch:
     """Many frame pairs of uneven shape per call (qmiv_batch_*)."""
 
-    GRAPH, SERIAL = 1, 2
+    GRAPH, AUTOTUNE = 1, 4
 
-    def __init__(self, ctx: Context, max_pairs: int, max_pixels: int, graph: bool = False, serial: bool = False,
+    def __init__(self, ctx: Context, max_pairs: int, max_pixels: int, graph: bool = False, autotune: bool = False,
                  **params):
         self._lib = library()
         self.ctx = ctx
         self.params = make_params(**params)
-        flags = (self.GRAPH if graph else 0) | (self.SERIAL if serial else 0)
+        flags = (self.GRAPH if graph else 0) | (self.AUTOTUNE if autotune else 0)
         h = ctypes.c_void_p()
         check(self._lib.qmiv_batch_create(ctx.handle, max_pairs, max_pixels, ctypes.byref(self.params),
                                           flags, ctypes.byref(h)), "qmiv_batch_create")
@@ -295,6 +295,7 @@ class Batch:
         return p.value or 0
 
     def tuning(self, width, height, bitdepth, search_range):
+        """(tile width, tile height, rows per thread) of the CPS work list for pairs of this kind."""
         tw, th, p = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         check(self._lib.qmiv_batch_tuning(self.handle, width, height, bitdepth, search_range, ctypes.byref(tw),
                                           ctypes.byref(th), ctypes.byref(p)), "qmiv_batch_tuning")
