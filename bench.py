@@ -149,6 +149,56 @@ def cps_candidates(R=2):
     return 2 * W * H * (2 * R + 1) ** 2
 
 
+def run_mixed(ctx, steps):
+    """The mixed-resolution set (64 pairs, resolution / bit depth / R drawn per pair; IV-PSNR + PSNR +
+    IV-SSIM): the plain form (one call per pair) against the batched form (one launch per stage,
+    graphs, autotuned tiles). Pairs of one (resolution, bit depth) share their synthetic content."""
+    import torch
+    import qmiv_b200
+    from qmiv_b200 import synth
+    specs = synth.config3_specs(64, 3)
+    pool = {}
+    for s in specs:
+        key = (s["width"], s["height"], s["bitdepth"])
+        if key not in pool:
+            f0, f1 = synth.make_pair(*key, seed=len(pool))
+            pool[key] = (tuple(torch.from_numpy(p).cuda() for p in f0), tuple(torch.from_numpy(p).cuda() for p in f1))
+    mask = qmiv_b200.IVPSNR | qmiv_b200.PSNR | qmiv_b200.IVSSIM
+    calcs = {}
+    for s in specs:
+        k = (s["width"], s["height"], s["bitdepth"], s["search_range"])
+        if k not in calcs:
+            calcs[k] = qmiv_b200.Calc(ctx, s["width"], s["height"], s["bitdepth"], 420, search_range=s["search_range"])
+
+    def plain():
+        return [calcs[(s["width"], s["height"], s["bitdepth"], s["search_range"])].compute(
+            *pool[(s["width"], s["height"], s["bitdepth"])], mask) for s in specs]
+
+    descs = [dict(frame0=pool[(s["width"], s["height"], s["bitdepth"])][0],
+                  frame1=pool[(s["width"], s["height"], s["bitdepth"])][1], width=s["width"], height=s["height"],
+                  bitdepth=s["bitdepth"], search_range=s["search_range"], metrics=mask) for s in specs]
+    batch = qmiv_b200.Batch(ctx, len(specs), sum(s["width"] * s["height"] for s in specs), graph=True, autotune=True)
+    out = {}
+    for name, fn in (("plain", plain), ("batched", lambda: batch.compute(descs))):
+        for _ in range(3):
+            r = fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            r = fn()
+        torch.cuda.synchronize()
+        out[name] = steps * len(specs) / (time.perf_counter() - t0)
+        out[name + "_results"] = r
+    assert out.pop("plain_results") == out.pop("batched_results"), "plain and batched forms differ on the mixed set"
+    batch.close()
+    for c in calcs.values():
+        c.close()
+    return {"plain_pairs_s": out["plain"], "batched_pairs_s": out["batched"],
+            "batched_over_plain": out["batched"] / out["plain"], "pairs": len(specs),
+            "set": "64 pairs, resolution from {1280x720, 1920x1080, 2048x2048, 4096x2048}, bit depth {8, 10}, "
+                   "R {2, 4}, IV-PSNR + PSNR + IV-SSIM, device frames"}
+
+
 def run_qmiv(args, world, rank, local):
     import torch
     import qmiv_b200
@@ -233,6 +283,7 @@ def run_qmiv(args, world, rank, local):
     assert host_results == results, "host-frame and device-frame results differ"
 
     cps_tile = batch.tuning(W, H, BD, 2)
+    mixed = run_mixed(ctx, max(3, args.steps // 4)) if (world == 1 and not args.no_mixed) else None
 
     # ---- probes for the search kernel's roofline denominator ----
     lib = qmiv_b200.library()
@@ -254,7 +305,7 @@ def run_qmiv(args, world, rank, local):
     return dict(value=value, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
                 achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
                 sample=results[0], launches=int(round(launches_per_step * args.steps)), plain=plain_value,
-                cps_tile=cps_tile)
+                cps_tile=cps_tile, mixed=mixed)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -313,6 +364,7 @@ def main():
     ap.add_argument("--impl", choices=["qmiv", "reference"], default="qmiv")
     ap.add_argument("--cpu-frames", type=int, default=4, help="frames of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the plain-vs-batched mixed-resolution comparison")
     ap.add_argument("--size", default=None, help="WxH of a smaller profiling case (not a bench line)")
     ap.add_argument("--pairs", type=int, default=None, help="pairs per step of a smaller profiling case")
     args = ap.parse_args()
@@ -397,6 +449,7 @@ def main():
                                  "picked_by": "autotuner (qmiv_batch_tuning)"}},
            "plain_form": {"value": r["plain"], "unit": "frame-pairs/s",
                           "what": "the same pairs, one qmiv_frame_pair_compute call per pair (device frames)"},
+           "mixed_set": r["mixed"],
            "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
            "clocks": r["clocks"],
            "cpu_baseline": cpu,
