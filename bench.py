@@ -149,6 +149,58 @@ def cps_candidates(R=2):
     return 2 * W * H * (2 * R + 1) ** 2
 
 
+def frame_pool(specs):
+    """Device-resident synthetic pairs, one per (width, height, bit depth) of the specs."""
+    import torch
+    from qmiv_b200 import synth
+    pool = {}
+    for s in specs:
+        key = (s["width"], s["height"], s["bitdepth"])
+        if key not in pool:
+            f0, f1 = synth.make_pair(*key, seed=len(pool))
+            pool[key] = (tuple(torch.from_numpy(p).cuda() for p in f0), tuple(torch.from_numpy(p).cuda() for p in f1))
+    return pool
+
+
+def run_serve(ctx, duration_s, rate=200.0):
+    """The serving loop on a seeded Poisson stream of requests (rate per second, each 1..32 pairs of one
+    shape and metric set drawn as the mixed set), frames resident on the device, 40 GB HBM budget."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    reqs = synth.config4_requests(duration_s, rate, seed=4)
+    pool = frame_pool([s for r in reqs for s in r.specs])
+    sctx = qmiv_b200.Context(ctx.device, hbm_budget=40 << 30)
+    srv = qmiv_b200.Server(sctx, max_batch_pairs=64, max_batch_pixels=64 * 4096 * 2048, workers=2)
+    # warm-up: every (shape, R) kind once, so kernels are configured and tiles tuned before the stream
+    seen = set()
+    for r in reqs:
+        s0 = r.specs[0]
+        k = (s0["width"], s0["height"], s0["bitdepth"], s0["search_range"], r.metrics)
+        if k not in seen:
+            seen.add(k)
+            srv.wait(srv.submit([pool[k[:3]]], *k[:3], search_range=k[3], metrics=r.metrics))
+    srv.stats(reset=True)
+    tickets = []
+    t0 = time.perf_counter()
+    for r in reqs:
+        delay = t0 + r.arrival_s - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        s0 = r.specs[0]
+        key = (s0["width"], s0["height"], s0["bitdepth"])
+        tickets.append(srv.submit([pool[key]] * len(r.specs), *key, search_range=s0["search_range"],
+                                  metrics=r.metrics))
+    for t in tickets:
+        srv.wait(t)
+    st = srv.stats()
+    srv.close()
+    sctx.close()
+    return {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "pairs_per_s": st["pairs_per_s"],
+            "requests": st["completed"], "pairs": sum(len(r.specs) for r in reqs), "rate_per_s": rate,
+            "duration_s": duration_s, "workers": 2, "hbm_budget_gb": 40,
+            "what": "Poisson arrivals, 1-32 pairs per request drawn as the mixed set, device-resident frames"}
+
+
 def run_mixed(ctx, steps):
     """The mixed-resolution set (64 pairs, resolution / bit depth / R drawn per pair; IV-PSNR + PSNR +
     IV-SSIM): the plain form (one call per pair) against the batched form (one launch per stage,
@@ -157,12 +209,7 @@ def run_mixed(ctx, steps):
     import qmiv_b200
     from qmiv_b200 import synth
     specs = synth.config3_specs(64, 3)
-    pool = {}
-    for s in specs:
-        key = (s["width"], s["height"], s["bitdepth"])
-        if key not in pool:
-            f0, f1 = synth.make_pair(*key, seed=len(pool))
-            pool[key] = (tuple(torch.from_numpy(p).cuda() for p in f0), tuple(torch.from_numpy(p).cuda() for p in f1))
+    pool = frame_pool(specs)
     mask = qmiv_b200.IVPSNR | qmiv_b200.PSNR | qmiv_b200.IVSSIM
     calcs = {}
     for s in specs:
@@ -284,6 +331,7 @@ def run_qmiv(args, world, rank, local):
 
     cps_tile = batch.tuning(W, H, BD, 2)
     mixed = run_mixed(ctx, max(3, args.steps // 4)) if (world == 1 and not args.no_mixed) else None
+    serve = run_serve(ctx, args.serve_seconds) if (world == 1 and args.serve_seconds > 0) else None
 
     # ---- probes for the search kernel's roofline denominator ----
     lib = qmiv_b200.library()
@@ -305,7 +353,7 @@ def run_qmiv(args, world, rank, local):
     return dict(value=value, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
                 achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
                 sample=results[0], launches=int(round(launches_per_step * args.steps)), plain=plain_value,
-                cps_tile=cps_tile, mixed=mixed)
+                cps_tile=cps_tile, mixed=mixed, serve=serve)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -365,6 +413,7 @@ def main():
     ap.add_argument("--cpu-frames", type=int, default=4, help="frames of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the plain-vs-batched mixed-resolution comparison")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="length of the serving-loop arrival stream (0: skip)")
     ap.add_argument("--size", default=None, help="WxH of a smaller profiling case (not a bench line)")
     ap.add_argument("--pairs", type=int, default=None, help="pairs per step of a smaller profiling case")
     args = ap.parse_args()
@@ -450,6 +499,7 @@ def main():
            "plain_form": {"value": r["plain"], "unit": "frame-pairs/s",
                           "what": "the same pairs, one qmiv_frame_pair_compute call per pair (device frames)"},
            "mixed_set": r["mixed"],
+           "serve": r["serve"],
            "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
            "clocks": r["clocks"],
            "cpu_baseline": cpu,

@@ -249,6 +249,53 @@ QMIV_API qmiv_status qmiv_batch_stream(qmiv_batch batch, void** cuda_stream);
 QMIV_API qmiv_status qmiv_batch_tuning(qmiv_batch batch, int32_t width, int32_t height, int32_t bitdepth, int32_t search_range,
                               int32_t* cps_tile_w, int32_t* cps_tile_h, int32_t* cps_rows_per_thread);
 
+/* ---- serving loop: sequences of frame pairs admitted by HBM budget, continuously batched ------ */
+/* No reference counterpart: the reference app processes one sequence per process.
+   A request is a sequence of frame pairs of one shape and metric set. At admission its frames are
+   made resident on the device (host frames are copied into memory counted against the context's
+   HBM budget; device frames are used in place and must stay valid until the request completes);
+   a request whose frames do not fit waits until completed requests free memory, and a request
+   larger than the whole budget is rejected at submission. Worker threads, each with its own batched
+   engine and stream, repeatedly take the next pending pairs of all admitted requests (in arrival
+   order, up to max_batch_pairs / max_batch_pixels per launch sequence), so requests that arrive
+   while others are on the GPU join the next batch and their work overlaps on the device. A pair's
+   result does not depend on the batch it ran in. */
+
+typedef struct qmiv_request
+{
+  int32_t           width, height, bitdepth, chroma_format;
+  int32_t           search_range;   /* 1..5 */
+  uint32_t          metric_mask;
+  int32_t           num_pairs;
+  const qmiv_frame* in0;            /* [num_pairs] */
+  const qmiv_frame* in1;            /* [num_pairs] */
+} qmiv_request;
+
+typedef struct qmiv_request_stats
+{
+  double  submit_ms, admit_ms, done_ms;  /* since the server's creation (steady clock) */
+  double  latency_ms;                    /* done - submit */
+  int32_t batches;                       /* launch sequences the request's pairs ran in */
+  /* sequence means over the request's pairs, as the reference's per-sequence averages:
+     compensated sum in frame order / number of frames (apps/QMIV/src/xMetricQMIV.cpp:98-102) */
+  double  mean_psnr_pic, mean_wspsnr_pic, mean_ivpsnr, mean_ssim_pic, mean_msssim_pic, mean_ivssim, mean_ivmsssim;
+} qmiv_request_stats;
+
+/* workers: engines running concurrently (1..4). params as for qmiv_batch_create. */
+QMIV_API qmiv_status qmiv_server_create(qmiv_ctx ctx, const qmiv_params* params, int32_t max_batch_pairs,
+                               int64_t max_batch_pixels, int32_t workers, qmiv_server* out_server);
+/* Waits for every admitted and queued request, then stops the workers. */
+QMIV_API qmiv_status qmiv_server_destroy(qmiv_server server);
+QMIV_API qmiv_status qmiv_server_submit(qmiv_server server, const qmiv_request* request, uint64_t* ticket);
+/* Waits up to timeout_ms (< 0: no limit) for a request; results: [num_pairs] or null; stats may be
+   null. A ticket is released by a successful wait. QMIV_ERR_TIMEOUT leaves it pending. */
+QMIV_API qmiv_status qmiv_server_wait(qmiv_server server, uint64_t ticket, int32_t timeout_ms, qmiv_result* results,
+                             qmiv_request_stats* stats);
+/* Latency percentiles (nearest rank) of the requests completed since the last reset (or creation), and
+   pairs completed per second from the reset to the last completion. */
+QMIV_API qmiv_status qmiv_server_stats(qmiv_server server, double* p50_ms, double* p99_ms, double* pairs_per_s,
+                              int64_t* completed_requests, int32_t reset);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,7 +27,7 @@ from ._lib import (ALL, IVMSSSIM, IVPSNR, IVSSIM, METRIC_BITS, MSSSIM, PSNR, SSI
                    PEL_STOP, PEL_WARN, QmivError, check)
 
 __all__ = ["Context", "Calc", "Batch", "make_params", "metric_mask", "QmivError", "library",
-           "PSNR", "WSPSNR", "IVPSNR", "SSIM", "MSSSIM", "IVSSIM", "IVMSSSIM", "ALL"]
+           "PSNR", "WSPSNR", "IVPSNR", "SSIM", "MSSSIM", "IVSSIM", "IVMSSSIM", "ALL", "Server"]
 
 
 def library():
@@ -300,3 +300,67 @@ class Batch:
         check(self._lib.qmiv_batch_tuning(self.handle, width, height, bitdepth, search_range, ctypes.byref(tw),
                                           ctypes.byref(th), ctypes.byref(p)), "qmiv_batch_tuning")
         return tw.value, th.value, p.value
+
+
+class Server:
+    """Serving loop (qmiv_server_*): sequences of frame pairs admitted by HBM budget and continuously
+    batched over `workers` engines. Frames handed to submit() must stay alive until wait() returns."""
+
+    def __init__(self, ctx: Context, max_batch_pairs: int = 64, max_batch_pixels: int = 64 * 4096 * 2048,
+                 workers: int = 2, **params):
+        self._lib = library()
+        self.ctx = ctx
+        self.params = make_params(**params)
+        h = ctypes.c_void_p()
+        check(self._lib.qmiv_server_create(ctx.handle, ctypes.byref(self.params), max_batch_pairs, max_batch_pixels,
+                                           workers, ctypes.byref(h)), "qmiv_server_create")
+        self.handle = h
+        self._keep = {}
+
+    def close(self):
+        if self.handle:
+            check(self._lib.qmiv_server_destroy(self.handle), "qmiv_server_destroy")
+            self.handle = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, pairs, width, height, bitdepth, chroma_format=420, search_range=2, metrics=None) -> int:
+        """pairs: list of (frame0, frame1); every frame a tuple of three planes (numpy or CUDA arrays)."""
+        pairs = list(pairs)
+        n = len(pairs)
+        a0, a1 = (_lib.QmivFrame * max(1, n))(), (_lib.QmivFrame * max(1, n))()
+        keep = [a0, a1]
+        for i, (f0, f1) in enumerate(pairs):
+            a0[i], k0 = make_frame(f0)
+            a1[i], k1 = make_frame(f1)
+            keep += [k0, k1]
+        req = _lib.QmivRequest(width, height, bitdepth, chroma_format, search_range, metric_mask(metrics), n,
+                               ctypes.cast(a0, ctypes.POINTER(_lib.QmivFrame)),
+                               ctypes.cast(a1, ctypes.POINTER(_lib.QmivFrame)))
+        t = ctypes.c_uint64()
+        check(self._lib.qmiv_server_submit(self.handle, ctypes.byref(req), ctypes.byref(t)), "qmiv_server_submit")
+        self._keep[t.value] = (keep, n)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(per-pair result dicts, request statistics dict)."""
+        entry = self._keep.get(ticket)
+        n = entry[1] if entry else 0
+        out = (_lib.QmivResult * max(1, n))()
+        st = _lib.QmivRequestStats()
+        check(self._lib.qmiv_server_wait(self.handle, ticket, timeout_ms, out if n else None, ctypes.byref(st)),
+              "qmiv_server_wait")
+        self._keep.pop(ticket, None)
+        return [out[i].as_dict() for i in range(n)], st.as_dict()
+
+    def stats(self, reset: bool = False) -> dict:
+        p50, p99, pps = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        done = ctypes.c_int64()
+        check(self._lib.qmiv_server_stats(self.handle, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(pps),
+                                          ctypes.byref(done), int(bool(reset))), "qmiv_server_stats")
+        return {"p50_ms": p50.value, "p99_ms": p99.value, "pairs_per_s": pps.value, "completed": done.value}

@@ -65,6 +65,24 @@ class QmivPairDesc(ctypes.Structure):
                 ("metric_mask", ctypes.c_uint32)]
 
 
+class QmivRequest(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("bitdepth", ctypes.c_int32),
+                ("chroma_format", ctypes.c_int32), ("search_range", ctypes.c_int32), ("metric_mask", ctypes.c_uint32),
+                ("num_pairs", ctypes.c_int32), ("in0", ctypes.POINTER(QmivFrame)), ("in1", ctypes.POINTER(QmivFrame))]
+
+
+class QmivRequestStats(ctypes.Structure):
+    _fields_ = [("submit_ms", ctypes.c_double), ("admit_ms", ctypes.c_double), ("done_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double), ("batches", ctypes.c_int32),
+                ("mean_psnr_pic", ctypes.c_double), ("mean_wspsnr_pic", ctypes.c_double),
+                ("mean_ivpsnr", ctypes.c_double), ("mean_ssim_pic", ctypes.c_double),
+                ("mean_msssim_pic", ctypes.c_double), ("mean_ivssim", ctypes.c_double),
+                ("mean_ivmsssim", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # name -> (restype, argtypes); every symbol include/qmiv_gpu.h declares
 _P = ctypes.c_void_p
 _PP = ctypes.POINTER(ctypes.c_void_p)
@@ -105,6 +123,14 @@ SIGNATURES = {
     "qmiv_batch_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                          ctypes.POINTER(ctypes.c_int32)]),
+    "qmiv_server_create": (ctypes.c_int, [_P, ctypes.POINTER(QmivParams), ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
+                                          _PP]),
+    "qmiv_server_destroy": (ctypes.c_int, [_P]),
+    "qmiv_server_submit": (ctypes.c_int, [_P, ctypes.POINTER(QmivRequest), ctypes.POINTER(ctypes.c_uint64)]),
+    "qmiv_server_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(QmivResult),
+                                        ctypes.POINTER(QmivRequestStats)]),
+    "qmiv_server_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
 }
 
 _lib = None

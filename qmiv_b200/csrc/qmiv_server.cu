@@ -1,0 +1,371 @@
+// Serving loop (qmiv_server_*): requests (sequences of frame pairs) admitted by HBM budget and
+// continuously batched over worker engines.
+//
+//   submit   validates the request and queues it (rejects one larger than the whole budget)
+//   admit    a worker moves queued requests, in arrival order, to the admitted set while their
+//            resident frames fit the budget: host frames are copied into device memory counted
+//            against the context's budget, device frames are used in place
+//   batch    each worker takes the next pending pairs of all admitted requests, in arrival order,
+//            up to max_batch_pairs / max_batch_pixels, and runs them through its own engine
+//            (own stream), so two workers keep two launch sequences in flight
+//   finish   when a request's last pair is done its resident frames are freed, the sequence means
+//            are formed, and waiters are woken
+#include "qmiv_engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+using namespace qmiv;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request
+{
+  uint64_t     ticket = 0;
+  qmiv_request desc{};
+  std::vector<qmiv_frame> in0, in1;       // caller frames (or resident copies after admission)
+  DevMem       resident;                  // device copies of host frames
+  size_t       resident_bytes = 0;
+  int32_t      next = 0;                  // next pair to schedule
+  int32_t      done = 0;                  // pairs finished
+  int32_t      batches = 0;
+  bool         admitted = false, finished = false;
+  qmiv_status  status = QMIV_OK;
+  std::vector<qmiv_result> results;
+  double       submit_ms = 0, admit_ms = 0, done_ms = 0;
+};
+
+// Neumaier compensated sum in order, then / n (xMetricQMIV.cpp:98-102 with xKBNS.h:36-43)
+double seq_mean(const std::vector<qmiv_result>& r, double qmiv_result::*field)
+{
+  double s = 0.0, c = 0.0;
+  for(const qmiv_result& x : r)
+  {
+    const double v = x.*field;
+    const double t = s + v;
+    if(std::fabs(s) >= std::fabs(v)) { c += (s - t) + v; } else { c += (v - t) + s; }
+    s = t;
+  }
+  return (s + c) / (double)r.size();
+}
+
+}  // namespace
+
+struct qmiv_server_s
+{
+  qmiv_ctx_s*  ctx = nullptr;
+  qmiv_params  prm{};
+  int32_t      max_batch_pairs = 0;
+  int64_t      max_batch_pixels = 0;
+  Clock::time_point t0;
+  std::mutex   mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<Request>> queued;      // not admitted yet
+  std::vector<std::shared_ptr<Request>> admitted;   // in arrival order
+  std::unordered_map<uint64_t, std::shared_ptr<Request>> by_ticket;
+  uint64_t     next_ticket = 1;
+  bool         stopping = false;
+  std::vector<std::unique_ptr<Engine>> engines;
+  std::vector<std::thread> workers;
+  // statistics since the last reset
+  std::vector<double> latencies;
+  int64_t      pairs_done = 0;
+  double       window_start_ms = 0;
+  double       last_done_ms = 0;
+
+  double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+  void   worker(int w);
+  bool   admit_locked();
+};
+
+static size_t frame_device_bytes(const Shape& S) { return 2 * S.staged_frame_bytes(); }
+
+// Moves queued requests into the admitted set while their resident frames fit. Called with mu held.
+bool qmiv_server_s::admit_locked()
+{
+  bool any = false;
+  while(!queued.empty())
+  {
+    std::shared_ptr<Request> r = queued.front();
+    Shape S;
+    S.init(r->desc.width, r->desc.height, r->desc.bitdepth, r->desc.chroma_format);
+    if(r->resident_bytes > 0 && r->resident.alloc(ctx, r->resident_bytes) != QMIV_OK)
+    {
+      bool busy = false;
+      for(auto& a : admitted) { busy = busy || !a->finished; }
+      if(busy) { break; }   // budget full: wait for admitted requests to free memory, keep the order
+      // nothing admitted will free memory: the request cannot fit beside the engines' working memory
+      r->status = fail(QMIV_ERR_BUDGET, "request frames do not fit the HBM budget beside the engines' working memory");
+      r->resident_bytes = 0;
+    }
+    if(r->resident_bytes > 0)
+    {
+      char* base = r->resident.as<char>();
+      cudaError_t e = cudaSuccess;
+      for(int i = 0; i < r->desc.num_pairs && e == cudaSuccess; i++)
+      {
+        for(int f = 0; f < 2 && e == cudaSuccess; f++)
+        {
+          qmiv_frame& fr = f ? r->in1[i] : r->in0[i];
+          if(fr.mem != QMIV_MEM_HOST) { continue; }
+          size_t off = ((size_t)i * 2 + f) * S.staged_frame_bytes();
+          for(int c = 0; c < 3 && e == cudaSuccess; c++)
+          {
+            char* dst = base + off;
+            const size_t row = S.plane_cols(c) * S.esz;
+            e = cudaMemcpy2D(dst, S.staged_pitch(c), fr.plane[c], (size_t)fr.pitch[c], row, S.plane_rows(c), cudaMemcpyHostToDevice);
+            fr.plane[c] = dst;
+            fr.pitch[c] = (int64_t)S.staged_pitch(c);
+            off += S.staged_plane_bytes(c);
+          }
+          fr.mem = QMIV_MEM_DEVICE;
+        }
+      }
+      if(e != cudaSuccess) { r->status = cuda_fail(e, "server frame upload"); }
+    }
+    queued.pop_front();
+    r->admitted = true;
+    r->admit_ms = now_ms();
+    admitted.push_back(r);
+    any = true;
+  }
+  return any;
+}
+
+void qmiv_server_s::worker(int w)
+{
+  cudaSetDevice(ctx->device);
+  Engine& eng = *engines[w];
+  std::vector<qmiv_pair_desc> descs;
+  std::vector<std::pair<std::shared_ptr<Request>, int>> owners;
+  std::vector<qmiv_result> out;
+  for(;;)
+  {
+    descs.clear();
+    owners.clear();
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      for(;;)
+      {
+        admit_locked();
+        // next pending pairs of the admitted requests, in arrival order
+        int64_t px = 0;
+        for(auto& r : admitted)
+        {
+          if(r->status != QMIV_OK) { continue; }
+          const int64_t ppx = (int64_t)r->desc.width * r->desc.height;
+          bool counted = false;
+          while(r->next < r->desc.num_pairs && (int)descs.size() < max_batch_pairs && px + ppx <= max_batch_pixels)
+          {
+            qmiv_pair_desc d{};
+            d.in0 = r->in0[r->next]; d.in1 = r->in1[r->next];
+            d.width = r->desc.width; d.height = r->desc.height; d.bitdepth = r->desc.bitdepth;
+            d.chroma_format = r->desc.chroma_format; d.search_range = r->desc.search_range; d.metric_mask = r->desc.metric_mask;
+            descs.push_back(d);
+            owners.emplace_back(r, r->next);
+            r->next++;
+            px += ppx;
+            if(!counted) { r->batches++; counted = true; }
+          }
+          if((int)descs.size() >= max_batch_pairs) { break; }
+        }
+        // requests that failed at admission finish without running
+        for(auto& r : admitted)
+        {
+          if(r->status != QMIV_OK && !r->finished)
+          {
+            r->finished = true;
+            r->done_ms = now_ms();
+            r->resident.release();
+            cv_done.notify_all();
+          }
+        }
+        if(!descs.empty()) { break; }
+        if(stopping && queued.empty())
+        {
+          bool busy = false;
+          for(auto& r : admitted) { busy = busy || !r->finished; }
+          if(!busy) { return; }
+        }
+        cv_work.wait_for(lk, std::chrono::milliseconds(2));
+      }
+    }
+    out.assign(descs.size(), qmiv_result{});
+    const qmiv_status st = eng.run(descs.data(), (int32_t)descs.size(), out.data());
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      const double t = now_ms();
+      for(size_t k = 0; k < owners.size(); k++)
+      {
+        Request& r = *owners[k].first;
+        r.results[owners[k].second] = out[k];
+        if(st != QMIV_OK && r.status == QMIV_OK) { r.status = st; }
+        r.done++;
+        pairs_done++;
+        if(r.done == r.desc.num_pairs && !r.finished)
+        {
+          r.finished = true;
+          r.done_ms = t;
+          r.resident.release();
+          latencies.push_back(r.done_ms - r.submit_ms);
+          last_done_ms = t;
+        }
+      }
+      // drop finished requests from the admitted list (their tickets stay until waited on)
+      std::vector<std::shared_ptr<Request>> keep;
+      for(auto& r : admitted) { if(!r->finished) { keep.push_back(r); } }
+      admitted.swap(keep);
+    }
+    cv_done.notify_all();
+    cv_work.notify_all();
+  }
+}
+
+extern "C" {
+
+qmiv_status qmiv_server_create(qmiv_ctx ctx, const qmiv_params* params, int32_t max_batch_pairs, int64_t max_batch_pixels,
+                               int32_t workers, qmiv_server* out_server)
+{
+  if(!ctx || !out_server || max_batch_pairs <= 0 || max_batch_pixels <= 0 || workers < 1 || workers > 4)
+  {
+    return fail(QMIV_ERR_INVALID_ARG, "bad server arguments");
+  }
+  *out_server = nullptr;
+  qmiv_params prm;
+  if(params) { prm = *params; } else { qmiv_params_default(&prm); }
+  QMIV_TRY(validate_params(prm));
+  std::unique_ptr<qmiv_server_s> s(new qmiv_server_s());
+  s->ctx = ctx; s->prm = prm; s->max_batch_pairs = max_batch_pairs; s->max_batch_pixels = max_batch_pixels;
+  s->t0 = Clock::now();
+  for(int w = 0; w < workers; w++)
+  {
+    s->engines.emplace_back(new Engine());
+    QMIV_TRY(s->engines.back()->init(ctx, prm, max_batch_pairs, max_batch_pixels, QMIV_BATCH_GRAPH | QMIV_BATCH_AUTOTUNE));
+  }
+  qmiv_server_s* sp = s.get();
+  for(int w = 0; w < workers; w++) { s->workers.emplace_back([sp, w] { sp->worker(w); }); }
+  *out_server = s.release();
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_server_destroy(qmiv_server s)
+{
+  if(!s) { return fail(QMIV_ERR_INVALID_ARG, "server is null"); }
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+  }
+  s->cv_work.notify_all();
+  for(std::thread& t : s->workers) { t.join(); }
+  delete s;
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_server_submit(qmiv_server s, const qmiv_request* req, uint64_t* ticket)
+{
+  if(!s || !req || !ticket) { return fail(QMIV_ERR_INVALID_ARG, "null argument"); }
+  if(req->num_pairs <= 0 || !req->in0 || !req->in1) { return fail(QMIV_ERR_INVALID_ARG, "a request needs at least one pair"); }
+  if((req->metric_mask & ~(uint32_t)QMIV_ALL) != 0) { return fail(QMIV_ERR_INVALID_ARG, "unknown metric bits"); }
+  if((int64_t)req->width * req->height > s->max_batch_pixels) { return fail(QMIV_ERR_INVALID_ARG, "picture larger than max_batch_pixels"); }
+  Shape S;
+  QMIV_TRY(S.init(req->width, req->height, req->bitdepth, req->chroma_format));
+  qmiv_params p = s->prm;
+  p.search_range = req->search_range;
+  QMIV_TRY(validate_params(p));
+  std::shared_ptr<Request> r(new Request());
+  r->desc = *req;
+  r->in0.assign(req->in0, req->in0 + req->num_pairs);
+  r->in1.assign(req->in1, req->in1 + req->num_pairs);
+  size_t host_frames = 0;
+  for(int i = 0; i < req->num_pairs; i++)
+  {
+    if(r->in0[i].mem == QMIV_MEM_HOST || r->in1[i].mem == QMIV_MEM_HOST) { host_frames++; }
+  }
+  // resident copies: a full pair slot for every pair with a host frame
+  r->resident_bytes = host_frames ? (size_t)req->num_pairs * frame_device_bytes(S) : 0;
+  uint64_t used = 0, budget = 0;
+  qmiv_ctx_memory(s->ctx, &used, &budget);
+  if(budget != 0 && r->resident_bytes > budget) { return fail(QMIV_ERR_BUDGET, "request larger than the whole HBM budget"); }
+  r->results.assign(req->num_pairs, qmiv_result{});
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if(s->stopping) { return fail(QMIV_ERR_INVALID_ARG, "server is stopping"); }
+    r->ticket = s->next_ticket++;
+    r->submit_ms = s->now_ms();
+    s->queued.push_back(r);
+    s->by_ticket[r->ticket] = r;
+    *ticket = r->ticket;
+  }
+  s->cv_work.notify_all();
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_server_wait(qmiv_server s, uint64_t ticket, int32_t timeout_ms, qmiv_result* results,
+                             qmiv_request_stats* stats)
+{
+  if(!s) { return fail(QMIV_ERR_INVALID_ARG, "server is null"); }
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->by_ticket.find(ticket);
+  if(it == s->by_ticket.end()) { return fail(QMIV_ERR_INVALID_ARG, "unknown ticket"); }
+  std::shared_ptr<Request> r = it->second;
+  auto ready = [&] { return r->finished; };
+  if(timeout_ms < 0) { s->cv_done.wait(lk, ready); }
+  else if(!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+  {
+    return fail(QMIV_ERR_TIMEOUT, "request not finished within the timeout");
+  }
+  s->by_ticket.erase(it);
+  if(results) { for(int i = 0; i < r->desc.num_pairs; i++) { results[i] = r->results[i]; } }
+  if(stats)
+  {
+    qmiv_request_stats& st = *stats;
+    st.submit_ms = r->submit_ms; st.admit_ms = r->admit_ms; st.done_ms = r->done_ms;
+    st.latency_ms = r->done_ms - r->submit_ms;
+    st.batches = r->batches;
+    st.mean_psnr_pic = seq_mean(r->results, &qmiv_result::psnr_pic);
+    st.mean_wspsnr_pic = seq_mean(r->results, &qmiv_result::wspsnr_pic);
+    st.mean_ivpsnr = seq_mean(r->results, &qmiv_result::ivpsnr);
+    st.mean_ssim_pic = seq_mean(r->results, &qmiv_result::ssim_pic);
+    st.mean_msssim_pic = seq_mean(r->results, &qmiv_result::msssim_pic);
+    st.mean_ivssim = seq_mean(r->results, &qmiv_result::ivssim);
+    st.mean_ivmsssim = seq_mean(r->results, &qmiv_result::ivmsssim);
+  }
+  return r->status;
+}
+
+qmiv_status qmiv_server_stats(qmiv_server s, double* p50_ms, double* p99_ms, double* pairs_per_s,
+                              int64_t* completed_requests, int32_t reset)
+{
+  if(!s) { return fail(QMIV_ERR_INVALID_ARG, "server is null"); }
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::vector<double> l = s->latencies;
+  std::sort(l.begin(), l.end());
+  auto pct = [&](double q) -> double {
+    if(l.empty()) { return 0.0; }
+    size_t k = (size_t)std::ceil(q * (double)l.size());   // nearest rank
+    k = k == 0 ? 0 : k - 1;
+    return l[std::min(k, l.size() - 1)];
+  };
+  if(p50_ms) { *p50_ms = pct(0.50); }
+  if(p99_ms) { *p99_ms = pct(0.99); }
+  const double span = s->last_done_ms - s->window_start_ms;
+  if(pairs_per_s) { *pairs_per_s = span > 0 ? (double)s->pairs_done / (span / 1e3) : 0.0; }
+  if(completed_requests) { *completed_requests = (int64_t)l.size(); }
+  if(reset)
+  {
+    s->latencies.clear();
+    s->pairs_done = 0;
+    s->window_start_ms = s->now_ms();
+    s->last_done_ms = s->window_start_ms;
+  }
+  return QMIV_OK;
+}
+
+}  // extern "C"
