@@ -5,7 +5,7 @@
 // needs to be stored) or from k_ssim_moments (plain SSIM, MS-SSIM scales, which also writes the
 // next scale's 2x2 mean, xPixelOpsSTD.cpp:50-67). k_ssim_pool evaluates every window in FP64 with the
 // reference's operation order and sums each window row in x order with the compensated sum, one
-// lane per row, from shared memory.
+// lane per row, while other warps evaluate the next windows.
 #include "qmiv_kernels.cuh"
 
 namespace qmiv {
@@ -107,63 +107,71 @@ template cudaError_t launch_ssim_moments<uint8_t>(const SsimMomArgs&, cudaStream
 template cudaError_t launch_ssim_moments<uint16_t>(const SsimMomArgs&, cudaStream_t);
 
 // =============================================================================================
-// windows + ordered row sums. A CTA owns kBandJ window rows of one job and walks the row in chunks
-// of 32 windows: the chunk's (kBandJ+1) x 33 sub-block moments are staged in shared memory (the
-// next chunk's global loads are issued before the current chunk is evaluated), every thread
-// evaluates one window, and lane j of warp 0 adds the chunk's 32 values of row j in x order.
+// windows + ordered row sums (xSSIM.cpp:353-369). A CTA owns kPoolRows = 32 window rows of one job
+// and walks them in chunks of kPoolCW = 8 windows. Eight producer warps stage the chunk's 33 x 9
+// sub-block moments in shared memory (double-buffered, the next chunk's global loads in flight) and
+// evaluate one window per thread; a ninth warp keeps the 32 compensated row sums, lane j adding row
+// j's values in x order. Window values pass through two shared buffers guarded by named barriers
+// (full: producers -> summing warp, empty: summing warp -> producers), so evaluation and the serial
+// sums overlap and one warp instruction advances 32 row sums.
 // =============================================================================================
-constexpr int kBandJ = 8;                       // window rows per CTA
-constexpr int kChunkI = 32;                     // windows per chunk
-constexpr int kSubR = kBandJ + 1, kSubC = kChunkI + 1;
-constexpr int kStageN = 5 * kSubR * kSubC;      // staged moment values per chunk
-constexpr int kStagePerThread = (kStageN + 255) / 256;
+constexpr int kPoolRows = 32, kPoolCW = 8, kPoolEval = 256, kPoolThreads = kPoolEval + 32;
+constexpr int kPSubR = kPoolRows + 1, kPSubC = kPoolCW + 1;
+constexpr int kPStage = 5 * kPSubR * kPSubC;                       // staged moment values per chunk
+constexpr int kPPer = (kPStage + kPoolEval - 1) / kPoolEval;       // per producer thread
+enum { kBarFull0 = 1, kBarEmpty0 = 3, kBarStage = 5 };            // named barrier ids (0 = __syncthreads)
+
+__device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ void bar_arrive(int id, int n) { asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 
 __device__ __forceinline__ void ssim_pool_body(const SsimPoolJob& J)
 {
-  __shared__ uint32_t st[2][5][kSubR][kSubC];
-  __shared__ double vals[kBandJ][kChunkI + 1];
-  const int j0 = blockIdx.x * kBandJ;
+  __shared__ uint32_t st[2][5][kPSubR][kPSubC];
+  __shared__ double vals[2][kPoolRows][kPoolCW + 1];
+  const int j0 = blockIdx.x * kPoolRows;
   if(j0 >= J.ny) { return; }
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int nchunks = (J.nx + kChunkI - 1) / kChunkI;
-  const int nby = J.ny + 1, nbx = J.nx + 1;  // sub-blocks any window of this job touches
-
-  uint32_t reg[kStagePerThread];
-  auto load = [&](int k) {
-    #pragma unroll
-    for(int r = 0; r < kStagePerThread; r++)
-    {
-      const int e = threadIdx.x + 256 * r;
-      uint32_t v = 0;
-      if(e < kStageN)
-      {
-        const int m = e / (kSubR * kSubC), rem = e - m * (kSubR * kSubC);
-        const int sy = rem / kSubC, sx = rem - sy * kSubC;
-        const int gy = j0 + sy, gx = k * kChunkI + sx;
-        if(gy < nby && gx < nbx) { v = __ldg(J.mom + (size_t)m * J.plane + (size_t)gy * J.pitch + gx); }
-      }
-      reg[r] = v;
-    }
-  };
-  auto store = [&](int buf) {
-    #pragma unroll
-    for(int r = 0; r < kStagePerThread; r++)
-    {
-      const int e = threadIdx.x + 256 * r;
-      if(e < kStageN) { (&st[buf][0][0][0])[e] = reg[r]; }
-    }
-  };
-
-  Kbns row;
-  load(0);
-  store(0);
-  __syncthreads();
-  for(int k = 0; k < nchunks; k++)
+  const int nchunks = (J.nx + kPoolCW - 1) / kPoolCW;
+  const int t = threadIdx.x;
+  if(t < kPoolEval)
   {
-    const int buf = k & 1;
-    if(k + 1 < nchunks) { load(k + 1); }
+    // ---- producers: stage, evaluate
+    const int jj = t >> 3, ii = t & 7;
+    const int nby = J.ny + 1, nbx = J.nx + 1;  // sub-blocks any window of this job touches
+    size_t off[kPPer];
+    int    sxs[kPPer];
+    bool   ok[kPPer];
+    #pragma unroll
+    for(int r = 0; r < kPPer; r++)
     {
-      const int i = k * kChunkI + tx, j = j0 + ty;
+      const int e = t + kPoolEval * r;
+      const int m = e / (kPSubR * kPSubC), rem = e - m * (kPSubR * kPSubC);
+      const int sy = rem / kPSubC, sx = rem - sy * kPSubC;
+      ok[r] = e < kPStage && j0 + sy < nby;
+      sxs[r] = sx;
+      off[r] = (size_t)m * J.plane + (size_t)(j0 + sy) * J.pitch + sx;
+    }
+    uint32_t reg[kPPer];
+    auto load = [&](int k) {
+      const int i0 = k * kPoolCW;
+      #pragma unroll
+      for(int r = 0; r < kPPer; r++) { reg[r] = (ok[r] && i0 + sxs[r] < nbx) ? __ldg(J.mom + off[r] + i0) : 0u; }
+    };
+    auto store = [&](int b) {
+      #pragma unroll
+      for(int r = 0; r < kPPer; r++)
+      {
+        const int e = t + kPoolEval * r;
+        if(e < kPStage) { (&st[b][0][0][0])[e] = reg[r]; }
+      }
+    };
+    load(0);
+    store(0);
+    bar_sync(kBarStage, kPoolEval);
+    if(nchunks > 1) { load(1); }
+    for(int k = 0; k < nchunks; k++)
+    {
+      const int b = k & 1;
+      const int i = k * kPoolCW + ii, j = j0 + jj;
       double v = 0.0;
       if(i < J.nx && j < J.ny)
       {
@@ -171,33 +179,51 @@ __device__ __forceinline__ void ssim_pool_body(const SsimPoolJob& J)
         #pragma unroll
         for(int m = 0; m < 5; m++)
         {
-          sm[m] = (uint64_t)st[buf][m][ty][tx] + st[buf][m][ty][tx + 1] + st[buf][m][ty + 1][tx] + st[buf][m][ty + 1][tx + 1];
+          sm[m] = (uint64_t)st[b][m][jj][ii] + st[b][m][jj][ii + 1] + st[b][m][jj + 1][ii] + st[b][m][jj + 1][ii + 1];
         }
         // moment 0/2 = "Tst" picture, 1/3 = "Ref" picture
         v = ssim_window(sm[1], sm[0], sm[3], sm[2], sm[4], J.C1, J.C2, J.calc_l != 0);
       }
-      vals[ty][tx] = v;
+      if(k >= 2) { bar_sync(kBarEmpty0 + b, kPoolThreads); }   // the summing warp is done with chunk k - 2
+      vals[b][jj][ii] = v;
+      bar_arrive(kBarFull0 + b, kPoolThreads);
+      if(k + 1 < nchunks)
+      {
+        store(b ^ 1);                                       // st[b ^ 1] was last read by chunk k - 1
+        bar_sync(kBarStage, kPoolEval);
+        if(k + 2 < nchunks) { load(k + 2); }
+      }
     }
-    __syncthreads();
-    if(ty == 0 && tx < kBandJ && j0 + tx < J.ny)
-    {
-      const int cnt = min(kChunkI, J.nx - k * kChunkI);
-      for(int u = 0; u < cnt; u++) { row.add(vals[tx][u]); }
-    }
-    if(k + 1 < nchunks) { store(buf ^ 1); }
-    __syncthreads();
   }
-  if(ty == 0 && tx < kBandJ && j0 + tx < J.ny) { J.row_sum[j0 + tx] = row.result(); }
+  else
+  {
+    // ---- summing warp: lane j owns window row j0 + j
+    const int j = t - kPoolEval;
+    const bool rowv = j0 + j < J.ny;
+    Kbns row;
+    for(int k = 0; k < nchunks; k++)
+    {
+      const int b = k & 1;
+      bar_sync(kBarFull0 + b, kPoolThreads);
+      const int cnt = min(kPoolCW, J.nx - k * kPoolCW);
+      if(rowv)
+      {
+        for(int u = 0; u < cnt; u++) { row.add(vals[b][j][u]); }
+      }
+      if(k + 2 < nchunks) { bar_arrive(kBarEmpty0 + b, kPoolThreads); }
+    }
+    if(rowv) { J.row_sum[j0 + j] = row.result(); }
+  }
 }
 
-__global__ void __launch_bounds__(256) k_ssim_pool(const __grid_constant__ SsimPoolArgs a) { ssim_pool_body(a.job[blockIdx.y]); }
+__global__ void __launch_bounds__(kPoolThreads, 2) k_ssim_pool(const __grid_constant__ SsimPoolArgs a) { ssim_pool_body(a.job[blockIdx.y]); }
 
-__global__ void __launch_bounds__(256) k_ssim_pool_multi(const SsimPoolJob* __restrict__ jobs) { ssim_pool_body(jobs[blockIdx.y]); }
+__global__ void __launch_bounds__(kPoolThreads, 2) k_ssim_pool_multi(const SsimPoolJob* __restrict__ jobs) { ssim_pool_body(jobs[blockIdx.y]); }
 
 cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_ny, cudaStream_t s)
 {
   if(njobs <= 0) { return cudaSuccess; }
-  k_ssim_pool_multi<<<dim3((max_ny + kBandJ - 1) / kBandJ, njobs), 256, 0, s>>>(d_jobs);
+  k_ssim_pool_multi<<<dim3((max_ny + kPoolRows - 1) / kPoolRows, njobs), kPoolThreads, 0, s>>>(d_jobs);
   return cudaGetLastError();
 }
 
@@ -206,8 +232,8 @@ cudaError_t launch_ssim_pool(const SsimPoolArgs& a, cudaStream_t s)
   if(a.njobs <= 0) { return cudaSuccess; }
   int maxny = 0;
   for(int k = 0; k < a.njobs; k++) { maxny = max(maxny, a.job[k].ny); }
-  const dim3 grid((maxny + kBandJ - 1) / kBandJ, a.njobs);
-  k_ssim_pool<<<grid, 256, 0, s>>>(a);
+  const dim3 grid((maxny + kPoolRows - 1) / kPoolRows, a.njobs);
+  k_ssim_pool<<<grid, kPoolThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
