@@ -8,6 +8,8 @@
 // lane per row, while other warps evaluate the next windows.
 #include "qmiv_kernels.cuh"
 
+#include <mutex>
+
 namespace qmiv {
 
 // =============================================================================================
@@ -108,98 +110,99 @@ template cudaError_t launch_ssim_moments<uint16_t>(const SsimMomArgs&, cudaStrea
 
 // =============================================================================================
 // windows + ordered row sums (xSSIM.cpp:353-369). A CTA owns kPoolRows = 32 window rows of one job
-// and walks them in chunks of kPoolCW = 8 windows. Eight producer warps stage the chunk's 33 x 9
-// sub-block moments in shared memory (double-buffered, the next chunk's global loads in flight) and
-// evaluate one window per thread; a ninth warp keeps the 32 compensated row sums, lane j adding row
-// j's values in x order. Window values pass through two shared buffers guarded by named barriers
-// (full: producers -> summing warp, empty: summing warp -> producers), so evaluation and the serial
-// sums overlap and one warp instruction advances 32 row sums.
+// and walks them in chunks of kPoolCW = 32 windows. Eight producer warps copy the chunk's 33 x 33
+// sub-block moments into shared memory with cp.async (double-buffered: chunk k+1 is in flight while
+// chunk k is evaluated) and evaluate four independent windows per thread; a ninth warp keeps the
+// 32 compensated row sums, lane j adding row j's values in x order. Window values pass through two
+// shared buffers guarded by named barriers (full: producers -> summing warp, empty: summing warp ->
+// producers), so evaluation and the serial sums overlap and one warp instruction advances 32 sums.
 // =============================================================================================
-constexpr int kPoolRows = 32, kPoolCW = 8, kPoolEval = 256, kPoolThreads = kPoolEval + 32;
-constexpr int kPSubR = kPoolRows + 1, kPSubC = kPoolCW + 1;
+constexpr int kPoolRows = 32, kPoolCW = 32, kPoolEval = 256, kPoolThreads = kPoolEval + 32;
+constexpr int kPSubR = kPoolRows + 1, kPSubC = kPoolCW + 1;        // 33 x 33 sub-blocks per chunk
 constexpr int kPStage = 5 * kPSubR * kPSubC;                       // staged moment values per chunk
-constexpr int kPPer = (kPStage + kPoolEval - 1) / kPoolEval;       // per producer thread
+constexpr size_t kPoolSmem = (size_t)2 * kPStage * 4 + (size_t)2 * kPoolRows * (kPoolCW + 1) * 8;
 enum { kBarFull0 = 1, kBarEmpty0 = 3, kBarStage = 5 };            // named barrier ids (0 = __syncthreads)
 
 __device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 __device__ __forceinline__ void bar_arrive(int id, int n) { asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+// 4-byte asynchronous global -> shared copy; src_bytes 0 writes a zero
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, uint32_t src_bytes)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src),
+               "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void ssim_pool_body(const SsimPoolJob& J)
 {
-  __shared__ uint32_t st[2][5][kPSubR][kPSubC];
-  __shared__ double vals[2][kPoolRows][kPoolCW + 1];
+  extern __shared__ __align__(16) unsigned char pool_smem[];
+  uint32_t (*st)[5][kPSubR][kPSubC] = reinterpret_cast<uint32_t (*)[5][kPSubR][kPSubC]>(pool_smem);
+  double (*vals)[kPoolRows][kPoolCW + 1] = reinterpret_cast<double (*)[kPoolRows][kPoolCW + 1]>(pool_smem + (size_t)2 * kPStage * 4);
   const int j0 = blockIdx.x * kPoolRows;
   if(j0 >= J.ny) { return; }
   const int nchunks = (J.nx + kPoolCW - 1) / kPoolCW;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   if(t < kPoolEval)
   {
-    // ---- producers: stage, evaluate
-    const int jj = t >> 3, ii = t & 7;
+    // ---- producers: copy, evaluate
     const int nby = J.ny + 1, nbx = J.nx + 1;  // sub-blocks any window of this job touches
-    size_t off[kPPer];
-    int    sxs[kPPer];
-    bool   ok[kPPer];
-    #pragma unroll
-    for(int r = 0; r < kPPer; r++)
-    {
-      const int e = t + kPoolEval * r;
-      const int m = e / (kPSubR * kPSubC), rem = e - m * (kPSubR * kPSubC);
-      const int sy = rem / kPSubC, sx = rem - sy * kPSubC;
-      ok[r] = e < kPStage && j0 + sy < nby;
-      sxs[r] = sx;
-      off[r] = (size_t)m * J.plane + (size_t)(j0 + sy) * J.pitch + sx;
-    }
-    uint32_t reg[kPPer];
-    auto load = [&](int k) {
+    auto issue = [&](int k) {
+      uint32_t* dst = &st[k & 1][0][0][0];
       const int i0 = k * kPoolCW;
-      #pragma unroll
-      for(int r = 0; r < kPPer; r++) { reg[r] = (ok[r] && i0 + sxs[r] < nbx) ? __ldg(J.mom + off[r] + i0) : 0u; }
-    };
-    auto store = [&](int b) {
-      #pragma unroll
-      for(int r = 0; r < kPPer; r++)
+      for(int rr = warp; rr < 5 * kPSubR; rr += kPoolEval / 32)
       {
-        const int e = t + kPoolEval * r;
-        if(e < kPStage) { (&st[b][0][0][0])[e] = reg[r]; }
+        const int m = rr / kPSubR, sy = rr - m * kPSubR, gy = j0 + sy;
+        const uint32_t* src = J.mom + (size_t)m * J.plane + (size_t)min(gy, nby - 1) * J.pitch;
+        for(int sx = lane; sx < kPSubC; sx += 32)
+        {
+          const int gx = i0 + sx;
+          const bool in = gy < nby && gx < nbx;
+          cp_async4(dst + (m * kPSubR + sy) * kPSubC + sx, src + (in ? gx : 0), in ? 4u : 0u);
+        }
       }
+      cp_async_commit();
     };
-    load(0);
-    store(0);
+    issue(0);
+    cp_async_wait_all();
     bar_sync(kBarStage, kPoolEval);
-    if(nchunks > 1) { load(1); }
     for(int k = 0; k < nchunks; k++)
     {
       const int b = k & 1;
-      const int i = k * kPoolCW + ii, j = j0 + jj;
-      double v = 0.0;
-      if(i < J.nx && j < J.ny)
+      if(k + 1 < nchunks) { issue(k + 1); }   // st[b ^ 1] was last read by chunk k - 1, before the stage barrier
+      double v[kPoolRows / 8];
+      #pragma unroll
+      for(int q = 0; q < kPoolRows / 8; q++)
       {
-        uint64_t sm[5];
-        #pragma unroll
-        for(int m = 0; m < 5; m++)
+        const int jj = warp + 8 * q, i = k * kPoolCW + lane, j = j0 + jj;
+        v[q] = 0.0;
+        if(i < J.nx && j < J.ny)
         {
-          sm[m] = (uint64_t)st[b][m][jj][ii] + st[b][m][jj][ii + 1] + st[b][m][jj + 1][ii] + st[b][m][jj + 1][ii + 1];
+          uint64_t sm[5];
+          #pragma unroll
+          for(int m = 0; m < 5; m++)
+          {
+            sm[m] = (uint64_t)st[b][m][jj][lane] + st[b][m][jj][lane + 1] + st[b][m][jj + 1][lane] + st[b][m][jj + 1][lane + 1];
+          }
+          // moment 0/2 = "Tst" picture, 1/3 = "Ref" picture
+          v[q] = ssim_window(sm[1], sm[0], sm[3], sm[2], sm[4], J.C1, J.C2, J.calc_l != 0);
         }
-        // moment 0/2 = "Tst" picture, 1/3 = "Ref" picture
-        v = ssim_window(sm[1], sm[0], sm[3], sm[2], sm[4], J.C1, J.C2, J.calc_l != 0);
       }
       if(k >= 2) { bar_sync(kBarEmpty0 + b, kPoolThreads); }   // the summing warp is done with chunk k - 2
-      vals[b][jj][ii] = v;
+      #pragma unroll
+      for(int q = 0; q < kPoolRows / 8; q++) { vals[b][warp + 8 * q][lane] = v[q]; }
       bar_arrive(kBarFull0 + b, kPoolThreads);
       if(k + 1 < nchunks)
       {
-        store(b ^ 1);                                       // st[b ^ 1] was last read by chunk k - 1
+        cp_async_wait_all();
         bar_sync(kBarStage, kPoolEval);
-        if(k + 2 < nchunks) { load(k + 2); }
       }
     }
   }
   else
   {
     // ---- summing warp: lane j owns window row j0 + j
-    const int j = t - kPoolEval;
-    const bool rowv = j0 + j < J.ny;
+    const bool rowv = j0 + lane < J.ny;
     Kbns row;
     for(int k = 0; k < nchunks; k++)
     {
@@ -208,11 +211,11 @@ __device__ __forceinline__ void ssim_pool_body(const SsimPoolJob& J)
       const int cnt = min(kPoolCW, J.nx - k * kPoolCW);
       if(rowv)
       {
-        for(int u = 0; u < cnt; u++) { row.add(vals[b][j][u]); }
+        for(int u = 0; u < cnt; u++) { row.add(vals[b][lane][u]); }
       }
       if(k + 2 < nchunks) { bar_arrive(kBarEmpty0 + b, kPoolThreads); }
     }
-    if(rowv) { J.row_sum[j0 + j] = row.result(); }
+    if(rowv) { J.row_sum[j0 + lane] = row.result(); }
   }
 }
 
@@ -220,20 +223,40 @@ __global__ void __launch_bounds__(kPoolThreads, 2) k_ssim_pool(const __grid_cons
 
 __global__ void __launch_bounds__(kPoolThreads, 2) k_ssim_pool_multi(const SsimPoolJob* __restrict__ jobs) { ssim_pool_body(jobs[blockIdx.y]); }
 
+static cudaError_t pool_configure()
+{
+  static std::mutex mu;
+  static uint64_t done = 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess) { return e; }
+  const uint64_t bit = 1ULL << (dev & 63);
+  std::lock_guard<std::mutex> lk(mu);
+  if(done & bit) { return cudaSuccess; }
+  e = cudaFuncSetAttribute(k_ssim_pool, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPoolSmem);
+  if(e == cudaSuccess) { e = cudaFuncSetAttribute(k_ssim_pool_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPoolSmem); }
+  if(e == cudaSuccess) { done |= bit; }
+  return e;
+}
+
 cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_ny, cudaStream_t s)
 {
   if(njobs <= 0) { return cudaSuccess; }
-  k_ssim_pool_multi<<<dim3((max_ny + kPoolRows - 1) / kPoolRows, njobs), kPoolThreads, 0, s>>>(d_jobs);
+  cudaError_t e = pool_configure();
+  if(e != cudaSuccess) { return e; }
+  k_ssim_pool_multi<<<dim3((max_ny + kPoolRows - 1) / kPoolRows, njobs), kPoolThreads, kPoolSmem, s>>>(d_jobs);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ssim_pool(const SsimPoolArgs& a, cudaStream_t s)
 {
   if(a.njobs <= 0) { return cudaSuccess; }
+  cudaError_t e = pool_configure();
+  if(e != cudaSuccess) { return e; }
   int maxny = 0;
   for(int k = 0; k < a.njobs; k++) { maxny = max(maxny, a.job[k].ny); }
   const dim3 grid((maxny + kPoolRows - 1) / kPoolRows, a.njobs);
-  k_ssim_pool<<<grid, kPoolThreads, 0, s>>>(a);
+  k_ssim_pool<<<grid, kPoolThreads, kPoolSmem, s>>>(a);
   return cudaGetLastError();
 }
 
