@@ -134,6 +134,8 @@ qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames
   {
     if(nx_[0] < 1 || ny_[0] < 1) { return fail(QMIV_ERR_INVALID_ARG, "picture smaller than one 8x8 SSIM window"); }
     QMIV_TRY(rowsum_.ensure(ctx_, (size_t)kMaxSsimSlots * 3 * ny_[0] * sizeof(double)));
+    // window values of up to 9 pool jobs (one flush) at scale 0, reused by later flushes
+    QMIV_TRY(win_.ensure(ctx_, (size_t)9 * pool_win_elems(nx_[0], ny_[0]) * sizeof(double)));
   }
   if(need_ms)
   {
@@ -277,7 +279,9 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
   auto add_pool = [&](const Moments& m, int scale, int slot, int calc_l, int use_ws) {
     for(int c = 0; c < 3; c++)
     {
-      SsimPoolJob& J = pool.job[pool.njobs++];
+      SsimPoolJob& J = pool.job[pool.njobs];
+      J.win = win_.as<double>() + (size_t)pool.njobs * pool_win_elems(nx_[0], ny_[0]);
+      pool.njobs++;
       J.mom = m.p + (size_t)c * 5 * m.plane(); J.plane = m.plane(); J.pitch = m.pitch;
       J.C1 = C1_; J.C2 = C2_;
       J.nx = nx_[scale]; J.ny = ny_[scale]; J.calc_l = calc_l;

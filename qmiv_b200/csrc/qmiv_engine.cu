@@ -271,6 +271,10 @@ qmiv_status Engine::run(const qmiv_pair_desc* pairs, int32_t n, qmiv_result* res
       p.mom_slot = mom_slot_elems(S);
       p.mom = take((size_t)slots * p.mom_slot * sizeof(uint32_t));
       p.rowsum = take((size_t)kMaxSsimSlots * 3 * K.ny[0] * sizeof(double));
+      // window values of the pair's scale-0 pool jobs, reused by the MS-SSIM scales
+      const int jobs0 = 3 * (((p.mask & QMIV_IVSSIM) ? 2 : 0) + ((p.mask & QMIV_SSIM) ? 1 : 0) +
+                             ((p.mask & QMIV_MSSSIM) ? 1 : 0) + ((p.mask & QMIV_IVMSSSIM) ? 2 : 0));
+      p.win = take((size_t)jobs0 * pool_win_elems(K.nx[0], K.ny[0]) * sizeof(double));
     }
     if(p.need_ms)
     {
@@ -727,14 +731,18 @@ void Engine::add_pool_jobs(int i, const PairKind& K, int ph, char* dbase, SsimPo
   const Shape& S = K.S;
   const int ns = p.need_ms ? K.ns : 0;
   double* rowsum = reinterpret_cast<double*>(dbase + p.rowsum);
+  double* win = reinterpret_cast<double*>(dbase + p.win);
+  int jobs_here = 0;
   auto add = [&](const Moments& m, int scale, int slot, int calc_l, int use_ws) {
     for(int c = 0; c < 3; c++)
     {
       SsimPoolJob& J = pj[np++];
+      J.win = win + (size_t)(jobs_here++) * pool_win_elems(K.nx[0], K.ny[0]);
       J.C1 = K.C1; J.C2 = K.C2;
       J.mom = m.p + (size_t)c * 5 * m.plane(); J.plane = m.plane(); J.pitch = m.pitch;
       J.nx = K.nx[scale]; J.ny = K.ny[scale]; J.calc_l = calc_l;
       J.row_sum = rowsum + (size_t)slot * 3 * K.ny[0] + (size_t)c * K.ny[scale];  // finalize reads [c][ny_scale]
+      PH.pool_max_nx = std::max(PH.pool_max_nx, J.nx);
       PH.pool_max_ny = std::max(PH.pool_max_ny, J.ny);
     }
     fa.slot[slot].row_sum = rowsum + (size_t)slot * 3 * K.ny[0];
@@ -792,7 +800,7 @@ qmiv_status Engine::launch_all(const Tables& T, cudaStream_t s)
     if(PH.pool_count > 0)
     {
       const int t = prof_begin(s);
-      QMIV_CUDA(launch_ssim_pool_multi(T.d_pool + PH.pool_first, (int)PH.pool_count, PH.pool_max_ny, s));
+      QMIV_CUDA(launch_ssim_pool_multi(T.d_pool + PH.pool_first, (int)PH.pool_count, PH.pool_max_nx, PH.pool_max_ny, s));
       prof_end(s, QMIV_STAGE_SSIM_ROWS, t);
     }
   }

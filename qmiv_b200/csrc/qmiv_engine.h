@@ -40,7 +40,7 @@ struct PairSlot
 {
   uint32_t mask = 0;
   bool     need_scp = false, need_search = false, need_ssim = false, need_ms = false, host = false;
-  size_t   out = 0, cps_rows = 0, row_sd = 0, row_ssd = 0, scp = 0, mom = 0, mom_slot = 0, rowsum = 0;
+  size_t   out = 0, cps_rows = 0, row_sd = 0, row_ssd = 0, scp = 0, mom = 0, mom_slot = 0, rowsum = 0, win = 0;
   size_t   pyr = 0, pyr_lv = 0, staging = 0;
 };
 
@@ -65,7 +65,7 @@ struct Phase
   size_t mom_first[2] = { 0, 0 }, mom_count[2] = { 0, 0 };
   int    mom_max_nbx = 0, mom_max_nby = 0;
   size_t pool_first = 0, pool_count = 0;
-  int    pool_max_ny = 0;
+  int    pool_max_nx = 0, pool_max_ny = 0;
 };
 
 // Argument tables of one set of pairs: host layout, device pointers, launch shapes.

@@ -170,7 +170,7 @@ private:
     return 3 * 5 * nby * ((nbx + 7) & ~(size_t)7);
   }
 
-  DevMem row_sd_, row_ssd_, cps_rows_, out_, ws_, scp_, pyr_, mom_, rowsum_, staging_;
+  DevMem row_sd_, row_ssd_, cps_rows_, out_, ws_, scp_, pyr_, mom_, rowsum_, win_, staging_;
   PairOut* h_out = nullptr;
   bool ws_uploaded_ = false;
   bool gcd_override_on_ = false;

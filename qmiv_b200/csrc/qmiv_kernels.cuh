@@ -81,6 +81,7 @@ struct SsimPoolJob
   int32_t         nx, ny;      // windows per row / column
   int32_t         calc_l;
   double*         row_sum;     // [ny]
+  double*         win;         // scratch window values [ceil(ny / 32)][nx][32] (pool_win_elems)
 };
 
 struct SsimPoolArgs
@@ -144,7 +145,8 @@ template <typename T> cudaError_t launch_prepass_multi(const PrepassArgs* d_jobs
 cudaError_t launch_reduce_multi(const ReduceArgs* d_jobs, int njobs, cudaStream_t s);
 template <typename T>
 cudaError_t launch_ssim_moments_multi(const SsimMomArgs* d_jobs, int njobs, int max_nbx, int max_nby, cudaStream_t s);
-cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_ny, cudaStream_t s);
+cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_nx, int max_ny, cudaStream_t s);
+size_t      pool_win_elems(int nx, int ny);   // doubles of SsimPoolJob::win
 cudaError_t launch_finalize_multi(const FinalizeArgs* d_pairs, const FinJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
 
 // CPS work-list form: one 64-byte aligned descriptor (tensor maps + tile geometry) per frame pair,

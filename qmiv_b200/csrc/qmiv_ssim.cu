@@ -3,12 +3,10 @@
 // Window moments are sums of 2x2 exact integer 4x4 sub-block moments. They come either from the
 // CPS search's epilogue (IV-SSIM: test picture vs its shift-compensated picture, so the SCP never
 // needs to be stored) or from k_ssim_moments (plain SSIM, MS-SSIM scales, which also writes the
-// next scale's 2x2 mean, xPixelOpsSTD.cpp:50-67). k_ssim_pool evaluates every window in FP64 with the
-// reference's operation order and sums each window row in x order with the compensated sum, one
-// lane per row, while other warps evaluate the next windows.
+// next scale's 2x2 mean, xPixelOpsSTD.cpp:50-67). k_ssim_win evaluates every window in FP64 with the
+// reference's operation order; k_ssim_rows sums each window row in x order with the compensated sum,
+// one lane per row.
 #include "qmiv_kernels.cuh"
-
-#include <mutex>
 
 namespace qmiv {
 
@@ -109,154 +107,141 @@ template cudaError_t launch_ssim_moments<uint8_t>(const SsimMomArgs&, cudaStream
 template cudaError_t launch_ssim_moments<uint16_t>(const SsimMomArgs&, cudaStream_t);
 
 // =============================================================================================
-// windows + ordered row sums (xSSIM.cpp:353-369). A CTA owns kPoolRows = 32 window rows of one job
-// and walks them in chunks of kPoolCW = 32 windows. Eight producer warps copy the chunk's 33 x 33
-// sub-block moments into shared memory with cp.async (double-buffered: chunk k+1 is in flight while
-// chunk k is evaluated) and evaluate four independent windows per thread; a ninth warp keeps the
-// 32 compensated row sums, lane j adding row j's values in x order. Window values pass through two
-// shared buffers guarded by named barriers (full: producers -> summing warp, empty: summing warp ->
-// producers), so evaluation and the serial sums overlap and one warp instruction advances 32 sums.
+// windows + ordered row sums (xSSIM.cpp:353-369), two kernels:
+//   k_ssim_win   a CTA evaluates a 32 x 32 tile of windows of one job: the tile's 33 x 33 sub-block
+//                moments are staged in shared memory, each thread evaluates four windows (FP64, the
+//                reference's operation order), and the values are written transposed to the job's
+//                scratch [band = y / 32][x][y % 32], so that
+//   k_ssim_rows  one warp per band of 32 window rows, lane j walking row j in x order with the
+//                compensated sum, reads 256 contiguous bytes per step (a deep register prefetch hides
+//                the memory latency of the serial chain).
+// All windows are independent work for the first kernel; only the second is order-dependent.
 // =============================================================================================
-constexpr int kPoolRows = 32, kPoolCW = 32, kPoolEval = 256, kPoolThreads = kPoolEval + 32;
-constexpr int kPSubR = kPoolRows + 1, kPSubC = kPoolCW + 1;        // 33 x 33 sub-blocks per chunk
-constexpr int kPStage = 5 * kPSubR * kPSubC;                       // staged moment values per chunk
-constexpr size_t kPoolSmem = (size_t)2 * kPStage * 4 + (size_t)2 * kPoolRows * (kPoolCW + 1) * 8;
-enum { kBarFull0 = 1, kBarEmpty0 = 3, kBarStage = 5 };            // named barrier ids (0 = __syncthreads)
+constexpr int kWinT = 32;                                  // windows per tile side
+constexpr int kWSub = kWinT + 1;                           // sub-blocks per tile side
+constexpr int kWStage = 5 * kWSub * kWSub;
+constexpr int kWPer = (kWStage + 255) / 256;
 
-__device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
-__device__ __forceinline__ void bar_arrive(int id, int n) { asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory"); }
-// 4-byte asynchronous global -> shared copy; src_bytes 0 writes a zero
-__device__ __forceinline__ void cp_async4(void* dst, const void* src, uint32_t src_bytes)
-{
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src),
-               "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+size_t pool_win_elems(int nx, int ny) { return (size_t)((ny + 31) / 32) * 32 * (size_t)nx; }
 
-__device__ __forceinline__ void ssim_pool_body(const SsimPoolJob& J)
+__device__ __forceinline__ void ssim_win_body(const SsimPoolJob& J, int tile_x, int tile_y)
 {
-  extern __shared__ __align__(16) unsigned char pool_smem[];
-  uint32_t (*st)[5][kPSubR][kPSubC] = reinterpret_cast<uint32_t (*)[5][kPSubR][kPSubC]>(pool_smem);
-  double (*vals)[kPoolRows][kPoolCW + 1] = reinterpret_cast<double (*)[kPoolRows][kPoolCW + 1]>(pool_smem + (size_t)2 * kPStage * 4);
-  const int j0 = blockIdx.x * kPoolRows;
-  if(j0 >= J.ny) { return; }
-  const int nchunks = (J.nx + kPoolCW - 1) / kPoolCW;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  if(t < kPoolEval)
+  __shared__ uint32_t st[5][kWSub][kWSub];
+  __shared__ double vals[kWinT][kWinT + 1];               // [x][y]
+  const int i0 = tile_x * kWinT, j0 = tile_y * kWinT;
+  if(i0 >= J.nx || j0 >= J.ny) { return; }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nby = J.ny + 1, nbx = J.nx + 1;
+  #pragma unroll
+  for(int r = 0; r < kWPer; r++)
   {
-    // ---- producers: copy, evaluate
-    const int nby = J.ny + 1, nbx = J.nx + 1;  // sub-blocks any window of this job touches
-    auto issue = [&](int k) {
-      uint32_t* dst = &st[k & 1][0][0][0];
-      const int i0 = k * kPoolCW;
-      for(int rr = warp; rr < 5 * kPSubR; rr += kPoolEval / 32)
-      {
-        const int m = rr / kPSubR, sy = rr - m * kPSubR, gy = j0 + sy;
-        const uint32_t* src = J.mom + (size_t)m * J.plane + (size_t)min(gy, nby - 1) * J.pitch;
-        for(int sx = lane; sx < kPSubC; sx += 32)
-        {
-          const int gx = i0 + sx;
-          const bool in = gy < nby && gx < nbx;
-          cp_async4(dst + (m * kPSubR + sy) * kPSubC + sx, src + (in ? gx : 0), in ? 4u : 0u);
-        }
-      }
-      cp_async_commit();
-    };
-    issue(0);
-    cp_async_wait_all();
-    bar_sync(kBarStage, kPoolEval);
-    for(int k = 0; k < nchunks; k++)
+    const int e = threadIdx.x + 256 * r;
+    if(e < kWStage)
     {
-      const int b = k & 1;
-      if(k + 1 < nchunks) { issue(k + 1); }   // st[b ^ 1] was last read by chunk k - 1, before the stage barrier
-      double v[kPoolRows / 8];
-      #pragma unroll
-      for(int q = 0; q < kPoolRows / 8; q++)
-      {
-        const int jj = warp + 8 * q, i = k * kPoolCW + lane, j = j0 + jj;
-        v[q] = 0.0;
-        if(i < J.nx && j < J.ny)
-        {
-          uint64_t sm[5];
-          #pragma unroll
-          for(int m = 0; m < 5; m++)
-          {
-            sm[m] = (uint64_t)st[b][m][jj][lane] + st[b][m][jj][lane + 1] + st[b][m][jj + 1][lane] + st[b][m][jj + 1][lane + 1];
-          }
-          // moment 0/2 = "Tst" picture, 1/3 = "Ref" picture
-          v[q] = ssim_window(sm[1], sm[0], sm[3], sm[2], sm[4], J.C1, J.C2, J.calc_l != 0);
-        }
-      }
-      if(k >= 2) { bar_sync(kBarEmpty0 + b, kPoolThreads); }   // the summing warp is done with chunk k - 2
-      #pragma unroll
-      for(int q = 0; q < kPoolRows / 8; q++) { vals[b][warp + 8 * q][lane] = v[q]; }
-      bar_arrive(kBarFull0 + b, kPoolThreads);
-      if(k + 1 < nchunks)
-      {
-        cp_async_wait_all();
-        bar_sync(kBarStage, kPoolEval);
-      }
+      const int m = e / (kWSub * kWSub), rem = e - m * (kWSub * kWSub);
+      const int sy = rem / kWSub, sx = rem - sy * kWSub;
+      const int gy = j0 + sy, gx = i0 + sx;
+      st[m][sy][sx] = (gy < nby && gx < nbx) ? __ldg(J.mom + (size_t)m * J.plane + (size_t)gy * J.pitch + gx) : 0u;
     }
   }
-  else
+  __syncthreads();
+  #pragma unroll
+  for(int q = 0; q < kWinT / 8; q++)
   {
-    // ---- summing warp: lane j owns window row j0 + j
-    const bool rowv = j0 + lane < J.ny;
-    Kbns row;
-    for(int k = 0; k < nchunks; k++)
+    const int jj = warp + 8 * q, i = i0 + lane, j = j0 + jj;
+    double v = 0.0;
+    if(i < J.nx && j < J.ny)
     {
-      const int b = k & 1;
-      bar_sync(kBarFull0 + b, kPoolThreads);
-      const int cnt = min(kPoolCW, J.nx - k * kPoolCW);
-      if(rowv)
+      uint64_t sm[5];
+      #pragma unroll
+      for(int m = 0; m < 5; m++)
       {
-        for(int u = 0; u < cnt; u++) { row.add(vals[b][lane][u]); }
+        sm[m] = (uint64_t)st[m][jj][lane] + st[m][jj][lane + 1] + st[m][jj + 1][lane] + st[m][jj + 1][lane + 1];
       }
-      if(k + 2 < nchunks) { bar_arrive(kBarEmpty0 + b, kPoolThreads); }
+      // moment 0/2 = "Tst" picture, 1/3 = "Ref" picture
+      v = ssim_window(sm[1], sm[0], sm[3], sm[2], sm[4], J.C1, J.C2, J.calc_l != 0);
     }
-    if(rowv) { J.row_sum[j0 + lane] = row.result(); }
+    vals[lane][jj] = v;
+  }
+  __syncthreads();
+  double* out = J.win + ((size_t)tile_y * J.nx + i0) * 32;
+  #pragma unroll
+  for(int q = 0; q < kWinT / 8; q++)
+  {
+    const int ii = warp + 8 * q;
+    if(i0 + ii < J.nx) { out[(size_t)ii * 32 + lane] = vals[ii][lane]; }
   }
 }
 
-__global__ void __launch_bounds__(kPoolThreads, 2) k_ssim_pool(const __grid_constant__ SsimPoolArgs a) { ssim_pool_body(a.job[blockIdx.y]); }
-
-__global__ void __launch_bounds__(kPoolThreads, 2) k_ssim_pool_multi(const SsimPoolJob* __restrict__ jobs) { ssim_pool_body(jobs[blockIdx.y]); }
-
-static cudaError_t pool_configure()
+__device__ __forceinline__ void ssim_rows_body(const SsimPoolJob& J, int band)
 {
-  static std::mutex mu;
-  static uint64_t done = 0;
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if(e != cudaSuccess) { return e; }
-  const uint64_t bit = 1ULL << (dev & 63);
-  std::lock_guard<std::mutex> lk(mu);
-  if(done & bit) { return cudaSuccess; }
-  e = cudaFuncSetAttribute(k_ssim_pool, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPoolSmem);
-  if(e == cudaSuccess) { e = cudaFuncSetAttribute(k_ssim_pool_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPoolSmem); }
-  if(e == cudaSuccess) { done |= bit; }
-  return e;
+  constexpr int U = 16;
+  const int lane = threadIdx.x & 31;
+  if(band * 32 >= J.ny) { return; }
+  const double* p = J.win + (size_t)band * J.nx * 32 + lane;
+  const int nx = J.nx;
+  Kbns row;
+  double cur[U], nxt[U];
+  #pragma unroll
+  for(int u = 0; u < U; u++) { cur[u] = u < nx ? __ldg(p + (size_t)u * 32) : 0.0; }
+  for(int i0 = 0; i0 < nx; i0 += U)
+  {
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      const int i = i0 + U + u;
+      nxt[u] = i < nx ? __ldg(p + (size_t)i * 32) : 0.0;
+    }
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      if(i0 + u < nx) { row.add(cur[u]); }
+    }
+    #pragma unroll
+    for(int u = 0; u < U; u++) { cur[u] = nxt[u]; }
+  }
+  const int j = band * 32 + lane;
+  if(j < J.ny) { J.row_sum[j] = row.result(); }
 }
 
-cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_ny, cudaStream_t s)
+__global__ void __launch_bounds__(256) k_ssim_win(const __grid_constant__ SsimPoolArgs a)
+{
+  ssim_win_body(a.job[blockIdx.z], blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(256) k_ssim_win_multi(const SsimPoolJob* __restrict__ jobs)
+{
+  ssim_win_body(jobs[blockIdx.z], blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(128) k_ssim_rows(const __grid_constant__ SsimPoolArgs a)
+{
+  ssim_rows_body(a.job[blockIdx.y], blockIdx.x * 4 + (threadIdx.x >> 5));
+}
+__global__ void __launch_bounds__(128) k_ssim_rows_multi(const SsimPoolJob* __restrict__ jobs)
+{
+  ssim_rows_body(jobs[blockIdx.y], blockIdx.x * 4 + (threadIdx.x >> 5));
+}
+
+cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_nx, int max_ny, cudaStream_t s)
 {
   if(njobs <= 0) { return cudaSuccess; }
-  cudaError_t e = pool_configure();
+  k_ssim_win_multi<<<dim3((max_nx + kWinT - 1) / kWinT, (max_ny + kWinT - 1) / kWinT, njobs), 256, 0, s>>>(d_jobs);
+  cudaError_t e = cudaGetLastError();
   if(e != cudaSuccess) { return e; }
-  k_ssim_pool_multi<<<dim3((max_ny + kPoolRows - 1) / kPoolRows, njobs), kPoolThreads, kPoolSmem, s>>>(d_jobs);
+  const int bands = (max_ny + 31) / 32;
+  k_ssim_rows_multi<<<dim3((bands + 3) / 4, njobs), 128, 0, s>>>(d_jobs);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ssim_pool(const SsimPoolArgs& a, cudaStream_t s)
 {
   if(a.njobs <= 0) { return cudaSuccess; }
-  cudaError_t e = pool_configure();
+  int maxnx = 0, maxny = 0;
+  for(int k = 0; k < a.njobs; k++) { maxnx = max(maxnx, a.job[k].nx); maxny = max(maxny, a.job[k].ny); }
+  k_ssim_win<<<dim3((maxnx + kWinT - 1) / kWinT, (maxny + kWinT - 1) / kWinT, a.njobs), 256, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
   if(e != cudaSuccess) { return e; }
-  int maxny = 0;
-  for(int k = 0; k < a.njobs; k++) { maxny = max(maxny, a.job[k].ny); }
-  const dim3 grid((maxny + kPoolRows - 1) / kPoolRows, a.njobs);
-  k_ssim_pool<<<grid, kPoolThreads, kPoolSmem, s>>>(a);
+  const int bands = (maxny + 31) / 32;
+  k_ssim_rows<<<dim3((bands + 3) / 4, a.njobs), 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 
