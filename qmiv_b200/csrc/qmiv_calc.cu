@@ -27,6 +27,16 @@ qmiv_status Shape::init(int32_t W_, int32_t H_, int32_t bd, int32_t cf)
   return QMIV_OK;
 }
 
+qmiv_status check_metrics(const Shape& S, uint32_t mask)
+{
+  if((mask & ~(uint32_t)QMIV_ALL) != 0) { return fail(QMIV_ERR_INVALID_ARG, "unknown metric bits"); }
+  if((mask & (QMIV_SSIM | QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM)) && S.bitdepth > 14)
+  {
+    return fail(QMIV_ERR_UNSUPPORTED, "SSIM metrics need bit depth <= 14");
+  }
+  return QMIV_OK;
+}
+
 qmiv_status validate_params(const qmiv_params& p)
 {
   if(p.search_range < 1 || p.search_range > 5) { return fail(QMIV_ERR_UNSUPPORTED, "search range must be 1..5"); }
@@ -284,7 +294,7 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
       pool.njobs++;
       J.mom = m.p + (size_t)c * 5 * m.plane(); J.plane = m.plane(); J.pitch = m.pitch;
       J.C1 = C1_; J.C2 = C2_;
-      J.nx = nx_[scale]; J.ny = ny_[scale]; J.calc_l = calc_l;
+      J.nx = nx_[scale]; J.ny = ny_[scale]; J.calc_l = calc_l; J.wide = shape_.bitdepth > 12 ? 1 : 0;
       J.row_sum = rowsum + (size_t)slot * 3 * ny_[0] + (size_t)c * ny_[scale];  // finalize reads [c][ny_scale]
     }
     fa.slot[slot].row_sum = rowsum + (size_t)slot * 3 * ny_[0];
@@ -410,7 +420,7 @@ static qmiv_status calc_submit(qmiv_calc calc, const qmiv_frame* in0, const qmiv
 {
   if(!calc || !in0 || !in1) { return fail(QMIV_ERR_INVALID_ARG, "null argument"); }
   if(calc->pending) { return fail(QMIV_ERR_BUSY, "a submission is already in flight on this calc"); }
-  if((mask & ~QMIV_ALL) != 0) { return fail(QMIV_ERR_INVALID_ARG, "unknown metric bits"); }
+  QMIV_TRY(check_metrics(calc->pipe.shape(), mask));
   QMIV_CUDA(cudaSetDevice(calc->ctx->device));
   const bool host = in0->mem == QMIV_MEM_HOST || in1->mem == QMIV_MEM_HOST;
   QMIV_TRY(calc->pipe.prepare(mask, want_scp, host));

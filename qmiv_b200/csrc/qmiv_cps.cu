@@ -297,14 +297,25 @@ __device__ __forceinline__ void search_fp32(const Thr& th, const float4* tst, co
     c2[p] = fmaf(m2, t.z, o2);
     best[p] = 0xffffffffu;
   }
+  // The code of candidate (dyi, dxi) = (ry - i, rx - j) of pixel p = (i, j) is
+  // C::of(ry, rx) - C::of(i, j). Where C::of(ry, rx) < 128 for every reference sample the thread
+  // reads, the key's constant part belongs to the reference sample alone (one register for all
+  // eight pixels) and C::of(i, j) is taken off after the minimum. Two candidates of a pixel go into
+  // one three-input minimum.
+  constexpr bool kShared = C::of(3 + 2 * R, 1 + 2 * R) < 128;
   const float4* rb = ref + at_hx<R, WY>(th.y0, th.hx, 0);
+  auto key = [&](const float4& r, int p, uint32_t k) -> uint32_t {
+    const float e = fmaf(c2[p], r.z, fmaf(c1[p], r.y, fmaf(c0[p], r.x, r.w)));
+    return (__float_as_uint(e) << 7) + k;
+  };
   #pragma unroll
   for(int ry = 0; ry < 4 + 2 * R; ry++)
   {
     #pragma unroll
-    for(int rx = 0; rx < 2 + 2 * R; rx++)
+    for(int rx = 0; rx < 2 + 2 * R; rx += 2)
     {
-      const float4 r = rb[ry * G::RP + (rx & 1) * G::Q + (rx >> 1)];
+      const float4 ra = rb[ry * G::RP + (rx & 1) * G::Q + (rx >> 1)];
+      const float4 rc = rb[ry * G::RP + ((rx + 1) & 1) * G::Q + ((rx + 1) >> 1)];
       #pragma unroll
       for(int i = 0; i < 4; i++)
       {
@@ -313,18 +324,23 @@ __device__ __forceinline__ void search_fp32(const Thr& th, const float4* tst, co
         #pragma unroll
         for(int j = 0; j < 2; j++)
         {
-          const int dxi = rx - j;
-          if(dxi < 0 || dxi >= D) { continue; }
           const int p = 2 * i + j;
-          const float e = fmaf(c2[p], r.z, fmaf(c1[p], r.y, fmaf(c0[p], r.x, r.w)));
-          const uint32_t key = (__float_as_uint(e) << 7) + C::of(dyi, dxi) - (kKeyBase << 7);
-          best[p] = min(best[p], key);
+          const bool va = rx - j >= 0 && rx - j < D, vc = rx + 1 - j >= 0 && rx + 1 - j < D;
+          const uint32_t ka = (kShared ? C::of(ry, rx) : C::of(dyi, rx - j)) - (kKeyBase << 7);
+          const uint32_t kc = (kShared ? C::of(ry, rx + 1) : C::of(dyi, rx + 1 - j)) - (kKeyBase << 7);
+          if(va && vc) { best[p] = __vimin3_u32(best[p], key(ra, p, ka), key(rc, p, kc)); }
+          else if(va) { best[p] = min(best[p], key(ra, p, ka)); }
+          else if(vc) { best[p] = min(best[p], key(rc, p, kc)); }
         }
       }
     }
   }
   #pragma unroll
-  for(int p = 0; p < 8; p++) { idx[p] = min(best[p] & 127u, C::kMax); }
+  for(int p = 0; p < 8; p++)
+  {
+    const uint32_t base = kShared ? C::of(p >> 1, p & 1) : 0u;
+    idx[p] = min((best[p] & 127u) - base, C::kMax);
+  }
 }
 
 template <int R, int WY>
@@ -390,6 +406,7 @@ __device__ __forceinline__ void epilogue_fp(const Thr& th, const CpsArgs& a, con
     #pragma unroll
     for(int m = 0; m < 5; m++) { mm[c][m] = 0.f; }
   }
+  uint32_t rs[12];
   #pragma unroll
   for(int i = 0; i < 4; i++)
   {
@@ -428,25 +445,40 @@ __device__ __forceinline__ void epilogue_fp(const Thr& th, const CpsArgs& a, con
     for(int c = 0; c < 3; c++)
     {
       // 2^23 + (a sum below 2^23) has the sum in its low bits; 32 lanes add 32 x 0x4B000000
-      const uint32_t s = __reduce_add_sync(kFull, __float_as_uint(frs[c] + kBias)) - 32u * kBiasBits;
-      if(th.lane == 0 && (!EDGE || y < a.H)) { atomicAdd(rows + (size_t)y * 3 + c, s); }
+      rs[3 * i + c] = __reduce_add_sync(kFull, __float_as_uint(frs[c] + kBias)) - 32u * kBiasBits;
     }
+  }
+  // the warp's twelve row sums (row yb + i, component c) go out in one atomic: lane 3 i + c adds
+  // rs[3 i + c] to rows[(yb + i) * 3 + c]
+  if(th.lane < 12)
+  {
+    uint32_t v = rs[0];
+    #pragma unroll
+    for(int q = 1; q < 12; q++) { v = th.lane == q ? rs[q] : v; }
+    if(!EDGE || yb + ((th.lane * 11) >> 5) < a.H) { atomicAdd(rows + (size_t)yb * 3 + th.lane, v); }
   }
   if(MOM)
   {
-    // lanes 2m and 2m + 1 hold the two column halves of block bx
+    // lanes 2m and 2m + 1 hold the two column halves of block bx; all shuffles first, then the even
+    // lanes store the fifteen moment planes' values
     const Moments mom = a.mom[dir];
     const int bx = xb >> 2, by = yb >> 2;
-    const bool store = (th.lane & 1) == 0 && bx < mom.nbx && by < mom.nby;
+    uint32_t mv[15];
     #pragma unroll
     for(int c = 0; c < 3; c++)
     {
       #pragma unroll
       for(int m = 0; m < 5; m++)
       {
-        const float f = mm[c][m] + __shfl_xor_sync(kFull, mm[c][m], 1);   // exact: integers below 2^24
-        if(store) { mom.p[((size_t)c * 5 + m) * mom.plane() + (size_t)by * mom.pitch + bx] = __float2uint_rn(f); }
+        mv[5 * c + m] = __float2uint_rn(mm[c][m] + __shfl_xor_sync(kFull, mm[c][m], 1));   // exact: integers below 2^24
       }
+    }
+    if((th.lane & 1) == 0 && bx < mom.nbx && by < mom.nby)
+    {
+      uint32_t* q = mom.p + (size_t)by * mom.pitch + bx;
+      const size_t plane = mom.plane();
+      #pragma unroll
+      for(int k = 0; k < 15; k++) { q[0] = mv[k]; q += plane; }
     }
   }
 }
@@ -873,7 +905,7 @@ cudaError_t launch_r(CpsKernelArgs& k, cudaStream_t s)
   {
     if(wy == 8) { return launch_inst<R, 8, T>(k, smem, dev, s); }
   }
-  if constexpr(R >= 4) { return launch_inst<R, 4, T>(k, smem, dev, s); }
+  if(wy == 4) { return launch_inst<R, 4, T>(k, smem, dev, s); }
   return cudaErrorInvalidConfiguration;
 }
 
@@ -891,8 +923,9 @@ cudaError_t launch_multi_r(const CpsKernelArgs* d, const int32_t* prefix, int np
 
 }  // namespace
 
-// 16 warps (128 x 32 tiles) where both float tiles and the raw boxes fit in shared memory: always
-// for R <= 3, for R = 4 unless 4:4:4 boxes do not fit; 8 warps (128 x 16 tiles) otherwise.
+// 16 warps (128 x 32 tiles) where both float tiles and the raw boxes fit in shared memory (R <= 4,
+// except 2-byte 4:4:4 pictures from R = 3 on, whose full-size chroma boxes are too large); 8 warps
+// (128 x 16 tiles) otherwise.
 int cps_pick_wy(int R, int esz, int sx, int sy)
 {
   if(R <= 4 && cps_tile_fits(R, 8, esz, sx, sy)) { return 8; }

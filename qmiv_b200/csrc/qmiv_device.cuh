@@ -65,20 +65,20 @@ struct Kbns
   __device__ __forceinline__ double result() const { return dadd(s, c); }
 };
 
-// SSIM of one window from exact integer moments (xStructSimSTD.cpp:420-461, same operation order;
-// AVX-512 CalcBlckAvg8 / CalcMultiBlckAvg8S4 give the same per-window value).
-__device__ __forceinline__ double ssim_window(uint64_t sr, uint64_t st, uint64_t srr, uint64_t stt, uint64_t srt,
-                                              double C1, double C2, bool calc_l)
+// SSIM of one window (xStructSimSTD.cpp:420-461, same operation order; AVX-512 CalcBlckAvg8 /
+// CalcMultiBlckAvg8S4 give the same per-window value) from its moments divided by the window area:
+// ar = SumR / 64, at = SumT / 64, qr = SumR2 / 64, qt = SumT2 / 64, qrt = SumRT / 64 (all exact).
+// 2 x is formed as x + x, which is the same double.
+__device__ __forceinline__ double ssim_window_avg(double ar, double at, double qr, double qt, double qrt, double C1,
+                                                  double C2, bool calc_l)
 {
-  const double inv   = 0.015625;  // 1/64, exact
-  const double avg_r = dmul((double)sr, inv);
-  const double avg_t = dmul((double)st, inv);
-  const double var_r = dsub(dmul((double)srr, inv), dmul(avg_r, avg_r));
-  const double var_t = dsub(dmul((double)stt, inv), dmul(avg_t, avg_t));
-  const double cov   = dsub(dmul((double)srt, inv), dmul(avg_r, avg_t));
-  const double cs    = ddiv(dadd(dmul(2.0, cov), C2), dadd(dadd(var_r, var_t), C2));
+  const double ar2 = dmul(ar, ar), at2 = dmul(at, at);
+  const double var_r = dsub(qr, ar2);
+  const double var_t = dsub(qt, at2);
+  const double cov   = dsub(qrt, dmul(ar, at));
+  const double cs    = ddiv(dadd(dadd(cov, cov), C2), dadd(dadd(var_r, var_t), C2));
   if(!calc_l) { return cs; }
-  const double l = ddiv(dadd(dmul(dmul(2.0, avg_r), avg_t), C1), dadd(dadd(dmul(avg_r, avg_r), dmul(avg_t, avg_t)), C1));
+  const double l = ddiv(dadd(dmul(dadd(ar, ar), at), C1), dadd(dadd(ar2, at2), C1));
   return dmul(l, cs);
 }
 

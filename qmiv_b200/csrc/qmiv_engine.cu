@@ -20,6 +20,7 @@
 #include "qmiv_engine.h"
 
 #include <algorithm>
+#include <cassert>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -234,8 +235,8 @@ qmiv_status Engine::run(const qmiv_pair_desc* pairs, int32_t n, qmiv_result* res
   for(int i = 0; i < n; i++)
   {
     const qmiv_pair_desc& d = pairs[i];
-    if((d.metric_mask & ~(uint32_t)QMIV_ALL) != 0) { return fail(QMIV_ERR_INVALID_ARG, "unknown metric bits"); }
     QMIV_TRY(kind_for(d, kind[i]));
+    QMIV_TRY(check_metrics(kind[i]->S, d.metric_mask));
     PairSlot& p = P[i];
     const Shape& S = kind[i]->S;
     p.mask = d.metric_mask;
@@ -740,8 +741,9 @@ void Engine::add_pool_jobs(int i, const PairKind& K, int ph, char* dbase, SsimPo
       J.win = win + (size_t)(jobs_here++) * pool_win_elems(K.nx[0], K.ny[0]);
       J.C1 = K.C1; J.C2 = K.C2;
       J.mom = m.p + (size_t)c * 5 * m.plane(); J.plane = m.plane(); J.pitch = m.pitch;
-      J.nx = K.nx[scale]; J.ny = K.ny[scale]; J.calc_l = calc_l;
+      J.nx = K.nx[scale]; J.ny = K.ny[scale]; J.calc_l = calc_l; J.wide = S.bitdepth > 12 ? 1 : 0;
       J.row_sum = rowsum + (size_t)slot * 3 * K.ny[0] + (size_t)c * K.ny[scale];  // finalize reads [c][ny_scale]
+      assert(pool_job_aligned(J));
       PH.pool_max_nx = std::max(PH.pool_max_nx, J.nx);
       PH.pool_max_ny = std::max(PH.pool_max_ny, J.ny);
     }

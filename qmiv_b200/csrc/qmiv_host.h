@@ -104,6 +104,9 @@ struct Shape
 };
 
 qmiv_status validate_params(const qmiv_params& p);
+// Known metric bits, and the SSIM family only where its exact 32-bit sub-block moments hold
+// (bit depth <= 14: 16 * (2^14 - 1)^2 < 2^32).
+qmiv_status check_metrics(const Shape& S, uint32_t mask);
 
 // The device pipeline of one frame pair of a fixed shape, with its scratch buffers.
 class PairPipeline

@@ -80,6 +80,8 @@ struct SsimPoolJob
   int32_t         pitch;
   int32_t         nx, ny;      // windows per row / column
   int32_t         calc_l;
+  int32_t         wide;        // window sums can exceed 32 bits (bit depth > 12)
+  int32_t         pad_;
   double*         row_sum;     // [ny]
   double*         win;         // scratch window values [ceil(ny / 32)][nx][32] (pool_win_elems)
 };
@@ -147,6 +149,8 @@ template <typename T>
 cudaError_t launch_ssim_moments_multi(const SsimMomArgs* d_jobs, int njobs, int max_nbx, int max_nby, cudaStream_t s);
 cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max_nx, int max_ny, cudaStream_t s);
 size_t      pool_win_elems(int nx, int ny);   // doubles of SsimPoolJob::win
+// 16-byte alignment of the moment rows and the scratch, which the pooling kernels copy with cp.async
+bool        pool_job_aligned(const SsimPoolJob& J);
 cudaError_t launch_finalize_multi(const FinalizeArgs* d_pairs, const FinJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
 
 // CPS work-list form: one 64-byte aligned descriptor (tensor maps + tile geometry) per frame pair,

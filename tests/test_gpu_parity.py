@@ -114,7 +114,8 @@ def test_ssim_windows_golden(golden, qctx):
 
 @pytest.mark.parametrize("shape", [(640, 360, 8, 420, 2, False), (416, 240, 10, 420, 4, True),
                                    (352, 288, 10, 422, 3, False), (258, 130, 8, 444, 1, True),
-                                   (1280, 720, 10, 420, 2, True)])
+                                   (1280, 720, 10, 420, 2, True), (320, 240, 14, 420, 2, False),
+                                   (200, 120, 13, 444, 3, True)])
 def test_against_oracle_seeded(shape, qctx, oracle_lib):
     import qmiv_b200
     from qmiv_b200 import synth
@@ -130,6 +131,19 @@ def test_against_oracle_seeded(shape, qctx, oracle_lib):
             assert got[k][:3] == exp[k][:3] if isinstance(exp[k], list) else got[k] == exp[k], k
         s0, s1 = calc.gen_shft_comp_pics(f0, f1)
         assert np.array_equal(s0, exp["scp0"]) and np.array_equal(s1, exp["scp1"])
+
+
+def test_ssim_family_rejected_above_14_bits(qctx):
+    """The SSIM family's exact 32-bit sub-block moments need bit depth <= 14; deeper pictures are
+    refused for those metrics and still served for the PSNR family."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    f0, f1 = synth.make_pair(64, 48, 15, seed=3)
+    with qmiv_b200.Calc(qctx, 64, 48, 15) as calc:
+        with pytest.raises(qmiv_b200.QmivError) as ei:
+            calc.compute(f0, f1, qmiv_b200.IVSSIM)
+        assert "bit depth" in str(ei.value)
+        assert calc.compute(f0, f1, qmiv_b200.IVPSNR | qmiv_b200.PSNR)["ivpsnr"] > 0
 
 
 def test_full_size_erp_4096x2048_10bit(qctx, oracle_lib):
