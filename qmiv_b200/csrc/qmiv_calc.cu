@@ -180,8 +180,15 @@ qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cuda
     {
       if(!staging_.p) { return fail(QMIV_ERR_INVALID_ARG, "staging not prepared"); }
       char* dst = staging_.as<char>() + off;
-      QMIV_CUDA(cudaMemcpy2DAsync(dst, S.staged_pitch(c), f->plane[c], (size_t)f->pitch[c], row_bytes, S.plane_rows(c),
-                                  cudaMemcpyHostToDevice, s));
+      if((size_t)f->pitch[c] == row_bytes && S.staged_pitch(c) == row_bytes)
+      {
+        QMIV_CUDA(cudaMemcpyAsync(dst, f->plane[c], row_bytes * S.plane_rows(c), cudaMemcpyHostToDevice, s));
+      }
+      else
+      {
+        QMIV_CUDA(cudaMemcpy2DAsync(dst, S.staged_pitch(c), f->plane[c], (size_t)f->pitch[c], row_bytes, S.plane_rows(c),
+                                    cudaMemcpyHostToDevice, s));
+      }
       out.p[c] = dst;
       out.pitch[c] = (int32_t)(S.staged_pitch(c) / S.esz);
       off += S.staged_plane_bytes(c);

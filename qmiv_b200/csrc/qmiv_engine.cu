@@ -352,8 +352,16 @@ qmiv_status Engine::run(const qmiv_pair_desc* pairs, int32_t n, qmiv_result* res
           else if(fr->mem == QMIV_MEM_HOST)
           {
             char* dst = dbase + off;
-            QMIV_CUDA(cudaMemcpy2DAsync(dst, S.staged_pitch(c), fr->plane[c], (size_t)fr->pitch[c], row_bytes, S.plane_rows(c),
-                                        cudaMemcpyHostToDevice, cs));
+            if((size_t)fr->pitch[c] == row_bytes && S.staged_pitch(c) == row_bytes)
+            {
+              // contiguous plane on both sides: one linear copy
+              QMIV_CUDA(cudaMemcpyAsync(dst, fr->plane[c], row_bytes * S.plane_rows(c), cudaMemcpyHostToDevice, cs));
+            }
+            else
+            {
+              QMIV_CUDA(cudaMemcpy2DAsync(dst, S.staged_pitch(c), fr->plane[c], (size_t)fr->pitch[c], row_bytes, S.plane_rows(c),
+                                          cudaMemcpyHostToDevice, cs));
+            }
             out.p[c] = dst;
             out.pitch[c] = (int32_t)(S.staged_pitch(c) / S.esz);
             off += S.staged_plane_bytes(c);
