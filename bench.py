@@ -33,6 +33,9 @@ sys.path.insert(0, ROOT)
 W, H, BD, CF = 4096, 2048, 10, 420
 PAIRS_PER_STEP = 8
 METRIC_NAME = "IV-PSNR frame-pairs/s @4096x2048 10b"
+# DRAM bytes of one 8-pair k_cps_multi launch: ncu dram__bytes_read.sum + dram__bytes_write.sum of a
+# 2-pair launch of the same kernel (100.8 MB + 86.0 MB) times the ratio of pairs, 4
+CPS_TRAFFIC_BYTES = 4 * (100.8e6 + 86.0e6)
 METRICS = ("IVPSNR", "WSPSNR", "IVSSIM")
 
 
@@ -489,7 +492,9 @@ def main():
                         "bound": "int32",
                         "achieved": r["achieved"], "peak": r["int_peak"], "unit": "TOP/s",
                         "frac": r["achieved"] / r["int_peak"] if r["int_peak"] else None,
-                        "traffic": None,
+                        "traffic": CPS_TRAFFIC_BYTES,
+                        "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one k_cps_multi launch over "
+                                        "2 pairs (ncu), scaled by 4 to the 8-pair launch; bytes",
                         "accounting": "8 int32 ops per candidate, 2*W*H*25 candidates per pair, "
                                       f"{PAIRS_PER_STEP} pairs per launch; peak measured by qmiv_probe_int32_peak on "
                                       "this GPU",
