@@ -105,6 +105,20 @@ class Oracle(_Lib):
             out["scp0"], out["scp1"] = scp0.reshape(shp), scp1.reshape(shp)
         return out
 
+    def compute_pair_masked(self, params: Params, frame0, frame1, mask_plane, mask_bitdepth, mask=PSNR | WSPSNR | IVPSNR):
+        """Mask mode (GCD-M, PSNR-M, WS-PSNR-M, IV-PSNR-M); returns (result dict, NumNonMasked)."""
+        a0, p0 = _planes(frame0)
+        a1, p1 = _planes(frame1)
+        m = np.ascontiguousarray(mask_plane, np.uint8 if mask_bitdepth <= 8 else np.uint16)
+        res = Result()
+        nnm = ctypes.c_int32()
+        rc = self.lib.qo_compute_pair_masked(ctypes.byref(params), p0, p1, m.ctypes.data_as(ctypes.c_void_p),
+                                             ctypes.c_int32(mask_bitdepth), ctypes.c_uint32(mask), ctypes.byref(res),
+                                             ctypes.byref(nnm))
+        if rc != 0:
+            raise RuntimeError(f"qo_compute_pair_masked failed ({rc})")
+        return res.as_dict(), int(nnm.value)
+
     def unpack444(self, frame, width, height, bitdepth, chroma_format):
         a, p = _planes(frame)
         dst = np.zeros((3, height, width), np.uint16)
@@ -226,6 +240,20 @@ class Reference(_Lib):
             shp = (3, params.height, params.width)
             out["scp0"], out["scp1"] = scp0.reshape(shp), scp1.reshape(shp)
         return out
+
+    def compute_pair_masked(self, params: Params, frame0, frame1, mask_plane, mask_bitdepth, mask=PSNR | WSPSNR | IVPSNR):
+        """The app's mask mode (GCD-M, PSNR-M, WS-PSNR-M, IV-PSNR-M); returns (result dict, NumNonMasked)."""
+        a0, p0 = _planes(frame0)
+        a1, p1 = _planes(frame1)
+        m = np.ascontiguousarray(mask_plane, np.uint8 if mask_bitdepth <= 8 else np.uint16)
+        res = Result()
+        nnm = ctypes.c_int32()
+        rc = self.lib.ref_compute_pair_masked(ctypes.byref(params), p0, p1, m.ctypes.data_as(ctypes.c_void_p),
+                                              ctypes.c_int32(mask_bitdepth), ctypes.c_uint32(mask), ctypes.byref(res),
+                                              ctypes.byref(nnm))
+        if rc != 0:
+            raise RuntimeError(f"ref_compute_pair_masked failed ({rc})")
+        return res.as_dict(), int(nnm.value)
 
     def cps_rows(self, tst444, ref444, bitdepth, gcd, search_range=2, cws=(4, 1, 1, 0)):
         t, r = _u16(tst444), _u16(ref444)

@@ -377,6 +377,218 @@ static double qo_ivpsnr_quality(const uint64_t* row_sse, int32_t W, int32_t H, i
 }
 
 /* ----------------------------------------------------------------------------------------------- */
+/* Mask mode: the mask picture's luma weights every sample (eCmp::LM in every *M call).            */
+/* ----------------------------------------------------------------------------------------------- */
+
+/* xPixelOpsSTD::CountNonZero, libs/pmbb-core/src/xPixelOpsSTD.cpp:273-284 */
+int32_t qo_count_nonzero(const uint16_t* msk, int32_t W, int32_t H)
+{
+  int32_t n = 0;
+  for(size_t i = 0; i < (size_t)W * H; i++) { n += msk[i] != 0; }
+  return n;
+}
+
+/* xGlobClrDiff::CalcGlobalColorDiffM, libs/pmbb-ivqm/src/xGlobClrDiff.cpp:60-91, with
+   xDistortionSTD::CalcWeightedSD (libs/pmbb-core/src/xDistortionSTD.cpp:45-56: int32 product). */
+void qo_gcd_masked(const uint16_t* tst, const uint16_t* ref, const uint16_t* msk, int32_t W, int32_t H, int32_t bitdepth,
+                   int32_t mask_bitdepth, const float coef[4], int32_t nnm, int32_t gcd[4])
+{
+  const int32_t maxv = qo_max_value(bitdepth);
+  int64_t sd[4] = { 0, 0, 0, 0 };
+  for(int32_t c = 0; c < 3; c++)
+  {
+    const uint16_t* t = tst + (size_t)c * W * H;
+    const uint16_t* r = ref + (size_t)c * W * H;
+    for(size_t i = 0; i < (size_t)W * H; i++) { sd[c] += ((int32_t)t[i] - (int32_t)r[i]) * (int32_t)msk[i]; }
+  }
+  const double den = (double)((int64_t)nnm * (int64_t)qo_max_value(mask_bitdepth));
+  for(int32_t c = 0; c < 4; c++)
+  {
+    const int32_t maxdiff = qo_round_f32(coef[c] * (float)maxv);
+    gcd[c] = qo_clampi(qo_round_f64((double)sd[c] / den), -maxdiff, maxdiff);
+  }
+}
+
+/* One masked CPS direction, xCorrespPixelShiftSTD::CalcDistAsymmetricRowM and
+   FindBestPixelWithinBlockM, libs/pmbb-ivqm/src/xCorrespPixelShiftSTD.cpp:151-215: masked test pixels
+   are skipped, masked candidates are skipped (the mask is edge-extended like the pictures), the
+   winner's squared differences are weighted by the test pixel's mask value, uint64 row sums. */
+void qo_cps_masked(const uint16_t* tst, const uint16_t* ref, const uint16_t* msk, int32_t W, int32_t H, const int32_t gcd[4],
+                   int32_t R, const int32_t cws[4], uint64_t* row_sse)
+{
+  const size_t pl = (size_t)W * H;
+  for(int32_t y = 0; y < H; y++)
+  {
+    uint64_t rowsum[3] = { 0, 0, 0 };
+    for(int32_t x = 0; x < W; x++)
+    {
+      const int32_t m = msk[(size_t)y * W + x];
+      if(m == 0) { continue; }
+      int32_t s[3];
+      for(int32_t c = 0; c < 3; c++) { s[c] = (int32_t)tst[c * pl + (size_t)y * W + x] + gcd[c]; }
+      int32_t best_err = INT32_MAX; int32_t best_pel[3] = { 0, 0, 0 };
+      for(int32_t dy = -R; dy <= R; dy++)
+      {
+        const int32_t yy = qo_clampi(y + dy, 0, H - 1);
+        for(int32_t dx = -R; dx <= R; dx++)
+        {
+          const int32_t xx = qo_clampi(x + dx, 0, W - 1);
+          if(msk[(size_t)yy * W + xx] == 0) { continue; }
+          uint32_t err = 0; int32_t pel[3];
+          for(int32_t c = 0; c < 3; c++)
+          {
+            pel[c] = ref[c * pl + (size_t)yy * W + xx];
+            const int32_t d = s[c] - pel[c];
+            err += (uint32_t)(d * d) * (uint32_t)cws[c];
+          }
+          if((int32_t)err < best_err) { best_err = (int32_t)err; for(int32_t c = 0; c < 3; c++) { best_pel[c] = pel[c]; } }
+        }
+      }
+      for(int32_t c = 0; c < 3; c++)
+      {
+        const int32_t d = s[c] - best_pel[c];
+        rowsum[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)m;
+      }
+    }
+    for(int32_t c = 0; c < 3; c++) { row_sse[(size_t)y * 3 + c] = rowsum[c]; }
+  }
+}
+
+/* xPSNR::CalcPSNRfromMaskedSSD, libs/pmbb-ivqm/src/xPSNR.cpp:198-205 (MAX formed in int64) */
+static double qo_psnr_from_masked_ssd(double ssd, int32_t nnm, int32_t bitdepth_pic, int32_t bitdepth_msk)
+{
+  const uint64_t mp = (uint64_t)qo_max_value(bitdepth_pic), mm = (uint64_t)qo_max_value(bitdepth_msk);
+  const int64_t  MAX = (int64_t)((uint64_t)(int64_t)nnm * (mp * mp) * mm);
+  return ssd > 0 ? 10.0 * log10((double)MAX / ssd) : DBL_MAX;
+}
+
+/* xIVPSNRM::xCalcQualAsymmetricPicM, libs/pmbb-ivqm/src/xIVPSNR.cpp:172-200 */
+static double qo_ivpsnr_quality_masked(const uint64_t* row_sse, int32_t H, int32_t bitdepth, int32_t mask_bitdepth, int32_t nnm,
+                                       const double* ws, const int32_t cwa[4])
+{
+  double err[3];
+  for(int32_t c = 0; c < 3; c++)
+  {
+    if(ws)
+    {
+      qo_kbns k = { 0.0, 0.0 };
+      for(int32_t y = 0; y < H; y++) { qo_kbns_add(&k, (double)row_sse[(size_t)y * 3 + c] * ws[y]); }
+      err[c] = qo_kbns_result(&k);
+    }
+    else
+    {
+      uint64_t t = 0;
+      for(int32_t y = 0; y < H; y++) { t += row_sse[(size_t)y * 3 + c]; }
+      err[c] = (double)t;
+    }
+  }
+  double q[4] = { 0, 0, 0, 0 };
+  for(int32_t c = 0; c < 3; c++) { q[c] = qo_psnr_from_masked_ssd(err[c] > 0 ? err[c] : 1.0, nnm, bitdepth, mask_bitdepth); }
+  const int32_t wsum = cwa[0] + cwa[1] + cwa[2] + cwa[3];
+  const double  inv  = 1.0 / (double)wsum;
+  return (q[0] * (double)cwa[0] + q[1] * (double)cwa[1] + q[2] * (double)cwa[2] + q[3] * (double)cwa[3]) * inv;
+}
+
+/* Mask mode of the app: apps/QMIV/src/xAppQMIV.cpp:900-906 (NumNonMasked), :930 (GCD-M), :971 (PSNR-M),
+   :999 (WS-PSNR-M), :1026-1028 (IV-PSNR-M); SSIM metrics are refused with a mask (:360-365).
+   mask_plane: W x H, 1 byte per sample for mask_bitdepth 8, else 2. */
+int qo_compute_pair_masked(const qo_params* p, const void* const planes0[3], const void* const planes1[3], const void* mask_plane,
+                           int32_t mask_bitdepth, uint32_t mask, qo_result* out, int32_t* num_non_masked)
+{
+  if(mask & (QO_SSIM | QO_MSSSIM | QO_IVSSIM | QO_IVMSSSIM)) { return 1; }
+  const int32_t W = p->width, H = p->height, BD = p->bitdepth;
+  const size_t  n = (size_t)W * H * 3, pl = (size_t)W * H;
+  const int64_t area = (int64_t)W * H;
+  memset(out, 0, sizeof(*out));
+
+  uint16_t* P0 = (uint16_t*)malloc(n * sizeof(uint16_t));
+  uint16_t* P1 = (uint16_t*)malloc(n * sizeof(uint16_t));
+  uint16_t* M  = (uint16_t*)malloc(pl * sizeof(uint16_t));
+  qo_unpack444(planes0, W, H, BD, p->chroma_format, P0);
+  qo_unpack444(planes1, W, H, BD, p->chroma_format, P1);
+  for(size_t i = 0; i < pl; i++) { M[i] = mask_bitdepth <= 8 ? ((const uint8_t*)mask_plane)[i] : ((const uint16_t*)mask_plane)[i]; }
+  const int32_t nnm = qo_count_nonzero(M, W, H);
+  *num_non_masked = nnm;
+
+  int32_t exact[3];
+  for(int32_t c = 0; c < 3; c++)
+  {
+    exact[c] = memcmp(P0 + (size_t)c * pl, P1 + (size_t)c * pl, pl * sizeof(uint16_t)) == 0;
+    out->exact[c] = exact[c];
+  }
+  double* ws = NULL; double ws_corr = 1.0;
+  if(p->erp) { ws = (double*)malloc((size_t)H * sizeof(double)); qo_ws_weights(H, p->lat_range, ws, &ws_corr); }
+  const double inv_cwa = 1.0 / (double)(p->cwa[0] + p->cwa[1] + p->cwa[2] + p->cwa[3]);
+  #define QO_PER_PIC(v) (((v)[0] * p->cwa[0] + (v)[1] * p->cwa[1] + (v)[2] * p->cwa[2]) * inv_cwa) /* xMetricQMIV.cpp:91-97 */
+  const double fake = qo_psnr_from_ssd(1, area, BD); /* getFakePSNR(area, picture bit depth), xAppQMIV.cpp:974-981 */
+
+  int32_t gcd[4] = { 0, 0, 0, 0 }, ngcd[4];
+  if(mask & QO_IVPSNR) { qo_gcd_masked(P1, P0, M, W, H, BD, mask_bitdepth, p->unc, nnm, gcd); } /* swap as xGlobClrDiff.h:42 */
+  for(int32_t c = 0; c < 4; c++) { out->gcd_r2t[c] = gcd[c]; ngcd[c] = -gcd[c]; }
+
+  if(mask & (QO_PSNR | QO_WSPSNR))
+  {
+    /* xDistortionSTD::CalcWeightedSSD, libs/pmbb-core/src/xDistortionSTD.cpp:57-68 */
+    uint64_t ssd[3] = { 0, 0, 0 };
+    for(int32_t c = 0; c < 3; c++)
+    {
+      const uint16_t* a = P0 + (size_t)c * pl; const uint16_t* b = P1 + (size_t)c * pl;
+      for(size_t i = 0; i < pl; i++) { const int32_t d = (int32_t)a[i] - (int32_t)b[i]; ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)M[i]; }
+    }
+    /* xPSNR::calcPicPSNRM, libs/pmbb-ivqm/src/xPSNR.cpp:54-66: the mask's bit depth stands for both
+       the picture's and the mask's (CalcPSNRsFromMaskedSSDs(.., Msk->getBitDepth(), Msk->getBitDepth())) */
+    double psnrm[3];
+    for(int32_t c = 0; c < 3; c++) { psnrm[c] = qo_psnr_from_masked_ssd((double)ssd[c], nnm, mask_bitdepth, mask_bitdepth); }
+    if(mask & QO_PSNR)
+    {
+      for(int32_t c = 0; c < 3; c++) { out->psnr[c] = exact[c] ? fake : psnrm[c]; }
+      out->psnr_pic = QO_PER_PIC(out->psnr);
+    }
+    if(mask & QO_WSPSNR) /* xWSPSNR.cpp:51-77 (no ERP: PSNR-M), :108-133 */
+    {
+      for(int32_t c = 0; c < 3; c++)
+      {
+        double v = psnrm[c];
+        if(ws)
+        {
+          const uint16_t* a = P0 + (size_t)c * pl; const uint16_t* b = P1 + (size_t)c * pl;
+          qo_kbns k = { 0.0, 0.0 };
+          for(int32_t y = 0; y < H; y++)
+          {
+            uint64_t rs = 0;
+            for(int32_t x = 0; x < W; x++)
+            {
+              const size_t i = (size_t)y * W + x;
+              const int32_t d = (int32_t)b[i] - (int32_t)a[i];
+              rs += (uint64_t)(int64_t)(d * d) * (uint64_t)M[i];
+            }
+            qo_kbns_add(&k, (double)rs * ws[y]);
+          }
+          const double e = qo_kbns_result(&k) * ws_corr;
+          v = qo_psnr_from_masked_ssd(e, nnm, BD, mask_bitdepth);
+        }
+        out->wspsnr[c] = exact[c] ? fake : v;
+      }
+      out->wspsnr_pic = QO_PER_PIC(out->wspsnr);
+    }
+  }
+  if(mask & QO_IVPSNR) /* xIVPSNRM::calcPicIVPSNRM, xIVPSNR.cpp:153-170: R2T searches In1 in In0 with -GCD */
+  {
+    uint64_t* rows = (uint64_t*)malloc((size_t)H * 3 * sizeof(uint64_t));
+    qo_cps_masked(P1, P0, M, W, H, ngcd, p->search_range, p->cws, rows);
+    const double r2t = qo_ivpsnr_quality_masked(rows, H, BD, mask_bitdepth, nnm, ws, p->cwa);
+    qo_cps_masked(P0, P1, M, W, H, gcd, p->search_range, p->cws, rows);
+    const double t2r = qo_ivpsnr_quality_masked(rows, H, BD, mask_bitdepth, nnm, ws, p->cwa);
+    free(rows);
+    out->ivpsnr_r2t = r2t; out->ivpsnr_t2r = t2r;
+    out->ivpsnr = t2r < r2t ? t2r : r2t;
+  }
+  #undef QO_PER_PIC
+  free(P0); free(P1); free(M); free(ws);
+  return 0;
+}
+
+/* ----------------------------------------------------------------------------------------------- */
 /* Full frame pipeline, apps/QMIV/src/xAppQMIV.cpp:761-827 and the calcFrame* functions :927-1108   */
 /* ----------------------------------------------------------------------------------------------- */
 int qo_compute_pair(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,

@@ -83,6 +83,16 @@ int32_t qo_num_scales(int32_t W, int32_t H);
 int qo_compute_pair(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,
                     qo_result* out, uint16_t* scp0, uint16_t* scp1);
 
+/* Mask mode (GCD-M, CPS-M, PSNR-M, WS-PSNR-M, IV-PSNR-M): mask_plane is the mask's luma, W x H,
+   1 byte per sample for mask_bitdepth 8, else 2. Returns nonzero for SSIM metric bits. */
+int qo_compute_pair_masked(const qo_params* p, const void* const planes0[3], const void* const planes1[3], const void* mask_plane,
+                           int32_t mask_bitdepth, uint32_t mask, qo_result* out, int32_t* num_non_masked);
+int32_t qo_count_nonzero(const uint16_t* msk, int32_t W, int32_t H);
+void qo_gcd_masked(const uint16_t* tst, const uint16_t* ref, const uint16_t* msk, int32_t W, int32_t H, int32_t bitdepth,
+                   int32_t mask_bitdepth, const float coef[4], int32_t nnm, int32_t gcd[4]);
+void qo_cps_masked(const uint16_t* tst, const uint16_t* ref, const uint16_t* msk, int32_t W, int32_t H, const int32_t gcd[4],
+                   int32_t R, const int32_t cws[4], uint64_t* row_sse);
+
 #ifdef __cplusplus
 }
 #endif

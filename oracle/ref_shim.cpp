@@ -13,6 +13,7 @@
     apps/QMIV/src/xAppQMIV.cpp:927-948   calcFrameGCD / calcFrameSCP
     apps/QMIV/src/xAppQMIV.cpp:967-1108  calcFrame____PSNR .. calcFrameIVMSSSIM
     apps/QMIV/src/xAppQMIV.cpp:680-744   createProcessors (parameter plumbing)
+    apps/QMIV/src/xAppQMIV.cpp:900-1030  mask mode (NumNonMasked, GCD-M, PSNR-M, WS-PSNR-M, IV-PSNR-M)
     libs/pmbb-core/src/xSeq.cpp:231-290  xUnpackFrame (8->16 bit, chroma upsampling)
 */
 #include "xPic.h"
@@ -240,6 +241,77 @@ int ref_compute_pair(const ref_params* P, const void* const Planes0[3], const vo
   }
 
   if(CalcSSIMs) { ProcSSIM.destroy(); }
+  return 0;
+}
+
+/* Mask mode of the reference app for one frame pair: the mask picture's luma (W x H, 1 byte per
+   sample for MaskBitDepth 8, else 2 bytes) weights every sample; metrics limited to PSNR, WS-PSNR and
+   IV-PSNR as the app requires (xAppQMIV.cpp:360-365). NumNonMasked receives CountNonZero(mask). */
+int ref_compute_pair_masked(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3],
+                            const void* MaskPlane, int32_t MaskBitDepth, uint32_t Mask, ref_result* Out, int32_t* NumNonMaskedOut)
+{
+  const int32   W = P->width, H = P->height, BD = P->bitdepth;
+  const int32V2 Size = { W, H };
+  const int32   Margin = xRoundUpToNearestMultiple(P->search_range, 2);
+  const int32V4 Cws = { P->cws[0], P->cws[1], P->cws[2], P->cws[3] };
+  const int32V4 Cwa = { P->cwa[0], P->cwa[1], P->cwa[2], P->cwa[3] };
+  const flt32V4 Unc = { P->unc[0], P->unc[1], P->unc[2], P->unc[3] };
+  if(Mask & (REF_SSIM | REF_MSSSIM | REF_IVSSIM | REF_IVMSSSIM)) { return 1; }
+
+  Pool TP(P->num_threads, H);
+
+  xPicP PicP[3]; xPicI PicI[2];
+  for(int32 i = 0; i < 2; i++) { PicP[i].create(Size, BD, Margin); PicI[i].create(Size, BD, Margin); }
+  PicP[2].create(Size, MaskBitDepth, Margin);
+  loadFrame(PicP[0], Planes0, W, H, BD, P->chroma_format);
+  loadFrame(PicP[1], Planes1, W, H, BD, P->chroma_format);
+  // the mask file is read like the inputs; only its luma is used (eCmp::LM in every *M call)
+  if(MaskBitDepth <= 8) { xPixelOps::Cvt(PicP[2].getAddr(eCmp::LM), (const uint8*)MaskPlane, PicP[2].getStride(), W, W, H); }
+  else                  { xPixelOps::Copy(PicP[2].getAddr(eCmp::LM), (const uint16*)MaskPlane, PicP[2].getStride(), W, W, H); }
+  for(int32 c = 1; c < 3; c++) { PicP[2].fill(0, (eCmp)c); }
+
+  std::memset(Out, 0, sizeof(ref_result));
+  bool Exact[3];
+  for(int32 c = 0; c < 3; c++) { Exact[c] = PicP[0].equalCmp(&PicP[1], (eCmp)c); Out->exact[c] = Exact[c]; }
+  for(int32 i = 0; i < 3; i++) { PicP[i].extend(); }
+  const int32 NumNonMasked = xPixelOps::CountNonZero(PicP[2].getAddr(eCmp::LM), PicP[2].getStride(), W, H);
+  *NumNonMaskedOut = NumNonMasked;
+  for(int32 i = 0; i < 2; i++) { PicI[i].rearrangeFromPlanar(&PicP[i]); }
+
+  xGlobClrDiffProc ProcGCD; xIVPSNRM ProcPSNR;
+  ProcGCD.setUnntcbCoef(Unc); ProcGCD.bindThrdPoolIntf(&TP.TPI);
+  ProcPSNR.setSearchRange(P->search_range); ProcPSNR.setCmpWeightsSearch(Cws); ProcPSNR.setCmpWeightsAverage(Cwa);
+  ProcPSNR.setUnntcbCoef(Unc); ProcPSNR.bindThrdPoolIntf(&TP.TPI); ProcPSNR.initRowBuffers(H);
+  if(P->erp) { ProcPSNR.initWS(true, W, H, BD, P->lon_range, P->lat_range); }
+
+  flt64 LastR2T = 0, LastT2R = 0;
+  ProcPSNR.setDebugCallbackQAP([&](flt64 R2T, flt64 T2R) { LastR2T = R2T; LastT2R = T2R; });
+  const flt64 InvDen = 1.0 / (flt64)Cwa.getSum();
+  auto PerPic = [&](const flt64V4& V) { return (V[0] * Cwa[0] + V[1] * Cwa[1] + V[2] * Cwa[2]) * InvDen; };
+
+  int32V4 GCD = { 0, 0, 0, 0 };
+  if(Mask & REF_IVPSNR) { GCD = ProcGCD.CalcGlobalColorDiffM(&PicP[0], &PicP[1], &PicP[2], NumNonMasked); }
+  for(int32 c = 0; c < 4; c++) { Out->gcd_r2t[c] = GCD[c]; }
+
+  if(Mask & REF_PSNR)
+  {
+    flt64V4 V = ProcPSNR.calcPicPSNRM(&PicP[0], &PicP[1], &PicP[2], NumNonMasked);
+    for(int32 c = 0; c < 3; c++) { if(Exact[c]) { V[c] = ProcPSNR.getFakePSNR(PicP[0].getArea(), PicP[0].getBitDepth()); } }
+    for(int32 c = 0; c < 3; c++) { Out->psnr[c] = V[c]; }
+    Out->psnr_pic = PerPic(V);
+  }
+  if(Mask & REF_WSPSNR)
+  {
+    flt64V4 V = ProcPSNR.calcPicWSPSNRM(&PicP[0], &PicP[1], &PicP[2], NumNonMasked);
+    for(int32 c = 0; c < 3; c++) { if(Exact[c]) { V[c] = ProcPSNR.getFakePSNR(PicP[0].getArea(), PicP[0].getBitDepth()); } }
+    for(int32 c = 0; c < 3; c++) { Out->wspsnr[c] = V[c]; }
+    Out->wspsnr_pic = PerPic(V);
+  }
+  if(Mask & REF_IVPSNR)
+  {
+    Out->ivpsnr = ProcPSNR.calcPicIVPSNRM(&PicI[0], &PicI[1], &PicP[2], NumNonMasked, GCD);
+    Out->ivpsnr_r2t = LastR2T; Out->ivpsnr_t2r = LastT2R;
+  }
   return 0;
 }
 

@@ -30,6 +30,12 @@ def golden():
 
 
 @pytest.fixture(scope="session")
+def golden_masked():
+    with open(os.path.join(GOLDEN, "golden_masked.json")) as f:
+        return json.load(f)["masked"]
+
+
+@pytest.fixture(scope="session")
 def cps_arrays():
     import numpy as np
     return dict(np.load(os.path.join(GOLDEN, "cps_fixtures.npz")))

@@ -77,3 +77,27 @@ def to444(frame, chroma_format=420):
     for c in (1, 2):
         out[c] = np.repeat(np.repeat(frame[c], 1 << sy, axis=0), 1 << sx, axis=1)[:h, :w]
     return out
+
+
+def det_mask(width, height, bitdepth, seed, kind="binary"):
+    """A mask picture's luma (H, W) for mask mode: 'binary' (0 or the maximum, about 60 % kept),
+    'weights' (0..maximum, about 80 % non-zero), 'sparse' (about 5 % non-zero), 'ones' (all maximum),
+    'region' (a rectangle kept, the rest masked)."""
+    maxv = (1 << bitdepth) - 1
+    dtype = np.uint8 if bitdepth <= 8 else np.uint16
+    r = _stream(seed, 300, 2 * width * height).astype(np.int64)
+    a, b = r[: width * height].reshape(height, width), r[width * height:].reshape(height, width)
+    if kind == "binary":
+        m = np.where(a % 100 < 60, maxv, 0)
+    elif kind == "weights":
+        m = np.where(a % 100 < 80, b % (maxv + 1), 0)
+    elif kind == "sparse":
+        m = np.where(a % 100 < 5, 1 + b % maxv, 0)
+    elif kind == "ones":
+        m = np.full((height, width), maxv)
+    elif kind == "region":
+        m = np.zeros((height, width), np.int64)
+        m[height // 4: (3 * height) // 4, width // 3: (2 * width) // 3] = maxv
+    else:
+        raise ValueError(kind)
+    return m.astype(dtype)

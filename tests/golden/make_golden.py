@@ -8,7 +8,8 @@ The x86-64-v3 (AVX2) build is used: the x86-64-v4 (AVX-512) build of the referen
 8-bit 4:2:0 chroma when the picture width is 64 modulo 128 (xPixelOpsAVX512.cpp CvtUpsampleHV builds
 a store mask with a 64-bit shift by 64), which the portable and AVX2 builds do not.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # golden.json
+    python tests/golden/make_golden.py masked     # golden_masked.json (mask mode)
 """
 from __future__ import annotations
 
@@ -25,7 +26,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
 import oracle  # noqa: E402
-from detgen import det_pair, hash32, to444  # noqa: E402
+from detgen import det_mask, det_pair, hash32, to444  # noqa: E402
 
 ARCH = "x86-64-v3"
 
@@ -167,6 +168,48 @@ def make_ssim_windows(ref):
     return cases
 
 
+# mask mode: (width, height, bitdepth, chroma_format, R, erp, seed, mask bit depth, mask kind)
+MASKED_CASES = [
+    (64, 64, 10, 420, 2, True, 21, 8, "binary"),
+    (64, 48, 8, 444, 3, False, 22, 10, "weights"),
+    (96, 64, 10, 422, 2, True, 23, 14, "weights"),
+    (130, 66, 8, 420, 1, False, 24, 8, "sparse"),
+    (128, 64, 12, 420, 2, True, 25, 10, "binary"),
+    (64, 64, 10, 420, 4, False, 26, 8, "ones"),
+    (256, 128, 10, 420, 2, True, 27, 8, "region"),
+    (200, 100, 8, 420, 5, False, 28, 12, "weights"),
+    (66, 34, 10, 420, 2, True, 29, 8, "binary"),
+    (1920, 1080, 8, 420, 2, False, 30, 8, "binary"),
+]
+
+
+def make_masked(ref):
+    """The app's mask mode (xAppQMIV.cpp:900-1030) run by the compiled reference: GCD-M, PSNR-M,
+    WS-PSNR-M, IV-PSNR-M and the number of non-masked samples. Frames and masks come from detgen."""
+    out = []
+    for (W, H, bd, cf, R, erp, seed, mbd, kind) in MASKED_CASES:
+        p = oracle.make_params(W, H, bd, cf, search_range=R, erp=erp, num_threads=8)
+        f0, f1 = det_pair(W, H, bd, seed, cf)
+        m = det_mask(W, H, mbd, seed, kind)
+        r, nnm = ref.compute_pair_masked(p, f0, f1, m, mbd)
+        keys = ["gcd_r2t", "exact", "psnr", "psnr_pic", "wspsnr", "wspsnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"]
+        exp = {k: ([fhex(x) if isinstance(x, float) else int(x) for x in r[k]] if isinstance(r[k], list)
+                   else fhex(r[k])) for k in keys}
+        exp["num_non_masked"] = nnm
+        out.append(dict(width=W, height=H, bitdepth=bd, chroma_format=cf, search_range=R, erp=erp, seed=seed,
+                        mask_bitdepth=mbd, mask_kind=kind, expected=exp))
+        print("masked", W, H, bd, cf, R, erp, mbd, kind, nnm, r["ivpsnr"])
+    return out
+
+
+def main_masked():
+    ref = oracle.Reference(ARCH)
+    data = dict(generator="tests/golden/make_golden.py masked", reference_build=ARCH, masked=make_masked(ref))
+    with open(os.path.join(HERE, "golden_masked.json"), "w") as f:
+        json.dump(data, f, separators=(",", ":"))
+    print("wrote", os.path.join(HERE, "golden_masked.json"))
+
+
 def main():
     ref = oracle.Reference(ARCH)
     data = dict(generator="tests/golden/make_golden.py", reference_build=ARCH,
@@ -177,4 +220,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["masked"]:
+        main_masked()
+    else:
+        main()

@@ -62,3 +62,22 @@ def compare_result(got, expected, mask, ignore=()):
 
 def sha256(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def masked_case_inputs(case):
+    """Frames and mask of a golden mask-mode case (detgen)."""
+    from detgen import det_mask
+    f0, f1 = det_pair(case["width"], case["height"], case["bitdepth"], case["seed"], case["chroma_format"])
+    m = det_mask(case["width"], case["height"], case["mask_bitdepth"], case["seed"], case["mask_kind"])
+    return f0, f1, m
+
+
+MASKED_METRICS = 1 | 2 | 4
+
+
+def compare_masked(got, nnm, expected):
+    """Bit-exact comparison of a mask-mode result against its golden block. Returns mismatches."""
+    bad = compare_result(got, expected, MASKED_METRICS)
+    if nnm != expected["num_non_masked"]:
+        bad.append(("num_non_masked", nnm, expected["num_non_masked"]))
+    return bad

@@ -112,3 +112,36 @@ def test_num_scales(oracle_lib):
     assert oracle_lib.num_scales(256, 128) == 3
     assert oracle_lib.num_scales(31, 500) == 0
     assert oracle_lib.num_scales(4096, 2048) == 5
+
+
+def _masked_ids():
+    import json, os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "golden_masked.json")) as f:
+        g = json.load(f)["masked"]
+    return [f"{c['width']}x{c['height']}_{c['bitdepth']}b_{c['chroma_format']}_R{c['search_range']}"
+            f"{'_erp' if c['erp'] else ''}_m{c['mask_bitdepth']}{c['mask_kind']}" for c in g]
+
+
+@pytest.mark.parametrize("idx", range(len(_masked_ids())), ids=_masked_ids())
+def test_masked_pipeline_matches_reference(idx, golden_masked, oracle_lib):
+    """Mask mode (GCD-M, CPS-M, PSNR-M, WS-PSNR-M, IV-PSNR-M) of the restatement against the compiled
+    reference's outputs, bit for bit, including the reference's bit-depth choice in PSNR-M and its
+    direction labels in IV-PSNR-M."""
+    import oracle
+    from golden_cases import compare_masked, masked_case_inputs
+    case = golden_masked[idx]
+    f0, f1, m = masked_case_inputs(case)
+    p = oracle.make_params(case["width"], case["height"], case["bitdepth"], case["chroma_format"],
+                           search_range=case["search_range"], erp=case["erp"])
+    got, nnm = oracle_lib.compute_pair_masked(p, f0, f1, m, case["mask_bitdepth"])
+    assert compare_masked(got, nnm, case["expected"]) == []
+
+
+def test_masked_refuses_ssim(oracle_lib):
+    import numpy as np
+    import oracle
+    from detgen import det_mask, det_pair
+    f0, f1 = det_pair(32, 32, 8, 1, 420)
+    p = oracle.make_params(32, 32, 8, 420)
+    with pytest.raises(RuntimeError):
+        oracle_lib.compute_pair_masked(p, f0, f1, det_mask(32, 32, 8, 1), 8, oracle.IVSSIM)
