@@ -180,6 +180,24 @@ QMIV_API qmiv_status qmiv_frame_pair_submit(qmiv_calc calc, const qmiv_frame* in
                                    uint32_t metric_mask);
 QMIV_API qmiv_status qmiv_frame_pair_wait(qmiv_calc calc, int32_t timeout_ms, qmiv_result* out);
 
+/* Mask mode, the app's -im option (apps/QMIV/src/xAppQMIV.cpp:900-1030): every sample is weighted by
+   the mask picture's luma value M(x, y) (plane[0] of `mask`, W x H, 1 byte per sample for
+   mask_bitdepth 8, else 2; mask_bitdepth 8..14). Replaces the reference's *M processor calls:
+     xGlobClrDiffProc::CalcGlobalColorDiffM   (xGlobClrDiff.h:42)     -> out->gcd_r2t
+     xPSNR::calcPicPSNRM                      (xPSNR.cpp:54-66)       -> out->psnr[], psnr_pic
+     xWSPSNR::calcPicWSPSNRM                  (xWSPSNR.cpp:51-77)     -> out->wspsnr[], wspsnr_pic
+     xIVPSNRM::calcPicIVPSNRM                 (xIVPSNR.cpp:153-170)   -> out->ivpsnr, _r2t, _t2r
+   with the reference's arithmetic, including two of its conventions: PSNR-M takes the mask's bit
+   depth for the picture's maximum (xPSNR.cpp:61), and IV-PSNR-M labels the search of In1 in In0
+   "R2T" (xIVPSNR.cpp:161). out->ssd holds the weighted SSDs, cps_sse_* the weighted CPS sums.
+   metric_mask may hold QMIV_PSNR, QMIV_WSPSNR and QMIV_IVPSNR; the SSIM family is refused with
+   QMIV_ERR_UNSUPPORTED as the app refuses it (xAppQMIV.cpp:360-365). num_non_masked (may be NULL)
+   receives the count of non-zero mask samples (xAppQMIV.cpp:904); an all-zero mask is
+   QMIV_ERR_INVALID_ARG. Blocks until done. */
+QMIV_API qmiv_status qmiv_frame_pair_compute_masked(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1,
+                                                    const qmiv_frame* mask, int32_t mask_bitdepth, uint32_t metric_mask,
+                                                    qmiv_result* out, int32_t* num_non_masked);
+
 /* xGlobClrDiffProc::CalcGlobalColorDiff(Tst=In0, Ref=In1) -> round(mean(In1 - In0)), clipped. */
 QMIV_API qmiv_status qmiv_calc_gcd(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, int32_t gcd_r2t[4]);
 

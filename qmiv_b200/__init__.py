@@ -173,6 +173,21 @@ class Calc:
                                                 metric_mask(metrics), ctypes.byref(res)), "qmiv_frame_pair_compute")
         return res.as_dict()
 
+    def compute_masked(self, frame0, frame1, mask, mask_bitdepth: int, metrics=None):
+        """Mask mode (qmiv_frame_pair_compute_masked): mask is the mask picture's luma plane (H x W;
+        uint8 for mask_bitdepth 8, else uint16; host array or CUDA tensor). Returns (result dict,
+        number of non-zero mask samples)."""
+        f0, k0 = make_frame(frame0)
+        f1, k1 = make_frame(frame1)
+        fm, km = make_frame((mask, mask, mask))
+        res = _lib.QmivResult()
+        nnm = ctypes.c_int32()
+        m = metric_mask(metrics) if metrics is not None else PSNR | WSPSNR | IVPSNR
+        check(self._lib.qmiv_frame_pair_compute_masked(self.handle, ctypes.byref(f0), ctypes.byref(f1), ctypes.byref(fm),
+                                                       mask_bitdepth, m, ctypes.byref(res), ctypes.byref(nnm)),
+              "qmiv_frame_pair_compute_masked")
+        return res.as_dict(), int(nnm.value)
+
     def submit(self, frame0, frame1, metrics=None):
         f0, k0 = make_frame(frame0)
         f1, k1 = make_frame(frame1)

@@ -101,6 +101,9 @@ SIGNATURES = {
     "qmiv_calc_destroy": (ctypes.c_int, [_P]),
     "qmiv_frame_pair_compute": (ctypes.c_int, [_P, ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame),
                                                ctypes.c_uint32, ctypes.POINTER(QmivResult)]),
+    "qmiv_frame_pair_compute_masked": (ctypes.c_int, [_P, ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame),
+                                                      ctypes.POINTER(QmivFrame), ctypes.c_int32, ctypes.c_uint32,
+                                                      ctypes.POINTER(QmivResult), ctypes.POINTER(ctypes.c_int32)]),
     "qmiv_frame_pair_submit": (ctypes.c_int, [_P, ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame), ctypes.c_uint32]),
     "qmiv_frame_pair_wait": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(QmivResult)]),
     "qmiv_calc_gcd": (ctypes.c_int, [_P, ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame), ctypes.c_int32 * 4]),

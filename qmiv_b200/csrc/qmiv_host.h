@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <memory>
 #include <vector>
 
 struct qmiv_ctx_s
@@ -124,6 +125,9 @@ public:
   // SCP planes (T samples, planar 3 x W*H) of the last run, or null
   const void* scp(int which) const;
   const uint32_t* cps_rows() const { return cps_rows_.as<uint32_t>(); }
+  const double* ws_device() const { return ws_.as<double>(); }   // ERP row weights, after prepare()
+  double ws_corr() const { return ws_corr_; }
+  const int32_t* maxdiff() const { return maxdiff_; }
   const Shape& shape() const { return shape_; }
   int32_t search_range() const { return R_; }
   void set_gcd_override(const int32_t* g)
@@ -183,6 +187,19 @@ private:
   std::vector<std::pair<int, int>> ev_pending_;  // (stage, index of the begin event)
 };
 
+// Mask mode of one calc (qmiv_masked.cu): its scratch and the synchronous run.
+class MaskedPipeline
+{
+public:
+  qmiv_status run(qmiv_calc_s* calc, const qmiv_frame* in0, const qmiv_frame* in1, const qmiv_frame* mask,
+                  int32_t mask_bitdepth, uint32_t metrics, qmiv_result* out, int32_t* num_non_masked);
+  ~MaskedPipeline();
+
+private:
+  DevMem out_, rows_, stage_;
+  void*  h_out_ = nullptr;
+};
+
 }  // namespace qmiv
 
 struct qmiv_calc_s
@@ -196,4 +213,5 @@ struct qmiv_calc_s
   bool                 pending = false;
   uint32_t             pending_mask = 0;
   bool                 has_last = false;
+  std::unique_ptr<qmiv::MaskedPipeline> masked;   // created by the first masked call
 };

@@ -1,0 +1,407 @@
+// Mask mode on B200: the reference app's -im option (apps/QMIV/src/xAppQMIV.cpp:900-1030), where a
+// mask picture's luma weights every sample of PSNR, WS-PSNR and IV-PSNR (the STD-only *M processor
+// calls; the app refuses the SSIM family with a mask, :360-365).
+//
+//   k_mask_prepass   one warp per 4:4:4 row: sum of (In1 - In0) * M (GCD-M), sum of (In1 - In0)^2 * M
+//                    per row (PSNR-M, WS-PSNR-M), non-zero mask samples, exactness, largest samples
+//   k_mask_reduce    GCD-M (xGlobClrDiff.cpp:60-91): IEEE divide by NumNonMasked * MaskMax,
+//                    round half away, clip
+//   k_cps_masked     the masked search (xCorrespPixelShiftSTD.cpp:151-215), both directions: masked
+//                    test pixels and masked candidates are skipped, the winner's squared differences
+//                    are weighted by the test pixel's mask value and summed per row in uint64
+//   k_mask_finalize  the ordered compensated sums (xKBNS.h:36-43) of the ERP row weights and the
+//                    row totals, one thread per chain
+// dB values, exact-component fake values and the picture averages are formed on the host in
+// qmiv_frame_pair_compute_masked with the reference's arithmetic, including its choice of the mask's
+// bit depth for the picture's maximum in PSNR-M (xPSNR.cpp:61) and its direction labels in
+// IV-PSNR-M (xIVPSNR.cpp:161-162: "R2T" searches In1 in In0).
+#include "qmiv_host.h"
+#include "qmiv_kernels.cuh"
+
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+
+namespace qmiv {
+
+struct MaskOut
+{
+  int32_t  gcd[4];
+  int32_t  flags;              // bit0 / bit1: frame 0 / 1 held samples above the maximum
+  int32_t  nnm;                // non-zero mask samples (xPixelOpsSTD.cpp:273-284)
+  uint32_t max_sample[2];
+  int64_t  sd[3];              // sum over 4:4:4 positions of (In1 - In0) * M
+  uint64_t ssd[3];             // sum of (In1 - In0)^2 * M
+  uint32_t differs[3];         // the component differs somewhere (whole-picture exactness)
+  uint32_t pad_;
+  double   ws_err[3];          // KBNS over rows of rowSSD_M * w[y]
+  uint64_t cps_sum[2][3];      // [R2T, T2R] in xIVPSNRM's labels
+  double   cps_ws[2][3];       // KBNS over rows of rowSSE_M * w[y]
+};
+
+struct MaskArgs
+{
+  Img         in0, in1;
+  const void* mask;            // luma of the mask picture, W x H
+  int32_t     mpitch;          // in samples
+  int32_t     W, H;
+  uint32_t    clip;            // samples above are clipped (conceal), 65535 = no clipping
+  int32_t     maxv, mask_max;
+  int32_t     maxdiff[4];
+  int32_t     cws[3];
+  uint64_t*   row_ssd;         // [3][H]
+  uint64_t*   row_cps;         // [2][H][3]
+  const double* ws;            // [H] or null
+  MaskOut*    out;
+};
+
+namespace {
+
+template <typename TM>
+__device__ __forceinline__ int32_t mask_at(const MaskArgs& a, int x, int y)
+{
+  return (int32_t)__ldg(static_cast<const TM*>(a.mask) + (size_t)y * a.mpitch + x);
+}
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v)
+{
+  #pragma unroll
+  for(int o = 16; o > 0; o >>= 1) { v += __shfl_down_sync(0xffffffffu, v, o); }
+  return v;
+}
+
+template <typename T, typename TM>
+__global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ MaskArgs a)
+{
+  const int lane = threadIdx.x & 31;
+  const int y = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if(y >= a.H) { return; }                                   // whole warps: no block barrier follows
+  int64_t  sd[3] = { 0, 0, 0 };
+  uint64_t ssd[3] = { 0, 0, 0 };
+  uint32_t nnm = 0, dif = 0, mx0 = 0, mx1 = 0;
+  for(int x = lane; x < a.W; x += 32)
+  {
+    const int32_t m = mask_at<TM>(a, x, y);
+    nnm += m != 0;
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      uint32_t va = (uint32_t)fetch<T>(a.in0, c, x, y), vb = (uint32_t)fetch<T>(a.in1, c, x, y);
+      mx0 = max(mx0, va); mx1 = max(mx1, vb);
+      va = min(va, a.clip); vb = min(vb, a.clip);
+      const int32_t d = (int32_t)vb - (int32_t)va;
+      sd[c] += (int64_t)(d * m);                             // int32 product, xDistortionSTD.cpp:50
+      ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)(uint32_t)m;    // xDistortionSTD.cpp:62
+      dif |= (d != 0 ? 1u : 0u) << c;
+    }
+  }
+  #pragma unroll
+  for(int c = 0; c < 3; c++)
+  {
+    sd[c] = (int64_t)warp_sum_u64((uint64_t)sd[c]);
+    ssd[c] = warp_sum_u64(ssd[c]);
+  }
+  nnm = __reduce_add_sync(0xffffffffu, nnm);
+  dif = __reduce_or_sync(0xffffffffu, dif);
+  mx0 = __reduce_max_sync(0xffffffffu, mx0);
+  mx1 = __reduce_max_sync(0xffffffffu, mx1);
+  if(lane == 0)
+  {
+    MaskOut* o = a.out;
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      a.row_ssd[(size_t)c * a.H + y] = ssd[c];
+      atomicAdd(reinterpret_cast<unsigned long long*>(&o->sd[c]), (unsigned long long)sd[c]);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&o->ssd[c]), (unsigned long long)ssd[c]);
+      if(dif & (1u << c)) { atomicOr(&o->differs[c], 1u); }
+    }
+    atomicAdd(&o->nnm, (int32_t)nnm);
+    atomicMax(&o->max_sample[0], mx0);
+    atomicMax(&o->max_sample[1], mx1);
+  }
+}
+
+// GCD-M, xGlobClrDiff.cpp:60-91 (called with swapped pictures, xGlobClrDiff.h:42: mean of In1 - In0)
+__global__ void k_mask_reduce(const __grid_constant__ MaskArgs a)
+{
+  if(threadIdx.x != 0) { return; }
+  MaskOut* o = a.out;
+  const double den = (double)((int64_t)o->nnm * (int64_t)a.mask_max);
+  #pragma unroll
+  for(int c = 0; c < 4; c++)
+  {
+    int32_t g = 0;
+    if(c < 3 && o->nnm > 0) { g = round_half_away(ddiv((double)o->sd[c], den)); }
+    o->gcd[c] = min(max(g, -a.maxdiff[c]), a.maxdiff[c]);
+  }
+  o->flags |= (o->max_sample[0] > (uint32_t)a.maxv ? 1 : 0) | (o->max_sample[1] > (uint32_t)a.maxv ? 2 : 0);
+}
+
+// The masked search. A CTA takes a 32 x 8 tile of test pixels of one direction (blockIdx.z: 0 = R2T,
+// test In1 searched in In0 with -GCD; 1 = T2R, test In0 searched in In1 with +GCD) and stages the
+// reference samples and mask of the tile plus an R halo at clamped coordinates (the reference's
+// edge-extended margin). Candidates run in raster order with a strict minimum of the int32 error.
+template <typename T, typename TM, int R>
+__global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ MaskArgs a)
+{
+  constexpr int TW = 32, TH = 8, SW = TW + 2 * R, SH = TH + 2 * R;
+  __shared__ int4 st[SH][SW];                                // (Y, Cb, Cr, mask)
+  const int dir = blockIdx.z;
+  const Img& tst = dir ? a.in0 : a.in1;
+  const Img& ref = dir ? a.in1 : a.in0;
+  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  for(int e = threadIdx.x; e < SH * SW; e += 256)
+  {
+    const int ly = e / SW, lx = e - ly * SW;
+    const int gx = clampi(x0 - R + lx, 0, a.W - 1), gy = clampi(y0 - R + ly, 0, a.H - 1);
+    st[ly][lx] = make_int4((int32_t)min((uint32_t)fetch<T>(ref, 0, gx, gy), a.clip),
+                           (int32_t)min((uint32_t)fetch<T>(ref, 1, gx, gy), a.clip),
+                           (int32_t)min((uint32_t)fetch<T>(ref, 2, gx, gy), a.clip), mask_at<TM>(a, gx, gy));
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int x = x0 + tx, y = y0 + ty;
+  uint64_t e[3] = { 0, 0, 0 };
+  if(x < a.W && y < a.H)
+  {
+    const int32_t m = st[ty + R][tx + R].w;
+    if(m != 0)
+    {
+      const int32_t sg = dir ? 1 : -1;
+      int32_t s[3];
+      #pragma unroll
+      for(int c = 0; c < 3; c++) { s[c] = (int32_t)min((uint32_t)fetch<T>(tst, c, x, y), a.clip) + sg * a.out->gcd[c]; }
+      int32_t best = 0x7fffffff;
+      int4 bp = st[ty + R][tx + R];
+      #pragma unroll
+      for(int dy = 0; dy <= 2 * R; dy++)
+      {
+        #pragma unroll
+        for(int dx = 0; dx <= 2 * R; dx++)
+        {
+          const int4 r = st[ty + dy][tx + dx];
+          if(r.w == 0) { continue; }
+          const int32_t d0 = s[0] - r.x, d1 = s[1] - r.y, d2 = s[2] - r.z;
+          const uint32_t err = (uint32_t)(d0 * d0) * (uint32_t)a.cws[0] + (uint32_t)(d1 * d1) * (uint32_t)a.cws[1] +
+                               (uint32_t)(d2 * d2) * (uint32_t)a.cws[2];
+          if((int32_t)err < best) { best = (int32_t)err; bp = r; }
+        }
+      }
+      const int32_t d0 = s[0] - bp.x, d1 = s[1] - bp.y, d2 = s[2] - bp.z;
+      e[0] = (uint64_t)(int64_t)(d0 * d0) * (uint64_t)m;
+      e[1] = (uint64_t)(int64_t)(d1 * d1) * (uint64_t)m;
+      e[2] = (uint64_t)(int64_t)(d2 * d2) * (uint64_t)m;
+    }
+  }
+  // a warp is 32 pixels of one row
+  #pragma unroll
+  for(int c = 0; c < 3; c++) { e[c] = warp_sum_u64(e[c]); }
+  if(tx == 0 && y < a.H)
+  {
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      if(e[c]) { atomicAdd(reinterpret_cast<unsigned long long*>(a.row_cps + ((size_t)dir * a.H + y) * 3 + c), (unsigned long long)e[c]); }
+    }
+  }
+}
+
+// Chains 0..2: WS rows of component c; chains 3..8: CPS rows of (direction, component). Each is the
+// reference's row-order compensated sum; the CPS chains also form the plain uint64 totals.
+__global__ void k_mask_finalize(const __grid_constant__ MaskArgs a)
+{
+  const int k = threadIdx.x;
+  if(k >= 9) { return; }
+  MaskOut* o = a.out;
+  const int H = a.H;
+  if(k < 3)
+  {
+    if(!a.ws) { return; }
+    const uint64_t* r = a.row_ssd + (size_t)k * H;
+    Kbns s;
+    for(int y = 0; y < H; y++) { s.add(dmul((double)r[y], a.ws[y])); }
+    o->ws_err[k] = s.result();
+    return;
+  }
+  const int d = (k - 3) / 3, c = (k - 3) % 3;
+  const uint64_t* r = a.row_cps + (size_t)d * H * 3 + c;
+  uint64_t total = 0;
+  Kbns s;
+  for(int y = 0; y < H; y++)
+  {
+    const uint64_t v = r[(size_t)y * 3];
+    total += v;
+    if(a.ws) { s.add(dmul((double)v, a.ws[y])); }
+  }
+  o->cps_sum[d][c] = total;
+  o->cps_ws[d][c] = a.ws ? s.result() : 0.0;
+}
+
+template <typename T, typename TM>
+cudaError_t launch_masked_t(const MaskArgs& a, int R, cudaStream_t s)
+{
+  k_mask_prepass<T, TM><<<(a.H + 7) / 8, 256, 0, s>>>(a);
+  k_mask_reduce<<<1, 32, 0, s>>>(a);
+  const dim3 grid((a.W + 31) / 32, (a.H + 7) / 8, 2);
+  switch(R)
+  {
+  case 1: k_cps_masked<T, TM, 1><<<grid, 256, 0, s>>>(a); break;
+  case 2: k_cps_masked<T, TM, 2><<<grid, 256, 0, s>>>(a); break;
+  case 3: k_cps_masked<T, TM, 3><<<grid, 256, 0, s>>>(a); break;
+  case 4: k_cps_masked<T, TM, 4><<<grid, 256, 0, s>>>(a); break;
+  case 5: k_cps_masked<T, TM, 5><<<grid, 256, 0, s>>>(a); break;
+  default: return cudaErrorInvalidValue;
+  }
+  k_mask_finalize<<<1, 32, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// xPSNR::CalcPSNRfromMaskedSSD, xPSNR.cpp:198-205: MAX = NumNonMasked * MaxPic^2 * MaxMsk in int64
+double psnr_masked(double ssd, int32_t nnm, int32_t bitdepth_pic, int32_t bitdepth_msk)
+{
+  const uint64_t mp = (uint64_t)((1 << bitdepth_pic) - 1), mm = (uint64_t)((1 << bitdepth_msk) - 1);
+  const int64_t  MAX = (int64_t)((uint64_t)(int64_t)nnm * (mp * mp) * mm);
+  return ssd > 0 ? 10.0 * log10((double)MAX / ssd) : DBL_MAX;
+}
+
+}  // namespace
+
+MaskedPipeline::~MaskedPipeline()
+{
+  if(h_out_) { cudaFreeHost(h_out_); }
+}
+
+qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const qmiv_frame* in1, const qmiv_frame* mask,
+                                int32_t mask_bitdepth, uint32_t metrics, qmiv_result* out, int32_t* num_non_masked)
+{
+  PairPipeline& pipe = calc->pipe;
+  const Shape& S = pipe.shape();
+  const qmiv_params& prm = calc->prm;
+  cudaStream_t s = calc->stream;
+  if(mask_bitdepth < 8 || mask_bitdepth > 14) { return fail(QMIV_ERR_INVALID_ARG, "mask bit depth must be in 8..14"); }
+  if(!mask || !mask->plane[0]) { return fail(QMIV_ERR_INVALID_ARG, "mask plane is null"); }
+  const size_t mesz = mask_bitdepth <= 8 ? 1 : 2;
+  const size_t mrow = (size_t)S.W * mesz;
+  if(mask->pitch[0] < (int64_t)mrow || (mask->pitch[0] % (int64_t)mesz) != 0) { return fail(QMIV_ERR_INVALID_ARG, "bad mask pitch"); }
+  if(S.bitdepth > 14) { return fail(QMIV_ERR_UNSUPPORTED, "mask mode needs bit depth <= 14"); }
+
+  const bool host = in0->mem == QMIV_MEM_HOST || in1->mem == QMIV_MEM_HOST;
+  QMIV_TRY(pipe.prepare(QMIV_PSNR, false, host));           // staging for host frames, ERP weights on the device
+  Img a0{}, a1{};
+  QMIV_TRY(pipe.resolve(in0, 0, a0, s));
+  QMIV_TRY(pipe.resolve(in1, 1, a1, s));
+
+  QMIV_TRY(out_.ensure(calc->ctx, sizeof(MaskOut)));
+  QMIV_TRY(rows_.ensure(calc->ctx, (size_t)9 * S.H * sizeof(uint64_t)));
+  if(!h_out_) { QMIV_CUDA(cudaMallocHost(&h_out_, sizeof(MaskOut))); }
+  MaskArgs a{};
+  a.in0 = a0; a.in1 = a1;
+  if(mask->mem == QMIV_MEM_DEVICE)
+  {
+    a.mask = mask->plane[0];
+    a.mpitch = (int32_t)(mask->pitch[0] / (int64_t)mesz);
+  }
+  else if(mask->mem == QMIV_MEM_HOST)
+  {
+    QMIV_TRY(stage_.ensure(calc->ctx, mrow * S.H));
+    QMIV_CUDA(cudaMemcpy2DAsync(stage_.p, mrow, mask->plane[0], (size_t)mask->pitch[0], mrow, S.H, cudaMemcpyHostToDevice, s));
+    a.mask = stage_.p;
+    a.mpitch = S.W;
+  }
+  else { return fail(QMIV_ERR_INVALID_ARG, "mask mem must be QMIV_MEM_HOST or QMIV_MEM_DEVICE"); }
+  a.W = S.W; a.H = S.H;
+  a.clip = prm.invalid_pel_action == QMIV_PEL_CNCL ? (uint32_t)S.maxv : 0xffffu;
+  a.maxv = S.maxv; a.mask_max = (1 << mask_bitdepth) - 1;
+  for(int c = 0; c < 4; c++) { a.maxdiff[c] = pipe.maxdiff()[c]; }
+  for(int c = 0; c < 3; c++) { a.cws[c] = prm.cws[c]; }
+  a.row_ssd = rows_.as<uint64_t>();
+  a.row_cps = rows_.as<uint64_t>() + (size_t)3 * S.H;
+  a.ws = prm.erp ? pipe.ws_device() : nullptr;
+  a.out = out_.as<MaskOut>();
+  QMIV_CUDA(cudaMemsetAsync(out_.p, 0, sizeof(MaskOut), s));
+  QMIV_CUDA(cudaMemsetAsync(a.row_cps, 0, (size_t)6 * S.H * sizeof(uint64_t), s));
+  cudaError_t e;
+  if(S.esz == 1) { e = mesz == 1 ? launch_masked_t<uint8_t, uint8_t>(a, prm.search_range, s) : launch_masked_t<uint8_t, uint16_t>(a, prm.search_range, s); }
+  else { e = mesz == 1 ? launch_masked_t<uint16_t, uint8_t>(a, prm.search_range, s) : launch_masked_t<uint16_t, uint16_t>(a, prm.search_range, s); }
+  if(e != cudaSuccess) { return cuda_fail(e, "masked launches"); }
+  QMIV_CUDA(cudaMemcpyAsync(h_out_, out_.p, sizeof(MaskOut), cudaMemcpyDeviceToHost, s));
+  QMIV_CUDA(cudaStreamSynchronize(s));
+  const MaskOut& o = *static_cast<const MaskOut*>(h_out_);
+
+  if(prm.invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3))
+  {
+    return fail(QMIV_ERR_INVALID_PIXEL, "input frame contains samples above the bit depth's maximum");
+  }
+  if(o.nnm == 0) { return fail(QMIV_ERR_INVALID_ARG, "the mask has no non-zero sample"); }
+  if(num_non_masked) { *num_non_masked = o.nnm; }
+  if(!out) { return QMIV_OK; }
+
+  std::memset(out, 0, sizeof(*out));
+  const int64_t area = (int64_t)S.W * S.H;
+  const int32_t bd = S.bitdepth, mbd = mask_bitdepth;
+  for(int c = 0; c < 4; c++) { out->gcd_r2t[c] = o.gcd[c]; }
+  for(int c = 0; c < 3; c++)
+  {
+    out->exact[c] = o.differs[c] == 0;
+    out->ssd[c] = o.ssd[c];
+    out->cps_sse_r2t[c] = o.cps_sum[0][c];
+    out->cps_sse_t2r[c] = o.cps_sum[1][c];
+  }
+  out->invalid_pel[0] = (o.flags & 1) != 0;
+  out->invalid_pel[1] = (o.flags & 2) != 0;
+  const double fake = psnr_from_ssd(1, area, bd);          // getFakePSNR(area, picture bit depth), xAppQMIV.cpp:976
+  const int32_t* cwa = prm.cwa;
+  const double inv = 1.0 / (double)(cwa[0] + cwa[1] + cwa[2] + cwa[3]);
+  auto per_pic3 = [&](const double v[4]) { return (v[0] * cwa[0] + v[1] * cwa[1] + v[2] * cwa[2]) * inv; };   // xMetricQMIV.cpp:91-97
+  if(metrics & QMIV_PSNR)                                     // xPSNR.cpp:54-66: the mask's bit depth for both
+  {
+    for(int c = 0; c < 3; c++) { out->psnr[c] = out->exact[c] ? fake : psnr_masked((double)o.ssd[c], o.nnm, mbd, mbd); }
+    out->psnr_pic = per_pic3(out->psnr);
+  }
+  if(metrics & QMIV_WSPSNR)                                   // xWSPSNR.cpp:51-77, :108-133
+  {
+    for(int c = 0; c < 3; c++)
+    {
+      const double v = prm.erp ? psnr_masked(o.ws_err[c] * pipe.ws_corr(), o.nnm, bd, mbd) : psnr_masked((double)o.ssd[c], o.nnm, mbd, mbd);
+      out->wspsnr[c] = out->exact[c] ? fake : v;
+    }
+    out->wspsnr_pic = per_pic3(out->wspsnr);
+  }
+  if(metrics & QMIV_IVPSNR)                                   // xIVPSNR.cpp:153-200
+  {
+    double q[2];
+    for(int d = 0; d < 2; d++)
+    {
+      double qc[4] = { 0, 0, 0, 0 };
+      for(int c = 0; c < 3; c++)
+      {
+        const double err = prm.erp ? o.cps_ws[d][c] : (double)o.cps_sum[d][c];
+        qc[c] = psnr_masked(err > 0 ? err : 1.0, o.nnm, bd, mbd);
+      }
+      q[d] = (qc[0] * (double)cwa[0] + qc[1] * (double)cwa[1] + qc[2] * (double)cwa[2] + qc[3] * (double)cwa[3]) * inv;
+    }
+    out->ivpsnr_r2t = q[0]; out->ivpsnr_t2r = q[1];
+    out->ivpsnr = (q[1] < q[0]) ? q[1] : q[0];
+  }
+  return QMIV_OK;
+}
+
+}  // namespace qmiv
+
+extern "C" qmiv_status qmiv_frame_pair_compute_masked(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1,
+                                                      const qmiv_frame* mask, int32_t mask_bitdepth, uint32_t metric_mask,
+                                                      qmiv_result* out, int32_t* num_non_masked)
+{
+  using namespace qmiv;
+  if(!calc || !in0 || !in1 || !mask) { return fail(QMIV_ERR_INVALID_ARG, "null argument"); }
+  if(calc->pending) { return fail(QMIV_ERR_BUSY, "a submission is already in flight on this calc"); }
+  if((metric_mask & ~(uint32_t)QMIV_ALL) != 0) { return fail(QMIV_ERR_INVALID_ARG, "unknown metric bits"); }
+  if(metric_mask & ~(uint32_t)(QMIV_PSNR | QMIV_WSPSNR | QMIV_IVPSNR))
+  {
+    return fail(QMIV_ERR_UNSUPPORTED, "mask mode computes PSNR, WS-PSNR and IV-PSNR only (as the reference)");
+  }
+  QMIV_CUDA(cudaSetDevice(calc->ctx->device));
+  if(!calc->masked) { calc->masked.reset(new MaskedPipeline()); }
+  return calc->masked->run(calc, in0, in1, mask, mask_bitdepth, metric_mask, out, num_non_masked);
+}

@@ -1,0 +1,107 @@
+"""Mask mode (qmiv_frame_pair_compute_masked): GCD-M, CPS-M, PSNR-M, WS-PSNR-M and IV-PSNR-M against
+the compiled reference's fixtures and the C restatement, bit for bit, with host and device frames."""
+import numpy as np
+import pytest
+
+import oracle
+from golden_cases import compare_masked, masked_case_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _ids():
+    import json, os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "golden_masked.json")) as f:
+        g = json.load(f)["masked"]
+    return [f"{c['width']}x{c['height']}_{c['bitdepth']}b_{c['chroma_format']}_R{c['search_range']}"
+            f"{'_erp' if c['erp'] else ''}_m{c['mask_bitdepth']}{c['mask_kind']}" for c in g]
+
+
+def _calc(qctx, case):
+    import qmiv_b200
+    return qmiv_b200.Calc(qctx, case["width"], case["height"], case["bitdepth"], case["chroma_format"],
+                          search_range=case["search_range"], erp=case["erp"])
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("idx", range(len(_ids())), ids=_ids())
+def test_masked_golden_host_frames(idx, golden_masked, qctx):
+    case = golden_masked[idx]
+    f0, f1, m = masked_case_inputs(case)
+    with _calc(qctx, case) as calc:
+        got, nnm = calc.compute_masked(f0, f1, m, case["mask_bitdepth"])
+    assert compare_masked(got, nnm, case["expected"]) == []
+
+
+@pytest.mark.parametrize("idx", [0, 2, 6, 9], ids=[_ids()[i] for i in [0, 2, 6, 9]])
+def test_masked_golden_device_frames(idx, golden_masked, qctx):
+    case = golden_masked[idx]
+    f0, f1, m = masked_case_inputs(case)
+    with _calc(qctx, case) as calc:
+        got, nnm = calc.compute_masked(tuple(_dev(p) for p in f0), tuple(_dev(p) for p in f1), _dev(m),
+                                       case["mask_bitdepth"])
+    assert compare_masked(got, nnm, case["expected"]) == []
+
+
+@pytest.mark.parametrize("shape", [(640, 360, 10, 420, 2, True, 8, "weights"), (352, 288, 8, 422, 5, False, 10, "binary"),
+                                   (258, 130, 10, 444, 3, True, 12, "sparse"),
+                                   (4096, 2048, 10, 420, 2, True, 8, "binary")])
+def test_masked_against_oracle_seeded(shape, qctx, oracle_lib):
+    """Seeded synthetic frames (the bench's generator) with detgen masks, up to the 4096x2048 workload."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    W, H, bd, cf, R, erp, mbd, kind = shape
+    f0, f1 = synth.make_pair(W, H, bd, seed=W + H, chroma_format=cf)
+    m = det_mask(W, H, mbd, W * 3 + H, kind)
+    p = oracle.make_params(W, H, bd, cf, search_range=R, erp=erp)
+    exp, n_exp = oracle_lib.compute_pair_masked(p, f0, f1, m, mbd)
+    with qmiv_b200.Calc(qctx, W, H, bd, cf, search_range=R, erp=erp) as calc:
+        got, nnm = calc.compute_masked(f0, f1, m, mbd)
+    assert nnm == n_exp
+    for k in ["gcd_r2t", "psnr", "wspsnr"]:
+        assert list(got[k][:3]) == list(exp[k][:3]), k
+    for k in ["psnr_pic", "wspsnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"]:
+        assert got[k] == exp[k], k
+
+
+def test_masked_ones_equals_plain_ivpsnr(qctx):
+    """With every mask sample at its maximum, IV-PSNR-M is the plain IV-PSNR (the weights and the
+    non-masked count cancel), while PSNR-M shows the reference's use of the mask's bit depth."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    W, H, bd = 320, 240, 10
+    f0, f1 = synth.make_pair(W, H, bd, seed=5)
+    ones = np.full((H, W), 255, np.uint8)
+    with qmiv_b200.Calc(qctx, W, H, bd) as calc:
+        plain = calc.compute(f0, f1, qmiv_b200.IVPSNR | qmiv_b200.PSNR)
+        got, nnm = calc.compute_masked(f0, f1, ones, 8)
+    assert nnm == W * H
+    assert got["ivpsnr"] == plain["ivpsnr"]
+    assert got["gcd_r2t"] == plain["gcd_r2t"]
+    # 10 log10(1023^2 / 255^2) apart
+    assert abs((plain["psnr"][0] - got["psnr"][0]) - 20 * np.log10(1023 / 255)) < 1e-9
+
+
+def test_masked_errors(qctx):
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    W, H = 64, 48
+    f0, f1 = synth.make_pair(W, H, 8, seed=1)
+    m = det_mask(W, H, 8, 1)
+    with qmiv_b200.Calc(qctx, W, H, 8) as calc:
+        with pytest.raises(qmiv_b200.QmivError) as ei:
+            calc.compute_masked(f0, f1, m, 8, qmiv_b200.IVSSIM)
+        assert ei.value.status == 2  # QMIV_ERR_UNSUPPORTED
+        with pytest.raises(qmiv_b200.QmivError):
+            calc.compute_masked(f0, f1, np.zeros((H, W), np.uint8), 8)
+        with pytest.raises(qmiv_b200.QmivError):
+            calc.compute_masked(f0, f1, m, 7)
+        # the calc still works after the refusals
+        got, nnm = calc.compute_masked(f0, f1, m, 8)
+        assert nnm == int((m != 0).sum())
