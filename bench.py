@@ -335,6 +335,7 @@ def run_qmiv(args, world, rank, local):
     cps_tile = batch.tuning(W, H, BD, 2)
     mixed = run_mixed(ctx, max(3, args.steps // 4)) if (world == 1 and not args.no_mixed) else None
     serve = run_serve(ctx, args.serve_seconds) if (world == 1 and args.serve_seconds > 0) else None
+    masked = run_masked(ctx, max(3, args.steps // 4)) if (world == 1 and not args.no_masked) else None
 
     # ---- probes for the search kernel's roofline denominator ----
     lib = qmiv_b200.library()
@@ -356,7 +357,7 @@ def run_qmiv(args, world, rank, local):
     return dict(value=value, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
                 achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
                 sample=results[0], launches=int(round(launches_per_step * args.steps)), plain=plain_value,
-                cps_tile=cps_tile, mixed=mixed, serve=serve)
+                cps_tile=cps_tile, mixed=mixed, serve=serve, masked=masked)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -400,6 +401,52 @@ def run_reference_app(n_frames, threads, seed=0):
                 ivpsnr=float(ivpsnr.group(1)) if ivpsnr else None)
 
 
+def run_masked(ctx, steps):
+    """Mask mode on one 4096x2048 10-bit 4:2:0 ERP pair with a block mask (60 % of 16x16 blocks kept,
+    8-bit): PSNR-M + WS-PSNR-M + IV-PSNR-M through qmiv_frame_pair_compute_masked, device frames."""
+    import torch
+    import qmiv_b200
+    from qmiv_b200 import synth
+    f0, f1 = synth.make_pair(W, H, BD, seed=77)
+    m = synth.make_mask(W, H, 8, seed=77)
+    d0 = tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in f0)
+    d1 = tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in f1)
+    dm = torch.from_numpy(m).cuda()
+    with qmiv_b200.Calc(ctx, W, H, BD, CF, search_range=2, erp=True) as calc:
+        for _ in range(3):
+            r, nnm = calc.compute_masked(d0, d1, dm, 8)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            r, nnm = calc.compute_masked(d0, d1, dm, 8)
+        dt = (time.perf_counter() - t0) / steps
+    return {"value": 1.0 / dt, "unit": "frame-pairs/s", "ms_per_pair": dt * 1e3, "num_non_masked": nnm,
+            "ivpsnr": r["ivpsnr"], "what": "one 4096x2048 10-bit 4:2:0 ERP pair, 8-bit block mask (60 % kept), "
+            "PSNR-M + WS-PSNR-M + IV-PSNR-M, device frames, one synchronous call per pair"}
+
+
+def run_reference_masked(threads, seed=77, reps=2):
+    """The reference's mask-mode processors (xGlobClrDiff::CalcGlobalColorDiffM, xPSNR::calcPicPSNRM,
+    xWSPSNR::calcPicWSPSNRM, xIVPSNRM::calcPicIVPSNRM) in the app's per-frame sequence, through the
+    reference library compiled from its sources (oracle/_ref) with a thread pool of `threads`, on the
+    masked workload: frame-pairs/s. The app binary itself cannot run its mask mode (its start-frame
+    check reads past a two-entry array for the mask input and always fails)."""
+    import oracle
+    from qmiv_b200 import synth
+    if not oracle.reference_available():
+        return None
+    ref = oracle.Reference()
+    a, b = synth.make_pair(W, H, BD, seed=seed)
+    m = synth.make_mask(W, H, 8, seed=seed)
+    p = oracle.make_params(W, H, BD, CF, search_range=2, erp=True, num_threads=threads)
+    r, _ = ref.compute_pair_masked(p, a, b, m, 8)           # warm-up
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        r, _ = ref.compute_pair_masked(p, a, b, m, 8)
+    secs = (time.perf_counter() - t0) / reps
+    return {"value": 1.0 / secs, "secs": secs, "threads": threads, "ivpsnr": r["ivpsnr"]}
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -417,6 +464,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the plain-vs-batched mixed-resolution comparison")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="length of the serving-loop arrival stream (0: skip)")
+    ap.add_argument("--no-masked", action="store_true", help="skip the mask-mode measurement")
     ap.add_argument("--size", default=None, help="WxH of a smaller profiling case (not a bench line)")
     ap.add_argument("--pairs", type=int, default=None, help="pairs per step of a smaller profiling case")
     args = ap.parse_args()
@@ -477,6 +525,16 @@ def main():
                                  f"(oracle/_ref) with -nth {c['threads']}, {c['secs']:.2f} s"}
         except Exception as e:  # the GPU number stands without the CPU baseline
             log("cpu baseline failed:", e)
+        if r["masked"] is not None:
+            try:
+                cm = run_reference_masked(host_threads())
+                if cm:
+                    r["masked"]["cpu_reference"] = {
+                        "value": cm["value"], "unit": "frame-pairs/s", "cores": cm["threads"], "ivpsnr": cm["ivpsnr"],
+                        "kind": "reference", "sample": "the same pair through the reference library's mask-mode processors "
+                        f"(oracle/_ref, {cm['threads']} pool threads), {cm['secs']:.2f} s per pair"}
+            except Exception as e:
+                log("masked cpu baseline failed:", e)
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -505,6 +563,7 @@ def main():
                           "what": "the same pairs, one qmiv_frame_pair_compute call per pair (device frames)"},
            "mixed_set": r["mixed"],
            "serve": r["serve"],
+           "masked_mode": r["masked"],
            "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
            "clocks": r["clocks"],
            "cpu_baseline": cpu,

@@ -138,3 +138,14 @@ def config4_requests(duration_s=1.0, rate=200.0, seed=4, max_pairs=32):
                  for _ in range(npairs)]
         reqs.append(Request(t, specs, metric_sets[rng.integers(0, 3)]))
     return reqs
+
+
+def make_mask(width, height, bitdepth=8, seed=0, keep=0.6, block=16):
+    """A mask picture's luma for mask mode: blocks of `block` x `block` samples kept (at the maximum
+    value) with probability `keep`, the rest masked (0), from a seeded generator."""
+    rng = np.random.default_rng(seed)
+    maxv = (1 << bitdepth) - 1
+    nby, nbx = -(-height // block), -(-width // block)
+    keepb = rng.random((nby, nbx)) < keep
+    m = np.repeat(np.repeat(keepb, block, axis=0), block, axis=1)[:height, :width]
+    return np.where(m, maxv, 0).astype(np.uint8 if bitdepth <= 8 else np.uint16)
