@@ -261,6 +261,14 @@ QMIV_API qmiv_status qmiv_batch_create(qmiv_ctx ctx, int32_t max_pairs, int64_t 
                               int32_t flags, qmiv_batch* out_batch);
 QMIV_API qmiv_status qmiv_batch_destroy(qmiv_batch batch);
 QMIV_API qmiv_status qmiv_batch_compute(qmiv_batch batch, const qmiv_pair_desc* pairs, int32_t num_pairs, qmiv_result* out);
+
+/* Asynchronous form of qmiv_batch_compute with two calls in flight: qmiv_batch_submit enqueues a
+   call's uploads and launches and returns at once with a ticket; qmiv_batch_wait(ticket) waits for
+   that call and writes its results. A third submission before a wait, or qmiv_batch_compute while
+   the first slot is held, returns QMIV_ERR_BUSY. Host frames must stay valid until the wait returns.
+   With host frames, the uploads of one call overlap the kernels of the other. */
+QMIV_API qmiv_status qmiv_batch_submit(qmiv_batch batch, const qmiv_pair_desc* pairs, int32_t num_pairs, uint64_t* ticket);
+QMIV_API qmiv_status qmiv_batch_wait(qmiv_batch batch, uint64_t ticket, qmiv_result* results);
 /* Device stream (cudaStream_t) the batch enqueues on. */
 QMIV_API qmiv_status qmiv_batch_stream(qmiv_batch batch, void** cuda_stream);
 /* Tile shapes picked by the autotuner for (width, height, bitdepth, R): for inspection and tests. */

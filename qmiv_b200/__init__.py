@@ -272,6 +272,7 @@ class Batch:
         check(self._lib.qmiv_batch_create(ctx.handle, max_pairs, max_pixels, ctypes.byref(self.params),
                                           flags, ctypes.byref(h)), "qmiv_batch_create")
         self.handle = h
+        self._inflight = {}
 
     def close(self):
         if self.handle:
@@ -284,9 +285,8 @@ class Batch:
     def __exit__(self, *exc):
         self.close()
 
-    def compute(self, pairs: Iterable[dict]) -> list[dict]:
-        """pairs: dicts with frame0, frame1, width, height, bitdepth, chroma_format, search_range, metrics."""
-        pairs = list(pairs)
+    @staticmethod
+    def _descs(pairs):
         descs = (_lib.QmivPairDesc * max(1, len(pairs)))()
         keep = []
         for i, p in enumerate(pairs):
@@ -299,9 +299,34 @@ class Batch:
             d.chroma_format = p.get("chroma_format", 420)
             d.search_range = p.get("search_range", 2)
             d.metric_mask = metric_mask(p.get("metrics"))
+        return descs, keep
+
+    def compute(self, pairs: Iterable[dict]) -> list[dict]:
+        """pairs: dicts with frame0, frame1, width, height, bitdepth, chroma_format, search_range, metrics."""
+        pairs = list(pairs)
+        descs, keep = self._descs(pairs)
         out = (_lib.QmivResult * max(1, len(pairs)))()
         check(self._lib.qmiv_batch_compute(self.handle, descs, len(pairs), out), "qmiv_batch_compute")
         return [out[i].as_dict() for i in range(len(pairs))]
+
+    def submit(self, pairs: Iterable[dict]) -> int:
+        """Asynchronous compute (qmiv_batch_submit): returns a ticket for wait(); up to two in flight.
+        The frames must stay alive and unchanged until the wait."""
+        pairs = list(pairs)
+        descs, keep = self._descs(pairs)
+        t = ctypes.c_uint64()
+        check(self._lib.qmiv_batch_submit(self.handle, descs, len(pairs), ctypes.byref(t)), "qmiv_batch_submit")
+        self._inflight[t.value] = (len(pairs), pairs, keep)
+        return t.value
+
+    def wait(self, ticket: int) -> list[dict]:
+        n = self._inflight[ticket][0] if ticket in self._inflight else 0
+        out = (_lib.QmivResult * max(1, n))()
+        try:
+            check(self._lib.qmiv_batch_wait(self.handle, ctypes.c_uint64(ticket), out), "qmiv_batch_wait")
+        finally:
+            self._inflight.pop(ticket, None)
+        return [out[i].as_dict() for i in range(n)]
 
     def stream(self) -> int:
         """cudaStream_t of the batch, as an integer (for torch.cuda.ExternalStream)."""

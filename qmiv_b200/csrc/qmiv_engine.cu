@@ -214,12 +214,19 @@ qmiv_status Engine::ensure_host(size_t mirror_bytes, int n)
 // ---------------------------------------------------------------------------------------------
 qmiv_status Engine::run(const qmiv_pair_desc* pairs, int32_t n, qmiv_result* results)
 {
+  QMIV_TRY(submit(pairs, n));
+  return collect(results);
+}
+
+qmiv_status Engine::submit(const qmiv_pair_desc* pairs, int32_t n)
+{
+  if(pend_n_ >= 0) { return fail(QMIV_ERR_BUSY, "the engine has a call in flight"); }
   if(!pairs && n > 0) { return fail(QMIV_ERR_INVALID_ARG, "null pairs"); }
   if(n > max_pairs_) { return fail(QMIV_ERR_INVALID_ARG, "more pairs than max_pairs"); }
   int64_t px = 0;
   for(int i = 0; i < n; i++) { px += (int64_t)pairs[i].width * pairs[i].height; }
   if(px > max_pixels_) { return fail(QMIV_ERR_INVALID_ARG, "more pixels than max_pixels"); }
-  if(n == 0) { return QMIV_OK; }
+  if(n == 0) { pend_n_ = 0; return QMIV_OK; }
   QMIV_CUDA(cudaSetDevice(ctx_->device));
   cudaStream_t s = stream_;
 
@@ -447,20 +454,34 @@ qmiv_status Engine::run(const qmiv_pair_desc* pairs, int32_t n, qmiv_result* res
     QMIV_CUDA(cudaGraphLaunch(ex, s));
   }
   else { QMIV_TRY(enqueue()); }
-  QMIV_CUDA(cudaStreamSynchronize(s));
+  pend_kind_ = kind;
+  pend_mask_.resize(n);
+  for(int i = 0; i < n; i++) { pend_mask_[i] = P[i].mask; }
+  pend_n_ = n;
+  return QMIV_OK;
+}
+
+qmiv_status Engine::collect(qmiv_result* results)
+{
+  if(pend_n_ < 0) { return fail(QMIV_ERR_INVALID_ARG, "nothing submitted"); }
+  const int n = pend_n_;
+  pend_n_ = -1;
+  if(n == 0) { return QMIV_OK; }
+  QMIV_CUDA(cudaSetDevice(ctx_->device));
+  QMIV_CUDA(cudaStreamSynchronize(stream_));
   harvest_profile();
 
   // ---- results ------------------------------------------------------------------------------------
   qmiv_status st = QMIV_OK;
   for(int i = 0; i < n; i++)
   {
-    const PairKind& K = *kind[i];
+    const PairKind& K = *pend_kind_[i];
     FinishInfo fi{};
-    fi.W = K.S.W; fi.H = K.S.H; fi.bitdepth = K.S.bitdepth; fi.mask = P[i].mask;
+    fi.W = K.S.W; fi.H = K.S.H; fi.bitdepth = K.S.bitdepth; fi.mask = pend_mask_[i];
     fi.erp = prm_.erp; fi.ws_corr = K.ws_corr;
     for(int c = 0; c < 4; c++) { fi.cwa[c] = prm_.cwa[c]; }
     fi.num_scales = K.ns;
-    finish_result(host_out_[i], fi, &results[i]);
+    if(results) { finish_result(host_out_[i], fi, &results[i]); }
     const qmiv_status ps = pair_status(host_out_[i], prm_.invalid_pel_action);
     if(ps != QMIV_OK && st == QMIV_OK) { st = ps; }
   }

@@ -98,6 +98,11 @@ public:
   qmiv_status init(qmiv_ctx_s* ctx, const qmiv_params& prm, int32_t max_pairs, int64_t max_pixels, int32_t flags);
   // Computes every pair and waits for the results.
   qmiv_status run(const qmiv_pair_desc* pairs, int32_t n, qmiv_result* results);
+  // The two halves of run(): enqueue every upload and launch on the engine's streams, then wait and
+  // finish the results. One call in flight per engine; host frames must stay valid until collect().
+  qmiv_status submit(const qmiv_pair_desc* pairs, int32_t n);
+  qmiv_status collect(qmiv_result* results);
+  bool        busy() const { return pend_n_ >= 0; }
   cudaStream_t stream() const { return stream_; }
   bool tuning(int32_t W, int32_t H, int32_t bd, int32_t R, int32_t* tile_w, int32_t* tile_h, int32_t* rows) const;
   size_t device_bytes() const { return arena_.bytes + arena_desc_.bytes + tune_scratch_.bytes; }
@@ -144,6 +149,9 @@ private:
   std::vector<cudaEvent_t> ev_pool_;
   size_t ev_used_ = 0;
   std::vector<std::pair<int, int>> ev_pending_;
+  int          pend_n_ = -1;                   // pairs of the call in flight, -1 = none
+  std::vector<PairKind*> pend_kind_;
+  std::vector<uint32_t>  pend_mask_;
 };
 
 }  // namespace qmiv

@@ -141,3 +141,31 @@ def test_batch_limits(qctx):
         with pytest.raises(qmiv_b200.QmivError):
             batch.compute([_desc(s, f0, f1)] * 2)
         assert batch.compute([]) == []
+
+
+def test_batch_submit_wait_two_in_flight(qctx):
+    """Asynchronous submissions (qmiv_batch_submit / qmiv_batch_wait): two calls in flight, host and
+    device frames, each call's results equal to the synchronous form; a third submission and a
+    synchronous call while the first slot is held are refused."""
+    import qmiv_b200
+    specs = _specs()[:4]
+    fa = [_frames(s, 1100 + i, device=(i % 2 == 0)) for i, s in enumerate(specs)]
+    fb = [_frames(s, 1200 + i) for i, s in enumerate(specs)]
+    px = sum(s[0] * s[1] for s in specs)
+    with qmiv_b200.Batch(qctx, max_pairs=len(specs), max_pixels=px, autotune=True) as batch:
+        da = [_desc(s, *f) for s, f in zip(specs, fa)]
+        db = [_desc(s, *f) for s, f in zip(specs, fb)]
+        exp_a, exp_b = batch.compute(da), batch.compute(db)
+        for _ in range(3):
+            ta = batch.submit(da)
+            tb = batch.submit(db)
+            with pytest.raises(qmiv_b200.QmivError) as ei:
+                batch.submit(da)
+            assert ei.value.status == 10  # QMIV_ERR_BUSY
+            with pytest.raises(qmiv_b200.QmivError):
+                batch.compute(da)
+            assert batch.wait(tb) == exp_b
+            assert batch.wait(ta) == exp_a
+        with pytest.raises(qmiv_b200.QmivError):
+            batch.wait(ta)
+        ta = batch.submit(da)   # left in flight: destroying the batch waits for it
