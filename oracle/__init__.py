@@ -22,6 +22,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 PSNR, WSPSNR, IVPSNR, SSIM, MSSSIM, IVSSIM, IVMSSSIM = 1, 2, 4, 8, 16, 32, 64
 ALL = 127
+# colour spaces of the app's -csi / -csm options (apps/QMIV/src/xUtilsQMIV.h:12-27)
+CS_RGB, CS_BGR, CS_GBR, CS_YCBCR = 2, 3, 4, 16
+CS_BT601, CS_SMPTE170M, CS_BT709, CS_SMPTE240M, CS_BT2020 = 17, 18, 19, 20, 21
 
 
 class Params(ctypes.Structure):
@@ -104,6 +107,17 @@ class Oracle(_Lib):
             shp = (3, params.height, params.width)
             out["scp0"], out["scp1"] = scp0.reshape(shp), scp1.reshape(shp)
         return out
+
+    def compute_pair_cs(self, params: Params, frame0, frame1, cs_in, cs_metric, mask=ALL & ~(MSSSIM | IVMSSSIM)):
+        """The pipeline after the app's colour-space conversion (-csi cs_in, -csm cs_metric)."""
+        a0, p0 = _planes(frame0)
+        a1, p1 = _planes(frame1)
+        res = Result()
+        rc = self.lib.qo_compute_pair_cs(ctypes.byref(params), p0, p1, ctypes.c_uint32(mask), ctypes.c_int32(cs_in),
+                                         ctypes.c_int32(cs_metric), ctypes.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"qo_compute_pair_cs failed ({rc})")
+        return res.as_dict()
 
     def compute_pair_masked(self, params: Params, frame0, frame1, mask_plane, mask_bitdepth, mask=PSNR | WSPSNR | IVPSNR):
         """Mask mode (GCD-M, PSNR-M, WS-PSNR-M, IV-PSNR-M); returns (result dict, NumNonMasked)."""
@@ -240,6 +254,17 @@ class Reference(_Lib):
             shp = (3, params.height, params.width)
             out["scp0"], out["scp1"] = scp0.reshape(shp), scp1.reshape(shp)
         return out
+
+    def compute_pair_cs(self, params: Params, frame0, frame1, cs_in, cs_metric, mask=ALL & ~(MSSSIM | IVMSSSIM)):
+        """The pipeline with the app's colour-space conversion (-csi cs_in, -csm cs_metric)."""
+        a0, p0 = _planes(frame0)
+        a1, p1 = _planes(frame1)
+        res = Result()
+        rc = self.lib.ref_compute_pair_cs(ctypes.byref(params), p0, p1, ctypes.c_uint32(mask), ctypes.c_int32(cs_in),
+                                          ctypes.c_int32(cs_metric), ctypes.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"ref_compute_pair_cs failed ({rc})")
+        return res.as_dict()
 
     def compute_pair_masked(self, params: Params, frame0, frame1, mask_plane, mask_bitdepth, mask=PSNR | WSPSNR | IVPSNR):
         """The app's mask mode (GCD-M, PSNR-M, WS-PSNR-M, IV-PSNR-M); returns (result dict, NumNonMasked)."""

@@ -377,6 +377,124 @@ static double qo_ivpsnr_quality(const uint64_t* row_sse, int32_t W, int32_t H, i
 }
 
 /* ----------------------------------------------------------------------------------------------- */
+/* Colour-space conversion before the metrics (f4): apps/QMIV/src/xAppQMIV.cpp:302-311 (which       */
+/* conversion), :853-891 (order). The app dispatches to the integer forms; their portable versions  */
+/* are libs/pmbb-core/src/xColorSpaceSTD.cpp:196-263. Fixed-point matrices with 16 fractional bits   */
+/* for BT.601 (= SMPTE 170M), BT.709, SMPTE 240M and BT.2020, the same integers as the reference's   */
+/* xColorSpaceCoeffYCbCr (xColorSpaceCoeff.h:59-73) so that rounding agrees.                         */
+/* ----------------------------------------------------------------------------------------------- */
+enum { QO_CS_RGB = 2, QO_CS_BGR = 3, QO_CS_GBR = 4, QO_CS_YCBCR = 16, QO_CS_BT601 = 17, QO_CS_SMPTE170M = 18,
+       QO_CS_BT709 = 19, QO_CS_SMPTE240M = 20, QO_CS_BT2020 = 21 };
+/* [space][0] = (Y<-R, Y<-G, Y<-B, Cb<-R, Cb<-G, Cr<-G, Cr<-B); [space][1] = (R<-Cr, G<-Cb, G<-Cr, B<-Cb) */
+static const int32_t qo_rgb2ycc[4][7] = {
+  { 19595, 38470, 7471, -11058, -21710, -27439, -5329 },   /* BT.601 */
+  { 13933, 46871, 4732,  -7509, -25259, -29763, -3005 },   /* BT.709 */
+  { 13894, 45941, 5701,  -7609, -25159, -29150, -3618 },   /* SMPTE 240M */
+  { 17216, 44434, 3886,  -9151, -23617, -30133, -2635 },   /* BT.2020 */
+};
+static const int32_t qo_ycc2rgb[4][4] = {
+  {  91881, -22553, -46802, 116130 },
+  { 103206, -12276, -30679, 121609 },
+  { 103285, -14852, -31236, 119669 },
+  {  96639, -10784, -37444, 123299 },
+};
+static int qo_cs_is_rgb(int32_t c) { return c == QO_CS_RGB || c == QO_CS_BGR || c == QO_CS_GBR; }
+static int qo_cs_is_defined_ycc(int32_t c) { return c > QO_CS_YCBCR; }
+static int qo_cs_index(int32_t c) /* eClrSpcLC of a defined YCbCr space, xUtilsQMIV.cpp:43-54 */
+{
+  switch(c) { case QO_CS_BT601: case QO_CS_SMPTE170M: return 0; case QO_CS_BT709: return 1; case QO_CS_SMPTE240M: return 2;
+              case QO_CS_BT2020: return 3; default: return -1; }
+}
+static inline int32_t qo_clipu(int32_t v, int32_t mx) { return v < 0 ? 0 : (v > mx ? mx : v); }
+
+/* Converts two 4:4:4 planar pictures in place as the app's preprocessFrames. Returns nonzero for a
+   combination the app refuses (xAppQMIV.cpp:302-306). */
+int qo_convert_colour(uint16_t* P0, uint16_t* P1, int32_t W, int32_t H, int32_t bitdepth, int32_t cs_in, int32_t cs_metric)
+{
+  if(cs_in != cs_metric)
+  {
+    if(cs_in >= QO_CS_YCBCR && cs_metric >= QO_CS_YCBCR) { return 1; }
+    if(cs_in == QO_CS_YCBCR || cs_metric == QO_CS_YCBCR) { return 1; }
+  }
+  const int ycc2rgb = qo_cs_is_defined_ycc(cs_in) && qo_cs_is_rgb(cs_metric);
+  const int rgb2ycc = qo_cs_is_rgb(cs_in) && qo_cs_is_defined_ycc(cs_metric);
+  const int reorder = qo_cs_is_rgb(cs_in) && cs_in != QO_CS_RGB && cs_metric == QO_CS_RGB;
+  const size_t pl = (size_t)W * H;
+  const int32_t mid = 1 << (bitdepth - 1), mx = (1 << bitdepth) - 1, add = 1 << 15;
+  uint16_t* pics[2] = { P0, P1 };
+  for(int i = 0; i < 2; i++)
+  {
+    uint16_t* a = pics[i]; uint16_t* b = a + pl; uint16_t* c = a + 2 * pl;
+    if(ycc2rgb) /* xColorSpaceSTD.cpp:231-263 */
+    {
+      const int32_t* k = qo_ycc2rgb[qo_cs_index(cs_in)];
+      for(size_t n = 0; n < pl; n++)
+      {
+        const int32_t iy = a[n], iu = (int32_t)b[n] - mid, iv = (int32_t)c[n] - mid;
+        const int32_t sy = (iy << 16) + add;
+        const int32_t r = (sy + k[0] * iv) >> 16, g = (sy + k[1] * iu + k[2] * iv) >> 16, bb = (sy + k[3] * iu) >> 16;
+        a[n] = (uint16_t)qo_clipu(r, mx); b[n] = (uint16_t)qo_clipu(g, mx); c[n] = (uint16_t)qo_clipu(bb, mx);
+      }
+    }
+    if(rgb2ycc) /* xColorSpaceSTD.cpp:196-229 */
+    {
+      const int32_t* k = qo_rgb2ycc[qo_cs_index(cs_metric)];
+      for(size_t n = 0; n < pl; n++)
+      {
+        const int32_t r = a[n], g = b[n], bb = c[n];
+        const int32_t ty = (k[0] * r + k[1] * g + k[2] * bb + add) >> 16;
+        const int32_t tu = (k[3] * r + k[4] * g + (bb << 15) + add) >> 16;
+        const int32_t tv = ((r << 15) + k[5] * g + k[6] * bb + add) >> 16;
+        a[n] = (uint16_t)qo_clipu(ty, mx); b[n] = (uint16_t)qo_clipu(tu + mid, mx); c[n] = (uint16_t)qo_clipu(tv + mid, mx);
+      }
+    }
+    if(reorder) /* xAppQMIV.cpp:878-891: BGR -> RGB swaps 0 and 2; GBR -> RGB swaps 0 and 1, then 0 and 2 */
+    {
+      for(size_t n = 0; n < pl; n++)
+      {
+        uint16_t t;
+        if(cs_in == QO_CS_BGR) { t = a[n]; a[n] = c[n]; c[n] = t; }
+        if(cs_in == QO_CS_GBR) { t = a[n]; a[n] = b[n]; b[n] = t; t = a[n]; a[n] = c[n]; c[n] = t; }
+      }
+    }
+  }
+  return 0;
+}
+
+/* The frame pipeline on colour-converted 4:4:4 pictures (conversion before the exactness check and
+   the metrics, as xAppQMIV::preprocessFrames). */
+int qo_compute_pair_cs(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask, int32_t cs_in,
+                       int32_t cs_metric, qo_result* out)
+{
+  const int32_t W = p->width, H = p->height, BD = p->bitdepth;
+  const size_t  pl = (size_t)W * H;
+  uint16_t* P0 = (uint16_t*)malloc(3 * pl * sizeof(uint16_t));
+  uint16_t* P1 = (uint16_t*)malloc(3 * pl * sizeof(uint16_t));
+  qo_unpack444(planes0, W, H, BD, p->chroma_format, P0);
+  qo_unpack444(planes1, W, H, BD, p->chroma_format, P1);
+  int rc = qo_convert_colour(P0, P1, W, H, BD, cs_in, cs_metric);
+  if(rc == 0)
+  {
+    qo_params q = *p;
+    q.chroma_format = 444;
+    const size_t esz = BD <= 8 ? 1 : 2;
+    unsigned char* B0 = (unsigned char*)malloc(3 * pl * esz);
+    unsigned char* B1 = (unsigned char*)malloc(3 * pl * esz);
+    for(size_t n = 0; n < 3 * pl; n++)
+    {
+      if(esz == 1) { B0[n] = (unsigned char)P0[n]; B1[n] = (unsigned char)P1[n]; }
+      else { ((uint16_t*)B0)[n] = P0[n]; ((uint16_t*)B1)[n] = P1[n]; }
+    }
+    const void* q0[3] = { B0, B0 + pl * esz, B0 + 2 * pl * esz };
+    const void* q1[3] = { B1, B1 + pl * esz, B1 + 2 * pl * esz };
+    rc = qo_compute_pair(&q, q0, q1, mask, out, NULL, NULL);
+    free(B0); free(B1);
+  }
+  free(P0); free(P1);
+  return rc;
+}
+
+/* ----------------------------------------------------------------------------------------------- */
 /* Mask mode: the mask picture's luma weights every sample (eCmp::LM in every *M call).            */
 /* ----------------------------------------------------------------------------------------------- */
 

@@ -83,6 +83,13 @@ int32_t qo_num_scales(int32_t W, int32_t H);
 int qo_compute_pair(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,
                     qo_result* out, uint16_t* scp0, uint16_t* scp1);
 
+/* Colour-space conversion of the app (-csi / -csm, codes as eClrSpcApp: RGB 2, BGR 3, GBR 4, YCbCr 16,
+   BT601 17, SMPTE170M 18, BT709 19, SMPTE240M 20, BT2020 21) on two 4:4:4 planar pictures, in place,
+   and the frame pipeline after it. Nonzero for combinations the app refuses. */
+int qo_convert_colour(uint16_t* P0, uint16_t* P1, int32_t W, int32_t H, int32_t bitdepth, int32_t cs_in, int32_t cs_metric);
+int qo_compute_pair_cs(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask, int32_t cs_in,
+                       int32_t cs_metric, qo_result* out);
+
 /* Mask mode (GCD-M, CPS-M, PSNR-M, WS-PSNR-M, IV-PSNR-M): mask_plane is the mask's luma, W x H,
    1 byte per sample for mask_bitdepth 8, else 2. Returns nonzero for SSIM metric bits. */
 int qo_compute_pair_masked(const qo_params* p, const void* const planes0[3], const void* const planes1[3], const void* mask_plane,

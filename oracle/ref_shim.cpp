@@ -28,6 +28,7 @@
 #include "xTestUtils.h"
 #include "xTestUtilsIVQM.h"
 #include "xKBNS.h"
+#include "xColorSpace.h"
 #include <cstring>
 #include <cstdint>
 #include <vector>
@@ -127,9 +128,85 @@ void copyPlanar(uint16_t* Dst, const xPicP& Src, int32 W, int32 H)
 
 extern "C" {
 
+/* Colour spaces of the app's -csi / -csm options (apps/QMIV/src/xUtilsQMIV.h:12-27). */
+enum { REF_CS_RGB = 2, REF_CS_BGR = 3, REF_CS_GBR = 4, REF_CS_YCBCR = 16, REF_CS_BT601 = 17, REF_CS_SMPTE170M = 18,
+       REF_CS_BT709 = 19, REF_CS_SMPTE240M = 20, REF_CS_BT2020 = 21 };
+
+} // extern "C"
+
+namespace {
+
+bool csIsRGB(int32 c) { return c == REF_CS_RGB || c == REF_CS_BGR || c == REF_CS_GBR; }
+bool csIsDefinedYCbCr(int32 c) { return c > REF_CS_YCBCR; }
+eClrSpcLC csToLC(int32 c)
+{
+  switch(c)
+  {
+  case REF_CS_BT601: return eClrSpcLC::BT601;
+  case REF_CS_SMPTE170M: return eClrSpcLC::SMPTE170M;
+  case REF_CS_BT709: return eClrSpcLC::BT709;
+  case REF_CS_SMPTE240M: return eClrSpcLC::SMPTE240M;
+  case REF_CS_BT2020: return eClrSpcLC::BT2020;
+  default: return eClrSpcLC::INVALID;
+  }
+}
+
+// The colour part of xAppQMIV::preprocessFrames (apps/QMIV/src/xAppQMIV.cpp:856-891, flags from :302-311)
+// on the two loaded 4:4:4 pictures.
+void convertColour(xPicP* Pic, int32 CsIn, int32 CsMetric)
+{
+  const bool CvtYCbCr2RGB = csIsDefinedYCbCr(CsIn) && csIsRGB(CsMetric);
+  const bool CvtRGB2YCbCr = csIsRGB(CsIn) && csIsDefinedYCbCr(CsMetric);
+  const bool ReorderRGB   = csIsRGB(CsIn) && CsIn != REF_CS_RGB && CsMetric == REF_CS_RGB;
+  for(int32 i = 0; i < 2; i++)
+  {
+    xPicP& P = Pic[i];
+    if(CvtYCbCr2RGB)
+    {
+      xColorSpace::ConvertYCbCr2RGB(P.getAddr(eCmp::R), P.getAddr(eCmp::G), P.getAddr(eCmp::B), P.getAddr(eCmp::LM), P.getAddr(eCmp::CB),
+                                    P.getAddr(eCmp::CR), P.getStride(), P.getStride(), P.getWidth(), P.getHeight(), P.getBitDepth(), csToLC(CsIn));
+    }
+    if(CvtRGB2YCbCr)
+    {
+      xColorSpace::ConvertRGB2YCbCr(P.getAddr(eCmp::LM), P.getAddr(eCmp::CB), P.getAddr(eCmp::CR), P.getAddr(eCmp::R), P.getAddr(eCmp::G),
+                                    P.getAddr(eCmp::B), P.getStride(), P.getStride(), P.getWidth(), P.getHeight(), P.getBitDepth(), csToLC(CsMetric));
+    }
+    if(ReorderRGB)
+    {
+      if(CsIn == REF_CS_BGR) { P.swapComponents(eCmp::C0, eCmp::C2); }
+      if(CsIn == REF_CS_GBR) { P.swapComponents(eCmp::C0, eCmp::C1); P.swapComponents(eCmp::C0, eCmp::C2); }
+    }
+  }
+}
+
+int computePairImpl(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask, ref_result* Out,
+                    uint16_t* Scp0, uint16_t* Scp1, int32 CsIn, int32 CsMetric);
+
+} // namespace
+
+extern "C" {
+
 /* Full per-frame pipeline of the reference app for one frame pair. scp0/scp1 (optional, 3*W*H uint16
    each, planar) receive the shift-compensated pictures m_PicSCP[0] / m_PicSCP[1]. Returns 0 on success. */
 int ref_compute_pair(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask, ref_result* Out, uint16_t* Scp0, uint16_t* Scp1)
+{
+  return computePairImpl(P, Planes0, Planes1, Mask, Out, Scp0, Scp1, REF_CS_YCBCR, REF_CS_YCBCR);
+}
+
+/* The same with the app's colour-space options: input colour space CsIn (-csi) and metric colour
+   space CsMetric (-csm), codes as eClrSpcApp. */
+int ref_compute_pair_cs(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask, int32_t CsIn,
+                        int32_t CsMetric, ref_result* Out)
+{
+  return computePairImpl(P, Planes0, Planes1, Mask, Out, nullptr, nullptr, CsIn, CsMetric);
+}
+
+} // extern "C"
+
+namespace {
+
+int computePairImpl(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask, ref_result* Out,
+                    uint16_t* Scp0, uint16_t* Scp1, int32 CsIn, int32 CsMetric)
 {
   const int32   W = P->width, H = P->height, BD = P->bitdepth;
   const int32V2 Size = { W, H };
@@ -152,6 +229,7 @@ int ref_compute_pair(const ref_params* P, const void* const Planes0[3], const vo
 
   loadFrame(PicP[0], Planes0, W, H, BD, P->chroma_format);
   loadFrame(PicP[1], Planes1, W, H, BD, P->chroma_format);
+  convertColour(PicP, CsIn, CsMetric);
 
   std::memset(Out, 0, sizeof(ref_result));
   bool Exact[3];
@@ -243,6 +321,10 @@ int ref_compute_pair(const ref_params* P, const void* const Planes0[3], const vo
   if(CalcSSIMs) { ProcSSIM.destroy(); }
   return 0;
 }
+
+} // namespace
+
+extern "C" {
 
 /* Mask mode of the reference app for one frame pair: the mask picture's luma (W x H, 1 byte per
    sample for MaskBitDepth 8, else 2 bytes) weights every sample; metrics limited to PSNR, WS-PSNR and

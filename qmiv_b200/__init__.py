@@ -26,7 +26,8 @@ from . import _lib
 from ._lib import (ALL, IVMSSSIM, IVPSNR, IVSSIM, METRIC_BITS, MSSSIM, PSNR, SSIM, WSPSNR, PEL_CNCL, PEL_SKIP,
                    PEL_STOP, PEL_WARN, QmivError, check)
 
-__all__ = ["Context", "Calc", "Batch", "make_params", "metric_mask", "QmivError", "library",
+__all__ = ["Context", "Calc", "Batch", "make_params", "metric_mask", "QmivError", "library", "frame_from_raw",
+           "raw_frame_bytes",
            "PSNR", "WSPSNR", "IVPSNR", "SSIM", "MSSSIM", "IVSSIM", "IVMSSSIM", "ALL", "Server"]
 
 
@@ -85,6 +86,41 @@ def _plane_info(plane):
     if arr.strides[1] != arr.itemsize:
         arr = np.ascontiguousarray(arr)
     return arr.ctypes.data, arr.strides[0], _lib.MEM_HOST, arr
+
+
+def raw_frame_bytes(width: int, height: int, bitdepth: int, chroma_format: int = 420) -> int:
+    """Bytes of one frame in a raw planar YUV file (xSeq's layout: Y, Cb, Cr; 1 byte per sample up
+    to 8 bits, else 2 bytes little endian)."""
+    esz = 1 if bitdepth <= 8 else 2
+    cw = width if chroma_format == 444 else width // 2
+    ch = height // 2 if chroma_format == 420 else height
+    return esz * (width * height + 2 * cw * ch)
+
+
+def frame_from_raw(buffer, width: int, height: int, bitdepth: int, chroma_format: int = 420, index: int = 0):
+    """The three planes of frame `index` of a raw planar YUV file held in `buffer` (1-D bytes: a numpy
+    uint8 array in host memory or a torch uint8 tensor on the device), as views with no copy and no
+    conversion: the kernels read 8-bit samples as bytes and deeper ones as 16-bit words, and never
+    upsample chroma (the reference's xSeqPic::xUnpackFrame, libs/pmbb-core/src/xSeq.cpp:231-290,
+    is not needed)."""
+    esz = 1 if bitdepth <= 8 else 2
+    cw = width if chroma_format == 444 else width // 2
+    ch = height // 2 if chroma_format == 420 else height
+    sizes = [(height, width), (ch, cw), (ch, cw)]
+    off = index * raw_frame_bytes(width, height, bitdepth, chroma_format)
+    planes = []
+    for h, w in sizes:
+        n = h * w * esz
+        seg = buffer[off:off + n]
+        if len(seg) != n:
+            raise ValueError("buffer shorter than the frame")
+        if hasattr(seg, "__cuda_array_interface__"):
+            import torch
+            planes.append(seg.view(torch.uint16 if esz == 2 else torch.uint8).view(h, w))
+        else:
+            planes.append(np.asarray(seg).view(np.uint16 if esz == 2 else np.uint8).reshape(h, w))
+        off += n
+    return tuple(planes)
 
 
 def make_frame(planes: Sequence) -> tuple[_lib.QmivFrame, list]:

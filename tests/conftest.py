@@ -36,6 +36,12 @@ def golden_masked():
 
 
 @pytest.fixture(scope="session")
+def golden_colour():
+    with open(os.path.join(GOLDEN, "golden_colour.json")) as f:
+        return json.load(f)["colour"]
+
+
+@pytest.fixture(scope="session")
 def cps_arrays():
     import numpy as np
     return dict(np.load(os.path.join(GOLDEN, "cps_fixtures.npz")))

@@ -10,6 +10,7 @@ a store mask with a 64-bit shift by 64), which the portable and AVX2 builds do n
 
     python tests/golden/make_golden.py            # golden.json
     python tests/golden/make_golden.py masked     # golden_masked.json (mask mode)
+    python tests/golden/make_golden.py colour     # golden_colour.json (colour-space conversion)
 """
 from __future__ import annotations
 
@@ -210,6 +211,45 @@ def main_masked():
     print("wrote", os.path.join(HERE, "golden_masked.json"))
 
 
+# colour-space conversion: (width, height, bitdepth, chroma_format, R, erp, seed, -csi, -csm)
+COLOUR_CASES = [
+    (64, 48, 8, 420, 2, False, 41, 19, 2),      # YCbCr BT.709 -> RGB
+    (64, 48, 10, 444, 2, True, 42, 2, 17),      # RGB -> YCbCr BT.601
+    (96, 64, 10, 444, 3, False, 43, 3, 2),      # BGR reordered to RGB
+    (96, 64, 8, 444, 2, True, 44, 4, 2),        # GBR reordered to RGB
+    (128, 64, 10, 420, 2, True, 45, 21, 2),     # YCbCr BT.2020 -> RGB
+    (64, 64, 12, 444, 2, False, 46, 2, 20),     # RGB -> YCbCr SMPTE 240M
+    (66, 34, 8, 444, 1, False, 47, 4, 21),      # GBR -> YCbCr BT.2020 (no reordering)
+    (64, 48, 10, 420, 4, True, 48, 18, 3),      # YCbCr SMPTE 170M -> BGR (plain RGB order)
+    (256, 128, 10, 444, 2, True, 49, 2, 19),    # RGB -> YCbCr BT.709
+]
+
+
+def make_colour(ref):
+    """The pipeline after the app's colour-space conversion (xAppQMIV.cpp:853-891), all metrics but the
+    multi-scale ones, run by the compiled reference. Frames come from detgen."""
+    out = []
+    mask = oracle.ALL & ~(oracle.MSSSIM | oracle.IVMSSSIM)
+    for (W, H, bd, cf, R, erp, seed, cs_in, cs_metric) in COLOUR_CASES:
+        p = oracle.make_params(W, H, bd, cf, search_range=R, erp=erp, num_threads=8)
+        f0, f1 = det_pair(W, H, bd, seed, cf)
+        r = ref.compute_pair_cs(p, f0, f1, cs_in, cs_metric, mask)
+        exp = {k: ([fhex(x) if isinstance(x, float) else int(x) for x in v] if isinstance(v, list)
+                   else (fhex(v) if isinstance(v, float) else int(v))) for k, v in r.items()}
+        out.append(dict(width=W, height=H, bitdepth=bd, chroma_format=cf, search_range=R, erp=erp, seed=seed,
+                        cs_in=cs_in, cs_metric=cs_metric, mask=mask, expected=exp))
+        print("colour", W, H, bd, cf, R, erp, cs_in, cs_metric, r["ivpsnr"])
+    return out
+
+
+def main_colour():
+    ref = oracle.Reference(ARCH)
+    data = dict(generator="tests/golden/make_golden.py colour", reference_build=ARCH, colour=make_colour(ref))
+    with open(os.path.join(HERE, "golden_colour.json"), "w") as f:
+        json.dump(data, f, separators=(",", ":"))
+    print("wrote", os.path.join(HERE, "golden_colour.json"))
+
+
 def main():
     ref = oracle.Reference(ARCH)
     data = dict(generator="tests/golden/make_golden.py", reference_build=ARCH,
@@ -222,5 +262,7 @@ def main():
 if __name__ == "__main__":
     if sys.argv[1:] == ["masked"]:
         main_masked()
+    elif sys.argv[1:] == ["colour"]:
+        main_colour()
     else:
         main()

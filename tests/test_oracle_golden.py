@@ -145,3 +145,33 @@ def test_masked_refuses_ssim(oracle_lib):
     p = oracle.make_params(32, 32, 8, 420)
     with pytest.raises(RuntimeError):
         oracle_lib.compute_pair_masked(p, f0, f1, det_mask(32, 32, 8, 1), 8, oracle.IVSSIM)
+
+
+def _colour_ids():
+    import json, os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "golden_colour.json")) as f:
+        g = json.load(f)["colour"]
+    return [f"{c['width']}x{c['height']}_{c['bitdepth']}b_{c['chroma_format']}_cs{c['cs_in']}to{c['cs_metric']}" for c in g]
+
+
+@pytest.mark.parametrize("idx", range(len(_colour_ids())), ids=_colour_ids())
+def test_colour_pipeline_matches_reference(idx, golden_colour, oracle_lib):
+    """Colour-space conversion before the metrics (YCbCr <-> RGB in four standards, BGR/GBR reordering)
+    of the restatement against the compiled reference, bit for bit."""
+    import oracle
+    case = golden_colour[idx]
+    f0, f1 = case_frames(case)
+    p = oracle.make_params(case["width"], case["height"], case["bitdepth"], case["chroma_format"],
+                           search_range=case["search_range"], erp=case["erp"])
+    got = oracle_lib.compute_pair_cs(p, f0, f1, case["cs_in"], case["cs_metric"], case["mask"])
+    assert compare_result(got, case["expected"], case["mask"]) == []
+
+
+def test_colour_refused_combinations(oracle_lib):
+    import oracle
+    from detgen import det_pair
+    f0, f1 = det_pair(32, 32, 8, 1, 444)
+    p = oracle.make_params(32, 32, 8, 444)
+    for cs_in, cs_metric in [(oracle.CS_BT601, oracle.CS_BT709), (oracle.CS_YCBCR, oracle.CS_RGB), (oracle.CS_RGB, oracle.CS_YCBCR)]:
+        with pytest.raises(RuntimeError):
+            oracle_lib.compute_pair_cs(p, f0, f1, cs_in, cs_metric)
