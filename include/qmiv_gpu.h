@@ -81,6 +81,14 @@ enum { QMIV_MEM_HOST = 0, QMIV_MEM_DEVICE = 1 };
 /* invalid-pixel action (apps/QMIV/src/xAppQMIV.cpp:834-852, README "InvalidPelActn") */
 enum { QMIV_PEL_SKIP = 0, QMIV_PEL_WARN = 1, QMIV_PEL_STOP = 2, QMIV_PEL_CNCL = 3 };
 
+/* Colour spaces of the app's ColorSpaceInput / ColorSpaceMetric options, same codes as its eClrSpcApp
+   (apps/QMIV/src/xUtilsQMIV.h:12-27). QMIV_CS_YCBCR is the generic (unspecified) YCbCr. */
+enum
+{
+  QMIV_CS_RGB = 2, QMIV_CS_BGR = 3, QMIV_CS_GBR = 4,
+  QMIV_CS_YCBCR = 16, QMIV_CS_BT601 = 17, QMIV_CS_SMPTE170M = 18, QMIV_CS_BT709 = 19, QMIV_CS_SMPTE240M = 20, QMIV_CS_BT2020 = 21
+};
+
 typedef struct qmiv_ctx_s*    qmiv_ctx;
 typedef struct qmiv_calc_s*   qmiv_calc;
 typedef struct qmiv_batch_s*  qmiv_batch;
@@ -197,6 +205,16 @@ QMIV_API qmiv_status qmiv_frame_pair_wait(qmiv_calc calc, int32_t timeout_ms, qm
 QMIV_API qmiv_status qmiv_frame_pair_compute_masked(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1,
                                                     const qmiv_frame* mask, int32_t mask_bitdepth, uint32_t metric_mask,
                                                     qmiv_result* out, int32_t* num_non_masked);
+
+/* The app's colour-space conversion (ColorSpaceInput -csi, ColorSpaceMetric -csm;
+   apps/QMIV/src/xAppQMIV.cpp:299-311, :853-891) for this calc's later qmiv_frame_pair_compute /
+   _submit calls: YCbCr (BT.601, SMPTE 170M, BT.709, SMPTE 240M, BT.2020) to RGB, RGB to YCbCr, or BGR /
+   GBR reordered to RGB, applied to the 4:4:4 pictures before the exactness check and every metric,
+   with the reference's integer arithmetic. Equal spaces (the default, QMIV_CS_YCBCR for both) convert
+   nothing. YCbCr to YCbCr is QMIV_ERR_UNSUPPORTED and the generic YCbCr in a conversion
+   QMIV_ERR_INVALID_ARG, as the app refuses them. While a conversion is set, qmiv_calc_gcd / _scp /
+   _cps_rows are QMIV_ERR_UNSUPPORTED. */
+QMIV_API qmiv_status qmiv_calc_set_color_space(qmiv_calc calc, int32_t color_space_input, int32_t color_space_metric);
 
 /* xGlobClrDiffProc::CalcGlobalColorDiff(Tst=In0, Ref=In1) -> round(mean(In1 - In0)), clipped. */
 QMIV_API qmiv_status qmiv_calc_gcd(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, int32_t gcd_r2t[4]);

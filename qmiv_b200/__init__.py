@@ -24,6 +24,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (ALL, IVMSSSIM, IVPSNR, IVSSIM, METRIC_BITS, MSSSIM, PSNR, SSIM, WSPSNR, PEL_CNCL, PEL_SKIP,
+                   CS_RGB, CS_BGR, CS_GBR, CS_YCBCR, CS_BT601, CS_SMPTE170M, CS_BT709, CS_SMPTE240M, CS_BT2020,
                    PEL_STOP, PEL_WARN, QmivError, check)
 
 __all__ = ["Context", "Calc", "Batch", "make_params", "metric_mask", "QmivError", "library", "frame_from_raw",
@@ -208,6 +209,11 @@ class Calc:
         check(self._lib.qmiv_frame_pair_compute(self.handle, ctypes.byref(f0), ctypes.byref(f1),
                                                 metric_mask(metrics), ctypes.byref(res)), "qmiv_frame_pair_compute")
         return res.as_dict()
+
+    def set_color_space(self, color_space_input: int, color_space_metric: int):
+        """Colour-space conversion before the metrics (qmiv_calc_set_color_space), codes CS_*."""
+        check(self._lib.qmiv_calc_set_color_space(self.handle, color_space_input, color_space_metric),
+              "qmiv_calc_set_color_space")
 
     def compute_masked(self, frame0, frame1, mask, mask_bitdepth: int, metrics=None):
         """Mask mode (qmiv_frame_pair_compute_masked): mask is the mask picture's luma plane (H x W;

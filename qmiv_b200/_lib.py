@@ -23,6 +23,9 @@ METRIC_BITS = {"PSNR": PSNR, "WSPSNR": WSPSNR, "IVPSNR": IVPSNR, "SSIM": SSIM, "
 MEM_HOST, MEM_DEVICE = 0, 1
 STAGES = ["h2d", "prepass", "reduce", "cps", "ssim_win", "ssim_rows", "finalize", "d2h"]
 PEL_SKIP, PEL_WARN, PEL_STOP, PEL_CNCL = 0, 1, 2, 3
+# colour spaces (ColorSpaceInput / ColorSpaceMetric), apps/QMIV/src/xUtilsQMIV.h:12-27
+CS_RGB, CS_BGR, CS_GBR, CS_YCBCR = 2, 3, 4, 16
+CS_BT601, CS_SMPTE170M, CS_BT709, CS_SMPTE240M, CS_BT2020 = 17, 18, 19, 20, 21
 
 
 class QmivParams(ctypes.Structure):
@@ -110,6 +113,7 @@ SIGNATURES = {
     "qmiv_calc_scp": (ctypes.c_int, [_P, ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame),
                                      ctypes.POINTER(ctypes.c_int32), _P, _P, ctypes.c_int32]),
     "qmiv_calc_set_gcd": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
+    "qmiv_calc_set_color_space": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "qmiv_calc_cps_rows": (ctypes.c_int, [_P, _P, _P]),
     "qmiv_calc_stream": (ctypes.c_int, [_P, _PP]),
     "qmiv_frame_pair_compute_static": (ctypes.c_int, [ctypes.POINTER(QmivFrame), ctypes.POINTER(QmivFrame),

@@ -430,14 +430,25 @@ static qmiv_status calc_submit(qmiv_calc calc, const qmiv_frame* in0, const qmiv
   QMIV_TRY(check_metrics(calc->pipe.shape(), mask));
   QMIV_CUDA(cudaSetDevice(calc->ctx->device));
   const bool host = in0->mem == QMIV_MEM_HOST || in1->mem == QMIV_MEM_HOST;
-  QMIV_TRY(calc->pipe.prepare(mask, want_scp, host));
+  const bool colour = calc->colour && calc->colour->active;
+  QMIV_TRY(calc->pipe.prepare(colour ? 0u : mask, colour ? false : want_scp, host));
   Img a{}, b{};
   QMIV_TRY(calc->pipe.resolve(in0, 0, a, calc->stream));
   QMIV_TRY(calc->pipe.resolve(in1, 1, b, calc->stream));
-  QMIV_TRY(calc->pipe.enqueue(a, b, mask, want_scp, want_gcd, calc->stream));
+  if(colour)
+  {
+    // metrics on the converted 4:4:4 pictures (xAppQMIV.cpp:853-891 before :893-1108)
+    ColourStage& cs = *calc->colour;
+    Img c0{}, c1{};
+    QMIV_TRY(cs.convert(calc->ctx, calc->shape, calc->prm, a, b, c0, c1, calc->stream));
+    QMIV_TRY(cs.pipe444.prepare(mask, want_scp, false));
+    QMIV_TRY(cs.pipe444.enqueue(c0, c1, mask, want_scp, want_gcd, calc->stream));
+  }
+  else { QMIV_TRY(calc->pipe.enqueue(a, b, mask, want_scp, want_gcd, calc->stream)); }
   QMIV_CUDA(cudaEventRecord(calc->done, calc->stream));
   calc->pending = true;
   calc->pending_mask = mask;
+  calc->pending_colour = colour;
   return QMIV_OK;
 }
 
@@ -446,8 +457,26 @@ static qmiv_status calc_collect(qmiv_calc calc, int32_t timeout_ms, qmiv_result*
   if(!calc->pending) { return fail(QMIV_ERR_INVALID_ARG, "nothing submitted"); }
   QMIV_TRY(wait_event(calc->done, timeout_ms));
   calc->pending = false;
-  calc->has_last = true;
+  calc->has_last = !calc->pending_colour;
   calc->pipe.harvest_profile();
+  if(calc->pending_colour)
+  {
+    ColourStage& cs = *calc->colour;
+    cs.pipe444.harvest_profile();
+    const PairOut& o = cs.pipe444.host_out();
+    const int32_t inv = cs.invalid_flags(calc->shape.maxv);   // the original frames, before conversion
+    if(out)
+    {
+      finish_result(o, cs.pipe444.finish_info(calc->pending_mask), out);
+      out->invalid_pel[0] = (inv & 1) != 0;
+      out->invalid_pel[1] = (inv & 2) != 0;
+    }
+    if(calc->prm.invalid_pel_action == QMIV_PEL_STOP && inv)
+    {
+      return fail(QMIV_ERR_INVALID_PIXEL, "input frame contains samples above the bit depth's maximum");
+    }
+    return pair_status(o, calc->prm.invalid_pel_action);
+  }
   const PairOut& o = calc->pipe.host_out();
   if(out) { finish_result(o, calc->pipe.finish_info(calc->pending_mask), out); }
   return pair_status(o, calc->prm.invalid_pel_action);
@@ -508,8 +537,22 @@ qmiv_status qmiv_frame_pair_wait(qmiv_calc calc, int32_t timeout_ms, qmiv_result
   return calc_collect(calc, timeout_ms, out);
 }
 
+qmiv_status qmiv_calc_set_color_space(qmiv_calc calc, int32_t color_space_input, int32_t color_space_metric)
+{
+  if(!calc) { return fail(QMIV_ERR_INVALID_ARG, "calc is null"); }
+  if(calc->pending) { return fail(QMIV_ERR_BUSY, "a submission is in flight on this calc"); }
+  std::unique_ptr<ColourStage> cs(new ColourStage());
+  QMIV_TRY(cs->configure(color_space_input, color_space_metric));
+  if(cs->active && calc->shape.bitdepth > 14) { return fail(QMIV_ERR_UNSUPPORTED, "colour conversion needs bit depth <= 14"); }
+  calc->colour = cs->active ? std::move(cs) : nullptr;
+  return QMIV_OK;
+}
+
+static bool colour_set(qmiv_calc calc) { return calc && calc->colour && calc->colour->active; }
+
 qmiv_status qmiv_calc_gcd(qmiv_calc calc, const qmiv_frame* in0, const qmiv_frame* in1, int32_t gcd_r2t[4])
 {
+  if(colour_set(calc)) { return fail(QMIV_ERR_UNSUPPORTED, "not available with a colour conversion set"); }
   if(!gcd_r2t) { return fail(QMIV_ERR_INVALID_ARG, "gcd_r2t is null"); }
   qmiv_result r;
   QMIV_TRY(calc_submit(calc, in0, in1, 0, false, true));
@@ -523,6 +566,7 @@ qmiv_status qmiv_calc_scp(qmiv_calc calc, const qmiv_frame* in0, const qmiv_fram
 {
   if(dst_mem != QMIV_MEM_HOST && dst_mem != QMIV_MEM_DEVICE) { return fail(QMIV_ERR_INVALID_ARG, "bad dst_mem"); }
   if(!calc) { return fail(QMIV_ERR_INVALID_ARG, "calc is null"); }
+  if(colour_set(calc)) { return fail(QMIV_ERR_UNSUPPORTED, "not available with a colour conversion set"); }
   int32_t saved[4];
   const bool had = calc->pipe.get_gcd_override(saved);
   if(gcd_r2t) { calc->pipe.set_gcd_override(gcd_r2t); }
@@ -559,6 +603,7 @@ qmiv_status qmiv_calc_scp(qmiv_calc calc, const qmiv_frame* in0, const qmiv_fram
 qmiv_status qmiv_calc_cps_rows(qmiv_calc calc, uint64_t* rows_r2t, uint64_t* rows_t2r)
 {
   if(!calc) { return fail(QMIV_ERR_INVALID_ARG, "calc is null"); }
+  if(colour_set(calc)) { return fail(QMIV_ERR_UNSUPPORTED, "not available with a colour conversion set"); }
   if(!calc->has_last || !calc->pipe.cps_rows()) { return fail(QMIV_ERR_INVALID_ARG, "no CPS result available"); }
   const Shape& S = calc->shape;
   std::vector<uint32_t> tmp((size_t)2 * S.H * 3);

@@ -187,6 +187,30 @@ private:
   std::vector<std::pair<int, int>> ev_pending_;  // (stage, index of the begin event)
 };
 
+// Colour-space conversion of one calc (qmiv_colour.cu): the converted 4:4:4 planes of the current pair
+// and the 4:4:4 pipeline that computes the metrics on them.
+class ColourStage
+{
+public:
+  qmiv_status configure(int32_t cs_in, int32_t cs_metric);
+  // Converts both frames into 4:4:4 planes (out0 / out1 describe them) on stream s.
+  qmiv_status convert(qmiv_ctx_s* ctx, const Shape& S, const qmiv_params& prm, const Img& in0, const Img& in1, Img& out0, Img& out1,
+                      cudaStream_t s);
+  // bit0 / bit1: frame 0 / 1 held samples above maxv (valid after the stream synced)
+  int32_t invalid_flags(int32_t maxv) const;
+  ~ColourStage();
+
+  bool         active = false;
+  PairPipeline pipe444;
+
+private:
+  int32_t  mode = 0, space = 0, perm[3] = { 0, 1, 2 };
+  bool     configured_ = false;
+  Shape    shape444_;
+  DevMem   planes_, max_;
+  uint32_t* h_max_ = nullptr;
+};
+
 // Mask mode of one calc (qmiv_masked.cu): its scratch and the synchronous run.
 class MaskedPipeline
 {
@@ -214,4 +238,6 @@ struct qmiv_calc_s
   uint32_t             pending_mask = 0;
   bool                 has_last = false;
   std::unique_ptr<qmiv::MaskedPipeline> masked;   // created by the first masked call
+  std::unique_ptr<qmiv::ColourStage>    colour;   // set by qmiv_calc_set_color_space
+  bool                 pending_colour = false;   // the submission in flight went through the colour stage
 };

@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _raw(frames):
-    return np.frombuffer(b"".join(np.ascontiguousarray(p).tobytes() for f in frames for p in f), np.uint8)
+    return np.frombuffer(b"".join(np.ascontiguousarray(p).tobytes() for f in frames for p in f), np.uint8).copy()
 
 
 @pytest.mark.parametrize("shape", [(640, 360, 10, 420), (320, 240, 8, 420), (256, 128, 10, 422), (192, 96, 8, 444)])
