@@ -25,6 +25,13 @@ ALL = 127
 # colour spaces of the app's -csi / -csm options (apps/QMIV/src/xUtilsQMIV.h:12-27)
 CS_RGB, CS_BGR, CS_GBR, CS_YCBCR = 2, 3, 4, 16
 CS_BT601, CS_SMPTE170M, CS_BT709, CS_SMPTE240M, CS_BT2020 = 17, 18, 19, 20, 21
+# structural similarity modes (xSSIM::eMode) and margin extension modes (eMrgExt) of the app's -ssm / -ssb
+SSM_REGULAR_GAUSSIAN_FLT, SSM_REGULAR_GAUSSIAN_INT, SSM_REGULAR_AVERAGED, SSM_BLOCK_GAUSSIAN_INT, SSM_BLOCK_AVERAGED = 0, 1, 2, 3, 4
+BRD_NONE, BRD_NEAREST, BRD_REFLECT, BRD_MIRROR, BRD_CONSTANT, BRD_ZERO = 0, 1, 2, 3, 4, 5
+
+
+class SsimCfg(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int32), ("border", ctypes.c_int32), ("window", ctypes.c_int32), ("stride", ctypes.c_int32)]
 
 
 class Params(ctypes.Structure):
@@ -117,6 +124,18 @@ class Oracle(_Lib):
                                          ctypes.c_int32(cs_metric), ctypes.byref(res))
         if rc != 0:
             raise RuntimeError(f"qo_compute_pair_cs failed ({rc})")
+        return res.as_dict()
+
+    def compute_pair_ssim(self, params: Params, frame0, frame1, mode, border, window, stride, mask=ALL):
+        """The pipeline with the app's structural similarity options (-ssm, -ssb, -ssw, -sss)."""
+        a0, p0 = _planes(frame0)
+        a1, p1 = _planes(frame1)
+        res = Result()
+        cfg = SsimCfg(mode, border, window, stride)
+        rc = self.lib.qo_compute_pair_ssim(ctypes.byref(params), p0, p1, ctypes.c_uint32(mask), ctypes.byref(cfg),
+                                           ctypes.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"qo_compute_pair_ssim failed ({rc})")
         return res.as_dict()
 
     def compute_pair_masked(self, params: Params, frame0, frame1, mask_plane, mask_bitdepth, mask=PSNR | WSPSNR | IVPSNR):
@@ -264,6 +283,18 @@ class Reference(_Lib):
                                           ctypes.c_int32(cs_metric), ctypes.byref(res))
         if rc != 0:
             raise RuntimeError(f"ref_compute_pair_cs failed ({rc})")
+        return res.as_dict()
+
+    def compute_pair_ssim(self, params: Params, frame0, frame1, mode, border, window, stride, mask=ALL):
+        """The pipeline with the app's structural similarity options (-ssm, -ssb, -ssw, -sss)."""
+        a0, p0 = _planes(frame0)
+        a1, p1 = _planes(frame1)
+        res = Result()
+        cfg = SsimCfg(mode, border, window, stride)
+        rc = self.lib.ref_compute_pair_ssim(ctypes.byref(params), p0, p1, ctypes.c_uint32(mask), ctypes.byref(cfg),
+                                            ctypes.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"ref_compute_pair_ssim failed ({rc})")
         return res.as_dict()
 
     def compute_pair_masked(self, params: Params, frame0, frame1, mask_plane, mask_bitdepth, mask=PSNR | WSPSNR | IVPSNR):

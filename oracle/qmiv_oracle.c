@@ -205,49 +205,176 @@ void qo_ws_weights(int32_t H, int32_t lat_range, double* w, double* correction)
 }
 
 /* ----------------------------------------------------------------------------------------------- */
-/* a9/a10: block-averaged SSIM, 8x8 windows at stride 4                                            */
-/* window: libs/pmbb-ivqm/src/xStructSimSTD.cpp:420-461 (AVX-512 CalcBlckAvg8 and                  */
-/*         CalcMultiBlckAvg8S4 give the same per-window value, test-xStructSim.cpp:169-170)         */
-/* loops:  libs/pmbb-ivqm/src/xSSIM.cpp:276-311 (ranges), :328-369 (row and picture KBNS)           */
-/* ERP:    libs/pmbb-ivqm/src/xIVSSIM.cpp:138-173 (row weight w[y + WndSize/2])                     */
+/* a9/a10: SSIM under every structural similarity option of the app                                */
+/* windows: libs/pmbb-ivqm/src/xStructSimSTD.cpp:19-193 (regular 11x11 centred windows: Gaussian   */
+/*          float, Gaussian integer, averaged), :353-461 (block windows anchored at their top-left  */
+/*          sample: Gaussian integer 8/16, averaged 8/16/32). The AVX form of the regular averaged  */
+/*          window (xStructSimAVX.h:20-23 -> CalcBlckAvg11) sums the same integers.                 */
+/* loops:   libs/pmbb-ivqm/src/xSSIM.cpp:161-196 (ranges, NumUnit), :381-404 (block counts),        */
+/*          :215-251 (row KBNS in x order, picture KBNS over rows / NumActive)                      */
+/* borders: libs/pmbb-core/src/xMarginOps.h:16-20 (Nearest, Reflect, Mirror, Constant = 65535 as   */
+/*          xPicP::extend passes it, xPic.cpp:94-101, Zero); regular windows only, xSSIM.cpp:90     */
+/* ERP:     libs/pmbb-ivqm/src/xIVSSIM.cpp:138-173 (row weight w[y] regular, w[y + WndSize/2] block)*/
 /* ----------------------------------------------------------------------------------------------- */
-static double qo_ssim_window(const uint16_t* t, const uint16_t* r, int32_t stride, double C1, double C2, int32_t calc_l)
+
+/* Integer Gaussian windows (xStructSimConsts.h:111-124 for 11x11, :145-173 for 8x8 and 16x16), each
+   the mirror image of its top-left quadrant in both directions; weights sum to 2^18 (16x16: 262140) and
+   the sums are scaled by 2^-18 (c_InvFltrIntMul). The 11x11 quadrant is not symmetric about its
+   diagonal ([4][5] = 14854, [5][4] = 14855). */
+static const int32_t qo_gq11[6][6] = {
+  { 0, 2, 10, 29, 57, 72 },           { 2, 15, 72, 218, 424, 530 },          { 10, 72, 340, 1032, 2010, 2510 },
+  { 29, 218, 1032, 3135, 6107, 7626 }, { 57, 424, 2010, 6107, 11894, 14854 }, { 72, 530, 2510, 7626, 14855, 18550 },
+};
+static const int32_t qo_gq8[4][4] = {
+  { 81, 308, 749, 1168 }, { 308, 1168, 2842, 4432 }, { 749, 2842, 6913, 10781 }, { 1168, 4432, 10781, 16814 },
+};
+static const int32_t qo_gq16[8][8] = {
+  { 0, 1, 4, 10, 19, 32, 45, 54 },                 { 1, 5, 13, 32, 64, 108, 152, 181 },
+  { 4, 13, 38, 91, 181, 305, 432, 514 },           { 10, 32, 91, 216, 432, 727, 1029, 1224 },
+  { 19, 64, 181, 432, 865, 1456, 2061, 2451 },     { 32, 108, 305, 727, 1456, 2451, 3469, 4126 },
+  { 45, 152, 432, 1029, 2061, 3469, 4909, 5839 },  { 54, 181, 514, 1224, 2451, 4126, 5839, 6947 },
+};
+
+static int32_t qo_gauss_int(int32_t N, int32_t y, int32_t x)
 {
-  const double inv = 1.0 / 64.0;
-  int64_t sr = 0, st = 0, srr = 0, stt = 0, srt = 0;
-  for(int32_t y = 0; y < 8; y++)
+  const int32_t qy = y < N - 1 - y ? y : N - 1 - y, qx = x < N - 1 - x ? x : N - 1 - x;
+  return N == 11 ? qo_gq11[qy][qx] : N == 8 ? qo_gq8[qy][qx] : qo_gq16[qy][qx];
+}
+
+/* Float Gaussian window (c_FilterRglrGaussFlt32, xStructSimConsts.h:55-68): the 11x11 Gaussian of
+   sigma 1.5 normalised to unit sum, rounded to float; each product is formed in double. */
+static double qo_gflt11[11][11];
+static int    qo_gflt_ready = 0;
+static void qo_gflt_init(void)
+{
+  if(qo_gflt_ready) { return; }
+  double g[11][11], sum = 0.0;
+  for(int32_t y = 0; y < 11; y++)
   {
-    for(int32_t x = 0; x < 8; x++)
-    {
-      const int32_t R = r[(size_t)y * stride + x], T = t[(size_t)y * stride + x];
-      sr += R; st += T; srr += R * R; stt += T * T; srt += R * T;
-    }
+    for(int32_t x = 0; x < 11; x++) { g[y][x] = exp(-(double)((x - 5) * (x - 5) + (y - 5) * (y - 5)) / 4.5); sum += g[y][x]; }
   }
-  const double avg_r = (double)sr * inv;
-  const double avg_t = (double)st * inv;
-  const double var_r = (double)srr * inv - avg_r * avg_r;
-  const double var_t = (double)stt * inv - avg_t * avg_t;
-  const double cov   = (double)srt * inv - avg_r * avg_t;
-  const double cs    = (2 * cov + C2) / (var_r + var_t + C2);
+  for(int32_t y = 0; y < 11; y++) { for(int32_t x = 0; x < 11; x++) { qo_gflt11[y][x] = (double)(float)(g[y][x] / sum); } }
+  qo_gflt_ready = 1;
+}
+
+static int qo_ssm_regular(int32_t mode) { return mode >= QO_SSM_REGULAR_GAUSSIAN_FLT && mode <= QO_SSM_REGULAR_AVERAGED; }
+static int32_t qo_ssm_window(const qo_ssim_cfg* cfg) { return qo_ssm_regular(cfg->mode) ? 11 : cfg->window; }
+
+/* position of sample i of a length-n line after margin extension, -1 for the constant modes */
+static int32_t qo_brd_index(int32_t i, int32_t n, int32_t border)
+{
+  if(i >= 0 && i < n) { return i; }
+  switch(border)
+  {
+  case QO_BRD_NEAREST: return i < 0 ? 0 : n - 1;              /* ( a a a | a b c d | d d d ) */
+  case QO_BRD_REFLECT: return i < 0 ? -1 - i : 2 * n - 1 - i; /* ( c b a | a b c d | d c b ) */
+  case QO_BRD_MIRROR:  return i < 0 ? -i : 2 * n - 2 - i;     /* ( d c b | a b c d | c b a ) */
+  default:             return -1;
+  }
+}
+static int32_t qo_brd_sample(const uint16_t* p, int32_t W, int32_t H, int32_t x, int32_t y, int32_t border)
+{
+  const int32_t xi = qo_brd_index(x, W, border), yi = qo_brd_index(y, H, border);
+  if(xi < 0 || yi < 0) { return border == QO_BRD_CONSTANT ? 65535 : 0; }
+  return p[(size_t)yi * W + xi];
+}
+
+static double qo_ssim_formula(double avg_r, double avg_t, double var_r, double var_t, double cov, double C1, double C2, int32_t calc_l)
+{
+  const double cs = (2 * cov + C2) / (var_r + var_t + C2);          /* "Contrast" * "Similarity" */
   if(!calc_l) { return cs; }
-  const double l = (2 * avg_r * avg_t + C1) / (avg_r * avg_r + avg_t * avg_t + C1);
+  const double l = (2 * avg_r * avg_t + C1) / (avg_r * avg_r + avg_t * avg_t + C1); /* "Luminance" */
   return l * cs;
 }
 
-static int32_t qo_num_windows(int32_t len) { return len < 8 ? 0 : (len - 8) / 4 + 1; } /* xSSIM.cpp:496-519 */
+/* One window whose top-left input sample is (x0, y0); t = "Tst", r = "Ref". */
+static double qo_ssim_window_cfg(const uint16_t* t, const uint16_t* r, int32_t W, int32_t H, int32_t x0, int32_t y0,
+                                 const qo_ssim_cfg* cfg, double C1, double C2, int32_t calc_l)
+{
+  const int32_t N = qo_ssm_window(cfg), brd = qo_ssm_regular(cfg->mode) ? cfg->border : QO_BRD_NONE;
+  if(cfg->mode == QO_SSM_REGULAR_GAUSSIAN_FLT) /* xStructSimSTD.cpp:19-88: double sums in dy, dx order */
+  {
+    double sr = 0, st = 0, srr = 0, stt = 0, srt = 0;
+    for(int32_t dy = 0; dy < 11; dy++)
+    {
+      for(int32_t dx = 0; dx < 11; dx++)
+      {
+        const double R = (double)qo_brd_sample(r, W, H, x0 + dx, y0 + dy, brd);
+        const double T = (double)qo_brd_sample(t, W, H, x0 + dx, y0 + dy, brd);
+        const double C = qo_gflt11[dy][dx];
+        sr += R * C; st += T * C; srr += (R * R) * C; stt += (T * T) * C; srt += (R * T) * C;
+      }
+    }
+    return qo_ssim_formula(sr, st, srr - sr * sr, stt - st * st, srt - sr * st, C1, C2, calc_l);
+  }
+  const int gauss = cfg->mode == QO_SSM_REGULAR_GAUSSIAN_INT || cfg->mode == QO_SSM_BLOCK_GAUSSIAN_INT;
+  int64_t sr = 0, st = 0, srr = 0, stt = 0, srt = 0;
+  for(int32_t dy = 0; dy < N; dy++)
+  {
+    for(int32_t dx = 0; dx < N; dx++)
+    {
+      const int64_t R = qo_brd_sample(r, W, H, x0 + dx, y0 + dy, brd);
+      const int64_t T = qo_brd_sample(t, W, H, x0 + dx, y0 + dy, brd);
+      const int64_t C = gauss ? qo_gauss_int(N, dy, dx) : 1;
+      sr += R * C; st += T * C; srr += R * R * C; stt += T * T * C; srt += R * T * C;
+    }
+  }
+  const double inv = gauss ? 1.0 / (double)(1 << 18)                                    /* c_InvFltrIntMul */
+                   : cfg->mode == QO_SSM_REGULAR_AVERAGED ? 1.0 / (double)121           /* c_InvFltrArea */
+                   : 1.0 / (double)(N * N);                                              /* c_InvBlockArea */
+  const double avg_r = (double)sr * inv, avg_t = (double)st * inv;
+  const double var_r = (double)srr * inv - avg_r * avg_r;
+  const double var_t = (double)stt * inv - avg_t * avg_t;
+  const double cov   = (double)srt * inv - avg_r * avg_t;
+  return qo_ssim_formula(avg_r, avg_t, var_r, var_t, cov, C1, C2, calc_l);
+}
+
+int qo_ssim_cfg_check(const qo_ssim_cfg* cfg, int32_t W, int32_t H)
+{
+  if(cfg->mode < QO_SSM_REGULAR_GAUSSIAN_FLT || cfg->mode > QO_SSM_BLOCK_AVERAGED) { return -1; }
+  if(cfg->border < QO_BRD_NONE || cfg->border > QO_BRD_ZERO) { return -1; }
+  const int32_t N = qo_ssm_window(cfg);
+  if(qo_ssm_regular(cfg->mode) && cfg->window != 11) { return -1; }                     /* xAppQMIV.cpp:332 */
+  if(cfg->mode == QO_SSM_BLOCK_AVERAGED && N != 8 && N != 16 && N != 32) { return -1; } /* xAppQMIV.cpp:104 */
+  if(cfg->mode == QO_SSM_BLOCK_GAUSSIAN_INT && N != 8 && N != 16) { return -1; }        /* xStructSimSTD.cpp:399-403 */
+  if(cfg->stride < 1 || cfg->stride > N) { return -1; }                                  /* xAppQMIV.cpp:331 */
+  /* the averaged 11x11 window squares samples in 32-bit lanes (xStructSimSTD.cpp:167-169, and as signed
+     16-bit products in its AVX form), which the constant 65535 margin overflows */
+  if(cfg->mode == QO_SSM_REGULAR_AVERAGED && cfg->border == QO_BRD_CONSTANT) { return -1; }
+  if(W < N || H < N) { return -1; }
+  return 0;
+}
+
+/* window rows/columns of one picture: first window origin, count and the top-left offset of the
+   window's input samples relative to the origin */
+static void qo_ssim_range(const qo_ssim_cfg* cfg, int32_t len, int32_t* beg, int32_t* num, int32_t* org)
+{
+  const int32_t S = cfg->stride, N = qo_ssm_window(cfg);
+  if(qo_ssm_regular(cfg->mode))
+  {
+    const int32_t b = cfg->border != QO_BRD_NONE ? 0 : 5, e = cfg->border != QO_BRD_NONE ? len : len - 5;
+    *beg = b; *num = (e - b + S - 1) / S; *org = -5;
+  }
+  else { *beg = 0; *num = (len - N) / S + 1; *org = 0; }
+}
 
 static void qo_ssim_consts(int32_t bitdepth, double* C1, double* C2)
 {
-  const double maxv = (double)qo_max_value(bitdepth);  /* xSSIM.cpp:165-167, K1=0.01, K2=0.03 */
+  const double maxv = (double)qo_max_value(bitdepth);  /* xSSIM.cpp:50-52, K1=0.01, K2=0.03 */
   const double a = 0.01 * maxv, b = 0.03 * maxv;
   *C1 = a * a; *C2 = b * b;
 }
 
-void qo_ssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, int32_t calc_l,
-                 const double* ws_weights, double out[3])
+int qo_ssim_pic_cfg(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, int32_t calc_l,
+                    const double* ws_weights, const qo_ssim_cfg* cfg, double out[3])
 {
+  if(qo_ssim_cfg_check(cfg, W, H)) { return -1; }
+  qo_gflt_init();
   double C1, C2; qo_ssim_consts(bitdepth, &C1, &C2);
-  const int32_t nx = qo_num_windows(W), ny = qo_num_windows(H);
+  int32_t bx, by, nx, ny, org;
+  qo_ssim_range(cfg, W, &bx, &nx, &org);
+  qo_ssim_range(cfg, H, &by, &ny, &org);
+  const int32_t S = cfg->stride, wsoff = qo_ssm_regular(cfg->mode) ? 0 : (qo_ssm_window(cfg) >> 1);
   for(int32_t c = 0; c < 3; c++)
   {
     const uint16_t* t = tst + (size_t)c * W * H;
@@ -255,15 +382,15 @@ void qo_ssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H,
     qo_kbns pic = { 0.0, 0.0 }, wacc = { 0.0, 0.0 };
     for(int32_t j = 0; j < ny; j++)
     {
-      const int32_t y = 4 * j;
+      const int32_t y = by + j * S;
       qo_kbns row = { 0.0, 0.0 };
       for(int32_t i = 0; i < nx; i++)
       {
-        const size_t o = (size_t)y * W + 4 * i;
-        qo_kbns_add(&row, qo_ssim_window(t + o, r + o, W, C1, C2, calc_l));
+        const int32_t x = bx + i * S;
+        qo_kbns_add(&row, qo_ssim_window_cfg(t, r, W, H, x + org, y + org, cfg, C1, C2, calc_l));
       }
       double rs = qo_kbns_result(&row);
-      if(ws_weights) { const double wt = ws_weights[y + 4]; rs = rs * wt; qo_kbns_add(&wacc, wt); }
+      if(ws_weights) { const double wt = ws_weights[y + wsoff]; rs = rs * wt; qo_kbns_add(&wacc, wt); }
       qo_kbns_add(&pic, rs);
     }
     const int64_t active = (int64_t)nx * ny;
@@ -274,11 +401,21 @@ void qo_ssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H,
     }
     else { out[c] = qo_kbns_result(&pic) / (double)active; }
   }
+  return 0;
+}
+
+static const qo_ssim_cfg qo_ssim_default = { QO_SSM_BLOCK_AVERAGED, QO_BRD_NONE, 8, 4 }; /* xSSIM.h:35-37 */
+
+void qo_ssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, int32_t calc_l,
+                 const double* ws_weights, double out[3])
+{
+  if(qo_ssim_pic_cfg(tst, ref, W, H, bitdepth, calc_l, ws_weights, &qo_ssim_default, out)) { out[0] = out[1] = out[2] = 0.0; }
 }
 
 /* ----------------------------------------------------------------------------------------------- */
-/* a11: MS-SSIM, libs/pmbb-ivqm/src/xSSIM.cpp:230-256, scales :520-532, exponents                  */
-/* libs/pmbb-ivqm/src/xStructSimConsts.h:42-49, downsampling xPixelOpsSTD.cpp:50-67                 */
+/* a11: MS-SSIM, libs/pmbb-ivqm/src/xSSIM.cpp:115-141, scales :405-417, exponents                  */
+/* libs/pmbb-ivqm/src/xStructSimConsts.h:42-49, downsampling xPixelOpsSTD.cpp:50-67; every scale   */
+/* uses the same window options, the sub-pictures extended by the same border mode (:127)          */
 /* ----------------------------------------------------------------------------------------------- */
 static const double qo_ms_exponents[5][5] = {
   { 1.0000, 0.0000, 0.0000, 0.0000, 0.0000 },
@@ -312,25 +449,27 @@ static void qo_downsample(uint16_t* dst, const uint16_t* src, int32_t W, int32_t
   }
 }
 
-int qo_msssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, double out[3])
+int qo_msssim_pic_cfg(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, const qo_ssim_cfg* cfg,
+                      double out[3])
 {
   const int32_t ns = qo_num_scales(W, H);
   if(ns < 1) { return -1; }
   double sub[5][3];
-  qo_ssim_pic(tst, ref, W, H, bitdepth, ns == 1, NULL, sub[0]);
+  int rc = qo_ssim_pic_cfg(tst, ref, W, H, bitdepth, ns == 1, NULL, cfg, sub[0]);
   uint16_t* bufT = NULL; uint16_t* bufR = NULL;
   const uint16_t* curT = tst; const uint16_t* curR = ref;
   int32_t w = W, h = H;
-  for(int32_t i = 1; i < ns; i++)
+  for(int32_t i = 1; i < ns && rc == 0; i++)
   {
     const int32_t nw = w >> 1, nh = h >> 1;
     uint16_t* nT = (uint16_t*)malloc((size_t)nw * nh * 3 * sizeof(uint16_t));
     uint16_t* nR = (uint16_t*)malloc((size_t)nw * nh * 3 * sizeof(uint16_t));
     qo_downsample(nT, curT, w, h); qo_downsample(nR, curR, w, h);
     free(bufT); free(bufR); bufT = nT; bufR = nR; curT = nT; curR = nR; w = nw; h = nh;
-    qo_ssim_pic(curT, curR, w, h, bitdepth, i == ns - 1, NULL, sub[i]);
+    rc = qo_ssim_pic_cfg(curT, curR, w, h, bitdepth, i == ns - 1, NULL, cfg, sub[i]);
   }
   free(bufT); free(bufR);
+  if(rc) { return -1; }
   for(int32_t c = 0; c < 3; c++)
   {
     double score = 1.0;
@@ -342,6 +481,11 @@ int qo_msssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H
     out[c] = score;
   }
   return 0;
+}
+
+int qo_msssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, double out[3])
+{
+  return qo_msssim_pic_cfg(tst, ref, W, H, bitdepth, &qo_ssim_default, out);
 }
 
 /* ----------------------------------------------------------------------------------------------- */
@@ -709,8 +853,23 @@ int qo_compute_pair_masked(const qo_params* p, const void* const planes0[3], con
 /* ----------------------------------------------------------------------------------------------- */
 /* Full frame pipeline, apps/QMIV/src/xAppQMIV.cpp:761-827 and the calcFrame* functions :927-1108   */
 /* ----------------------------------------------------------------------------------------------- */
+static int qo_compute_pair_impl(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,
+                                qo_result* out, uint16_t* scp0, uint16_t* scp1, const qo_ssim_cfg* cfg);
+
 int qo_compute_pair(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,
                     qo_result* out, uint16_t* scp0, uint16_t* scp1)
+{
+  return qo_compute_pair_impl(p, planes0, planes1, mask, out, scp0, scp1, &qo_ssim_default);
+}
+
+int qo_compute_pair_ssim(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,
+                         const qo_ssim_cfg* cfg, qo_result* out)
+{
+  return qo_compute_pair_impl(p, planes0, planes1, mask, out, NULL, NULL, cfg);
+}
+
+static int qo_compute_pair_impl(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,
+                                qo_result* out, uint16_t* scp0, uint16_t* scp1, const qo_ssim_cfg* cfg)
 {
   const int32_t W = p->width, H = p->height, BD = p->bitdepth;
   const size_t  n = (size_t)W * H * 3;
@@ -804,30 +963,30 @@ int qo_compute_pair(const qo_params* p, const void* const planes0[3], const void
     out->ivpsnr = t2r < r2t ? t2r : r2t; /* std::min */
   }
 
-  if(mask & QO_SSIM) /* xSSIM.h:83 -> xSSIM.cpp:315-352, no ERP weighting */
+  int rc = 0;
+  if(mask & QO_SSIM) /* xSSIM.h:83 -> xSSIM.cpp:199-234, no ERP weighting */
   {
-    qo_ssim_pic(P0, P1, W, H, BD, 1, NULL, out->ssim);
+    rc |= qo_ssim_pic_cfg(P0, P1, W, H, BD, 1, NULL, cfg, out->ssim);
     out->ssim_pic = QO_PER_PIC(out->ssim);
   }
-  int rc = 0;
   if(mask & QO_MSSSIM)
   {
-    rc |= qo_msssim_pic(P0, P1, W, H, BD, out->msssim);
+    rc |= qo_msssim_pic_cfg(P0, P1, W, H, BD, cfg, out->msssim);
     out->msssim_pic = QO_PER_PIC(out->msssim);
   }
   if(mask & QO_IVSSIM) /* xIVSSIM.cpp:31-61 */
   {
     double t2r[3], r2t[3];
-    qo_ssim_pic(P0, S1, W, H, BD, 1, ws, t2r);
-    qo_ssim_pic(P1, S0, W, H, BD, 1, ws, r2t);
+    rc |= qo_ssim_pic_cfg(P0, S1, W, H, BD, 1, ws, cfg, t2r);
+    rc |= qo_ssim_pic_cfg(P1, S0, W, H, BD, 1, ws, cfg, r2t);
     out->ivssim_t2r = QO_PER_PIC4(t2r); out->ivssim_r2t = QO_PER_PIC4(r2t);
     out->ivssim = out->ivssim_r2t < out->ivssim_t2r ? out->ivssim_r2t : out->ivssim_t2r;
   }
   if(mask & QO_IVMSSSIM) /* xIVSSIM.cpp:62-92, no ERP weighting */
   {
     double t2r[3], r2t[3];
-    rc |= qo_msssim_pic(P0, S1, W, H, BD, t2r);
-    rc |= qo_msssim_pic(P1, S0, W, H, BD, r2t);
+    rc |= qo_msssim_pic_cfg(P0, S1, W, H, BD, cfg, t2r);
+    rc |= qo_msssim_pic_cfg(P1, S0, W, H, BD, cfg, r2t);
     out->ivmsssim_t2r = QO_PER_PIC4(t2r); out->ivmsssim_r2t = QO_PER_PIC4(r2t);
     out->ivmsssim = out->ivmsssim_r2t < out->ivmsssim_t2r ? out->ivmsssim_r2t : out->ivmsssim_t2r;
   }

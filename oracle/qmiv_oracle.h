@@ -76,6 +76,33 @@ void qo_ssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H,
 /* Per-channel MS-SSIM of one 4:4:4 picture pair. Returns 0, or -1 when the picture is too small. */
 int qo_msssim_pic(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, double out[3]);
 
+/* Structural similarity options of the app (-ssm, -ssb, -ssw, -sss; apps/QMIV/src/xAppQMIV.cpp:99-104):
+   mode as xSSIM::eMode (libs/pmbb-ivqm/src/xSSIM.h:23-31), border as eMrgExt
+   (libs/pmbb-core/src/xCommonDefCORE.h:322-331). The app's default is BlockAveraged, None, 8, 4. */
+enum
+{
+  QO_SSM_REGULAR_GAUSSIAN_FLT = 0, QO_SSM_REGULAR_GAUSSIAN_INT = 1, QO_SSM_REGULAR_AVERAGED = 2,
+  QO_SSM_BLOCK_GAUSSIAN_INT = 3, QO_SSM_BLOCK_AVERAGED = 4
+};
+enum { QO_BRD_NONE = 0, QO_BRD_NEAREST = 1, QO_BRD_REFLECT = 2, QO_BRD_MIRROR = 3, QO_BRD_CONSTANT = 4, QO_BRD_ZERO = 5 };
+typedef struct qo_ssim_cfg
+{
+  int32_t mode, border, window, stride;
+} qo_ssim_cfg;
+
+/* Per-channel SSIM of one 4:4:4 picture pair under any structural similarity option. ws_weights (ERP,
+   may be NULL) weight the window rows as xIVSSIM does. Returns 0, or -1 for an option the reference
+   cannot evaluate (see qo_ssim_cfg_check). */
+int qo_ssim_pic_cfg(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, int32_t calc_l,
+                    const double* ws_weights, const qo_ssim_cfg* cfg, double out[3]);
+int qo_msssim_pic_cfg(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_t H, int32_t bitdepth, const qo_ssim_cfg* cfg,
+                      double out[3]);
+/* 0 when the option set is one this restatement evaluates for a W x H picture, else -1. */
+int qo_ssim_cfg_check(const qo_ssim_cfg* cfg, int32_t W, int32_t H);
+/* The frame pipeline with the given structural similarity options. */
+int qo_compute_pair_ssim(const qo_params* p, const void* const planes0[3], const void* const planes1[3], uint32_t mask,
+                         const qo_ssim_cfg* cfg, qo_result* out);
+
 /* Number of MS-SSIM scales (xSSIM::xCalcNumScales). */
 int32_t qo_num_scales(int32_t W, int32_t H);
 

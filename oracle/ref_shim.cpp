@@ -63,6 +63,14 @@ struct ref_result
 
 enum { REF_PSNR = 1, REF_WSPSNR = 2, REF_IVPSNR = 4, REF_SSIM = 8, REF_MSSSIM = 16, REF_IVSSIM = 32, REF_IVMSSSIM = 64 };
 
+/* Structural similarity options of the app (-ssm, -ssb, -ssw, -sss; apps/QMIV/src/xAppQMIV.cpp:99-104,
+   325-332): mode as xSSIM::eMode (0 RegularGaussianFlt, 1 RegularGaussianInt, 2 RegularAveraged,
+   3 BlockGaussianInt, 4 BlockAveraged), border as eMrgExt (0 None .. 5 Zero). */
+struct ref_ssim_cfg
+{
+  int32_t mode, border, window, stride;
+};
+
 } // extern "C"
 
 namespace {
@@ -180,7 +188,9 @@ void convertColour(xPicP* Pic, int32 CsIn, int32 CsMetric)
 }
 
 int computePairImpl(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask, ref_result* Out,
-                    uint16_t* Scp0, uint16_t* Scp1, int32 CsIn, int32 CsMetric);
+                    uint16_t* Scp0, uint16_t* Scp1, int32 CsIn, int32 CsMetric, const ref_ssim_cfg* Ssim);
+
+const ref_ssim_cfg c_DefaultSsim = { (int32_t)xSSIM::eMode::BlockAveraged, (int32_t)eMrgExt::None, 8, 4 };
 
 } // namespace
 
@@ -190,7 +200,7 @@ extern "C" {
    each, planar) receive the shift-compensated pictures m_PicSCP[0] / m_PicSCP[1]. Returns 0 on success. */
 int ref_compute_pair(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask, ref_result* Out, uint16_t* Scp0, uint16_t* Scp1)
 {
-  return computePairImpl(P, Planes0, Planes1, Mask, Out, Scp0, Scp1, REF_CS_YCBCR, REF_CS_YCBCR);
+  return computePairImpl(P, Planes0, Planes1, Mask, Out, Scp0, Scp1, REF_CS_YCBCR, REF_CS_YCBCR, &c_DefaultSsim);
 }
 
 /* The same with the app's colour-space options: input colour space CsIn (-csi) and metric colour
@@ -198,7 +208,16 @@ int ref_compute_pair(const ref_params* P, const void* const Planes0[3], const vo
 int ref_compute_pair_cs(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask, int32_t CsIn,
                         int32_t CsMetric, ref_result* Out)
 {
-  return computePairImpl(P, Planes0, Planes1, Mask, Out, nullptr, nullptr, CsIn, CsMetric);
+  return computePairImpl(P, Planes0, Planes1, Mask, Out, nullptr, nullptr, CsIn, CsMetric, &c_DefaultSsim);
+}
+
+/* The same with the app's structural similarity options. With a border mode the pictures get a margin
+   of at least 6 so that every 11x11 window read lands in the extended margin (the app's own margin is
+   roundUp(R, 2), xAppQMIV.cpp:353, narrower than the 5-sample window reach for R <= 4). */
+int ref_compute_pair_ssim(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask,
+                          const ref_ssim_cfg* Ssim, ref_result* Out)
+{
+  return computePairImpl(P, Planes0, Planes1, Mask, Out, nullptr, nullptr, REF_CS_YCBCR, REF_CS_YCBCR, Ssim);
 }
 
 } // extern "C"
@@ -206,11 +225,12 @@ int ref_compute_pair_cs(const ref_params* P, const void* const Planes0[3], const
 namespace {
 
 int computePairImpl(const ref_params* P, const void* const Planes0[3], const void* const Planes1[3], uint32_t Mask, ref_result* Out,
-                    uint16_t* Scp0, uint16_t* Scp1, int32 CsIn, int32 CsMetric)
+                    uint16_t* Scp0, uint16_t* Scp1, int32 CsIn, int32 CsMetric, const ref_ssim_cfg* Ssim)
 {
   const int32   W = P->width, H = P->height, BD = P->bitdepth;
   const int32V2 Size = { W, H };
-  const int32   Margin = xRoundUpToNearestMultiple(P->search_range, 2);
+  const eMrgExt Border = (eMrgExt)Ssim->border;
+  const int32   Margin = xRoundUpToNearestMultiple(Border != eMrgExt::None ? xMax(P->search_range, 5) : P->search_range, 2);
   const int32V4 Cws = { P->cws[0], P->cws[1], P->cws[2], P->cws[3] };
   const int32V4 Cwa = { P->cwa[0], P->cwa[1], P->cwa[2], P->cwa[3] };
   const flt32V4 Unc = { P->unc[0], P->unc[1], P->unc[2], P->unc[3] };
@@ -251,7 +271,7 @@ int computePairImpl(const ref_params* P, const void* const Planes0[3], const voi
     ProcSSIM.create(Size, BD, Margin, CalcMSs);
     ProcSSIM.setSearchRange(P->search_range); ProcSSIM.setCmpWeightsSearch(Cws); ProcSSIM.setCmpWeightsAverage(Cwa);
     ProcSSIM.setUnntcbCoef(Unc);
-    ProcSSIM.setStructSimParams(xSSIM::eMode::BlockAveraged, eMrgExt::None, 8, 4);
+    ProcSSIM.setStructSimParams((xSSIM::eMode)Ssim->mode, Border, Ssim->window, Ssim->stride);
     ProcSSIM.bindThrdPoolIntf(&TP.TPI); ProcSSIM.initRowBuffers(H);
     if(P->erp) { ProcSSIM.initWS(true, W, H, BD, P->lon_range, P->lat_range); }
   }
@@ -294,6 +314,11 @@ int computePairImpl(const ref_params* P, const void* const Planes0[3], const voi
   {
     Out->ivpsnr = ProcPSNR.calcPicIVPSNR(&PicI[0], &PicI[1], GCD);
     Out->ivpsnr_r2t = LastR2T; Out->ivpsnr_t2r = LastT2R;
+  }
+  if(Border != eMrgExt::None)  // xAppQMIV::addStructSimMargs (xAppQMIV.cpp:798, 918-926)
+  {
+    for(int32 i = 0; i < 2; i++) { PicP[i].extend(Border); }
+    if(CalcSCP) { for(int32 i = 0; i < 2; i++) { SCP[i].extend(Border); } }
   }
   if(Mask & REF_SSIM)
   {

@@ -42,6 +42,12 @@ def golden_colour():
 
 
 @pytest.fixture(scope="session")
+def golden_ssim_modes():
+    with open(os.path.join(GOLDEN, "golden_ssim_modes.json")) as f:
+        return json.load(f)["ssim_modes"]
+
+
+@pytest.fixture(scope="session")
 def cps_arrays():
     import numpy as np
     return dict(np.load(os.path.join(GOLDEN, "cps_fixtures.npz")))

@@ -11,6 +11,12 @@ a store mask with a 64-bit shift by 64), which the portable and AVX2 builds do n
     python tests/golden/make_golden.py            # golden.json
     python tests/golden/make_golden.py masked     # golden_masked.json (mask mode)
     python tests/golden/make_golden.py colour     # golden_colour.json (colour-space conversion)
+    python tests/golden/make_golden.py ssim_modes # golden_ssim_modes.json (structural similarity options)
+
+The structural similarity option fixtures come from the x86-64-v2 build. GCC contracts a*b+c into
+fused multiply-adds by default in C++ (-ffp-contract=fast) wherever the target has FMA (x86-64-v3 and
+up), which moves the last bits of the non-power-of-two-scaled window formulas; the v2 build evaluates
+the arithmetic as written. The v3 values are stored beside them to bound that difference.
 """
 from __future__ import annotations
 
@@ -250,6 +256,73 @@ def main_colour():
     print("wrote", os.path.join(HERE, "golden_colour.json"))
 
 
+# structural similarity options: (width, height, bitdepth, chroma_format, R, erp, seed, -ssm, -ssb, -ssw, -sss)
+SSM_FLT, SSM_INT, SSM_AVG, SSM_BGI, SSM_BAVG = 0, 1, 2, 3, 4
+SSIM_MODE_CASES = [
+    (64, 48, 10, 420, 2, True, 61, SSM_FLT, 0, 11, 1),      # the original paper's setting
+    (96, 64, 8, 420, 2, False, 62, SSM_FLT, 0, 11, 4),
+    (72, 40, 10, 444, 3, True, 63, SSM_FLT, 1, 11, 1),      # Nearest
+    (66, 34, 8, 422, 1, False, 64, SSM_FLT, 2, 11, 3),      # Reflect
+    (64, 64, 12, 420, 2, True, 65, SSM_FLT, 3, 11, 2),      # Mirror
+    (48, 40, 10, 444, 2, False, 66, SSM_FLT, 4, 11, 5),     # Constant (65535)
+    (64, 48, 8, 420, 5, True, 67, SSM_FLT, 5, 11, 11),      # Zero
+    (128, 64, 10, 420, 2, True, 68, SSM_INT, 0, 11, 1),
+    (80, 48, 14, 444, 2, False, 69, SSM_INT, 1, 11, 4),
+    (64, 64, 10, 420, 4, True, 70, SSM_INT, 4, 11, 3),
+    (96, 64, 10, 420, 2, True, 71, SSM_AVG, 0, 11, 1),
+    (64, 48, 8, 444, 2, False, 72, SSM_AVG, 3, 11, 2),
+    (130, 66, 10, 422, 2, True, 73, SSM_AVG, 5, 11, 4),
+    (64, 64, 10, 420, 2, True, 74, SSM_BGI, 0, 8, 4),
+    (96, 64, 8, 420, 3, False, 75, SSM_BGI, 0, 8, 8),
+    (128, 96, 10, 444, 2, True, 76, SSM_BGI, 0, 16, 4),
+    (64, 48, 12, 420, 2, False, 77, SSM_BGI, 0, 16, 1),
+    (64, 64, 10, 420, 2, True, 78, SSM_BAVG, 0, 8, 1),
+    (96, 64, 8, 420, 2, False, 79, SSM_BAVG, 0, 8, 8),
+    (72, 56, 10, 444, 2, True, 80, SSM_BAVG, 0, 8, 3),
+    (128, 96, 10, 420, 2, True, 81, SSM_BAVG, 0, 16, 4),
+    (96, 64, 14, 444, 2, False, 82, SSM_BAVG, 0, 16, 16),
+    (160, 96, 10, 420, 2, True, 83, SSM_BAVG, 0, 32, 4),
+    (130, 70, 8, 422, 2, False, 84, SSM_BAVG, 0, 32, 7),
+    (256, 128, 10, 420, 2, True, 85, SSM_FLT, 0, 11, 1),
+]
+SSIM_KEYS = ("ssim", "ssim_pic", "msssim", "msssim_pic", "ivssim", "ivssim_r2t", "ivssim_t2r", "ivmsssim", "ivmsssim_r2t",
+             "ivmsssim_t2r")
+
+
+def make_ssim_modes(ref, ref_fma):
+    """Every metric of the pipeline under the app's -ssm / -ssb / -ssw / -sss options, run by the
+    compiled reference (xSSIM::setStructSimParams, xAppQMIV.cpp:722; border extension of the pictures
+    and the SCPs, :798 and :918-926). Frames come from detgen."""
+    out = []
+    for (W, H, bd, cf, R, erp, seed, mode, border, window, stride) in SSIM_MODE_CASES:
+        p = oracle.make_params(W, H, bd, cf, search_range=R, erp=erp, num_threads=8)
+        f0, f1 = det_pair(W, H, bd, seed, cf)
+        mask = oracle.ALL
+        if oracle.Oracle().num_scales(W, H) < 1:
+            mask &= ~(oracle.MSSSIM | oracle.IVMSSSIM)
+        r = ref.compute_pair_ssim(p, f0, f1, mode, border, window, stride, mask)
+        r3 = ref_fma.compute_pair_ssim(p, f0, f1, mode, border, window, stride, mask)
+        enc = lambda d: {k: ([fhex(x) if isinstance(x, float) else int(x) for x in v] if isinstance(v, list)
+                             else (fhex(v) if isinstance(v, float) else int(v))) for k, v in d.items()}
+        out.append(dict(width=W, height=H, bitdepth=bd, chroma_format=cf, search_range=R, erp=erp, seed=seed,
+                        ssim_mode=mode, ssim_border=border, ssim_window=window, ssim_stride=stride, mask=mask,
+                        expected=enc(r), expected_fma_build={k: v for k, v in enc(r3).items() if k in SSIM_KEYS}))
+        dev = max(abs(a - b) for k in SSIM_KEYS for a, b in zip(r[k] if isinstance(r[k], list) else [r[k]],
+                                                                 r3[k] if isinstance(r3[k], list) else [r3[k]]))
+        print("ssim_modes", W, H, bd, cf, R, erp, mode, border, window, stride, r["ssim_pic"], r["ivssim"], "v3 dev", dev)
+    return out
+
+
+def main_ssim_modes():
+    ref = oracle.Reference("x86-64-v2")
+    ref_fma = oracle.Reference("x86-64-v3")
+    data = dict(generator="tests/golden/make_golden.py ssim_modes", reference_build="x86-64-v2",
+                fma_build="x86-64-v3", ssim_modes=make_ssim_modes(ref, ref_fma))
+    with open(os.path.join(HERE, "golden_ssim_modes.json"), "w") as f:
+        json.dump(data, f, separators=(",", ":"))
+    print("wrote", os.path.join(HERE, "golden_ssim_modes.json"))
+
+
 def main():
     ref = oracle.Reference(ARCH)
     data = dict(generator="tests/golden/make_golden.py", reference_build=ARCH,
@@ -264,5 +337,7 @@ if __name__ == "__main__":
         main_masked()
     elif sys.argv[1:] == ["colour"]:
         main_colour()
+    elif sys.argv[1:] == ["ssim_modes"]:
+        main_ssim_modes()
     else:
         main()

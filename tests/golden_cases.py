@@ -60,6 +60,31 @@ def compare_result(got, expected, mask, ignore=()):
     return bad
 
 
+SSIM_KEYS = ["ssim", "ssim_pic", "msssim", "msssim_pic", "ivssim", "ivssim_r2t", "ivssim_t2r", "ivmsssim", "ivmsssim_r2t",
+             "ivmsssim_t2r"]
+
+
+def ssim_mode_ids():
+    import json, os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "golden_ssim_modes.json")) as f:
+        g = json.load(f)["ssim_modes"]
+    names = {0: "RglrFlt", 1: "RglrInt", 2: "RglrAvg", 3: "BlckInt", 4: "BlckAvg"}
+    return [f"{names[c['ssim_mode']]}_b{c['ssim_border']}_w{c['ssim_window']}_s{c['ssim_stride']}_{c['width']}x{c['height']}_"
+            f"{c['bitdepth']}b_{c['chroma_format']}{'_erp' if c['erp'] else ''}" for c in g]
+
+
+def max_ssim_deviation(got, expected, mask):
+    """Largest absolute difference over the SSIM-family values of a result dict and a golden block."""
+    dev = 0.0
+    for k in SSIM_KEYS:
+        if not metric_enabled(k, mask) or k not in expected:
+            continue
+        e, g = unhex(expected[k]), got[k]
+        es, gs = (e[:3], g[:3]) if isinstance(e, list) else ([e], [g])
+        dev = max(dev, max(abs(float(a) - float(b)) for a, b in zip(gs, es)))
+    return dev
+
+
 def sha256(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 

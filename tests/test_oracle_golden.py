@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import oracle
-from golden_cases import case_frames, case_params, compare_result, sha256, unhex
+from golden_cases import ssim_mode_ids, max_ssim_deviation, case_frames, case_params, compare_result, sha256, unhex
 
 
 def _pipeline_ids(golden_json=None):
@@ -175,3 +175,34 @@ def test_colour_refused_combinations(oracle_lib):
     for cs_in, cs_metric in [(oracle.CS_BT601, oracle.CS_BT709), (oracle.CS_YCBCR, oracle.CS_RGB), (oracle.CS_RGB, oracle.CS_YCBCR)]:
         with pytest.raises(RuntimeError):
             oracle_lib.compute_pair_cs(p, f0, f1, cs_in, cs_metric)
+
+
+@pytest.mark.parametrize("idx", range(len(ssim_mode_ids())), ids=ssim_mode_ids())
+def test_ssim_modes_match_reference(idx, golden_ssim_modes, oracle_lib):
+    """Every metric under the app's structural similarity options (regular 11x11 Gaussian float /
+    Gaussian integer / averaged windows with the five border extensions, block Gaussian integer 8/16 and
+    averaged 8/16/32 windows, strides 1..window) of the restatement against the compiled reference's
+    portable-arithmetic build, bit for bit, and within 1e-14 of its FMA-contracted build."""
+    import oracle
+    case = golden_ssim_modes[idx]
+    f0, f1 = case_frames(case)
+    p = oracle.make_params(case["width"], case["height"], case["bitdepth"], case["chroma_format"],
+                           search_range=case["search_range"], erp=case["erp"])
+    got = oracle_lib.compute_pair_ssim(p, f0, f1, case["ssim_mode"], case["ssim_border"], case["ssim_window"],
+                                       case["ssim_stride"], case["mask"])
+    assert compare_result(got, case["expected"], case["mask"]) == []
+    assert max_ssim_deviation(got, case["expected_fma_build"], case["mask"]) < 1e-14
+
+
+def test_ssim_mode_refusals(oracle_lib):
+    """Option sets the reference cannot evaluate: regular windows other than 11, Gaussian 32x32 blocks
+    (CalcBlckInt returns NaN), stride 0 or above the window, the averaged 11x11 window over the constant
+    65535 margin (32-bit overflow), pictures smaller than the window."""
+    import oracle
+    from detgen import det_pair
+    f0, f1 = det_pair(48, 48, 8, 1, 444)
+    p = oracle.make_params(48, 48, 8, 444)
+    for cfg in [(0, 0, 8, 1), (3, 0, 32, 4), (4, 0, 8, 0), (4, 0, 8, 9), (2, 4, 11, 1), (4, 0, 64, 4), (7, 0, 8, 4),
+                (0, 6, 11, 1)]:
+        with pytest.raises(RuntimeError):
+            oracle_lib.compute_pair_ssim(p, f0, f1, *cfg, mask=oracle.SSIM)
