@@ -81,6 +81,22 @@ enum { QMIV_MEM_HOST = 0, QMIV_MEM_DEVICE = 1 };
 /* invalid-pixel action (apps/QMIV/src/xAppQMIV.cpp:834-852, README "InvalidPelActn") */
 enum { QMIV_PEL_SKIP = 0, QMIV_PEL_WARN = 1, QMIV_PEL_STOP = 2, QMIV_PEL_CNCL = 3 };
 
+/* Structural similarity window modes of the app's StructSimMode option, same codes as xSSIM::eMode
+   (libs/pmbb-ivqm/src/xSSIM.h:23-31): regular 11x11 windows centred on every pixel (Gaussian float,
+   Gaussian integer or averaged weights), block windows of 8, 16 or 32 samples anchored at their
+   top-left sample (Gaussian integer 8/16 or averaged). */
+enum
+{
+  QMIV_SSM_REGULAR_GAUSSIAN_FLT = 0, QMIV_SSM_REGULAR_GAUSSIAN_INT = 1, QMIV_SSM_REGULAR_AVERAGED = 2,
+  QMIV_SSM_BLOCK_GAUSSIAN_INT = 3, QMIV_SSM_BLOCK_AVERAGED = 4
+};
+
+/* Border extension of the regular windows (StructSimBrdExt), same codes as eMrgExt
+   (libs/pmbb-core/src/xCommonDefCORE.h:322-331). QMIV_BRD_NONE evaluates only the windows inside the
+   picture; the others evaluate a window at every pixel and extend the picture like xMarginOps
+   (Constant = 65535). */
+enum { QMIV_BRD_NONE = 0, QMIV_BRD_NEAREST = 1, QMIV_BRD_REFLECT = 2, QMIV_BRD_MIRROR = 3, QMIV_BRD_CONSTANT = 4, QMIV_BRD_ZERO = 5 };
+
 /* Colour spaces of the app's ColorSpaceInput / ColorSpaceMetric options, same codes as its eClrSpcApp
    (apps/QMIV/src/xUtilsQMIV.h:12-27). QMIV_CS_YCBCR is the generic (unspecified) YCbCr. */
 enum
@@ -96,7 +112,9 @@ typedef struct qmiv_server_s* qmiv_server;
 
 /* Processor parameters. qmiv_params_default() gives the reference defaults:
    R=2, weights 4:1:1:0 (xCorrespPixelShiftPrms.h:22-24), unnoticeable coef 0.01 (xGlobClrDiff.h:20),
-   BlockAveraged SSIM with 8x8 windows at stride 4 (xSSIM.h:35-37), no ERP, STOP on invalid pixels. */
+   BlockAveraged SSIM with 8x8 windows at stride 4 and no border extension (xSSIM.h:35-37), no ERP,
+   STOP on invalid pixels. The SSIM options follow xSSIM::setStructSimParams (xSSIM.cpp:86-113) with
+   the app's checks (xAppQMIV.cpp:325-332); the batched and serving forms run the default options only. */
 typedef struct qmiv_params
 {
   int32_t search_range;        /* 1..5 */
@@ -106,9 +124,11 @@ typedef struct qmiv_params
   int32_t erp;                 /* equirectangular (WS) weighting on/off */
   int32_t lon_range_deg;       /* 360 */
   int32_t lat_range_deg;       /* 180 */
-  int32_t ssim_window;         /* 8 (BlockAveraged) */
-  int32_t ssim_stride;         /* 4 */
+  int32_t ssim_window;         /* 8; 11 for the regular modes; 8, 16 or 32 for the block modes */
+  int32_t ssim_stride;         /* 4; 1..ssim_window */
   int32_t invalid_pel_action;  /* QMIV_PEL_* */
+  int32_t ssim_mode;           /* QMIV_SSM_*, default QMIV_SSM_BLOCK_AVERAGED */
+  int32_t ssim_border;         /* QMIV_BRD_*, regular modes only, default QMIV_BRD_NONE */
 } qmiv_params;
 
 /* One frame: planar Y, Cb, Cr. Samples are 1 byte for bitdepth <= 8, else 2 bytes little endian.

@@ -25,7 +25,9 @@ import numpy as np
 from . import _lib
 from ._lib import (ALL, IVMSSSIM, IVPSNR, IVSSIM, METRIC_BITS, MSSSIM, PSNR, SSIM, WSPSNR, PEL_CNCL, PEL_SKIP,
                    CS_RGB, CS_BGR, CS_GBR, CS_YCBCR, CS_BT601, CS_SMPTE170M, CS_BT709, CS_SMPTE240M, CS_BT2020,
-                   PEL_STOP, PEL_WARN, QmivError, check)
+                   PEL_STOP, PEL_WARN, QmivError, check, SSM_REGULAR_GAUSSIAN_FLT, SSM_REGULAR_GAUSSIAN_INT,
+                   SSM_REGULAR_AVERAGED, SSM_BLOCK_GAUSSIAN_INT, SSM_BLOCK_AVERAGED, BRD_NONE, BRD_NEAREST, BRD_REFLECT,
+                   BRD_MIRROR, BRD_CONSTANT, BRD_ZERO)
 
 __all__ = ["Context", "Calc", "Batch", "make_params", "metric_mask", "QmivError", "library", "frame_from_raw",
            "raw_frame_bytes",
@@ -54,7 +56,10 @@ def metric_mask(metrics) -> int:
 
 
 def make_params(search_range=2, cws=(4, 1, 1, 0), cwa=(4, 1, 1, 0), unc=(0.01, 0.01, 0.01, 0.0), erp=False,
-                lon_range=360, lat_range=180, invalid_pel_action=PEL_STOP) -> _lib.QmivParams:
+                lon_range=360, lat_range=180, invalid_pel_action=PEL_STOP, ssim_mode=SSM_BLOCK_AVERAGED,
+                ssim_border=BRD_NONE, ssim_window=None, ssim_stride=4) -> _lib.QmivParams:
+    """Processor parameters; the SSIM options are the app's StructSimMode / StructSimBrdExt /
+    StructSimWindow / StructSimStride (ssim_window defaults to 11 for the regular modes, else 8)."""
     p = _lib.QmivParams()
     library().qmiv_params_default(ctypes.byref(p))
     p.search_range = search_range
@@ -65,6 +70,10 @@ def make_params(search_range=2, cws=(4, 1, 1, 0), cwa=(4, 1, 1, 0), unc=(0.01, 0
     p.lon_range_deg = lon_range
     p.lat_range_deg = lat_range
     p.invalid_pel_action = invalid_pel_action
+    p.ssim_mode = ssim_mode
+    p.ssim_border = ssim_border
+    p.ssim_window = ssim_window if ssim_window is not None else (11 if ssim_mode <= SSM_REGULAR_AVERAGED else 8)
+    p.ssim_stride = ssim_stride
     return p
 
 

@@ -26,6 +26,9 @@ PEL_SKIP, PEL_WARN, PEL_STOP, PEL_CNCL = 0, 1, 2, 3
 # colour spaces (ColorSpaceInput / ColorSpaceMetric), apps/QMIV/src/xUtilsQMIV.h:12-27
 CS_RGB, CS_BGR, CS_GBR, CS_YCBCR = 2, 3, 4, 16
 CS_BT601, CS_SMPTE170M, CS_BT709, CS_SMPTE240M, CS_BT2020 = 17, 18, 19, 20, 21
+# structural similarity modes (StructSimMode, xSSIM::eMode) and border extensions (StructSimBrdExt, eMrgExt)
+SSM_REGULAR_GAUSSIAN_FLT, SSM_REGULAR_GAUSSIAN_INT, SSM_REGULAR_AVERAGED, SSM_BLOCK_GAUSSIAN_INT, SSM_BLOCK_AVERAGED = 0, 1, 2, 3, 4
+BRD_NONE, BRD_NEAREST, BRD_REFLECT, BRD_MIRROR, BRD_CONSTANT, BRD_ZERO = 0, 1, 2, 3, 4, 5
 
 
 class QmivParams(ctypes.Structure):
@@ -33,7 +36,7 @@ class QmivParams(ctypes.Structure):
         ("search_range", ctypes.c_int32), ("cws", ctypes.c_int32 * 4), ("cwa", ctypes.c_int32 * 4),
         ("unc", ctypes.c_float * 4), ("erp", ctypes.c_int32), ("lon_range_deg", ctypes.c_int32),
         ("lat_range_deg", ctypes.c_int32), ("ssim_window", ctypes.c_int32), ("ssim_stride", ctypes.c_int32),
-        ("invalid_pel_action", ctypes.c_int32),
+        ("invalid_pel_action", ctypes.c_int32), ("ssim_mode", ctypes.c_int32), ("ssim_border", ctypes.c_int32),
     ]
 
 
@@ -124,6 +127,7 @@ SIGNATURES = {
                                          ctypes.c_int32, _PP]),
     "qmiv_probe_int32_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "qmiv_probe_fp32_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
+    "qmiv_probe_fp64_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "qmiv_batch_destroy": (ctypes.c_int, [_P]),
     "qmiv_batch_stream": (ctypes.c_int, [_P, _PP]),
     "qmiv_batch_compute": (ctypes.c_int, [_P, ctypes.POINTER(QmivPairDesc), ctypes.c_int32, ctypes.POINTER(QmivResult)]),

@@ -43,9 +43,55 @@ qmiv_status validate_params(const qmiv_params& p)
   if(p.cws[3] != 0) { return fail(QMIV_ERR_UNSUPPORTED, "the fourth search weight must be 0"); }
   for(int c = 0; c < 3; c++) { if(p.cws[c] < 0 || p.cwa[c] < 0) { return fail(QMIV_ERR_INVALID_ARG, "weights must be >= 0"); } }
   if(p.cwa[0] + p.cwa[1] + p.cwa[2] + p.cwa[3] <= 0) { return fail(QMIV_ERR_INVALID_ARG, "averaging weights sum to 0"); }
-  if(p.ssim_window != 8 || p.ssim_stride != 4) { return fail(QMIV_ERR_UNSUPPORTED, "only BlockAveraged SSIM with 8x8 windows at stride 4 is implemented"); }
+  // structural similarity options: the app's checks (xAppQMIV.cpp:325-332) and the sets the reference's
+  // windows evaluate (xStructSimSTD.cpp:399-403 returns NaN for Gaussian 32x32 blocks)
+  if(p.ssim_mode < QMIV_SSM_REGULAR_GAUSSIAN_FLT || p.ssim_mode > QMIV_SSM_BLOCK_AVERAGED) { return fail(QMIV_ERR_INVALID_ARG, "unknown SSIM mode"); }
+  if(p.ssim_border < QMIV_BRD_NONE || p.ssim_border > QMIV_BRD_ZERO) { return fail(QMIV_ERR_INVALID_ARG, "unknown SSIM border mode"); }
+  if(ssim_regular(p.ssim_mode) && p.ssim_window != 11) { return fail(QMIV_ERR_INVALID_ARG, "regular SSIM modes use 11x11 windows"); }
+  if(p.ssim_mode == QMIV_SSM_BLOCK_AVERAGED && p.ssim_window != 8 && p.ssim_window != 16 && p.ssim_window != 32)
+  {
+    return fail(QMIV_ERR_UNSUPPORTED, "BlockAveraged SSIM windows are 8, 16 or 32");
+  }
+  if(p.ssim_mode == QMIV_SSM_BLOCK_GAUSSIAN_INT && p.ssim_window != 8 && p.ssim_window != 16)
+  {
+    return fail(QMIV_ERR_UNSUPPORTED, "BlockGaussianInt SSIM windows are 8 or 16");
+  }
+  if(p.ssim_stride < 1 || p.ssim_stride > ssim_window_size(p)) { return fail(QMIV_ERR_INVALID_ARG, "SSIM stride must be in 1..window"); }
+  // the averaged 11x11 window squares samples in 32-bit lanes (xStructSimSTD.cpp:167-169; signed 16-bit
+  // products in its AVX form), which the constant margin of 65535 overflows
+  if(p.ssim_mode == QMIV_SSM_REGULAR_AVERAGED && p.ssim_border == QMIV_BRD_CONSTANT)
+  {
+    return fail(QMIV_ERR_UNSUPPORTED, "RegularAveraged SSIM with the Constant border overflows in the reference");
+  }
   if(p.erp && (p.lat_range_deg <= 0 || p.lat_range_deg > 180)) { return fail(QMIV_ERR_INVALID_ARG, "lat range must be in 1..180"); }
   if(p.invalid_pel_action < QMIV_PEL_SKIP || p.invalid_pel_action > QMIV_PEL_CNCL) { return fail(QMIV_ERR_INVALID_ARG, "bad invalid pixel action"); }
+  return QMIV_OK;
+}
+
+void ssim_line(const qmiv_params& p, int32_t len, int32_t& first_sample, int32_t& count)
+{
+  const int32_t S = p.ssim_stride, N = ssim_window_size(p);
+  if(ssim_regular(p.ssim_mode))
+  {
+    const bool margin = p.ssim_border != QMIV_BRD_NONE;
+    const int32_t beg = margin ? 0 : 5, end = margin ? len : len - 5;   // c_FilterRange = 5
+    count = end > beg ? (end - beg + S - 1) / S : 0;
+    first_sample = beg - 5;
+  }
+  else
+  {
+    count = len >= N ? (len - N) / S + 1 : 0;
+    first_sample = 0;
+  }
+}
+
+qmiv_status check_batched_ssim(const qmiv_params& p, uint32_t mask)
+{
+  if((mask & kSsimFamily) && !ssim_is_default(p))
+  {
+    return fail(QMIV_ERR_UNSUPPORTED, "the batched and serving forms compute SSIM with BlockAveraged 8x8 windows at stride 4 only; "
+                                      "other structural similarity options run through qmiv_calc");
+  }
   return QMIV_OK;
 }
 
@@ -105,6 +151,15 @@ qmiv_status PairPipeline::configure(qmiv_ctx_s* ctx, const Shape& shape, const q
     w >>= 1; h >>= 1;
   }
   nxp_ = (nx_[0] + 31) & ~31;
+  gen_ = !ssim_is_default(prm);
+  for(int s = 0; s < 5; s++)
+  {
+    int32_t f = 0;
+    ssim_line(prm, shape.W >> s, f, gnx_[s]);
+    ssim_line(prm, shape.H >> s, gfirst_, gny_[s]);
+  }
+  // ERP weight of window row j: its centre row (regular) or top row + WndSize / 2 (xIVSSIM.cpp:153)
+  gws_base_ = ssim_regular(prm.ssim_mode) ? gfirst_ + 5 : ssim_window_size(prm) / 2;
   const double maxd = (double)shape.maxv;  // xSSIM.cpp:165-167
   const double k1 = 0.01 * maxd, k2 = 0.03 * maxd;
   C1_ = k1 * k1; C2_ = k2 * k2;
@@ -122,13 +177,13 @@ qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames
   QMIV_TRY(row_sd_.ensure(ctx_, rows_total * sizeof(int64_t)));
   QMIV_TRY(row_ssd_.ensure(ctx_, rows_total * sizeof(uint64_t)));
   QMIV_TRY(out_.ensure(ctx_, sizeof(PairOut)));
-  const bool need_scp = want_scp || (mask & QMIV_IVMSSSIM);
+  const bool need_scp = need_scp_for(mask, want_scp);
   const bool need_search = need_scp || (mask & (QMIV_IVPSNR | QMIV_IVSSIM));
   const bool need_ssim = mask & (QMIV_SSIM | QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM);
   const bool need_ms = mask & (QMIV_MSSSIM | QMIV_IVMSSSIM);
   if(need_search) { QMIV_TRY(cps_rows_.ensure(ctx_, (size_t)2 * S.H * 3 * sizeof(uint32_t))); }
   if(need_scp) { QMIV_TRY(scp_.ensure(ctx_, (size_t)2 * 3 * S.W * S.H * S.esz)); }
-  if(need_ssim)
+  if(need_ssim && !gen_)
   {
     // moment slots: 0, 1 = IV-SSIM directions (written by the search), 2 = SSIM / MS-SSIM pair,
     // 3, 4 = IV-MS-SSIM pairs
@@ -140,12 +195,19 @@ qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames
     QMIV_TRY(ws_.ensure(ctx_, (size_t)S.H * sizeof(double)));
     if(!ws_uploaded_) { QMIV_CUDA(cudaMemcpy(ws_.p, ws_host_.data(), S.H * sizeof(double), cudaMemcpyHostToDevice)); ws_uploaded_ = true; }
   }
-  if(need_ssim)
+  if(need_ssim && !gen_)
   {
     if(nx_[0] < 1 || ny_[0] < 1) { return fail(QMIV_ERR_INVALID_ARG, "picture smaller than one 8x8 SSIM window"); }
     QMIV_TRY(rowsum_.ensure(ctx_, (size_t)kMaxSsimSlots * 3 * ny_[0] * sizeof(double)));
     // window values of up to 9 pool jobs (one flush) at scale 0, reused by later flushes
     QMIV_TRY(win_.ensure(ctx_, (size_t)9 * pool_win_elems(nx_[0], ny_[0]) * sizeof(double)));
+  }
+  if(need_ssim && gen_)
+  {
+    const int32_t N = ssim_window_size(prm_);
+    if(S.W < N || S.H < N || gnx_[0] < 1 || gny_[0] < 1) { return fail(QMIV_ERR_INVALID_ARG, "picture smaller than one SSIM window"); }
+    QMIV_TRY(rowsum_.ensure(ctx_, (size_t)kMaxSsimSlots * 3 * gny_[0] * sizeof(double)));
+    QMIV_TRY(win_.ensure(ctx_, (size_t)kGenMaxJobs * pool_win_elems(gnx_[0], gny_[0]) * sizeof(double)));
   }
   if(need_ms)
   {
@@ -242,7 +304,7 @@ template <typename T>
 qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mask, bool want_scp, bool want_gcd, cudaStream_t s)
 {
   const Shape& S = shape_;
-  const bool need_scp = want_scp || (mask & QMIV_IVMSSSIM);
+  const bool need_scp = need_scp_for(mask, want_scp);
   const bool need_search = need_scp || (mask & (QMIV_IVPSNR | QMIV_IVSSIM));
   const uint32_t clip = prm_.invalid_pel_action == QMIV_PEL_CNCL ? (uint32_t)S.maxv : 0xffffu;
   PairOut* dout = out_.as<PairOut>();
@@ -281,7 +343,7 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
     ca.gcd_src = dout; ca.rows = cps_rows_.as<uint32_t>();
     ca.scp0 = need_scp ? const_cast<void*>(scp(0)) : nullptr;
     ca.scp1 = need_scp ? const_cast<void*>(scp(1)) : nullptr;
-    if(mask & QMIV_IVSSIM) { ca.mom[0] = mom_at(0, 0); ca.mom[1] = mom_at(1, 0); }  // (In0, SCP1), (In1, SCP0)
+    if((mask & QMIV_IVSSIM) && !gen_) { ca.mom[0] = mom_at(0, 0); ca.mom[1] = mom_at(1, 0); }  // (In0, SCP1), (In1, SCP0)
     const int t = prof_begin(s);
     QMIV_CUDA(launch_cps<T>(ca, R_, s));
     prof_end(s, QMIV_STAGE_CPS, t);
@@ -290,100 +352,110 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
   // 3. SSIM family
   FinalizeArgs fa{};
   fa.nslots = kMaxSsimSlots;
-  double* rowsum = rowsum_.as<double>();
-  // window pooling of up to three pictures pairs (x 3 components) from their moments, one launch
-  SsimPoolArgs pool{};
-  auto add_pool = [&](const Moments& m, int scale, int slot, int calc_l, int use_ws) {
-    for(int c = 0; c < 3; c++)
-    {
-      SsimPoolJob& J = pool.job[pool.njobs];
-      J.win = win_.as<double>() + (size_t)pool.njobs * pool_win_elems(nx_[0], ny_[0]);
-      pool.njobs++;
-      J.mom = m.p + (size_t)c * 5 * m.plane(); J.plane = m.plane(); J.pitch = m.pitch;
-      J.C1 = C1_; J.C2 = C2_;
-      J.nx = nx_[scale]; J.ny = ny_[scale]; J.calc_l = calc_l; J.wide = shape_.bitdepth > 12 ? 1 : 0;
-      J.row_sum = rowsum + (size_t)slot * 3 * ny_[0] + (size_t)c * ny_[scale];  // finalize reads [c][ny_scale]
-    }
-    fa.slot[slot].row_sum = rowsum + (size_t)slot * 3 * ny_[0];
-    fa.slot[slot].nx = nx_[scale]; fa.slot[slot].ny = ny_[scale]; fa.slot[slot].use_ws = use_ws;
-  };
-  auto flush_pool = [&]() -> qmiv_status {
-    if(pool.njobs == 0) { return QMIV_OK; }
-    const int t = prof_begin(s);
-    QMIV_CUDA(launch_ssim_pool(pool, s));
-    prof_end(s, QMIV_STAGE_SSIM_ROWS, t);
-    pool.njobs = 0;
-    return QMIV_OK;
-  };
-  auto moments = [&](const Img& a, const Img& b, int W, int H, const Moments& m, const MutImg* down_a,
-                     const MutImg* down_b) -> qmiv_status {
-    SsimMomArgs ma{};
-    ma.a = a; ma.b = b; ma.W = W; ma.H = H; ma.clip = clip; ma.mom = m;
-    if(down_a) { ma.down_a = *down_a; }
-    if(down_b) { ma.down_b = *down_b; }
-    const int t = prof_begin(s);
-    QMIV_CUDA(launch_ssim_moments<T>(ma, s));
-    prof_end(s, QMIV_STAGE_SSIM_WIN, t);
-    return QMIV_OK;
-  };
+  if(gen_ && (mask & kSsimFamily))
+  {
+    const Img scp0 = need_scp ? img444(scp(0), S.W, S.H, S.esz) : Img{};
+    const Img scp1 = need_scp ? img444(scp(1), S.W, S.H, S.esz) : Img{};
+    QMIV_TRY(enqueue_ssim_gen<T>(in0, in1, scp0, scp1, mask, clip, fa, s));
+  }
+  else
+  {
+    double* rowsum = rowsum_.as<double>();
+    // window pooling of up to three pictures pairs (x 3 components) from their moments, one launch
+    SsimPoolArgs pool{};
+    auto add_pool = [&](const Moments& m, int scale, int slot, int calc_l, int use_ws) {
+      for(int c = 0; c < 3; c++)
+      {
+        SsimPoolJob& J = pool.job[pool.njobs];
+        J.win = win_.as<double>() + (size_t)pool.njobs * pool_win_elems(nx_[0], ny_[0]);
+        pool.njobs++;
+        J.mom = m.p + (size_t)c * 5 * m.plane(); J.plane = m.plane(); J.pitch = m.pitch;
+        J.C1 = C1_; J.C2 = C2_;
+        J.nx = nx_[scale]; J.ny = ny_[scale]; J.calc_l = calc_l; J.wide = shape_.bitdepth > 12 ? 1 : 0;
+        J.row_sum = rowsum + (size_t)slot * 3 * ny_[0] + (size_t)c * ny_[scale];  // finalize reads [c][ny_scale]
+      }
+      fa.slot[slot].row_sum = rowsum + (size_t)slot * 3 * ny_[0];
+      fa.slot[slot].nx = nx_[scale]; fa.slot[slot].ny = ny_[scale]; fa.slot[slot].use_ws = use_ws;
+      fa.slot[slot].ws_base = 4; fa.slot[slot].ws_step = 4;  // window row j covers rows 4j..4j+7 (xIVSSIM.cpp:153)
+    };
+    auto flush_pool = [&]() -> qmiv_status {
+      if(pool.njobs == 0) { return QMIV_OK; }
+      const int t = prof_begin(s);
+      QMIV_CUDA(launch_ssim_pool(pool, s));
+      prof_end(s, QMIV_STAGE_SSIM_ROWS, t);
+      pool.njobs = 0;
+      return QMIV_OK;
+    };
+    auto moments = [&](const Img& a, const Img& b, int W, int H, const Moments& m, const MutImg* down_a,
+                       const MutImg* down_b) -> qmiv_status {
+      SsimMomArgs ma{};
+      ma.a = a; ma.b = b; ma.W = W; ma.H = H; ma.clip = clip; ma.mom = m;
+      if(down_a) { ma.down_a = *down_a; }
+      if(down_b) { ma.down_b = *down_b; }
+      const int t = prof_begin(s);
+      QMIV_CUDA(launch_ssim_moments<T>(ma, s));
+      prof_end(s, QMIV_STAGE_SSIM_WIN, t);
+      return QMIV_OK;
+    };
 
-  const Img scp0 = need_scp ? img444(scp(0), S.W, S.H, S.esz) : Img{};
-  const Img scp1 = need_scp ? img444(scp(1), S.W, S.H, S.esz) : Img{};
-  const int use_ws = prm_.erp ? 1 : 0;
-  if(mask & QMIV_IVSSIM)  // moments written by the search: (In0, SCP1) = T2R, (In1, SCP0) = R2T (xIVSSIM.cpp:46-47)
-  {
-    add_pool(mom_at(0, 0), 0, kSlotIvT2R, 1, use_ws);
-    add_pool(mom_at(1, 0), 0, kSlotIvR2T, 1, use_ws);
-  }
-  if(mask & QMIV_SSIM)  // xSSIM.h:83
-  {
-    QMIV_TRY(moments(in0, in1, S.W, S.H, mom_at(2, 0), nullptr, nullptr));
-    if(pool.njobs + 3 > 9) { QMIV_TRY(flush_pool()); }
-    add_pool(mom_at(2, 0), 0, kSlotSsim, 1, 0);
-  }
-  QMIV_TRY(flush_pool());
-  if(mask & (QMIV_MSSSIM | QMIV_IVMSSSIM))                                                                      // xSSIM.cpp:230-256
-  {
-    // pyramid levels 1..ns-1 of In0, In1, SCP0, SCP1
-    size_t lv = 0;
-    for(int s2 = 1; s2 < ns_; s2++) { lv += (size_t)(S.W >> s2) * (S.H >> s2) * 3; }
-    auto level_base = [&](int img, int scale) -> char* {
-      size_t o = (size_t)img * lv;
-      for(int s2 = 1; s2 < scale; s2++) { o += (size_t)(S.W >> s2) * (S.H >> s2) * 3; }
-      return pyr_.as<char>() + o * S.esz;
-    };
-    auto level_img = [&](int img, int scale) -> Img {
-      if(scale == 0) { return img == 0 ? in0 : img == 1 ? in1 : img == 2 ? scp0 : scp1; }
-      return img444(level_base(img, scale), S.W >> scale, S.H >> scale, S.esz);
-    };
-    for(int sc = 0; sc < ns_; sc++)
+    const Img scp0 = need_scp ? img444(scp(0), S.W, S.H, S.esz) : Img{};
+    const Img scp1 = need_scp ? img444(scp(1), S.W, S.H, S.esz) : Img{};
+    const int use_ws = prm_.erp ? 1 : 0;
+    if(mask & QMIV_IVSSIM)  // moments written by the search: (In0, SCP1) = T2R, (In1, SCP0) = R2T (xIVSSIM.cpp:46-47)
     {
-      const int Ws = S.W >> sc, Hs = S.H >> sc;
-      const bool last = sc == ns_ - 1;
-      bool written[4] = { false, false, false, false };
-      auto down = [&](int img, MutImg& m) -> const MutImg* {
-        if(last || written[img]) { return nullptr; }
-        written[img] = true;
-        m = mut444(level_base(img, sc + 1), S.W >> (sc + 1), S.H >> (sc + 1), S.esz);
-        return &m;
+      add_pool(mom_at(0, 0), 0, kSlotIvT2R, 1, use_ws);
+      add_pool(mom_at(1, 0), 0, kSlotIvR2T, 1, use_ws);
+    }
+    if(mask & QMIV_SSIM)  // xSSIM.h:83
+    {
+      QMIV_TRY(moments(in0, in1, S.W, S.H, mom_at(2, 0), nullptr, nullptr));
+      if(pool.njobs + 3 > 9) { QMIV_TRY(flush_pool()); }
+      add_pool(mom_at(2, 0), 0, kSlotSsim, 1, 0);
+    }
+    QMIV_TRY(flush_pool());
+    if(mask & (QMIV_MSSSIM | QMIV_IVMSSSIM))                                                                      // xSSIM.cpp:230-256
+    {
+      // pyramid levels 1..ns-1 of In0, In1, SCP0, SCP1
+      size_t lv = 0;
+      for(int s2 = 1; s2 < ns_; s2++) { lv += (size_t)(S.W >> s2) * (S.H >> s2) * 3; }
+      auto level_base = [&](int img, int scale) -> char* {
+        size_t o = (size_t)img * lv;
+        for(int s2 = 1; s2 < scale; s2++) { o += (size_t)(S.W >> s2) * (S.H >> s2) * 3; }
+        return pyr_.as<char>() + o * S.esz;
       };
-      MutImg m0, m1, m2, m3, m4, m5;
-      if(mask & QMIV_MSSSIM)
+      auto level_img = [&](int img, int scale) -> Img {
+        if(scale == 0) { return img == 0 ? in0 : img == 1 ? in1 : img == 2 ? scp0 : scp1; }
+        return img444(level_base(img, scale), S.W >> scale, S.H >> scale, S.esz);
+      };
+      for(int sc = 0; sc < ns_; sc++)
       {
-        const MutImg* d0 = down(0, m0); const MutImg* d1 = down(1, m1);
-        QMIV_TRY(moments(level_img(0, sc), level_img(1, sc), Ws, Hs, mom_at(2, sc), d0, d1));
-        add_pool(mom_at(2, sc), sc, kSlotMs + sc, last ? 1 : 0, 0);
+        const int Ws = S.W >> sc, Hs = S.H >> sc;
+        const bool last = sc == ns_ - 1;
+        bool written[4] = { false, false, false, false };
+        auto down = [&](int img, MutImg& m) -> const MutImg* {
+          if(last || written[img]) { return nullptr; }
+          written[img] = true;
+          m = mut444(level_base(img, sc + 1), S.W >> (sc + 1), S.H >> (sc + 1), S.esz);
+          return &m;
+        };
+        MutImg m0, m1, m2, m3, m4, m5;
+        if(mask & QMIV_MSSSIM)
+        {
+          const MutImg* d0 = down(0, m0); const MutImg* d1 = down(1, m1);
+          QMIV_TRY(moments(level_img(0, sc), level_img(1, sc), Ws, Hs, mom_at(2, sc), d0, d1));
+          add_pool(mom_at(2, sc), sc, kSlotMs + sc, last ? 1 : 0, 0);
+        }
+        if(mask & QMIV_IVMSSSIM)  // xIVSSIM.cpp:77-78, no ERP weighting
+        {
+          const MutImg* d0 = down(0, m2); const MutImg* d3 = down(3, m3);
+          QMIV_TRY(moments(level_img(0, sc), level_img(3, sc), Ws, Hs, mom_at(3, sc), d0, d3));
+          add_pool(mom_at(3, sc), sc, kSlotIvmsT2R + sc, last ? 1 : 0, 0);
+          const MutImg* d1 = down(1, m4); const MutImg* d2 = down(2, m5);
+          QMIV_TRY(moments(level_img(1, sc), level_img(2, sc), Ws, Hs, mom_at(4, sc), d1, d2));
+          add_pool(mom_at(4, sc), sc, kSlotIvmsR2T + sc, last ? 1 : 0, 0);
+        }
+        QMIV_TRY(flush_pool());
       }
-      if(mask & QMIV_IVMSSSIM)  // xIVSSIM.cpp:77-78, no ERP weighting
-      {
-        const MutImg* d0 = down(0, m2); const MutImg* d3 = down(3, m3);
-        QMIV_TRY(moments(level_img(0, sc), level_img(3, sc), Ws, Hs, mom_at(3, sc), d0, d3));
-        add_pool(mom_at(3, sc), sc, kSlotIvmsT2R + sc, last ? 1 : 0, 0);
-        const MutImg* d1 = down(1, m4); const MutImg* d2 = down(2, m5);
-        QMIV_TRY(moments(level_img(1, sc), level_img(2, sc), Ws, Hs, mom_at(4, sc), d1, d2));
-        add_pool(mom_at(4, sc), sc, kSlotIvmsR2T + sc, last ? 1 : 0, 0);
-      }
-      QMIV_TRY(flush_pool());
     }
   }
 
@@ -397,6 +469,105 @@ qmiv_status PairPipeline::enqueue_t(const Img& in0, const Img& in1, uint32_t mas
   fa.out = dout;
   { const int t = prof_begin(s); QMIV_CUDA(launch_finalize(fa, s)); prof_end(s, QMIV_STAGE_FINALIZE, t); }
   { const int t = prof_begin(s); QMIV_CUDA(cudaMemcpyAsync(h_out, dout, sizeof(PairOut), cudaMemcpyDeviceToHost, s)); prof_end(s, QMIV_STAGE_D2H, t); }
+  return QMIV_OK;
+}
+
+// Structural similarity options other than BlockAveraged 8/4 (xSSIM.cpp:199-234 SSIM and MS-SSIM,
+// xIVSSIM.cpp:31-92 IV-SSIM and IV-MS-SSIM): window values of every (picture pair, component) job
+// from k_ssim_gen, row sums from k_ssim_rows, MS-SSIM levels from k_downsample2.
+template <typename T>
+qmiv_status PairPipeline::enqueue_ssim_gen(const Img& in0, const Img& in1, const Img& scp0, const Img& scp1, uint32_t mask,
+                                           uint32_t clip, FinalizeArgs& fa, cudaStream_t s)
+{
+  const Shape& S = shape_;
+  const int32_t N = ssim_window_size(prm_);
+  double* rowsum = rowsum_.as<double>();
+  const size_t wstride = pool_win_elems(gnx_[0], gny_[0]);
+  SsimGenArgs ga{};
+  SsimPoolArgs rows{};
+  auto add = [&](const Img& a, const Img& b, int scale, int slot, int calc_l, int use_ws) {
+    for(int c = 0; c < 3; c++)
+    {
+      SsimGenJob& J = ga.job[ga.njobs];
+      J = SsimGenJob{};
+      J.a = a; J.b = b; J.comp = c; J.W = S.W >> scale; J.H = S.H >> scale;
+      J.x0 = gfirst_; J.y0 = gfirst_; J.nx = gnx_[scale]; J.ny = gny_[scale];
+      J.calc_l = calc_l; J.clip = clip; J.esz = (int32_t)S.esz; J.C1 = C1_; J.C2 = C2_;
+      J.win = win_.as<double>() + (size_t)ga.njobs * wstride;
+      SsimPoolJob& P = rows.job[rows.njobs];
+      P = SsimPoolJob{};
+      P.win = J.win; P.nx = J.nx; P.ny = J.ny;
+      P.row_sum = rowsum + (size_t)slot * 3 * gny_[0] + (size_t)c * gny_[scale];   // finalize reads [c][ny_scale]
+      ga.njobs++; rows.njobs++;
+    }
+    SsimSlot& sl = fa.slot[slot];
+    sl.row_sum = rowsum + (size_t)slot * 3 * gny_[0];
+    sl.nx = gnx_[scale]; sl.ny = gny_[scale]; sl.use_ws = use_ws;
+    sl.ws_base = gws_base_; sl.ws_step = prm_.ssim_stride;
+  };
+  auto flush = [&]() -> qmiv_status {
+    if(ga.njobs == 0) { return QMIV_OK; }
+    int t = prof_begin(s);
+    QMIV_CUDA(launch_ssim_gen(ga, prm_.ssim_mode, N, prm_.ssim_stride, prm_.ssim_border, s));
+    prof_end(s, QMIV_STAGE_SSIM_WIN, t);
+    t = prof_begin(s);
+    QMIV_CUDA(launch_ssim_rows(rows, s));
+    prof_end(s, QMIV_STAGE_SSIM_ROWS, t);
+    ga.njobs = 0; rows.njobs = 0;
+    return QMIV_OK;
+  };
+
+  const int use_ws = prm_.erp ? 1 : 0;
+  if(mask & QMIV_IVSSIM)   // T2R = SSIM(In0, SCP1), R2T = SSIM(In1, SCP0) with ERP row weights (xIVSSIM.cpp:46-47)
+  {
+    add(in0, scp1, 0, kSlotIvT2R, 1, use_ws);
+    add(in1, scp0, 0, kSlotIvR2T, 1, use_ws);
+  }
+  if(mask & QMIV_SSIM) { add(in0, in1, 0, kSlotSsim, 1, 0); }   // xSSIM.h:83
+  QMIV_TRY(flush());
+  if(mask & (QMIV_MSSSIM | QMIV_IVMSSSIM))   // xSSIM.cpp:115-141, every scale with the same option
+  {
+    size_t lv = 0;
+    for(int s2 = 1; s2 < ns_; s2++) { lv += (size_t)(S.W >> s2) * (S.H >> s2) * 3; }
+    auto level_base = [&](int img, int scale) -> char* {
+      size_t o = (size_t)img * lv;
+      for(int s2 = 1; s2 < scale; s2++) { o += (size_t)(S.W >> s2) * (S.H >> s2) * 3; }
+      return pyr_.as<char>() + o * S.esz;
+    };
+    auto level_img = [&](int img, int scale) -> Img {
+      if(scale == 0) { return img == 0 ? in0 : img == 1 ? in1 : img == 2 ? scp0 : scp1; }
+      return img444(level_base(img, scale), S.W >> scale, S.H >> scale, S.esz);
+    };
+    auto down = [&](int ia, int ib, int scale) -> qmiv_status {   // level scale - 1 -> scale of pictures ia, ib
+      const int t = prof_begin(s);
+      QMIV_CUDA(launch_downsample2<T>(level_img(ia, scale - 1), level_img(ib, scale - 1),
+                                      mut444(level_base(ia, scale), S.W >> scale, S.H >> scale, S.esz),
+                                      mut444(level_base(ib, scale), S.W >> scale, S.H >> scale, S.esz), S.W >> scale,
+                                      S.H >> scale, clip, s));
+      prof_end(s, QMIV_STAGE_SSIM_WIN, t);
+      return QMIV_OK;
+    };
+    for(int sc = 0; sc < ns_; sc++)
+    {
+      const int last = sc == ns_ - 1 ? 1 : 0;
+      if(sc > 0)
+      {
+        if(mask & QMIV_MSSSIM) { QMIV_TRY(down(0, 1, sc)); }
+        if(mask & QMIV_IVMSSSIM)
+        {
+          if(!(mask & QMIV_MSSSIM)) { QMIV_TRY(down(0, 1, sc)); }
+          QMIV_TRY(down(2, 3, sc));
+        }
+      }
+      if(mask & QMIV_MSSSIM) { add(level_img(0, sc), level_img(1, sc), sc, kSlotMs + sc, last, 0); }
+      if(mask & QMIV_IVMSSSIM)   // no ERP weighting (xIVSSIM.cpp:77-78)
+      {
+        add(level_img(0, sc), level_img(3, sc), sc, kSlotIvmsT2R + sc, last, 0);
+        add(level_img(1, sc), level_img(2, sc), sc, kSlotIvmsR2T + sc, last, 0);
+      }
+      QMIV_TRY(flush());
+    }
+  }
   return QMIV_OK;
 }
 

@@ -273,6 +273,7 @@ void qmiv_params_default(qmiv_params* p)
   p->erp = 0; p->lon_range_deg = 360; p->lat_range_deg = 180;
   p->ssim_window = 8; p->ssim_stride = 4;
   p->invalid_pel_action = QMIV_PEL_STOP;
+  p->ssim_mode = QMIV_SSM_BLOCK_AVERAGED; p->ssim_border = QMIV_BRD_NONE;
 }
 
 qmiv_status qmiv_ctx_create(int32_t device, uint64_t hbm_budget_bytes, qmiv_ctx* out_ctx)

@@ -244,6 +244,7 @@ qmiv_status Engine::submit(const qmiv_pair_desc* pairs, int32_t n)
     const qmiv_pair_desc& d = pairs[i];
     QMIV_TRY(kind_for(d, kind[i]));
     QMIV_TRY(check_metrics(kind[i]->S, d.metric_mask));
+    QMIV_TRY(check_batched_ssim(prm_, d.metric_mask));
     PairSlot& p = P[i];
     const Shape& S = kind[i]->S;
     p.mask = d.metric_mask;
@@ -778,6 +779,7 @@ void Engine::add_pool_jobs(int i, const PairKind& K, int ph, char* dbase, SsimPo
     }
     fa.slot[slot].row_sum = rowsum + (size_t)slot * 3 * K.ny[0];
     fa.slot[slot].nx = K.nx[scale]; fa.slot[slot].ny = K.ny[scale]; fa.slot[slot].use_ws = use_ws;
+    fa.slot[slot].ws_base = 4; fa.slot[slot].ws_step = 4;  // window row j covers rows 4j..4j+7 (xIVSSIM.cpp:153)
   };
   const int use_ws = prm_.erp ? 1 : 0;
   if(ph == 0 && (p.mask & QMIV_IVSSIM))  // (In0, SCP1) = T2R, (In1, SCP0) = R2T (xIVSSIM.cpp:46-47)

@@ -105,6 +105,18 @@ struct Shape
 };
 
 qmiv_status validate_params(const qmiv_params& p);
+
+// Structural similarity options of a parameter set (xSSIM::setStructSimParams, xSSIM.cpp:86-113).
+constexpr uint32_t kSsimFamily = QMIV_SSIM | QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM;
+inline bool    ssim_regular(int32_t mode) { return mode >= QMIV_SSM_REGULAR_GAUSSIAN_FLT && mode <= QMIV_SSM_REGULAR_AVERAGED; }
+// BlockAveraged 8x8 windows at stride 4: the moment-based path (qmiv_ssim.cu)
+inline bool    ssim_is_default(const qmiv_params& p) { return p.ssim_mode == QMIV_SSM_BLOCK_AVERAGED && p.ssim_window == 8 && p.ssim_stride == 4; }
+inline int32_t ssim_window_size(const qmiv_params& p) { return ssim_regular(p.ssim_mode) ? 11 : p.ssim_window; }
+// Windows along a picture line of length len (xSSIM::xInitLoopRanges, xSSIM.cpp:161-196, counts
+// :381-404) and the line position of the first window's first input sample.
+void ssim_line(const qmiv_params& p, int32_t len, int32_t& first_sample, int32_t& count);
+// The batched and serving forms evaluate the default structural similarity option only.
+qmiv_status check_batched_ssim(const qmiv_params& p, uint32_t mask);
 // Known metric bits, and the SSIM family only where its exact 32-bit sub-block moments hold
 // (bit depth <= 14: 16 * (2^14 - 1)^2 < 2^32).
 qmiv_status check_metrics(const Shape& S, uint32_t mask);
@@ -148,6 +160,15 @@ public:
 
 private:
   template <typename T> qmiv_status enqueue_t(const Img& in0, const Img& in1, uint32_t mask, bool want_scp, bool want_gcd, cudaStream_t s);
+  // SSIM family under a non-default structural similarity option (qmiv_ssim_gen.cu windows on the
+  // pictures and their SCPs)
+  template <typename T>
+  qmiv_status enqueue_ssim_gen(const Img& in0, const Img& in1, const Img& scp0, const Img& scp1, uint32_t mask, uint32_t clip,
+                               FinalizeArgs& fa, cudaStream_t s);
+  bool need_scp_for(uint32_t mask, bool want_scp) const
+  {
+    return want_scp || (mask & QMIV_IVMSSSIM) || (gen_ && (mask & QMIV_IVSSIM));
+  }
 
   qmiv_ctx_s*  ctx_ = nullptr;
   Shape        shape_;
@@ -157,6 +178,9 @@ private:
   bool         fp32_ok_ = true;
   int32_t      ns_ = 0;
   int32_t      nx_[5] = {}, ny_[5] = {}, nxp_ = 0;
+  bool         gen_ = false;                       // non-default structural similarity option
+  int32_t      gnx_[5] = {}, gny_[5] = {};         // its windows per row / column at each MS-SSIM scale
+  int32_t      gfirst_ = 0, gws_base_ = 0;         // first window's first input sample; ERP weight of window row 0
   std::vector<double> ws_host_;
   double       ws_corr_ = 1.0;
   double       C1_ = 0, C2_ = 0;

@@ -171,7 +171,7 @@ cudaError_t launch_reduce_multi(const ReduceArgs* d_jobs, int njobs, cudaStream_
 // waits on its own floating-point dependency.
 //   WS-PSNR   KBNS over rows of rowSSD * w[y]            (xWSPSNR.cpp:123-132)
 //   IV-PSNR   KBNS over rows of rowSSE * w[y] (ERP)       (xIVPSNR.cpp:171-175) + exact uint64 sums
-//   SSIM      KBNS over window rows (ERP: row * w[y + 4], weights KBNS) (xSSIM.cpp:348-351,
+//   SSIM      KBNS over window rows (ERP: row * w[base + step j], weights KBNS) (xSSIM.cpp:348-351,
 //             xIVSSIM.cpp:148-172)
 // =============================================================================================
 // One CTA per chain: all threads stage the chain's inputs (independent loads) into shared memory,
@@ -192,7 +192,7 @@ __device__ __forceinline__ double chain_value(const FinalizeArgs& a, const FinCh
   }
   const SsimSlot& sl = a.slot[ch.a];
   const double v = sl.row_sum[(size_t)ch.b * sl.ny + y];
-  return sl.use_ws ? dmul(v, a.ws[4 * y + 4]) : v;
+  return sl.use_ws ? dmul(v, a.ws[sl.ws_base + sl.ws_step * y]) : v;
 }
 
 __device__ __forceinline__ void finalize_body(const FinalizeArgs& a, int chain, double* stage)
@@ -227,7 +227,7 @@ __device__ __forceinline__ void finalize_body(const FinalizeArgs& a, int chain, 
   for(int y = threadIdx.x; y < len; y += blockDim.x)
   {
     vals[y] = chain_value(a, ch, y);
-    if(wsum) { wts[y] = a.ws[4 * y + 4]; }
+    if(wsum) { wts[y] = a.ws[a.slot[ch.a].ws_base + a.slot[ch.a].ws_step * y]; }
   }
   __syncthreads();
   if(threadIdx.x != 0) { return; }

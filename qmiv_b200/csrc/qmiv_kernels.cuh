@@ -93,13 +93,43 @@ struct SsimPoolArgs
 };
 
 // ---------------------------------------------------------------------------------------------
+// SSIM under any structural similarity option (qmiv_ssim_gen.cu): window values of up to 9
+// (picture pair, component) jobs into their band-transposed scratch, then k_ssim_rows
+// ---------------------------------------------------------------------------------------------
+struct SsimGenJob
+{
+  Img      a, b;       // a = "Tst", b = "Ref" (xSSIM::xCalcPicSSIM argument order)
+  int32_t  comp;
+  int32_t  W, H;       // picture size in 4:4:4 samples
+  int32_t  x0, y0;     // input position of the first window's top-left sample
+  int32_t  nx, ny;     // windows per row / column
+  int32_t  calc_l;
+  uint32_t clip;       // conceal: samples above are clipped (65535 = no clipping)
+  int32_t  esz;        // bytes per sample of a and b
+  double   C1, C2;
+  double*  win;        // [ceil(ny / 32)][nx][32] (pool_win_elems)
+};
+
+constexpr int kGenMaxJobs = 9;
+struct SsimGenArgs
+{
+  int32_t    njobs;
+  int32_t    S, border, coef;   // stride, QMIV_BRD_*, offset of the window's coefficients (set by the launcher)
+  double     inv;               // scale of the integer sums: 2^-18, 1 / 121 or 1 / N^2 (set by the launcher)
+  int32_t    tw, th, cw;        // tile width / height in samples, columns per phase (set by the launcher)
+  int32_t    pad_;
+  SsimGenJob job[kGenMaxJobs];
+};
+
+// ---------------------------------------------------------------------------------------------
 // finalize: every serial KBNS chain of one frame pair, one thread per chain
 // ---------------------------------------------------------------------------------------------
 struct SsimSlot
 {
   const double* row_sum;       // [3][ny]
   int32_t       nx, ny;
-  int32_t       use_ws;        // ERP row weights w[4j + 4] (xIVSSIM.cpp:148-165)
+  int32_t       use_ws;        // ERP row weights w[ws_base + ws_step j] (xIVSSIM.cpp:148-165)
+  int32_t       ws_base, ws_step;
 };
 
 enum { kChainWsPsnr = 0, kChainIvPsnr = 1, kChainSsim = 2 };
@@ -138,6 +168,13 @@ cudaError_t launch_reduce(const ReduceArgs& a, cudaStream_t s);
 template <typename T> cudaError_t launch_cps(const CpsArgs& a, int R, cudaStream_t s);
 template <typename T> cudaError_t launch_ssim_moments(const SsimMomArgs& a, cudaStream_t s);
 cudaError_t launch_ssim_pool(const SsimPoolArgs& a, cudaStream_t s);
+cudaError_t launch_ssim_rows(const SsimPoolArgs& a, cudaStream_t s);   // row sums of ready window values
+// SSIM windows of one option set for up to kGenMaxJobs jobs: mode QMIV_SSM_*, window N, stride S,
+// border QMIV_BRD_* (regular modes)
+cudaError_t launch_ssim_gen(SsimGenArgs& a, int mode, int N, int S, int border, cudaStream_t s);
+template <typename T>
+cudaError_t launch_downsample2(const Img& a, const Img& b, const MutImg& da, const MutImg& db, int dw, int dh, uint32_t clip,
+                               cudaStream_t s);
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
 int         finalize_plan(FinalizeArgs& a);          // fills a.chain / a.nchains, returns the CTA count
 size_t      finalize_smem(const FinalizeArgs& a);

@@ -44,6 +44,25 @@ __global__ void __launch_bounds__(256) k_fp32_peak(float* out, int iters, float 
   if(r == 1234.5f) { out[blockIdx.x] = r; }
 }
 
+// Eight independent chains of separately rounded multiply and add per thread: the instruction mix of
+// the Gaussian-float SSIM window sums. Each DMUL and each DADD counts as one operation.
+__global__ void __launch_bounds__(256) k_fp64_peak(double* out, int iters, double seed)
+{
+  double x[kChains];
+  #pragma unroll
+  for(int k = 0; k < kChains; k++) { x[k] = seed + 0.001 * (threadIdx.x + k); }
+  const double a = 0.9999999, b = 1e-9;
+  for(int i = 0; i < iters; i++)
+  {
+    #pragma unroll
+    for(int k = 0; k < kChains; k++) { x[k] = __dadd_rn(__dmul_rn(x[k], a), b); }
+  }
+  double r = 0.0;
+  #pragma unroll
+  for(int k = 0; k < kChains; k++) { r += x[k]; }
+  if(r == 1234.5) { out[blockIdx.x] = r; }
+}
+
 template <typename K>
 qmiv_status time_kernel(int32_t device, K launch, double* ms_out)
 {
@@ -104,6 +123,24 @@ qmiv_status qmiv_probe_fp32_peak(int32_t device, int32_t iters, double* tflops)
   QMIV_TRY(st);
   const double flops = 2.0 * kChains * (double)iters * blocks * threads;
   *tflops = flops / (ms * 1e-3) / 1e12;
+  return QMIV_OK;
+}
+
+qmiv_status qmiv_probe_fp64_peak(int32_t device, int32_t iters, double* tops)
+{
+  if(!tops || iters <= 0) { return fail(QMIV_ERR_INVALID_ARG, "bad probe arguments"); }
+  int sms = 0;
+  QMIV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const int blocks = sms * 8, threads = 256;
+  double* out = nullptr;
+  QMIV_CUDA(cudaSetDevice(device));
+  QMIV_CUDA(cudaMalloc(&out, blocks * sizeof(double)));
+  double ms = 0;
+  const qmiv_status st = time_kernel(device, [&] { k_fp64_peak<<<blocks, threads>>>(out, iters, 1.0); }, &ms);
+  cudaFree(out);
+  QMIV_TRY(st);
+  const double ops = 2.0 * kChains * (double)iters * blocks * threads;
+  *tops = ops / (ms * 1e-3) / 1e12;
   return QMIV_OK;
 }
 

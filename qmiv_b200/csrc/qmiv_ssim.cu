@@ -323,6 +323,19 @@ cudaError_t launch_ssim_pool_multi(const SsimPoolJob* d_jobs, int njobs, int max
   return cudaGetLastError();
 }
 
+cudaError_t launch_ssim_rows(const SsimPoolArgs& a, cudaStream_t s)
+{
+  if(a.njobs <= 0) { return cudaSuccess; }
+  int maxny = 0;
+  for(int k = 0; k < a.njobs; k++)
+  {
+    if(((uintptr_t)a.job[k].win & 15) != 0) { return cudaErrorMisalignedAddress; }
+    maxny = max(maxny, a.job[k].ny);
+  }
+  k_ssim_rows<<<dim3((maxny + 31) / 32, a.njobs), 32, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ssim_pool(const SsimPoolArgs& a, cudaStream_t s)
 {
   if(a.njobs <= 0) { return cudaSuccess; }

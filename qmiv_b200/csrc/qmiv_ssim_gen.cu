@@ -1,0 +1,409 @@
+// Structural similarity under every window option of the reference (xSSIM::setStructSimParams,
+// libs/pmbb-ivqm/src/xSSIM.cpp:86-113; the app's -ssm / -ssb / -ssw / -sss, apps/QMIV/src/xAppQMIV.cpp:99-104):
+//   regular 11x11 windows centred on (x, y), x, y in [5, W - 5) without a border mode or [0, W) with one
+//   (xSSIM.cpp:161-196), whose reads beyond the picture see the margin extension (libs/pmbb-core/src/
+//   xMarginOps.h:16-20: Nearest, Reflect, Mirror, Constant 65535 as xPicP::extend passes it, Zero):
+//     Gaussian float   (xStructSimSTD.cpp:19-88)  five double sums in dy, dx order of value x coefficient,
+//                      each product and sum rounded separately
+//     Gaussian integer (xStructSimSTD.cpp:89-154) exact integer sums of value x integer coefficient, x 2^-18
+//     averaged         (xStructSimSTD.cpp:155-193, AVX CalcBlckAvg11) exact integer sums x (1 / 121)
+//   block N x N windows with their top-left sample at (x, y), x in [0, W - N] (xSSIM.cpp:182-195):
+//     Gaussian integer 8 / 16 (xStructSimSTD.cpp:353-419), averaged 8 / 16 / 32 (:420-461) x (1 / N^2)
+// Integer sums stay below 2^53 for 16-bit samples (65535^2 * 2^18 < 2^51), so they are formed exactly in
+// double with fused multiply-adds in any order; the float Gaussian sums keep the reference's order and
+// roundings (separate multiply and add). The window formula uses separately rounded operations in the
+// reference's order, so every window value equals the portable reference's bit for bit.
+//
+// k_ssim_gen: a CTA of 32 x WY threads stages the samples its windows read, both pictures packed
+// (a | b << 16) in shared memory after clipping and margin extension, then lane l of warp w evaluates
+// window column x0 + l for K consecutive window rows: it walks the input rows the K windows cover, and
+// each sample loaded from shared memory feeds every window whose rows include it. With stride S > 1
+// the tile's columns are stored by phase (column c at (c % S) * cw + c / S), so the 32 lanes of a warp
+// read 32 consecutive words. Window values go to the band-transposed scratch [ny / 32][nx][32] that
+// k_ssim_rows (qmiv_ssim.cu) sums in x order, one lane per window row.
+#include "qmiv_host.h"
+
+#include <cmath>
+#include <mutex>
+
+namespace qmiv {
+
+namespace {
+
+enum { kGenFlt = 0, kGenInt = 1, kGenAvg = 2 };
+
+// window coefficients, row-major dy * N + dx
+constexpr int kCoefFlt11 = 0, kCoefInt11 = 121, kCoefInt8 = 242, kCoefInt16 = 306, kCoefTotal = 562;
+__constant__ double c_gen_coef[kCoefTotal];
+
+// Integer Gaussian windows (xStructSimConsts.h:111-124 for 11x11, :145-173 for 8x8 and 16x16), each the
+// mirror image of its top-left quadrant in both directions. These integers define the reference's
+// metric, so they are kept as they are. The 11x11 quadrant is not symmetric about its diagonal.
+const int32_t kGq11[6][6] = {
+  { 0, 2, 10, 29, 57, 72 },           { 2, 15, 72, 218, 424, 530 },          { 10, 72, 340, 1032, 2010, 2510 },
+  { 29, 218, 1032, 3135, 6107, 7626 }, { 57, 424, 2010, 6107, 11894, 14854 }, { 72, 530, 2510, 7626, 14855, 18550 },
+};
+const int32_t kGq8[4][4] = {
+  { 81, 308, 749, 1168 }, { 308, 1168, 2842, 4432 }, { 749, 2842, 6913, 10781 }, { 1168, 4432, 10781, 16814 },
+};
+const int32_t kGq16[8][8] = {
+  { 0, 1, 4, 10, 19, 32, 45, 54 },                 { 1, 5, 13, 32, 64, 108, 152, 181 },
+  { 4, 13, 38, 91, 181, 305, 432, 514 },           { 10, 32, 91, 216, 432, 727, 1029, 1224 },
+  { 19, 64, 181, 432, 865, 1456, 2061, 2451 },     { 32, 108, 305, 727, 1456, 2451, 3469, 4126 },
+  { 45, 152, 432, 1029, 2061, 3469, 4909, 5839 },  { 54, 181, 514, 1224, 2451, 4126, 5839, 6947 },
+};
+
+int32_t gauss_int(int N, int y, int x)
+{
+  const int qy = y < N - 1 - y ? y : N - 1 - y, qx = x < N - 1 - x ? x : N - 1 - x;
+  return N == 11 ? kGq11[qy][qx] : N == 8 ? kGq8[qy][qx] : kGq16[qy][qx];
+}
+
+// The float Gaussian (c_FilterRglrGaussFlt32, xStructSimConsts.h:55-68) is the 11x11 Gaussian of sigma
+// 1.5 normalised to unit sum and rounded to float.
+void build_coefs(double* c)
+{
+  double g[11][11], sum = 0.0;
+  for(int y = 0; y < 11; y++)
+  {
+    for(int x = 0; x < 11; x++) { g[y][x] = std::exp(-(double)((x - 5) * (x - 5) + (y - 5) * (y - 5)) / 4.5); sum += g[y][x]; }
+  }
+  for(int y = 0; y < 11; y++) { for(int x = 0; x < 11; x++) { c[kCoefFlt11 + 11 * y + x] = (double)(float)(g[y][x] / sum); } }
+  for(int y = 0; y < 11; y++) { for(int x = 0; x < 11; x++) { c[kCoefInt11 + 11 * y + x] = gauss_int(11, y, x); } }
+  for(int y = 0; y < 8; y++) { for(int x = 0; x < 8; x++) { c[kCoefInt8 + 8 * y + x] = gauss_int(8, y, x); } }
+  for(int y = 0; y < 16; y++) { for(int x = 0; x < 16; x++) { c[kCoefInt16 + 16 * y + x] = gauss_int(16, y, x); } }
+}
+
+// exact double of a 16-bit integer: 2^52 + v has a unit ulp
+__device__ __forceinline__ double u16_to_f64(uint32_t v) { return dsub(__hiloint2double(0x43300000, (int)v), 4503599627370496.0); }
+
+// position of sample i of a length-n line after margin extension; in = false for the constant modes
+__device__ __forceinline__ int brd_map(int i, int n, int border, bool& in)
+{
+  in = true;
+  if(i >= 0 && i < n) { return i; }
+  int j;
+  switch(border)
+  {
+  case QMIV_BRD_REFLECT: j = i < 0 ? -1 - i : 2 * n - 1 - i; break;   // ( c b a | a b c d | d c b )
+  case QMIV_BRD_MIRROR:  j = i < 0 ? -i : 2 * n - 2 - i; break;       // ( d c b | a b c d | c b a )
+  case QMIV_BRD_CONSTANT:
+  case QMIV_BRD_ZERO:    in = false; return 0;
+  default:               j = i;                                        // Nearest; None reads only unused tile parts
+  }
+  return min(max(j, 0), n - 1);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// window kernel
+// ---------------------------------------------------------------------------------------------
+template <int MODE, int N>
+__device__ __forceinline__ double gen_window(const double (&m)[5], double inv, double C1, double C2, bool calc_l)
+{
+  // m: sums of R, T, R^2, T^2, R*T (R = "Ref" = b, T = "Tst" = a)
+  double ar, at, var_r, var_t, cov;
+  if(MODE == kGenFlt)                                         // xStructSimSTD.cpp:41-45
+  {
+    ar = m[0]; at = m[1];
+    var_r = dsub(m[2], dmul(ar, ar));
+    var_t = dsub(m[3], dmul(at, at));
+    cov   = dsub(m[4], dmul(ar, at));
+  }
+  else                                                        // xStructSimSTD.cpp:110-114, :171-175
+  {
+    ar = dmul(m[0], inv); at = dmul(m[1], inv);
+    var_r = dsub(dmul(m[2], inv), dmul(ar, ar));
+    var_t = dsub(dmul(m[3], inv), dmul(at, at));
+    cov   = dsub(dmul(m[4], inv), dmul(ar, at));
+  }
+  // 2 x is formed as x + x, which is the same double
+  const double cs = ddiv(dadd(dadd(cov, cov), C2), dadd(dadd(var_r, var_t), C2));
+  if(!calc_l) { return cs; }
+  const double l = ddiv(dadd(dmul(dadd(ar, ar), at), C1), dadd(dadd(dmul(ar, ar), dmul(at, at)), C1));
+  return dmul(l, cs);
+}
+
+template <int MODE, int N, int K>
+__global__ void __launch_bounds__(128) k_ssim_gen(const __grid_constant__ SsimGenArgs a)
+{
+  extern __shared__ uint32_t tile[];                          // [th][S * cw], sample a | b << 16
+  const SsimGenJob& J = a.job[blockIdx.z];
+  const int S = a.S, WY = blockDim.y, lane = threadIdx.x, w = threadIdx.y;
+  const int wx0 = blockIdx.x * 32, wy0 = blockIdx.y * WY * K;
+  if(wx0 >= J.nx || wy0 >= J.ny) { return; }                 // uniform over the CTA
+  const int pitch = S * a.cw;
+  // staged part: the columns and rows the CTA's existing windows read
+  const int tw = (min(32, J.nx - wx0) - 1) * S + N;
+  const int th = (min(WY * K, J.ny - wy0) - 1) * S + N;
+  const int X0 = J.x0 + wx0 * S, Y0 = J.y0 + wy0 * S;
+  const int c = J.comp;
+  for(int r = w; r < th; r += WY)
+  {
+    bool yin;
+    const int yi = brd_map(Y0 + r, J.H, a.border, yin);
+    uint32_t* dst = tile + (size_t)r * pitch;
+    for(int col = lane; col < tw; col += 32)
+    {
+      bool xin;
+      const int xi = brd_map(X0 + col, J.W, a.border, xin);
+      uint32_t va, vb;
+      if(xin && yin)
+      {
+        if(J.esz == 1) { va = (uint32_t)fetch<uint8_t>(J.a, c, xi, yi); vb = (uint32_t)fetch<uint8_t>(J.b, c, xi, yi); }
+        else { va = (uint32_t)fetch<uint16_t>(J.a, c, xi, yi); vb = (uint32_t)fetch<uint16_t>(J.b, c, xi, yi); }
+        va = min(va, J.clip); vb = min(vb, J.clip);
+      }
+      else { va = vb = a.border == QMIV_BRD_CONSTANT ? 0xffffu : 0u; }
+      const int q = col / S;
+      dst[(col - q * S) * a.cw + q] = va | (vb << 16);
+    }
+  }
+  __syncthreads();
+
+  int co[N];                                                  // tile column of tap dx for this lane
+  #pragma unroll
+  for(int dx = 0; dx < N; dx++) { const int q = dx / S; co[dx] = (dx - q * S) * a.cw + q + lane; }
+  double acc[K][5];
+  #pragma unroll
+  for(int k = 0; k < K; k++)
+  {
+    #pragma unroll
+    for(int m = 0; m < 5; m++) { acc[k][m] = 0.0; }
+  }
+  const uint32_t* rowp = tile + (size_t)(w * K * S) * pitch;
+  const int nr = (K - 1) * S + N;                             // input rows of the thread's K windows
+  #pragma unroll 1
+  for(int r = 0; r < nr; r++, rowp += pitch)
+  {
+    // window k takes this input row as its row dy = r - k S (rows in order, so each window's
+    // contributions arrive in dy-major, dx-minor order)
+    unsigned valid = 0;
+    int crow[K];
+    #pragma unroll
+    for(int k = 0; k < K; k++)
+    {
+      const int dy = r - k * S;
+      if(dy >= 0 && dy < N) { valid |= 1u << k; }
+      crow[k] = a.coef + min(max(dy, 0), N - 1) * N;       // in range also where unused
+    }
+    #pragma unroll
+    for(int dx = 0; dx < N; dx++)
+    {
+      const uint32_t v = rowp[co[dx]];
+      const double T = u16_to_f64(v & 0xffffu), R = u16_to_f64(v >> 16);
+      const double RR = dmul(R, R), TT = dmul(T, T), RT = dmul(R, T);   // exact (< 2^32)
+      #pragma unroll
+      for(int k = 0; k < K; k++)
+      {
+        if(!(valid & (1u << k))) { continue; }
+        if(MODE == kGenAvg)
+        {
+          acc[k][0] = dadd(acc[k][0], R); acc[k][1] = dadd(acc[k][1], T);
+          acc[k][2] = dadd(acc[k][2], RR); acc[k][3] = dadd(acc[k][3], TT); acc[k][4] = dadd(acc[k][4], RT);
+        }
+        else
+        {
+          const double C = c_gen_coef[crow[k] + dx];
+          if(MODE == kGenFlt)                                 // SumR += R * C, ... (xStructSimSTD.cpp:34-38)
+          {
+            acc[k][0] = dadd(acc[k][0], dmul(R, C)); acc[k][1] = dadd(acc[k][1], dmul(T, C));
+            acc[k][2] = dadd(acc[k][2], dmul(RR, C)); acc[k][3] = dadd(acc[k][3], dmul(TT, C));
+            acc[k][4] = dadd(acc[k][4], dmul(RT, C));
+          }
+          else                                                // exact integers
+          {
+            acc[k][0] = __fma_rn(R, C, acc[k][0]); acc[k][1] = __fma_rn(T, C, acc[k][1]);
+            acc[k][2] = __fma_rn(RR, C, acc[k][2]); acc[k][3] = __fma_rn(TT, C, acc[k][3]);
+            acc[k][4] = __fma_rn(RT, C, acc[k][4]);
+          }
+        }
+      }
+    }
+  }
+  const int wx = wx0 + lane;
+  if(wx >= J.nx) { return; }
+  #pragma unroll
+  for(int k = 0; k < K; k++)
+  {
+    const int wy = wy0 + w * K + k;
+    if(wy < J.ny)
+    {
+      J.win[((size_t)(wy >> 5) * J.nx + wx) * 32 + (wy & 31)] = gen_window<MODE, N>(acc[k], a.inv, J.C1, J.C2, J.calc_l != 0);
+    }
+  }
+}
+
+// 2x2 mean of both pictures of a pair for the next MS-SSIM scale (xPixelOpsSTD.cpp:50-67), after clipping
+struct DownArgs
+{
+  Img      src[2];
+  MutImg   dst[2];     // null planes are skipped
+  int32_t  dw, dh;
+  uint32_t clip;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_downsample2(const __grid_constant__ DownArgs a)
+{
+  const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5), c = blockIdx.z;
+  if(x >= a.dw || y >= a.dh) { return; }
+  #pragma unroll
+  for(int i = 0; i < 2; i++)
+  {
+    T* d = static_cast<T*>(a.dst[i].p[c]);
+    if(!d) { continue; }
+    const uint32_t v = min((uint32_t)fetch<T>(a.src[i], c, 2 * x, 2 * y), a.clip) + min((uint32_t)fetch<T>(a.src[i], c, 2 * x + 1, 2 * y), a.clip) +
+                       min((uint32_t)fetch<T>(a.src[i], c, 2 * x, 2 * y + 1), a.clip) +
+                       min((uint32_t)fetch<T>(a.src[i], c, 2 * x + 1, 2 * y + 1), a.clip);
+    d[(size_t)y * a.dst[i].pitch[c] + x] = (T)((v + 2) >> 2);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kGenSmemPreferred = 96 * 1024;   // two CTAs per SM
+constexpr size_t kGenSmemMax = 200 * 1024;
+
+struct GenPlan
+{
+  int    WY, K;
+  int    tw, th, cw;
+  size_t smem;
+};
+
+// The largest window block (WY warps x K window rows per thread) whose tile fits the preferred shared
+// memory; one window row per thread when even that does not (wide strides of 32x32 windows).
+bool gen_plan(int N, int S, GenPlan& p)
+{
+  static const int kShapes[6][2] = { { 4, 8 }, { 2, 8 }, { 4, 2 }, { 2, 2 }, { 1, 2 }, { 1, 1 } };
+  for(int i = 0; i < 6; i++)
+  {
+    p.WY = kShapes[i][0]; p.K = kShapes[i][1];
+    p.tw = 31 * S + N;
+    p.th = (p.WY * p.K - 1) * S + N;
+    p.cw = (p.tw + S - 1) / S;
+    p.smem = (size_t)p.th * S * p.cw * sizeof(uint32_t);
+    if(p.smem <= kGenSmemPreferred) { return true; }
+  }
+  return p.smem <= kGenSmemMax;
+}
+
+template <int MODE, int N, int K>
+cudaError_t gen_attr()
+{
+  return cudaFuncSetAttribute(k_ssim_gen<MODE, N, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmemMax);
+}
+
+template <int MODE, int N>
+cudaError_t gen_attr_k()
+{
+  cudaError_t e = gen_attr<MODE, N, 8>();
+  if(e == cudaSuccess) { e = gen_attr<MODE, N, 2>(); }
+  if(e == cudaSuccess) { e = gen_attr<MODE, N, 1>(); }
+  return e;
+}
+
+// coefficient upload and shared-memory limits, once per device
+cudaError_t gen_configure()
+{
+  static std::mutex mu;
+  static uint64_t done = 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess) { return e; }
+  const uint64_t bit = 1ULL << (dev & 63);
+  std::lock_guard<std::mutex> lk(mu);
+  if(done & bit) { return cudaSuccess; }
+  double c[kCoefTotal];
+  build_coefs(c);
+  e = cudaMemcpyToSymbol(c_gen_coef, c, sizeof(c));
+  if(e == cudaSuccess) { e = gen_attr_k<kGenFlt, 11>(); }
+  if(e == cudaSuccess) { e = gen_attr_k<kGenInt, 11>(); }
+  if(e == cudaSuccess) { e = gen_attr_k<kGenInt, 8>(); }
+  if(e == cudaSuccess) { e = gen_attr_k<kGenInt, 16>(); }
+  if(e == cudaSuccess) { e = gen_attr_k<kGenAvg, 11>(); }
+  if(e == cudaSuccess) { e = gen_attr_k<kGenAvg, 8>(); }
+  if(e == cudaSuccess) { e = gen_attr_k<kGenAvg, 16>(); }
+  if(e == cudaSuccess) { e = gen_attr_k<kGenAvg, 32>(); }
+  if(e == cudaSuccess) { done |= bit; }
+  return e;
+}
+
+template <int MODE, int N>
+cudaError_t gen_launch_k(const SsimGenArgs& a, const GenPlan& p, dim3 grid, cudaStream_t s)
+{
+  const dim3 block(32, p.WY);
+  if(p.K == 8) { k_ssim_gen<MODE, N, 8><<<grid, block, p.smem, s>>>(a); }
+  else if(p.K == 2) { k_ssim_gen<MODE, N, 2><<<grid, block, p.smem, s>>>(a); }
+  else { k_ssim_gen<MODE, N, 1><<<grid, block, p.smem, s>>>(a); }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_ssim_gen(SsimGenArgs& a, int mode, int N, int S, int border, cudaStream_t s)
+{
+  if(a.njobs <= 0) { return cudaSuccess; }
+  if(a.njobs > kGenMaxJobs || S < 1 || S > N) { return cudaErrorInvalidValue; }
+  GenPlan p;
+  if(!gen_plan(N, S, p)) { return cudaErrorInvalidValue; }
+  cudaError_t e = gen_configure();
+  if(e != cudaSuccess) { return e; }
+  int maxnx = 0, maxny = 0;
+  for(int k = 0; k < a.njobs; k++)
+  {
+    const SsimGenJob& J = a.job[k];
+    if(J.nx < 1 || J.ny < 1 || !J.win || (J.esz != 1 && J.esz != 2)) { return cudaErrorInvalidValue; }
+    maxnx = max(maxnx, J.nx); maxny = max(maxny, J.ny);
+  }
+  a.S = S; a.border = border; a.tw = p.tw; a.th = p.th; a.cw = p.cw;
+  const dim3 grid((maxnx + 31) / 32, (maxny + p.WY * p.K - 1) / (p.WY * p.K), a.njobs);
+  switch(mode)
+  {
+  case QMIV_SSM_REGULAR_GAUSSIAN_FLT:
+    if(N != 11) { return cudaErrorInvalidValue; }
+    a.coef = kCoefFlt11; a.inv = 1.0;
+    return gen_launch_k<kGenFlt, 11>(a, p, grid, s);
+  case QMIV_SSM_REGULAR_GAUSSIAN_INT:
+    if(N != 11) { return cudaErrorInvalidValue; }
+    a.coef = kCoefInt11; a.inv = 1.0 / (double)(1 << 18);          // c_InvFltrIntMul
+    return gen_launch_k<kGenInt, 11>(a, p, grid, s);
+  case QMIV_SSM_REGULAR_AVERAGED:
+    if(N != 11) { return cudaErrorInvalidValue; }
+    a.coef = 0; a.inv = 1.0 / (double)121;                          // c_InvFltrArea
+    return gen_launch_k<kGenAvg, 11>(a, p, grid, s);
+  case QMIV_SSM_BLOCK_GAUSSIAN_INT:
+    a.inv = 1.0 / (double)(1 << 18);
+    if(N == 8) { a.coef = kCoefInt8; return gen_launch_k<kGenInt, 8>(a, p, grid, s); }
+    if(N == 16) { a.coef = kCoefInt16; return gen_launch_k<kGenInt, 16>(a, p, grid, s); }
+    return cudaErrorInvalidValue;
+  case QMIV_SSM_BLOCK_AVERAGED:
+    a.coef = 0; a.inv = 1.0 / (double)(N * N);                      // c_InvBlockArea
+    if(N == 8) { return gen_launch_k<kGenAvg, 8>(a, p, grid, s); }
+    if(N == 16) { return gen_launch_k<kGenAvg, 16>(a, p, grid, s); }
+    if(N == 32) { return gen_launch_k<kGenAvg, 32>(a, p, grid, s); }
+    return cudaErrorInvalidValue;
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T>
+cudaError_t launch_downsample2(const Img& a, const Img& b, const MutImg& da, const MutImg& db, int dw, int dh, uint32_t clip,
+                               cudaStream_t s)
+{
+  if(dw <= 0 || dh <= 0) { return cudaSuccess; }
+  DownArgs d{};
+  d.src[0] = a; d.src[1] = b; d.dst[0] = da; d.dst[1] = db; d.dw = dw; d.dh = dh; d.clip = clip;
+  const dim3 grid((dw + 31) / 32, (dh + 7) / 8, 3);
+  k_downsample2<T><<<grid, 256, 0, s>>>(d);
+  return cudaGetLastError();
+}
+template cudaError_t launch_downsample2<uint8_t>(const Img&, const Img&, const MutImg&, const MutImg&, int, int, uint32_t, cudaStream_t);
+template cudaError_t launch_downsample2<uint16_t>(const Img&, const Img&, const MutImg&, const MutImg&, int, int, uint32_t, cudaStream_t);
+
+}  // namespace qmiv

@@ -51,7 +51,11 @@ def test_params_default_match_reference_defaults():
     assert list(p.cws) == [4, 1, 1, 0] and list(p.cwa) == [4, 1, 1, 0]
     assert [round(x, 6) for x in p.unc] == [0.01, 0.01, 0.01, 0.0]
     assert (p.ssim_window, p.ssim_stride) == (8, 4)
+    assert (p.ssim_mode, p.ssim_border) == (qmiv_b200.SSM_BLOCK_AVERAGED, qmiv_b200.BRD_NONE)
     assert p.invalid_pel_action == qmiv_b200.PEL_STOP
+    # the regular modes take 11x11 windows unless told otherwise
+    q = qmiv_b200.make_params(ssim_mode=qmiv_b200.SSM_REGULAR_GAUSSIAN_FLT, ssim_stride=1)
+    assert (q.ssim_mode, q.ssim_window, q.ssim_stride) == (0, 11, 1)
 
 
 @pytest.mark.skipif(cuda_available(), reason="checks the no-GPU error path")

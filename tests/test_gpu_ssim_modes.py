@@ -1,0 +1,124 @@
+"""Structural similarity options (qmiv_params.ssim_mode / ssim_border / ssim_window / ssim_stride): regular
+11x11 Gaussian float, Gaussian integer and averaged windows with every border extension, block Gaussian
+integer and averaged windows of every size and stride, through SSIM, MS-SSIM, IV-SSIM and IV-MS-SSIM,
+bit-exact against the compiled reference's fixtures and the C restatement."""
+import numpy as np
+import pytest
+
+import oracle
+from golden_cases import case_frames, compare_result, max_ssim_deviation, ssim_mode_ids
+
+pytestmark = pytest.mark.gpu
+
+
+def _calc(qctx, case, **kw):
+    import qmiv_b200
+    return qmiv_b200.Calc(qctx, case["width"], case["height"], case["bitdepth"], case["chroma_format"],
+                          search_range=case["search_range"], erp=case["erp"], ssim_mode=case["ssim_mode"],
+                          ssim_border=case["ssim_border"], ssim_window=case["ssim_window"],
+                          ssim_stride=case["ssim_stride"], **kw)
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("idx", range(len(ssim_mode_ids())), ids=ssim_mode_ids())
+def test_ssim_modes_golden(idx, golden_ssim_modes, qctx):
+    case = golden_ssim_modes[idx]
+    f0, f1 = case_frames(case)
+    with _calc(qctx, case) as calc:
+        got = calc.compute(f0, f1, case["mask"])
+    assert compare_result(got, case["expected"], case["mask"]) == []
+    # the reference's FMA-contracted build moves only the last bits
+    assert max_ssim_deviation(got, case["expected_fma_build"], case["mask"]) < 1e-14
+
+
+@pytest.mark.parametrize("idx", [0, 3, 8, 15, 22], ids=[ssim_mode_ids()[i] for i in [0, 3, 8, 15, 22]])
+def test_ssim_modes_golden_device_frames(idx, golden_ssim_modes, qctx):
+    case = golden_ssim_modes[idx]
+    f0, f1 = case_frames(case)
+    with _calc(qctx, case) as calc:
+        got = calc.compute(tuple(_dev(p) for p in f0), tuple(_dev(p) for p in f1), case["mask"])
+    assert compare_result(got, case["expected"], case["mask"]) == []
+
+
+@pytest.mark.parametrize("shape", [
+    # (W, H, bitdepth, chroma, R, erp, mode, border, window, stride, metrics)
+    (640, 360, 10, 420, 2, True, 0, 0, 11, 1, oracle.ALL),                       # the paper's setting
+    (1920, 1080, 8, 420, 2, False, 0, 0, 11, 4, oracle.SSIM | oracle.MSSSIM),
+    (352, 288, 10, 422, 3, True, 1, 2, 11, 2, oracle.SSIM | oracle.IVSSIM),
+    (500, 260, 12, 444, 2, True, 2, 3, 11, 1, oracle.SSIM | oracle.IVSSIM),
+    (720, 480, 10, 420, 2, False, 3, 0, 16, 3, oracle.SSIM | oracle.IVMSSSIM),
+    (1280, 720, 10, 420, 2, True, 4, 0, 32, 4, oracle.SSIM | oracle.IVSSIM | oracle.MSSSIM),
+    (300, 200, 14, 444, 2, False, 0, 4, 11, 11, oracle.SSIM | oracle.IVSSIM),
+    (256, 256, 8, 420, 1, True, 4, 0, 8, 1, oracle.ALL),
+])
+def test_ssim_modes_against_oracle_seeded(shape, qctx, oracle_lib):
+    """Seeded synthetic frames (the bench's generator) at sizes beyond the fixtures."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    W, H, bd, cf, R, erp, mode, brd, win, st, mask = shape
+    f0, f1 = synth.make_pair(W, H, bd, seed=W * 7 + H, chroma_format=cf)
+    p = oracle.make_params(W, H, bd, cf, search_range=R, erp=erp)
+    exp = oracle_lib.compute_pair_ssim(p, f0, f1, mode, brd, win, st, mask)
+    with qmiv_b200.Calc(qctx, W, H, bd, cf, search_range=R, erp=erp, ssim_mode=mode, ssim_border=brd, ssim_window=win,
+                        ssim_stride=st) as calc:
+        got = calc.compute(f0, f1, mask)
+    exp_enc = {k: ([float(x).hex() for x in v] if isinstance(v, list) and v and isinstance(v[0], float)
+                   else (float(v).hex() if isinstance(v, float) else v)) for k, v in exp.items()}
+    assert compare_result(got, exp_enc, mask) == []
+
+
+@pytest.mark.parametrize("mode,border,window,stride", [(0, 0, 11, 1), (1, 3, 11, 4), (2, 1, 11, 2), (3, 0, 16, 4),
+                                                       (4, 0, 32, 8)])
+def test_ssim_modes_identical_full_size(mode, border, window, stride, qctx):
+    """4096x2048 10-bit 4:2:0 (the IV-PSNR benchmark picture): a picture against itself gives SSIM and
+    MS-SSIM of exactly 1 under every option (each window's numerators equal its denominators, and the
+    compensated sums count the windows exactly); the ERP-weighted IV-SSIM divides a weighted sum by the
+    weight mean times the window count, which rounds to within a few ulp of 1."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    W, H = 4096, 2048
+    f0, _ = synth.make_pair(W, H, 10, seed=11)
+    f0d = tuple(_dev(p) for p in f0)
+    with qmiv_b200.Calc(qctx, W, H, 10, 420, erp=True, ssim_mode=mode, ssim_border=border, ssim_window=window,
+                        ssim_stride=stride) as calc:
+        got = calc.compute(f0d, f0d, qmiv_b200.SSIM | qmiv_b200.IVSSIM | qmiv_b200.MSSSIM)
+    assert list(got["ssim"][:3]) == [1.0, 1.0, 1.0]
+    assert got["msssim_pic"] == 1.0
+    assert abs(got["ivssim"] - 1.0) < 1e-15
+
+
+def test_ssim_mode_refusals(qctx):
+    import qmiv_b200
+    bad = [dict(ssim_mode=0, ssim_window=8), dict(ssim_mode=3, ssim_window=32), dict(ssim_mode=4, ssim_window=8, ssim_stride=0),
+           dict(ssim_mode=4, ssim_window=16, ssim_stride=17), dict(ssim_mode=2, ssim_border=4), dict(ssim_mode=4, ssim_window=12),
+           dict(ssim_mode=5), dict(ssim_mode=0, ssim_border=6)]
+    for kw in bad:
+        with pytest.raises(qmiv_b200.QmivError):
+            qmiv_b200.Calc(qctx, 64, 64, 10, 420, **kw)
+    # a picture smaller than the window
+    with qmiv_b200.Calc(qctx, 40, 24, 8, 420, ssim_mode=4, ssim_window=32) as calc:
+        from qmiv_b200 import synth
+        f0, f1 = synth.make_pair(40, 24, 8, seed=1)
+        with pytest.raises(qmiv_b200.QmivError):
+            calc.compute(f0, f1, qmiv_b200.SSIM)
+        got = calc.compute(f0, f1, qmiv_b200.PSNR)   # the calc still works for the other metrics
+        assert got["psnr_pic"] > 0
+
+
+def test_batched_forms_refuse_other_ssim_options(qctx):
+    """The batched form evaluates the default BlockAveraged 8/4 SSIM only; other options are refused
+    there when an SSIM metric is asked for, and accepted for the PSNR family."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    f0, f1 = synth.make_pair(128, 64, 10, seed=2)
+    pair = dict(frame0=f0, frame1=f1, width=128, height=64, bitdepth=10, chroma_format=420, search_range=2)
+    with qmiv_b200.Batch(qctx, max_pairs=2, max_pixels=128 * 64, ssim_mode=0, ssim_window=11, ssim_stride=1) as b:
+        with pytest.raises(qmiv_b200.QmivError) as ei:
+            b.compute([dict(pair, metrics=qmiv_b200.SSIM)])
+        assert ei.value.status == 2
+        res = b.compute([dict(pair, metrics=qmiv_b200.PSNR | qmiv_b200.IVPSNR)])
+        assert res[0]["ivpsnr"] > 0
