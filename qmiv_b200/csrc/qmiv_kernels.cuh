@@ -117,7 +117,7 @@ struct SsimGenArgs
   int32_t    S, border, coef;   // stride, QMIV_BRD_*, offset of the window's coefficients (set by the launcher)
   double     inv;               // scale of the integer sums: 2^-18, 1 / 121 or 1 / N^2 (set by the launcher)
   int32_t    tw, th, cw;        // tile width / height in samples, columns per phase (set by the launcher)
-  int32_t    pad_;
+  int32_t    wr;                // window rows per CTA of the row-walking form (set by the launcher)
   SsimGenJob job[kGenMaxJobs];
 };
 

@@ -14,13 +14,13 @@
 // roundings (separate multiply and add). The window formula uses separately rounded operations in the
 // reference's order, so every window value equals the portable reference's bit for bit.
 //
-// k_ssim_gen: a CTA of 32 x WY threads stages the samples its windows read, both pictures packed
-// (a | b << 16) in shared memory after clipping and margin extension, then lane l of warp w evaluates
-// window column x0 + l for K consecutive window rows: it walks the input rows the K windows cover, and
-// each sample loaded from shared memory feeds every window whose rows include it. With stride S > 1
-// the tile's columns are stored by phase (column c at (c % S) * cw + c / S), so the 32 lanes of a warp
-// read 32 consecutive words. Window values go to the band-transposed scratch [ny / 32][nx][32] that
-// k_ssim_rows (qmiv_ssim.cu) sums in x order, one lane per window row.
+// Two window kernels, both staging the samples a CTA's windows read in shared memory, both pictures
+// packed (a | b << 16) after clipping and margin extension:
+//   k_ssim_gen_rows (strides 1, 2, 4): each lane evaluates K neighbouring windows of a window row and
+//     walks that row's input rows; a sample loaded once feeds every window that covers it.
+//   k_ssim_gen (other strides): one window per thread.
+// Window values go to the band-transposed scratch [ny / 32][nx][32] that k_ssim_rows (qmiv_ssim.cu)
+// sums in x order, one lane per window row.
 #include "qmiv_host.h"
 
 #include <cmath>
@@ -125,6 +125,9 @@ __device__ __forceinline__ double gen_window(const double (&m)[5], double inv, d
   return dmul(l, cs);
 }
 
+// One window per thread (K = 1) for strides other than 1, 2 and 4: lane l of warp w evaluates window
+// column x0 + l of window row y0 + w. With stride S > 1 the tile's columns are stored by phase (column c
+// at (c % S) * cw + c / S), so the 32 lanes of a warp read 32 consecutive words.
 template <int MODE, int N, int K>
 __global__ void __launch_bounds__(128) k_ssim_gen(const __grid_constant__ SsimGenArgs a)
 {
@@ -235,6 +238,114 @@ __global__ void __launch_bounds__(128) k_ssim_gen(const __grid_constant__ SsimGe
   }
 }
 
+// Row-walking form for strides 1, 2 and 4 (the original paper's and the app's default stride): lane l of
+// warp w evaluates the K windows x0 + l K .. x0 + l K + K - 1 of window rows w, w + 4, ... of the CTA.
+// For each window row it walks the N input rows in order; in input row dy, input column j of the lane's
+// span (j in [0, (K - 1) S + N)) is loaded and converted once and feeds window k as its tap
+// dx = j - k S wherever that lies in [0, N): every (j, k) pair is resolved at compile time, so no
+// instruction is spent on a tap a window does not have, and each window still receives its taps in
+// dy-major, dx-minor order. The N coefficients of row dy are loaded once per row. The tile's columns are
+// stored by phase modulo K S, so the lanes of a warp read consecutive words.
+template <int MODE, int N, int K, int S>
+__global__ void __launch_bounds__(128) k_ssim_gen_rows(const __grid_constant__ SsimGenArgs a)
+{
+  constexpr int KS = K * S;
+  constexpr int J = (K - 1) * S + N;                          // input columns of one lane's windows
+  extern __shared__ uint32_t tile[];                          // [th][KS * cw], sample a | b << 16
+  const SsimGenJob& Jb = a.job[blockIdx.z];
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int WR = a.wr;                                        // window rows per CTA
+  const int wx0 = blockIdx.x * 32 * K, wy0 = blockIdx.y * WR;
+  if(wx0 >= Jb.nx || wy0 >= Jb.ny) { return; }
+  const int cw = a.cw, pitch = KS * cw;
+  const int tw = (min(32 * K, Jb.nx - wx0) - 1) * S + N;
+  const int rows = min(WR, Jb.ny - wy0);
+  const int th = (rows - 1) * S + N;
+  const int X0 = Jb.x0 + wx0 * S, Y0 = Jb.y0 + wy0 * S;
+  const int c = Jb.comp;
+  for(int r = w; r < th; r += blockDim.y)
+  {
+    bool yin;
+    const int yi = brd_map(Y0 + r, Jb.H, a.border, yin);
+    uint32_t* dst = tile + (size_t)r * pitch;
+    for(int col = lane; col < tw; col += 32)
+    {
+      bool xin;
+      const int xi = brd_map(X0 + col, Jb.W, a.border, xin);
+      uint32_t va, vb;
+      if(xin && yin)
+      {
+        if(Jb.esz == 1) { va = (uint32_t)fetch<uint8_t>(Jb.a, c, xi, yi); vb = (uint32_t)fetch<uint8_t>(Jb.b, c, xi, yi); }
+        else { va = (uint32_t)fetch<uint16_t>(Jb.a, c, xi, yi); vb = (uint32_t)fetch<uint16_t>(Jb.b, c, xi, yi); }
+        va = min(va, Jb.clip); vb = min(vb, Jb.clip);
+      }
+      else { va = vb = a.border == QMIV_BRD_CONSTANT ? 0xffffu : 0u; }
+      dst[(col % KS) * cw + col / KS] = va | (vb << 16);
+    }
+  }
+  __syncthreads();
+
+  const int wx = wx0 + lane * K;
+  for(int wr = w; wr < rows; wr += blockDim.y)
+  {
+    double acc[K][5];
+    #pragma unroll
+    for(int k = 0; k < K; k++)
+    {
+      #pragma unroll
+      for(int m = 0; m < 5; m++) { acc[k][m] = 0.0; }
+    }
+    const uint32_t* rowp = tile + (size_t)(wr * S) * pitch + lane;
+    #pragma unroll 1
+    for(int dy = 0; dy < N; dy++, rowp += pitch)
+    {
+      double C[N];
+      if(MODE != kGenAvg)
+      {
+        #pragma unroll
+        for(int dx = 0; dx < N; dx++) { C[dx] = c_gen_coef[a.coef + dy * N + dx]; }
+      }
+      #pragma unroll
+      for(int j = 0; j < J; j++)
+      {
+        const uint32_t v = rowp[(j % KS) * cw + j / KS];
+        const double T = u16_to_f64(v & 0xffffu), R = u16_to_f64(v >> 16);
+        const double RR = dmul(R, R), TT = dmul(T, T), RT = dmul(R, T);   // exact (< 2^32)
+        #pragma unroll
+        for(int k = 0; k < K; k++)
+        {
+          const int dx = j - k * S;
+          if(dx < 0 || dx >= N) { continue; }                 // resolved at compile time
+          if(MODE == kGenAvg)
+          {
+            acc[k][0] = dadd(acc[k][0], R); acc[k][1] = dadd(acc[k][1], T);
+            acc[k][2] = dadd(acc[k][2], RR); acc[k][3] = dadd(acc[k][3], TT); acc[k][4] = dadd(acc[k][4], RT);
+          }
+          else if(MODE == kGenFlt)                            // SumR += R * C, ... (xStructSimSTD.cpp:34-38)
+          {
+            acc[k][0] = dadd(acc[k][0], dmul(R, C[dx])); acc[k][1] = dadd(acc[k][1], dmul(T, C[dx]));
+            acc[k][2] = dadd(acc[k][2], dmul(RR, C[dx])); acc[k][3] = dadd(acc[k][3], dmul(TT, C[dx]));
+            acc[k][4] = dadd(acc[k][4], dmul(RT, C[dx]));
+          }
+          else                                                // exact integers
+          {
+            acc[k][0] = __fma_rn(R, C[dx], acc[k][0]); acc[k][1] = __fma_rn(T, C[dx], acc[k][1]);
+            acc[k][2] = __fma_rn(RR, C[dx], acc[k][2]); acc[k][3] = __fma_rn(TT, C[dx], acc[k][3]);
+            acc[k][4] = __fma_rn(RT, C[dx], acc[k][4]);
+          }
+        }
+      }
+    }
+    const int wy = wy0 + wr;
+    double* out = Jb.win + ((size_t)(wy >> 5) * Jb.nx) * 32 + (wy & 31);
+    #pragma unroll
+    for(int k = 0; k < K; k++)
+    {
+      if(wx + k < Jb.nx) { out[(size_t)(wx + k) * 32] = gen_window<MODE, N>(acc[k], a.inv, Jb.C1, Jb.C2, Jb.calc_l != 0); }
+    }
+  }
+}
+
 // 2x2 mean of both pictures of a pair for the next MS-SSIM scale (xPixelOpsSTD.cpp:50-67), after clipping
 struct DownArgs
 {
@@ -272,39 +383,55 @@ constexpr size_t kGenSmemMax = 200 * 1024;
 struct GenPlan
 {
   int    WY, K;
-  int    tw, th, cw;
+  int    tw, th, cw, wr;
   size_t smem;
 };
 
-// The largest window block (WY warps x K window rows per thread) whose tile fits the preferred shared
-// memory; one window row per thread when even that does not (wide strides of 32x32 windows).
+// Windows per lane of the row-walking form (strides 1, 2, 4): enough that a loaded sample feeds several
+// windows, few enough that the tile of 32 K windows stays small.
+constexpr int rows_k(int S, int N) { return S == 1 ? 8 : (S == 2 || N < 32) ? 4 : 2; }
+
+// Launch shape of either form: the row-walking form for strides 1, 2 and 4 with as many window rows per
+// CTA as fit 96 KB of tile; one window per thread otherwise (every tap of a thread's window is its own,
+// so no instruction is spent on taps a window does not have).
 bool gen_plan(int N, int S, GenPlan& p)
 {
-  static const int kShapes[6][2] = { { 4, 8 }, { 2, 8 }, { 4, 2 }, { 2, 2 }, { 1, 2 }, { 1, 1 } };
-  for(int i = 0; i < 6; i++)
+  if(S == 1 || S == 2 || S == 4)
   {
-    p.WY = kShapes[i][0]; p.K = kShapes[i][1];
-    p.tw = 31 * S + N;
-    p.th = (p.WY * p.K - 1) * S + N;
-    p.cw = (p.tw + S - 1) / S;
-    p.smem = (size_t)p.th * S * p.cw * sizeof(uint32_t);
-    if(p.smem <= kGenSmemPreferred) { return true; }
+    const int K = rows_k(S, N), KS = K * S;
+    p.K = K; p.WY = 4;
+    p.tw = (32 * K - 1) * S + N;
+    p.cw = (p.tw + KS - 1) / KS;
+    for(int wr = 32; wr >= 4; wr >>= 1)
+    {
+      p.wr = wr;
+      p.th = (wr - 1) * S + N;
+      p.smem = (size_t)p.th * KS * p.cw * sizeof(uint32_t);
+      if(p.smem <= kGenSmemPreferred) { return true; }
+    }
+    return p.smem <= kGenSmemMax;
   }
+  p.K = 1; p.WY = 4; p.wr = 0;
+  p.tw = 31 * S + N;
+  p.th = (p.WY - 1) * S + N;
+  p.cw = (p.tw + S - 1) / S;
+  p.smem = (size_t)p.th * S * p.cw * sizeof(uint32_t);
   return p.smem <= kGenSmemMax;
 }
 
-template <int MODE, int N, int K>
-cudaError_t gen_attr()
+template <int MODE, int N, int S>
+cudaError_t gen_attr_rows()
 {
-  return cudaFuncSetAttribute(k_ssim_gen<MODE, N, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmemMax);
+  return cudaFuncSetAttribute(k_ssim_gen_rows<MODE, N, rows_k(S, N), S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmemMax);
 }
 
 template <int MODE, int N>
-cudaError_t gen_attr_k()
+cudaError_t gen_attr_all()
 {
-  cudaError_t e = gen_attr<MODE, N, 8>();
-  if(e == cudaSuccess) { e = gen_attr<MODE, N, 2>(); }
-  if(e == cudaSuccess) { e = gen_attr<MODE, N, 1>(); }
+  cudaError_t e = cudaFuncSetAttribute(k_ssim_gen<MODE, N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmemMax);
+  if(e == cudaSuccess) { e = gen_attr_rows<MODE, N, 1>(); }
+  if(e == cudaSuccess) { e = gen_attr_rows<MODE, N, 2>(); }
+  if(e == cudaSuccess) { e = gen_attr_rows<MODE, N, 4>(); }
   return e;
 }
 
@@ -322,25 +449,34 @@ cudaError_t gen_configure()
   double c[kCoefTotal];
   build_coefs(c);
   e = cudaMemcpyToSymbol(c_gen_coef, c, sizeof(c));
-  if(e == cudaSuccess) { e = gen_attr_k<kGenFlt, 11>(); }
-  if(e == cudaSuccess) { e = gen_attr_k<kGenInt, 11>(); }
-  if(e == cudaSuccess) { e = gen_attr_k<kGenInt, 8>(); }
-  if(e == cudaSuccess) { e = gen_attr_k<kGenInt, 16>(); }
-  if(e == cudaSuccess) { e = gen_attr_k<kGenAvg, 11>(); }
-  if(e == cudaSuccess) { e = gen_attr_k<kGenAvg, 8>(); }
-  if(e == cudaSuccess) { e = gen_attr_k<kGenAvg, 16>(); }
-  if(e == cudaSuccess) { e = gen_attr_k<kGenAvg, 32>(); }
+  if(e == cudaSuccess) { e = gen_attr_all<kGenFlt, 11>(); }
+  if(e == cudaSuccess) { e = gen_attr_all<kGenInt, 11>(); }
+  if(e == cudaSuccess) { e = gen_attr_all<kGenInt, 8>(); }
+  if(e == cudaSuccess) { e = gen_attr_all<kGenInt, 16>(); }
+  if(e == cudaSuccess) { e = gen_attr_all<kGenAvg, 11>(); }
+  if(e == cudaSuccess) { e = gen_attr_all<kGenAvg, 8>(); }
+  if(e == cudaSuccess) { e = gen_attr_all<kGenAvg, 16>(); }
+  if(e == cudaSuccess) { e = gen_attr_all<kGenAvg, 32>(); }
   if(e == cudaSuccess) { done |= bit; }
   return e;
 }
 
 template <int MODE, int N>
-cudaError_t gen_launch_k(const SsimGenArgs& a, const GenPlan& p, dim3 grid, cudaStream_t s)
+cudaError_t gen_launch_k(const SsimGenArgs& a, const GenPlan& p, int S, int maxnx, int maxny, cudaStream_t s)
 {
   const dim3 block(32, p.WY);
-  if(p.K == 8) { k_ssim_gen<MODE, N, 8><<<grid, block, p.smem, s>>>(a); }
-  else if(p.K == 2) { k_ssim_gen<MODE, N, 2><<<grid, block, p.smem, s>>>(a); }
-  else { k_ssim_gen<MODE, N, 1><<<grid, block, p.smem, s>>>(a); }
+  if(p.wr > 0)
+  {
+    const dim3 grid((maxnx + 32 * p.K - 1) / (32 * p.K), (maxny + p.wr - 1) / p.wr, a.njobs);
+    if(S == 1) { k_ssim_gen_rows<MODE, N, rows_k(1, N), 1><<<grid, block, p.smem, s>>>(a); }
+    else if(S == 2) { k_ssim_gen_rows<MODE, N, rows_k(2, N), 2><<<grid, block, p.smem, s>>>(a); }
+    else { k_ssim_gen_rows<MODE, N, rows_k(4, N), 4><<<grid, block, p.smem, s>>>(a); }
+  }
+  else
+  {
+    const dim3 grid((maxnx + 31) / 32, (maxny + p.WY - 1) / p.WY, a.njobs);
+    k_ssim_gen<MODE, N, 1><<<grid, block, p.smem, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
@@ -361,32 +497,31 @@ cudaError_t launch_ssim_gen(SsimGenArgs& a, int mode, int N, int S, int border, 
     if(J.nx < 1 || J.ny < 1 || !J.win || (J.esz != 1 && J.esz != 2)) { return cudaErrorInvalidValue; }
     maxnx = max(maxnx, J.nx); maxny = max(maxny, J.ny);
   }
-  a.S = S; a.border = border; a.tw = p.tw; a.th = p.th; a.cw = p.cw;
-  const dim3 grid((maxnx + 31) / 32, (maxny + p.WY * p.K - 1) / (p.WY * p.K), a.njobs);
+  a.S = S; a.border = border; a.tw = p.tw; a.th = p.th; a.cw = p.cw; a.wr = p.wr;
   switch(mode)
   {
   case QMIV_SSM_REGULAR_GAUSSIAN_FLT:
     if(N != 11) { return cudaErrorInvalidValue; }
     a.coef = kCoefFlt11; a.inv = 1.0;
-    return gen_launch_k<kGenFlt, 11>(a, p, grid, s);
+    return gen_launch_k<kGenFlt, 11>(a, p, S, maxnx, maxny, s);
   case QMIV_SSM_REGULAR_GAUSSIAN_INT:
     if(N != 11) { return cudaErrorInvalidValue; }
     a.coef = kCoefInt11; a.inv = 1.0 / (double)(1 << 18);          // c_InvFltrIntMul
-    return gen_launch_k<kGenInt, 11>(a, p, grid, s);
+    return gen_launch_k<kGenInt, 11>(a, p, S, maxnx, maxny, s);
   case QMIV_SSM_REGULAR_AVERAGED:
     if(N != 11) { return cudaErrorInvalidValue; }
     a.coef = 0; a.inv = 1.0 / (double)121;                          // c_InvFltrArea
-    return gen_launch_k<kGenAvg, 11>(a, p, grid, s);
+    return gen_launch_k<kGenAvg, 11>(a, p, S, maxnx, maxny, s);
   case QMIV_SSM_BLOCK_GAUSSIAN_INT:
     a.inv = 1.0 / (double)(1 << 18);
-    if(N == 8) { a.coef = kCoefInt8; return gen_launch_k<kGenInt, 8>(a, p, grid, s); }
-    if(N == 16) { a.coef = kCoefInt16; return gen_launch_k<kGenInt, 16>(a, p, grid, s); }
+    if(N == 8) { a.coef = kCoefInt8; return gen_launch_k<kGenInt, 8>(a, p, S, maxnx, maxny, s); }
+    if(N == 16) { a.coef = kCoefInt16; return gen_launch_k<kGenInt, 16>(a, p, S, maxnx, maxny, s); }
     return cudaErrorInvalidValue;
   case QMIV_SSM_BLOCK_AVERAGED:
     a.coef = 0; a.inv = 1.0 / (double)(N * N);                      // c_InvBlockArea
-    if(N == 8) { return gen_launch_k<kGenAvg, 8>(a, p, grid, s); }
-    if(N == 16) { return gen_launch_k<kGenAvg, 16>(a, p, grid, s); }
-    if(N == 32) { return gen_launch_k<kGenAvg, 32>(a, p, grid, s); }
+    if(N == 8) { return gen_launch_k<kGenAvg, 8>(a, p, S, maxnx, maxny, s); }
+    if(N == 16) { return gen_launch_k<kGenAvg, 16>(a, p, S, maxnx, maxny, s); }
+    if(N == 32) { return gen_launch_k<kGenAvg, 32>(a, p, S, maxnx, maxny, s); }
     return cudaErrorInvalidValue;
   default: return cudaErrorInvalidValue;
   }
