@@ -345,6 +345,7 @@ def run_qmiv(args, world, rank, local):
     mixed = run_mixed(ctx, max(3, args.steps // 4)) if (world == 1 and not args.no_mixed) else None
     serve = run_serve(ctx, args.serve_seconds) if (world == 1 and args.serve_seconds > 0) else None
     masked = run_masked(ctx, max(3, args.steps // 4)) if (world == 1 and not args.no_masked) else None
+    ssim_modes = run_ssim_modes(ctx, max(3, args.steps // 4)) if (world == 1 and not args.no_ssim_modes) else None
 
     # ---- probes for the search kernel's roofline denominator ----
     lib = qmiv_b200.library()
@@ -366,7 +367,7 @@ def run_qmiv(args, world, rank, local):
     return dict(value=value, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
                 achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
                 sample=results[0], launches=int(round(launches_per_step * args.steps)), plain=plain_value,
-                cps_tile=cps_tile, mixed=mixed, serve=serve, masked=masked)
+                cps_tile=cps_tile, mixed=mixed, serve=serve, masked=masked, ssim_modes=ssim_modes)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -456,6 +457,85 @@ def run_reference_masked(threads, seed=77, reps=2):
     return {"value": 1.0 / secs, "secs": secs, "threads": threads, "ivpsnr": r["ivpsnr"]}
 
 
+# structural similarity options measured besides the default (BlockAveraged 8/4): (name, mode, border,
+# window, stride); the first is the original paper's SSIM (11x11 Gaussian, every pixel)
+SSIM_OPTIONS = [("RegularGaussianFlt/None/11/1", 0, 0, 11, 1), ("RegularGaussianInt/None/11/1", 1, 0, 11, 1),
+                ("BlockAveraged/None/16/4", 4, 0, 16, 4)]
+
+
+def ssim_option_windows(mode, window, stride):
+    """Windows of one SSIM evaluation of a 4:4:4 picture of W x H (all three components)."""
+    if mode <= 2:
+        nx, ny = (W - 10 + stride - 1) // stride, (H - 10 + stride - 1) // stride
+    else:
+        nx, ny = (W - window) // stride + 1, (H - window) // stride + 1
+    return 3 * nx * ny
+
+
+def run_ssim_modes(ctx, steps):
+    """SSIM + IV-SSIM (ERP) of one 4096x2048 10-bit 4:2:0 pair per call under other structural similarity
+    options, device frames, with the window kernel's FP64 rate against the FP64 multiply/add rate
+    measured on this GPU by qmiv_probe_fp64_peak."""
+    import ctypes
+    import torch
+    import qmiv_b200
+    from qmiv_b200 import _lib, synth
+    f0, f1 = synth.make_pair(W, H, BD, seed=91)
+    d0 = tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in f0)
+    d1 = tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in f1)
+    mask = qmiv_b200.SSIM | qmiv_b200.IVSSIM
+    peak = ctypes.c_double()
+    _lib.check(qmiv_b200.library().qmiv_probe_fp64_peak(ctx.device, 4096, ctypes.byref(peak)), "probe")
+    out = {"what": "SSIM + IV-SSIM (ERP) of one 4096x2048 10-bit 4:2:0 pair per synchronous call, device frames",
+           "fp64_peak_tops": peak.value, "options": []}
+    for name, mode, border, window, stride in SSIM_OPTIONS:
+        with qmiv_b200.Calc(ctx, W, H, BD, CF, search_range=2, erp=True, ssim_mode=mode, ssim_border=border,
+                            ssim_window=window, ssim_stride=stride) as calc:
+            for _ in range(3):
+                r = calc.compute(d0, d1, mask)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                r = calc.compute(d0, d1, mask)
+            dt = (time.perf_counter() - t0) / steps
+            ctx.stage_times(reset=True)
+            ctx.set_profiling(True)
+            for _ in range(steps):
+                calc.compute(d0, d1, mask)
+            ctx.set_profiling(False)
+            st = ctx.stage_times(reset=True)
+        win_ms, win_n = st["ssim_win"]
+        # one window launch evaluates SSIM (In0, In1) and IV-SSIM (In0, SCP1), (In1, SCP0): 3 evaluations
+        windows = 3 * ssim_option_windows(mode, window, stride)
+        n = 11 if mode <= 2 else window
+        ops_per_window = n * n * (10 if mode == 0 else 5)   # float Gaussian: multiply + add per moment and tap
+        avg_ms = win_ms / max(win_n, 1)
+        achieved = windows * ops_per_window / (avg_ms * 1e-3) / 1e12
+        out["options"].append({"option": name, "value": 1.0 / dt, "unit": "frame-pairs/s", "ms_per_pair": dt * 1e3,
+                               "ssim_pic": r["ssim_pic"], "ivssim": r["ivssim"],
+                               "window_kernel": {"avg_launch_ms": avg_ms, "windows_per_launch": windows,
+                                                 "fp64_ops_per_window": ops_per_window, "achieved_tops": achieved,
+                                                 "frac": achieved / peak.value if peak.value else None}})
+    return out
+
+
+def run_reference_ssim_option(threads, option, seed=91):
+    """The same pair and metrics through the reference library (oracle/_ref, xSSIM / xIVSSIM with
+    setStructSimParams) with a thread pool of `threads`: frame-pairs/s of one call."""
+    import oracle
+    from qmiv_b200 import synth
+    if not oracle.reference_available():
+        return None
+    _, mode, border, window, stride = option
+    ref = oracle.Reference()
+    a, b = synth.make_pair(W, H, BD, seed=seed)
+    p = oracle.make_params(W, H, BD, CF, search_range=2, erp=True, num_threads=threads)
+    t0 = time.perf_counter()
+    r = ref.compute_pair_ssim(p, a, b, mode, border, window, stride, oracle.SSIM | oracle.IVSSIM)
+    secs = time.perf_counter() - t0
+    return {"value": 1.0 / secs, "secs": secs, "threads": threads, "ivssim": r["ivssim"], "ssim_pic": r["ssim_pic"]}
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -474,6 +554,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the plain-vs-batched mixed-resolution comparison")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="length of the serving-loop arrival stream (0: skip)")
     ap.add_argument("--no-masked", action="store_true", help="skip the mask-mode measurement")
+    ap.add_argument("--no-ssim-modes", action="store_true", help="skip the structural similarity option measurement")
     ap.add_argument("--size", default=None, help="WxH of a smaller profiling case (not a bench line)")
     ap.add_argument("--pairs", type=int, default=None, help="pairs per step of a smaller profiling case")
     args = ap.parse_args()
@@ -544,6 +625,16 @@ def main():
                         f"(oracle/_ref, {cm['threads']} pool threads), {cm['secs']:.2f} s per pair"}
             except Exception as e:
                 log("masked cpu baseline failed:", e)
+        if r["ssim_modes"] is not None:
+            try:
+                cs = run_reference_ssim_option(host_threads(), SSIM_OPTIONS[0])
+                if cs:
+                    r["ssim_modes"]["options"][0]["cpu_reference"] = {
+                        "value": cs["value"], "unit": "frame-pairs/s", "cores": cs["threads"], "ivssim": cs["ivssim"],
+                        "kind": "reference", "sample": "the same pair through the reference library's xSSIM / xIVSSIM "
+                        f"(oracle/_ref, {cs['threads']} pool threads), {cs['secs']:.2f} s per pair"}
+            except Exception as e:
+                log("ssim option cpu baseline failed:", e)
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -573,6 +664,7 @@ def main():
            "mixed_set": r["mixed"],
            "serve": r["serve"],
            "masked_mode": r["masked"],
+           "ssim_modes": r["ssim_modes"],
            "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
            "clocks": r["clocks"],
            "cpu_baseline": cpu,
