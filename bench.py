@@ -174,7 +174,9 @@ def run_serve(ctx, duration_s, rate=200.0):
     pool = frame_pool([s for r in reqs for s in r.specs])
     sctx = qmiv_b200.Context(ctx.device, hbm_budget=40 << 30)
     srv = qmiv_b200.Server(sctx, max_batch_pairs=64, max_batch_pixels=64 * 4096 * 2048, workers=2)
-    # warm-up: every (shape, R) kind once, so kernels are configured and tiles tuned before the stream
+    # warm-up: every (shape, R) kind once, so kernels are configured and tiles tuned before the stream,
+    # then two concurrent requests of the largest size, so that both workers' device scratch has grown
+    # to a full batch before the stream (a server reserves its working memory at start-up)
     seen = set()
     for r in reqs:
         s0 = r.specs[0]
@@ -182,6 +184,10 @@ def run_serve(ctx, duration_s, rate=200.0):
         if k not in seen:
             seen.add(k)
             srv.wait(srv.submit([pool[k[:3]]], *k[:3], search_range=k[3], metrics=r.metrics))
+    big = max(seen, key=lambda k: k[0] * k[1] * k[2] * (2 * k[3] + 1))
+    warm = [srv.submit([pool[big[:3]]] * 32, *big[:3], search_range=big[3], metrics=big[4]) for _ in range(2)]
+    for t in warm:
+        srv.wait(t)
     srv.stats(reset=True)
     tickets = []
     t0 = time.perf_counter()

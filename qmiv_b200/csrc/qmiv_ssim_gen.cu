@@ -96,6 +96,48 @@ __device__ __forceinline__ int brd_map(int i, int n, int border, bool& in)
 
 }  // namespace
 
+// Stages rows r0, r0 + rstep, ... < th of the tile: tile column col holds input column X0 + col of both
+// pictures (a | b << 16), after conceal clipping and margin extension; idx(col) is its word in the row.
+// Rows read through row pointers; columns map through the margin only where the tile crosses the
+// picture's left or right edge.
+template <typename IDX>
+__device__ __forceinline__ void stage_tile(const SsimGenJob& J, int border, int X0, int Y0, int tw, int th, int r0, int rstep,
+                                           int lane, uint32_t* tile, int pitch, IDX idx)
+{
+  const int c = J.comp;
+  const bool x_inside = X0 >= 0 && X0 + tw <= J.W;
+  const uint32_t fill = border == QMIV_BRD_CONSTANT ? 0xffffu : 0u;
+  const int sxa = J.a.sx[c], sxb = J.b.sx[c];
+  for(int r = r0; r < th; r += rstep)
+  {
+    bool yin;
+    const int yi = brd_map(Y0 + r, J.H, border, yin);
+    uint32_t* dst = tile + (size_t)r * pitch;
+    const size_t oa = (size_t)(yi >> J.a.sy[c]) * J.a.pitch[c], ob = (size_t)(yi >> J.b.sy[c]) * J.b.pitch[c];
+    for(int col = lane; col < tw; col += 32)
+    {
+      bool xin = true;
+      const int xi = x_inside ? X0 + col : brd_map(X0 + col, J.W, border, xin);
+      uint32_t va = fill, vb = fill;   // the margin constant is not clipped
+      if(xin && yin)
+      {
+        if(J.esz == 1)
+        {
+          va = __ldg(static_cast<const uint8_t*>(J.a.p[c]) + oa + (xi >> sxa));
+          vb = __ldg(static_cast<const uint8_t*>(J.b.p[c]) + ob + (xi >> sxb));
+        }
+        else
+        {
+          va = __ldg(static_cast<const uint16_t*>(J.a.p[c]) + oa + (xi >> sxa));
+          vb = __ldg(static_cast<const uint16_t*>(J.b.p[c]) + ob + (xi >> sxb));
+        }
+        va = min(va, J.clip); vb = min(vb, J.clip);
+      }
+      dst[idx(col)] = va | (vb << 16);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // window kernel
 // ---------------------------------------------------------------------------------------------
@@ -141,28 +183,7 @@ __global__ void __launch_bounds__(128) k_ssim_gen(const __grid_constant__ SsimGe
   const int tw = (min(32, J.nx - wx0) - 1) * S + N;
   const int th = (min(WY * K, J.ny - wy0) - 1) * S + N;
   const int X0 = J.x0 + wx0 * S, Y0 = J.y0 + wy0 * S;
-  const int c = J.comp;
-  for(int r = w; r < th; r += WY)
-  {
-    bool yin;
-    const int yi = brd_map(Y0 + r, J.H, a.border, yin);
-    uint32_t* dst = tile + (size_t)r * pitch;
-    for(int col = lane; col < tw; col += 32)
-    {
-      bool xin;
-      const int xi = brd_map(X0 + col, J.W, a.border, xin);
-      uint32_t va, vb;
-      if(xin && yin)
-      {
-        if(J.esz == 1) { va = (uint32_t)fetch<uint8_t>(J.a, c, xi, yi); vb = (uint32_t)fetch<uint8_t>(J.b, c, xi, yi); }
-        else { va = (uint32_t)fetch<uint16_t>(J.a, c, xi, yi); vb = (uint32_t)fetch<uint16_t>(J.b, c, xi, yi); }
-        va = min(va, J.clip); vb = min(vb, J.clip);
-      }
-      else { va = vb = a.border == QMIV_BRD_CONSTANT ? 0xffffu : 0u; }
-      const int q = col / S;
-      dst[(col - q * S) * a.cw + q] = va | (vb << 16);
-    }
-  }
+  stage_tile(J, a.border, X0, Y0, tw, th, w, WY, lane, tile, pitch, [S, cw = a.cw](int col) { const int q = col / S; return (col - q * S) * cw + q; });
   __syncthreads();
 
   int co[N];                                                  // tile column of tap dx for this lane
@@ -262,27 +283,7 @@ __global__ void __launch_bounds__(128) k_ssim_gen_rows(const __grid_constant__ S
   const int rows = min(WR, Jb.ny - wy0);
   const int th = (rows - 1) * S + N;
   const int X0 = Jb.x0 + wx0 * S, Y0 = Jb.y0 + wy0 * S;
-  const int c = Jb.comp;
-  for(int r = w; r < th; r += blockDim.y)
-  {
-    bool yin;
-    const int yi = brd_map(Y0 + r, Jb.H, a.border, yin);
-    uint32_t* dst = tile + (size_t)r * pitch;
-    for(int col = lane; col < tw; col += 32)
-    {
-      bool xin;
-      const int xi = brd_map(X0 + col, Jb.W, a.border, xin);
-      uint32_t va, vb;
-      if(xin && yin)
-      {
-        if(Jb.esz == 1) { va = (uint32_t)fetch<uint8_t>(Jb.a, c, xi, yi); vb = (uint32_t)fetch<uint8_t>(Jb.b, c, xi, yi); }
-        else { va = (uint32_t)fetch<uint16_t>(Jb.a, c, xi, yi); vb = (uint32_t)fetch<uint16_t>(Jb.b, c, xi, yi); }
-        va = min(va, Jb.clip); vb = min(vb, Jb.clip);
-      }
-      else { va = vb = a.border == QMIV_BRD_CONSTANT ? 0xffffu : 0u; }
-      dst[(col % KS) * cw + col / KS] = va | (vb << 16);
-    }
-  }
+  stage_tile(Jb, a.border, X0, Y0, tw, th, w, blockDim.y, lane, tile, pitch, [cw](int col) { return (col % KS) * cw + col / KS; });
   __syncthreads();
 
   const int wx = wx0 + lane * K;
