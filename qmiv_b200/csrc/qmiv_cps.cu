@@ -47,6 +47,8 @@ namespace {
 
 constexpr float    kBias     = 8388608.0f;   // 2^23
 constexpr uint32_t kKeyBase  = 0x49800000u;  // bit pattern of 2^20f
+// 128, the key's scale, read from constant memory so that the key is one integer multiply-add
+__constant__ uint32_t c_key_scale = 128u;
 constexpr uint32_t kBiasBits = 0x4B000000u;  // bit pattern of 2^23f
 constexpr unsigned kFull     = 0xffffffffu;
 constexpr long long kWaitCycles = 1LL << 31; // bound of one tile-load wait (about a second)
@@ -306,7 +308,7 @@ __device__ __forceinline__ void search_fp32(const Thr& th, const float4* tst, co
   const float4* rb = ref + at_hx<R, WY>(th.y0, th.hx, 0);
   auto key = [&](const float4& r, int p, uint32_t k) -> uint32_t {
     const float e = fmaf(c2[p], r.z, fmaf(c1[p], r.y, fmaf(c0[p], r.x, r.w)));
-    return (__float_as_uint(e) << 7) + k;
+    return __float_as_uint(e) * c_key_scale + k;
   };
   #pragma unroll
   for(int ry = 0; ry < 4 + 2 * R; ry++)
