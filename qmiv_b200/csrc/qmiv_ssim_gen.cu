@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(256) k_downsample2(const __grid_constant__ Dow
 // ---------------------------------------------------------------------------------------------
 namespace {
 
-constexpr size_t kGenSmemPreferred = 96 * 1024;   // two CTAs per SM
+constexpr size_t kGenSmemPreferred = 48 * 1024;   // four CTAs per SM: the staging of one hides behind the others
 constexpr size_t kGenSmemMax = 200 * 1024;
 
 struct GenPlan
@@ -393,7 +393,7 @@ struct GenPlan
 constexpr int rows_k(int S, int N) { return S == 1 ? 8 : (S == 2 || N < 32) ? 4 : 2; }
 
 // Launch shape of either form: the row-walking form for strides 1, 2 and 4 with as many window rows per
-// CTA as fit 96 KB of tile; one window per thread otherwise (every tap of a thread's window is its own,
+// CTA as fit 48 KB of tile; one window per thread otherwise (every tap of a thread's window is its own,
 // so no instruction is spent on taps a window does not have).
 bool gen_plan(int N, int S, GenPlan& p)
 {
