@@ -36,15 +36,44 @@ __device__ __forceinline__ void prepass_body(const PrepassArgs& a, int warp)
   int64_t  sd  = 0;
   uint64_t ssd = 0;
   uint32_t m0 = 0, m1 = 0;
-  for(int x = lane; x < n; x += 32)
-  {
-    uint32_t v0 = __ldg(p0 + x), v1 = __ldg(p1 + x);
+  auto sample = [&](uint32_t v0, uint32_t v1) {
     m0 = max(m0, v0); m1 = max(m1, v1);
     v0 = min(v0, a.clip); v1 = min(v1, a.clip);
     const int32_t d = (int32_t)v1 - (int32_t)v0;
     sd  += d;
-    ssd += (uint64_t)((int64_t)d * d);
+    ssd += (uint32_t)d * (uint32_t)d;                    // d^2 < 2^32 for 16-bit samples
+  };
+  // 16-byte loads where both rows allow them (each lane then holds 8 or 16 samples of each frame in
+  // flight), the rest of the row sample by sample
+  int x0 = 0;
+  if((((uintptr_t)p0 | (uintptr_t)p1) & 15) == 0)
+  {
+    constexpr int V = 16 / (int)sizeof(T);
+    const int nv = n / V;
+    const uint4* q0 = reinterpret_cast<const uint4*>(p0);
+    const uint4* q1 = reinterpret_cast<const uint4*>(p1);
+    for(int v = lane; v < nv; v += 32)
+    {
+      const uint4 A = __ldg(q0 + v), B = __ldg(q1 + v);
+      const uint32_t wa[4] = { A.x, A.y, A.z, A.w }, wb[4] = { B.x, B.y, B.z, B.w };
+      #pragma unroll
+      for(int k = 0; k < 4; k++)
+      {
+        if(sizeof(T) == 2)
+        {
+          sample(wa[k] & 0xffffu, wb[k] & 0xffffu);
+          sample(wa[k] >> 16, wb[k] >> 16);
+        }
+        else
+        {
+          #pragma unroll
+          for(int b = 0; b < 4; b++) { sample((wa[k] >> (8 * b)) & 0xffu, (wb[k] >> (8 * b)) & 0xffu); }
+        }
+      }
+    }
+    x0 = nv * V;
   }
+  for(int x = x0 + lane; x < n; x += 32) { sample(__ldg(p0 + x), __ldg(p1 + x)); }
   #pragma unroll
   for(int o = 16; o > 0; o >>= 1)
   {
