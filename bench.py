@@ -294,8 +294,30 @@ def run_qmiv(args, world, rank, local):
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
-    ms = ev0.elapsed_time(ev1)
-    ms_max = max_over_ranks(ms, world, local)
+    ms_sync = max_over_ranks(ev0.elapsed_time(ev1), world, local)
+
+    # ---- the same steps with two batches in flight (qmiv_batch_submit / qmiv_batch_wait on two engines
+    # and streams): one step's serial pooling chains overlap the next step's search. Every step still
+    # computes all of its pairs; the results are checked against the synchronous run. ----
+    for _ in range(2):
+        ta, tb = batch.submit(dev_desc), batch.submit(dev_desc)
+        batch.wait(ta)
+        batch.wait(tb)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        ticket = batch.submit(dev_desc)
+        for _ in range(args.steps - 1):
+            nxt = batch.submit(dev_desc)
+            assert batch.wait(ticket) == results, "pipelined and synchronous batches differ"
+            ticket = nxt
+        assert batch.wait(ticket) == results, "pipelined and synchronous batches differ"
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    ms_max = max_over_ranks(ev0.elapsed_time(ev1), world, local)
 
     # ---- per-stage kernel times: the same steps with the library's stage timers (CUDA events on the
     # batch stream around every stage's launch; graphs are not replayed while the timers are on) ----
@@ -370,7 +392,8 @@ def run_qmiv(args, world, rank, local):
     achieved = ops_per_launch / (cps_avg_ms * 1e-3) / 1e12
     h2d = sum(frame_bytes(a) + frame_bytes(b) for a, b in pairs)
     d2h = PAIRS_PER_STEP * 632  # sizeof(PairOut), the device result block read back per pair
-    return dict(value=value, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
+    value_sync = units / (ms_sync / 1e3)
+    return dict(value=value, value_sync=value_sync, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
                 achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
                 sample=results[0], launches=int(round(launches_per_step * args.steps)), plain=plain_value,
                 cps_tile=cps_tile, mixed=mixed, serve=serve, masked=masked, ssim_modes=ssim_modes)
@@ -665,6 +688,8 @@ def main():
                         "avg_launch_ms": r["cps_avg_ms"],
                         "tile": {"w": r["cps_tile"][0], "h": r["cps_tile"][1], "pixels_per_thread": 8,
                                  "picked_by": "autotuner (qmiv_batch_tuning)"}},
+           "one_batch_in_flight": {"value": r["value_sync"], "unit": "frame-pairs/s",
+                                   "what": "the same steps with one synchronous qmiv_batch_compute each"},
            "plain_form": {"value": r["plain"], "unit": "frame-pairs/s",
                           "what": "the same pairs, one qmiv_frame_pair_compute call per pair (device frames)"},
            "mixed_set": r["mixed"],
