@@ -114,7 +114,8 @@ typedef struct qmiv_server_s* qmiv_server;
    R=2, weights 4:1:1:0 (xCorrespPixelShiftPrms.h:22-24), unnoticeable coef 0.01 (xGlobClrDiff.h:20),
    BlockAveraged SSIM with 8x8 windows at stride 4 and no border extension (xSSIM.h:35-37), no ERP,
    STOP on invalid pixels. The SSIM options follow xSSIM::setStructSimParams (xSSIM.cpp:86-113) with
-   the app's checks (xAppQMIV.cpp:325-332); the batched and serving forms run the default options only. */
+   the app's checks (xAppQMIV.cpp:325-332). The batched and serving forms compute SSIM metrics under a
+   non-default option pair by pair after the batch (the qmiv_calc path); every other metric batched. */
 typedef struct qmiv_params
 {
   int32_t search_range;        /* 1..5 */

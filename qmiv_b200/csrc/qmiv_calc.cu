@@ -85,16 +85,6 @@ void ssim_line(const qmiv_params& p, int32_t len, int32_t& first_sample, int32_t
   }
 }
 
-qmiv_status check_batched_ssim(const qmiv_params& p, uint32_t mask)
-{
-  if((mask & kSsimFamily) && !ssim_is_default(p))
-  {
-    return fail(QMIV_ERR_UNSUPPORTED, "the batched and serving forms compute SSIM with BlockAveraged 8x8 windows at stride 4 only; "
-                                      "other structural similarity options run through qmiv_calc");
-  }
-  return QMIV_OK;
-}
-
 // ---------------------------------------------------------------------------------------------
 // PairPipeline
 // ---------------------------------------------------------------------------------------------

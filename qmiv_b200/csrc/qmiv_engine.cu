@@ -232,6 +232,7 @@ qmiv_status Engine::submit(const qmiv_pair_desc* pairs, int32_t n)
 
   // ---- per-pair kinds, masks, arena layout ---------------------------------------------------
   std::vector<PairKind*> kind(n);
+  std::vector<int> gen_idx;
   std::vector<PairSlot>& P = slots_;
   P.assign(n, PairSlot{});
   std::string sig;
@@ -244,10 +245,21 @@ qmiv_status Engine::submit(const qmiv_pair_desc* pairs, int32_t n)
     const qmiv_pair_desc& d = pairs[i];
     QMIV_TRY(kind_for(d, kind[i]));
     QMIV_TRY(check_metrics(kind[i]->S, d.metric_mask));
-    QMIV_TRY(check_batched_ssim(prm_, d.metric_mask));
     PairSlot& p = P[i];
     const Shape& S = kind[i]->S;
     p.mask = d.metric_mask;
+    if(!ssim_is_default(prm_) && (p.mask & kSsimFamily))
+    {
+      int32_t f, nx, ny;
+      ssim_line(prm_, S.W, f, nx);
+      ssim_line(prm_, S.H, f, ny);
+      if(S.W < ssim_window_size(prm_) || S.H < ssim_window_size(prm_) || nx < 1 || ny < 1)
+      {
+        return fail(QMIV_ERR_INVALID_ARG, "picture smaller than one SSIM window");
+      }
+      gen_idx.push_back(i);
+      p.mask &= ~kSsimFamily;
+    }
     p.need_scp = (p.mask & QMIV_IVMSSSIM) != 0;
     p.need_search = p.need_scp || (p.mask & (QMIV_IVPSNR | QMIV_IVSSIM));
     p.need_ssim = (p.mask & (QMIV_SSIM | QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM)) != 0;
@@ -458,6 +470,9 @@ qmiv_status Engine::submit(const qmiv_pair_desc* pairs, int32_t n)
   pend_kind_ = kind;
   pend_mask_.resize(n);
   for(int i = 0; i < n; i++) { pend_mask_[i] = P[i].mask; }
+  pend_gen_ = gen_idx;
+  pend_gen_desc_.clear();
+  for(int i : gen_idx) { pend_gen_desc_.push_back(pairs[i]); }
   pend_n_ = n;
   return QMIV_OK;
 }
@@ -486,7 +501,46 @@ qmiv_status Engine::collect(qmiv_result* results)
     const qmiv_status ps = pair_status(host_out_[i], prm_.invalid_pel_action);
     if(ps != QMIV_OK && st == QMIV_OK) { st = ps; }
   }
+  if(results && st == QMIV_OK && !pend_gen_.empty()) { st = collect_gen(results); }
   return st;
+}
+
+qmiv_status Engine::collect_gen(qmiv_result* results)
+{
+  for(size_t g = 0; g < pend_gen_.size(); g++)
+  {
+    const int i = pend_gen_[g];
+    const qmiv_pair_desc& d = pend_gen_desc_[g];
+    const uint32_t mask = d.metric_mask & kSsimFamily;
+    const KindKey key{ d.width, d.height, d.bitdepth, d.chroma_format, d.search_range };
+    std::unique_ptr<PairPipeline>& pp = gen_pipes_[key];
+    if(!pp)
+    {
+      pp.reset(new PairPipeline());
+      qmiv_params prm = prm_;
+      prm.search_range = d.search_range;
+      QMIV_TRY(pp->configure(ctx_, pend_kind_[i]->S, prm, d.search_range));
+    }
+    const bool host = d.in0.mem == QMIV_MEM_HOST || d.in1.mem == QMIV_MEM_HOST;
+    QMIV_TRY(pp->prepare(mask, false, host));
+    Img a, b;
+    QMIV_TRY(pp->resolve(&d.in0, 0, a, stream_));
+    QMIV_TRY(pp->resolve(&d.in1, 1, b, stream_));
+    QMIV_TRY(pp->enqueue(a, b, mask, false, false, stream_));
+    QMIV_CUDA(cudaStreamSynchronize(stream_));
+    qmiv_result r{};
+    finish_result(pp->host_out(), pp->finish_info(mask), &r);
+    qmiv_result& o = results[i];
+    for(int c = 0; c < 4; c++) { o.ssim[c] = r.ssim[c]; o.msssim[c] = r.msssim[c]; }
+    o.ssim_pic = r.ssim_pic; o.msssim_pic = r.msssim_pic;
+    o.ivssim = r.ivssim; o.ivssim_r2t = r.ivssim_r2t; o.ivssim_t2r = r.ivssim_t2r;
+    o.ivmsssim = r.ivmsssim; o.ivmsssim_r2t = r.ivmsssim_r2t; o.ivmsssim_t2r = r.ivmsssim_t2r;
+    if(mask & (QMIV_IVSSIM | QMIV_IVMSSSIM))   // the search's side outputs, as the plain form reports them
+    {
+      for(int c = 0; c < 4; c++) { o.gcd_r2t[c] = r.gcd_r2t[c]; o.cps_sse_r2t[c] = r.cps_sse_r2t[c]; o.cps_sse_t2r[c] = r.cps_sse_t2r[c]; }
+    }
+  }
+  return QMIV_OK;
 }
 
 // ---------------------------------------------------------------------------------------------

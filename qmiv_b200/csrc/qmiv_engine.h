@@ -152,6 +152,13 @@ private:
   int          pend_n_ = -1;                   // pairs of the call in flight, -1 = none
   std::vector<PairKind*> pend_kind_;
   std::vector<uint32_t>  pend_mask_;
+  // SSIM metrics under a structural similarity option other than BlockAveraged 8/4: the batch computes
+  // every other metric, then collect() computes these pair by pair through a PairPipeline of the
+  // pair's kind (the qmiv_calc path) and merges them into the results
+  std::vector<int>            pend_gen_;       // indices of the call's pairs with such metrics
+  std::vector<qmiv_pair_desc> pend_gen_desc_;
+  std::map<KindKey, std::unique_ptr<PairPipeline>> gen_pipes_;
+  qmiv_status collect_gen(qmiv_result* results);
 };
 
 }  // namespace qmiv

@@ -115,8 +115,7 @@ inline int32_t ssim_window_size(const qmiv_params& p) { return ssim_regular(p.ss
 // Windows along a picture line of length len (xSSIM::xInitLoopRanges, xSSIM.cpp:161-196, counts
 // :381-404) and the line position of the first window's first input sample.
 void ssim_line(const qmiv_params& p, int32_t len, int32_t& first_sample, int32_t& count);
-// The batched and serving forms evaluate the default structural similarity option only.
-qmiv_status check_batched_ssim(const qmiv_params& p, uint32_t mask);
+
 // Known metric bits, and the SSIM family only where its exact 32-bit sub-block moments hold
 // (bit depth <= 14: 16 * (2^14 - 1)^2 < 2^32).
 qmiv_status check_metrics(const Shape& S, uint32_t mask);

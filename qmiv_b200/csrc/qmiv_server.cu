@@ -280,7 +280,6 @@ qmiv_status qmiv_server_submit(qmiv_server s, const qmiv_request* req, uint64_t*
   qmiv_params p = s->prm;
   p.search_range = req->search_range;
   QMIV_TRY(validate_params(p));
-  QMIV_TRY(check_batched_ssim(p, req->metric_mask));
   std::shared_ptr<Request> r(new Request());
   r->desc = *req;
   r->in0.assign(req->in0, req->in0 + req->num_pairs);

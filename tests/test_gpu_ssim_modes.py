@@ -109,16 +109,30 @@ def test_ssim_mode_refusals(qctx):
         assert got["psnr_pic"] > 0
 
 
-def test_batched_forms_refuse_other_ssim_options(qctx):
-    """The batched form evaluates the default BlockAveraged 8/4 SSIM only; other options are refused
-    there when an SSIM metric is asked for, and accepted for the PSNR family."""
+@pytest.mark.parametrize("mode,border,window,stride", [(0, 0, 11, 1), (1, 2, 11, 4), (3, 0, 16, 4)])
+def test_batched_and_serving_forms_take_ssim_options(mode, border, window, stride, qctx):
+    """The batched form (synchronous and submit / wait) and the serving loop give, under other
+    structural similarity options, the same results as the plain form: the SSIM metrics of such pairs
+    are computed pair by pair after the batch, the others in the batch."""
     import qmiv_b200
     from qmiv_b200 import synth
-    f0, f1 = synth.make_pair(128, 64, 10, seed=2)
-    pair = dict(frame0=f0, frame1=f1, width=128, height=64, bitdepth=10, chroma_format=420, search_range=2)
-    with qmiv_b200.Batch(qctx, max_pairs=2, max_pixels=128 * 64, ssim_mode=0, ssim_window=11, ssim_stride=1) as b:
-        with pytest.raises(qmiv_b200.QmivError) as ei:
-            b.compute([dict(pair, metrics=qmiv_b200.SSIM)])
-        assert ei.value.status == 2
-        res = b.compute([dict(pair, metrics=qmiv_b200.PSNR | qmiv_b200.IVPSNR)])
-        assert res[0]["ivpsnr"] > 0
+    opts = dict(ssim_mode=mode, ssim_border=border, ssim_window=window, ssim_stride=stride, erp=True)
+    shapes = [(128, 64, 10, 420, 2), (96, 96, 8, 444, 3), (160, 96, 10, 422, 2)]
+    frames = [synth.make_pair(W, H, bd, seed=W + bd, chroma_format=cf) for (W, H, bd, cf, R) in shapes]
+    masks = [qmiv_b200.ALL, qmiv_b200.SSIM | qmiv_b200.IVSSIM, qmiv_b200.PSNR | qmiv_b200.IVPSNR | qmiv_b200.MSSSIM]
+    plain = []
+    for (W, H, bd, cf, R), (f0, f1), m in zip(shapes, frames, masks):
+        with qmiv_b200.Calc(qctx, W, H, bd, cf, search_range=R, **opts) as calc:
+            plain.append(calc.compute(f0, f1, m))
+    descs = [dict(frame0=f0, frame1=f1, width=W, height=H, bitdepth=bd, chroma_format=cf, search_range=R, metrics=m)
+             for (W, H, bd, cf, R), (f0, f1), m in zip(shapes, frames, masks)]
+    px = sum(W * H for (W, H, _, _, _) in shapes)
+    with qmiv_b200.Batch(qctx, max_pairs=len(descs), max_pixels=px, **opts) as b:
+        assert b.compute(descs) == plain
+        t0, t1 = b.submit(descs), b.submit(descs)
+        assert b.wait(t0) == plain and b.wait(t1) == plain
+    with qmiv_b200.Server(qctx, max_batch_pairs=4, max_batch_pixels=px, **opts) as srv:
+        tickets = [srv.submit([fr], W, H, bd, cf, search_range=R, metrics=m)
+                   for (W, H, bd, cf, R), fr, m in zip(shapes, frames, masks)]
+        got = [srv.wait(t)[0][0] for t in tickets]
+    assert got == plain
