@@ -27,12 +27,20 @@ qmiv_status Shape::init(int32_t W_, int32_t H_, int32_t bd, int32_t cf)
   return QMIV_OK;
 }
 
-qmiv_status check_metrics(const Shape& S, uint32_t mask)
+qmiv_status check_metrics(const Shape& S, uint32_t mask, const qmiv_params& p)
 {
   if((mask & ~(uint32_t)QMIV_ALL) != 0) { return fail(QMIV_ERR_INVALID_ARG, "unknown metric bits"); }
   if((mask & (QMIV_SSIM | QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM)) && S.bitdepth > 14)
   {
-    return fail(QMIV_ERR_UNSUPPORTED, "SSIM metrics need bit depth <= 14");
+    // plain SSIM only: the reference's SIMD 2x2 downsampling (MS-SSIM) adds sample pairs in signed 16-bit
+    // lanes (xPixelOpsSSE.cpp:186-189), and the IV metrics' search errors overflow int32, above 14 bits
+    const bool wide_ok = (p.ssim_mode == QMIV_SSM_REGULAR_GAUSSIAN_FLT || p.ssim_mode == QMIV_SSM_REGULAR_GAUSSIAN_INT) &&
+                         !(mask & (QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM));
+    if(!wide_ok)
+    {
+      return fail(QMIV_ERR_UNSUPPORTED, "SSIM metrics at a bit depth above 14 need the RegularGaussianFlt or RegularGaussianInt "
+                                        "option (plain SSIM only)");
+    }
   }
   return QMIV_OK;
 }
@@ -588,7 +596,7 @@ static qmiv_status calc_submit(qmiv_calc calc, const qmiv_frame* in0, const qmiv
 {
   if(!calc || !in0 || !in1) { return fail(QMIV_ERR_INVALID_ARG, "null argument"); }
   if(calc->pending) { return fail(QMIV_ERR_BUSY, "a submission is already in flight on this calc"); }
-  QMIV_TRY(check_metrics(calc->pipe.shape(), mask));
+  QMIV_TRY(check_metrics(calc->pipe.shape(), mask, calc->prm));
   QMIV_CUDA(cudaSetDevice(calc->ctx->device));
   const bool host = in0->mem == QMIV_MEM_HOST || in1->mem == QMIV_MEM_HOST;
   const bool colour = calc->colour && calc->colour->active;

@@ -244,7 +244,7 @@ qmiv_status Engine::submit(const qmiv_pair_desc* pairs, int32_t n)
   {
     const qmiv_pair_desc& d = pairs[i];
     QMIV_TRY(kind_for(d, kind[i]));
-    QMIV_TRY(check_metrics(kind[i]->S, d.metric_mask));
+    QMIV_TRY(check_metrics(kind[i]->S, d.metric_mask, prm_));
     PairSlot& p = P[i];
     const Shape& S = kind[i]->S;
     p.mask = d.metric_mask;

@@ -116,9 +116,11 @@ inline int32_t ssim_window_size(const qmiv_params& p) { return ssim_regular(p.ss
 // :381-404) and the line position of the first window's first input sample.
 void ssim_line(const qmiv_params& p, int32_t len, int32_t& first_sample, int32_t& count);
 
-// Known metric bits, and the SSIM family only where its exact 32-bit sub-block moments hold
-// (bit depth <= 14: 16 * (2^14 - 1)^2 < 2^32).
-qmiv_status check_metrics(const Shape& S, uint32_t mask);
+// Known metric bits, and the SSIM family only where it is exact: up to 14 bits for the default
+// windows (exact 32-bit sub-block moments: 16 * (2^14 - 1)^2 < 2^32) and for every option whose
+// reference arithmetic squares samples in 32 bits; plain SSIM up to 16 bits under the regular Gaussian
+// windows, whose reference sums are double or 64-bit (xStructSimSTD.cpp:19-154).
+qmiv_status check_metrics(const Shape& S, uint32_t mask, const qmiv_params& p);
 
 // The device pipeline of one frame pair of a fixed shape, with its scratch buffers.
 class PairPipeline

@@ -276,10 +276,10 @@ qmiv_status qmiv_server_submit(qmiv_server s, const qmiv_request* req, uint64_t*
   if((int64_t)req->width * req->height > s->max_batch_pixels) { return fail(QMIV_ERR_INVALID_ARG, "picture larger than max_batch_pixels"); }
   Shape S;
   QMIV_TRY(S.init(req->width, req->height, req->bitdepth, req->chroma_format));
-  QMIV_TRY(check_metrics(S, req->metric_mask));
   qmiv_params p = s->prm;
   p.search_range = req->search_range;
   QMIV_TRY(validate_params(p));
+  QMIV_TRY(check_metrics(S, req->metric_mask, p));
   std::shared_ptr<Request> r(new Request());
   r->desc = *req;
   r->in0.assign(req->in0, req->in0 + req->num_pairs);

@@ -284,6 +284,12 @@ SSIM_MODE_CASES = [
     (160, 96, 10, 420, 2, True, 83, SSM_BAVG, 0, 32, 4),
     (130, 70, 8, 422, 2, False, 84, SSM_BAVG, 0, 32, 7),
     (256, 128, 10, 420, 2, True, 85, SSM_FLT, 0, 11, 1),
+    # 15- and 16-bit pictures: the regular Gaussian windows sum in double / int64 in the reference, so
+    # plain SSIM is defined there (not MS-SSIM: the SIMD downsampling adds in signed 16-bit lanes; not the
+    # IV metrics: the search's int32 errors overflow)
+    (64, 48, 16, 444, 2, False, 86, SSM_FLT, 0, 11, 1, 1 | 8),
+    (96, 64, 15, 420, 2, True, 87, SSM_INT, 1, 11, 2, 1 | 2 | 8),
+    (72, 72, 16, 422, 2, False, 88, SSM_FLT, 4, 11, 3, 8),
 ]
 SSIM_KEYS = ("ssim", "ssim_pic", "msssim", "msssim_pic", "ivssim", "ivssim_r2t", "ivssim_t2r", "ivmsssim", "ivmsssim_r2t",
              "ivmsssim_t2r")
@@ -294,10 +300,11 @@ def make_ssim_modes(ref, ref_fma):
     compiled reference (xSSIM::setStructSimParams, xAppQMIV.cpp:722; border extension of the pictures
     and the SCPs, :798 and :918-926). Frames come from detgen."""
     out = []
-    for (W, H, bd, cf, R, erp, seed, mode, border, window, stride) in SSIM_MODE_CASES:
+    for case in SSIM_MODE_CASES:
+        (W, H, bd, cf, R, erp, seed, mode, border, window, stride), extra = case[:11], case[11:]
         p = oracle.make_params(W, H, bd, cf, search_range=R, erp=erp, num_threads=8)
         f0, f1 = det_pair(W, H, bd, seed, cf)
-        mask = oracle.ALL
+        mask = extra[0] if extra else oracle.ALL
         if oracle.Oracle().num_scales(W, H) < 1:
             mask &= ~(oracle.MSSSIM | oracle.IVMSSSIM)
         r = ref.compute_pair_ssim(p, f0, f1, mode, border, window, stride, mask)

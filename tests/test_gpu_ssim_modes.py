@@ -107,6 +107,16 @@ def test_ssim_mode_refusals(qctx):
             calc.compute(f0, f1, qmiv_b200.SSIM)
         got = calc.compute(f0, f1, qmiv_b200.PSNR)   # the calc still works for the other metrics
         assert got["psnr_pic"] > 0
+    # above 14 bits: plain SSIM under the regular Gaussian windows only
+    f0, f1 = synth.make_pair(64, 48, 16, seed=2, chroma_format=444)
+    with qmiv_b200.Calc(qctx, 64, 48, 16, 444, ssim_mode=0, ssim_stride=1) as calc:
+        assert 0.0 < calc.compute(f0, f1, qmiv_b200.SSIM)["ssim_pic"] <= 1.0
+        for m in (qmiv_b200.MSSSIM, qmiv_b200.IVSSIM, qmiv_b200.IVMSSSIM):
+            with pytest.raises(qmiv_b200.QmivError):
+                calc.compute(f0, f1, m)
+    with qmiv_b200.Calc(qctx, 64, 48, 15, 420, ssim_mode=2) as calc:
+        with pytest.raises(qmiv_b200.QmivError):
+            calc.compute(*synth.make_pair(64, 48, 15, seed=3), qmiv_b200.SSIM)
 
 
 @pytest.mark.parametrize("mode,border,window,stride", [(0, 0, 11, 1), (1, 2, 11, 4), (3, 0, 16, 4)])
