@@ -10,7 +10,7 @@
 //                    test pixels and masked candidates are skipped, the winner's squared differences
 //                    are weighted by the test pixel's mask value and summed per row in uint64
 //   k_mask_finalize  the ordered compensated sums (xKBNS.h:36-43) of the ERP row weights and the
-//                    row totals, one thread per chain
+//                    row totals, one CTA per chain (terms staged in shared memory, one thread sums)
 // dB values, exact-component fake values and the picture averages are formed on the host in
 // qmiv_frame_pair_compute_masked with the reference's arithmetic, including its choice of the mask's
 // bit depth for the picture's maximum in PSNR-M (xPSNR.cpp:61) and its direction labels in
@@ -208,34 +208,52 @@ __global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ Mask
 }
 
 // Chains 0..2: WS rows of component c; chains 3..8: CPS rows of (direction, component). Each is the
-// reference's row-order compensated sum; the CPS chains also form the plain uint64 totals.
-__global__ void k_mask_finalize(const __grid_constant__ MaskArgs a)
+// reference's row-order compensated sum; the CPS chains also form the plain uint64 totals. One CTA per
+// chain: all threads stage a chunk of the chain's terms (the products with the ERP weights, the same
+// doubles the serial loop would form) in shared memory, then thread 0 adds them in row order, so the
+// serial chain never waits on global memory.
+constexpr int kMaskFinChunk = 4096;
+__global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ MaskArgs a)
 {
-  const int k = threadIdx.x;
-  if(k >= 9) { return; }
+  __shared__ double vals[kMaskFinChunk];
+  __shared__ unsigned long long tot;
+  const int k = blockIdx.x;
+  if(k < 3 && !a.ws) { return; }                              // uniform over the CTA
   MaskOut* o = a.out;
   const int H = a.H;
-  if(k < 3)
+  const bool cps = k >= 3;
+  const int d = cps ? (k - 3) / 3 : 0, c = cps ? (k - 3) % 3 : 0;
+  const uint64_t* r = cps ? a.row_cps + (size_t)d * H * 3 + c : a.row_ssd + (size_t)k * H;
+  const size_t step = cps ? 3 : 1;
+  if(threadIdx.x == 0) { tot = 0ull; }
+  unsigned long long loc = 0ull;
+  Kbns s;                                                     // used by thread 0
+  for(int base = 0; base < H; base += kMaskFinChunk)
   {
-    if(!a.ws) { return; }
-    const uint64_t* r = a.row_ssd + (size_t)k * H;
-    Kbns s;
-    for(int y = 0; y < H; y++) { s.add(dmul((double)r[y], a.ws[y])); }
-    o->ws_err[k] = s.result();
-    return;
+    const int n = min(kMaskFinChunk, H - base);
+    __syncthreads();                                          // the previous chunk has been summed
+    for(int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+      const uint64_t v = r[(size_t)(base + i) * step];
+      loc += v;
+      vals[i] = a.ws ? dmul((double)v, a.ws[base + i]) : 0.0;
+    }
+    __syncthreads();
+    if(threadIdx.x == 0 && a.ws)
+    {
+      #pragma unroll 8
+      for(int i = 0; i < n; i++) { s.add(vals[i]); }
+    }
   }
-  const int d = (k - 3) / 3, c = (k - 3) % 3;
-  const uint64_t* r = a.row_cps + (size_t)d * H * 3 + c;
-  uint64_t total = 0;
-  Kbns s;
-  for(int y = 0; y < H; y++)
+  atomicAdd(&tot, loc);                                       // exact: integer sum in any order
+  __syncthreads();
+  if(threadIdx.x != 0) { return; }
+  if(cps)
   {
-    const uint64_t v = r[(size_t)y * 3];
-    total += v;
-    if(a.ws) { s.add(dmul((double)v, a.ws[y])); }
+    o->cps_sum[d][c] = tot;
+    o->cps_ws[d][c] = a.ws ? s.result() : 0.0;
   }
-  o->cps_sum[d][c] = total;
-  o->cps_ws[d][c] = a.ws ? s.result() : 0.0;
+  else { o->ws_err[k] = s.result(); }
 }
 
 template <typename T, typename TM>
@@ -253,7 +271,7 @@ cudaError_t launch_masked_t(const MaskArgs& a, int R, cudaStream_t s)
   case 5: k_cps_masked<T, TM, 5><<<grid, 256, 0, s>>>(a); break;
   default: return cudaErrorInvalidValue;
   }
-  k_mask_finalize<<<1, 32, 0, s>>>(a);
+  k_mask_finalize<<<9, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
