@@ -172,22 +172,26 @@ __global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ Mask
       int32_t s[3];
       #pragma unroll
       for(int c = 0; c < 3; c++) { s[c] = (int32_t)min((uint32_t)fetch<T>(tst, c, x, y), a.clip) + sg * a.out->gcd[c]; }
+      // the winner is tracked by its raster index (one select per candidate) and read back after the
+      // search; the centre is never masked here, so some candidate always wins
+      constexpr int D = 2 * R + 1;
       int32_t best = 0x7fffffff;
-      int4 bp = st[ty + R][tx + R];
+      int bidx = R * D + R;
       #pragma unroll
-      for(int dy = 0; dy <= 2 * R; dy++)
+      for(int dy = 0; dy < D; dy++)
       {
         #pragma unroll
-        for(int dx = 0; dx <= 2 * R; dx++)
+        for(int dx = 0; dx < D; dx++)
         {
           const int4 r = st[ty + dy][tx + dx];
           if(r.w == 0) { continue; }
           const int32_t d0 = s[0] - r.x, d1 = s[1] - r.y, d2 = s[2] - r.z;
           const uint32_t err = (uint32_t)(d0 * d0) * (uint32_t)a.cws[0] + (uint32_t)(d1 * d1) * (uint32_t)a.cws[1] +
                                (uint32_t)(d2 * d2) * (uint32_t)a.cws[2];
-          if((int32_t)err < best) { best = (int32_t)err; bp = r; }
+          if((int32_t)err < best) { best = (int32_t)err; bidx = dy * D + dx; }
         }
       }
+      const int4 bp = st[ty + bidx / D][tx + bidx % D];
       const int32_t d0 = s[0] - bp.x, d1 = s[1] - bp.y, d2 = s[2] - bp.z;
       e[0] = (uint64_t)(int64_t)(d0 * d0) * (uint64_t)m;
       e[1] = (uint64_t)(int64_t)(d1 * d1) * (uint64_t)m;
