@@ -8,7 +8,9 @@
 //                    round half away, clip
 //   k_cps_masked     the masked search (xCorrespPixelShiftSTD.cpp:151-215), both directions: masked
 //                    test pixels and masked candidates are skipped, the winner's squared differences
-//                    are weighted by the test pixel's mask value and summed per row in uint64
+//                    are weighted by the test pixel's mask value and summed per row in uint64;
+//                    k_cps_masked_key is the same search by exact integer keys, four pixels per
+//                    thread, where the bit depth, weights and GCD range bound every error
 //   k_mask_finalize  the ordered compensated sums (xKBNS.h:36-43) of the ERP row weights and the
 //                    row totals, one CTA per chain (terms staged in shared memory, one thread sums)
 // dB values, exact-component fake values and the picture averages are formed on the host in
@@ -18,8 +20,10 @@
 #include "qmiv_host.h"
 #include "qmiv_kernels.cuh"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace qmiv {
@@ -53,6 +57,8 @@ struct MaskArgs
   uint64_t*   row_cps;         // [2][H][3]
   const double* ws;            // [H] or null
   MaskOut*    out;
+  uint32_t    key_off;         // k_cps_masked_key: bound B of every error and every sum of w s^2
+  uint32_t    kscale;          // 128, read from the parameter bank so the key stays one integer multiply-add
 };
 
 namespace {
@@ -211,6 +217,115 @@ __global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ Mask
   }
 }
 
+// The same search where every error and every sum of w s^2 is at most B with 2B < 2^25 - 1 (the host
+// checks this from the bit depth, weights and GCD clip range; samples are in range under STOP and CNCL).
+// Expanding e = sum_c w_c (s_c - r_c)^2 = K_s + q_r + sum_c a_c r_c with K_s = sum w s^2 (constant per
+// test pixel), q_r = sum w r^2 (staged once per reference sample) and a_c = -2 w_c s_c gives
+// t = B + q_r + sum_c a_c r_c = e + (B - K_s), an integer in [0, 2B] that orders the candidates of a
+// pixel exactly as e does. The key t * 128 + k (k the raster index of the candidate) then orders them
+// as (error, raster index), so one unsigned minimum per candidate keeps the reference's first strict
+// minimum. A masked reference sample is staged as (0, 0, 0, 2^25 - 1): its key is above every real
+// one, so it never wins. Each thread searches four vertically adjacent pixels, so one staged sample
+// read from shared memory feeds up to four candidates.
+template <typename T, typename TM, int R>
+__global__ void __launch_bounds__(256, 4) k_cps_masked_key(const __grid_constant__ MaskArgs a)
+{
+  constexpr int P = 4, TW = 32, TH = 8 * P, SW = TW + 2 * R, SH = TH + 2 * R, D = 2 * R + 1;
+  constexpr uint32_t kMaskedT = (1u << 25) - 1u;
+  static_assert(D * D <= 128, "the raster index must fit the key's low 7 bits");
+  __shared__ int4 st[SH][SW];                                // (Y, Cb, Cr, B + sum w r^2)
+  const int dir = blockIdx.z;
+  const Img& tst = dir ? a.in0 : a.in1;
+  const Img& ref = dir ? a.in1 : a.in0;
+  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  const uint32_t w0 = (uint32_t)a.cws[0], w1 = (uint32_t)a.cws[1], w2 = (uint32_t)a.cws[2];
+  // the test pixels are read before the tile is staged so that their loads overlap the staging
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int x = x0 + tx, xc = min(x, a.W - 1);
+  const int32_t sg = dir ? 1 : -1;
+  int32_t s[P][3], c0[P], c1[P], c2[P], m[P];
+  uint32_t best[P];
+  #pragma unroll
+  for(int p = 0; p < P; p++)
+  {
+    const int y = y0 + ty * P + p, yc = min(y, a.H - 1);     // rows past the picture search a clamped pixel, discarded below
+    #pragma unroll
+    for(int c = 0; c < 3; c++) { s[p][c] = (int32_t)min((uint32_t)fetch<T>(tst, c, xc, yc), a.clip) + sg * a.out->gcd[c]; }
+    c0[p] = -2 * (int32_t)w0 * s[p][0];
+    c1[p] = -2 * (int32_t)w1 * s[p][1];
+    c2[p] = -2 * (int32_t)w2 * s[p][2];
+    m[p] = (x < a.W && y < a.H) ? mask_at<TM>(a, x, y) : 0;  // 0 for masked and out-of-picture pixels
+    best[p] = 0xffffffffu;
+  }
+  for(int e = threadIdx.x; e < SH * SW; e += 256)
+  {
+    const int ly = e / SW, lx = e - ly * SW;
+    const int gx = clampi(x0 - R + lx, 0, a.W - 1), gy = clampi(y0 - R + ly, 0, a.H - 1);
+    int4 v = make_int4(0, 0, 0, (int32_t)kMaskedT);
+    if(mask_at<TM>(a, gx, gy) != 0)
+    {
+      const uint32_t r0 = min((uint32_t)fetch<T>(ref, 0, gx, gy), a.clip);
+      const uint32_t r1 = min((uint32_t)fetch<T>(ref, 1, gx, gy), a.clip);
+      const uint32_t r2 = min((uint32_t)fetch<T>(ref, 2, gx, gy), a.clip);
+      v = make_int4((int32_t)r0, (int32_t)r1, (int32_t)r2, (int32_t)(a.key_off + w0 * r0 * r0 + w1 * r1 * r1 + w2 * r2 * r2));
+    }
+    st[ly][lx] = v;
+  }
+  __syncthreads();
+  #pragma unroll
+  for(int j = 0; j < D + P - 1; j++)
+  {
+    #pragma unroll
+    for(int dx = 0; dx < D; dx++)
+    {
+      const int4 r = st[ty * P + j][tx + dx];
+      #pragma unroll
+      for(int p = 0; p < P; p++)
+      {
+        const int dy = j - p;
+        if(dy < 0 || dy >= D) { continue; }                  // resolved at compile time
+        const uint32_t t = (uint32_t)r.w + (uint32_t)(c0[p] * r.x) + (uint32_t)(c1[p] * r.y) + (uint32_t)(c2[p] * r.z);
+        best[p] = min(best[p], t * a.kscale + (uint32_t)(dy * D + dx));
+      }
+    }
+  }
+  // Row sums. Each term d^2 M is below 2^38 here (d^2 < 2^24 is checked with the key bound, M < 2^14),
+  // so its low 16 bits and the rest (< 2^22) are summed over the warp's 32 pixels of a row in 32 bits each, exactly, by one
+  // redux.sync apiece.
+  uint32_t lo[P][3], hi[P][3];
+  #pragma unroll
+  for(int p = 0; p < P; p++)
+  {
+    // the minimum is always some candidate's key (no key has low bits 127), so k < D * D; the clamp
+    // keeps the read in the tile whatever the data
+    const int k = min((int)(best[p] & 127u), D * D - 1);
+    const int4 bp = st[ty * P + p + k / D][tx + k % D];
+    const int32_t d[3] = { s[p][0] - bp.x, s[p][1] - bp.y, s[p][2] - bp.z };
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      const uint64_t t = (uint64_t)(uint32_t)(d[c] * d[c]) * (uint64_t)(uint32_t)m[p];
+      lo[p][c] = __reduce_add_sync(0xffffffffu, (uint32_t)t & 0xffffu);
+      hi[p][c] = __reduce_add_sync(0xffffffffu, (uint32_t)(t >> 16));
+    }
+  }
+  if(tx == 0)
+  {
+    #pragma unroll
+    for(int p = 0; p < P; p++)
+    {
+      const int y = y0 + ty * P + p;
+      if(y >= a.H) { continue; }
+      #pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const uint64_t v = ((uint64_t)hi[p][c] << 16) + lo[p][c];
+        if(v) { atomicAdd(reinterpret_cast<unsigned long long*>(a.row_cps + ((size_t)dir * a.H + y) * 3 + c), (unsigned long long)v); }
+      }
+    }
+  }
+}
+
 // Chains 0..2: WS rows of component c; chains 3..8: CPS rows of (direction, component). Each is the
 // reference's row-order compensated sum; the CPS chains also form the plain uint64 totals. One CTA per
 // chain: all threads stage a chunk of the chain's terms (the products with the ERP weights, the same
@@ -261,12 +376,25 @@ __global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ M
 }
 
 template <typename T, typename TM>
-cudaError_t launch_masked_t(const MaskArgs& a, int R, cudaStream_t s)
+cudaError_t launch_masked_t(const MaskArgs& a, int R, bool key, cudaStream_t s)
 {
   k_mask_prepass<T, TM><<<(a.H + 7) / 8, 256, 0, s>>>(a);
   k_mask_reduce<<<1, 32, 0, s>>>(a);
   const dim3 grid((a.W + 31) / 32, (a.H + 7) / 8, 2);
-  switch(R)
+  const dim3 grid_key((a.W + 31) / 32, (a.H + 31) / 32, 2);
+  if(key)
+  {
+    switch(R)
+    {
+    case 1: k_cps_masked_key<T, TM, 1><<<grid_key, 256, 0, s>>>(a); break;
+    case 2: k_cps_masked_key<T, TM, 2><<<grid_key, 256, 0, s>>>(a); break;
+    case 3: k_cps_masked_key<T, TM, 3><<<grid_key, 256, 0, s>>>(a); break;
+    case 4: k_cps_masked_key<T, TM, 4><<<grid_key, 256, 0, s>>>(a); break;
+    case 5: k_cps_masked_key<T, TM, 5><<<grid_key, 256, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
+  }
+  else switch(R)
   {
   case 1: k_cps_masked<T, TM, 1><<<grid, 256, 0, s>>>(a); break;
   case 2: k_cps_masked<T, TM, 2><<<grid, 256, 0, s>>>(a); break;
@@ -343,9 +471,24 @@ qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const 
   a.out = out_.as<MaskOut>();
   QMIV_CUDA(cudaMemsetAsync(out_.p, 0, sizeof(MaskOut), s));
   QMIV_CUDA(cudaMemsetAsync(a.row_cps, 0, (size_t)6 * S.H * sizeof(uint64_t), s));
+  // the key search needs samples in range (STOP fails on any other, CNCL clips), 2B < 2^25 - 1 with
+  // B = sum_c w_c (Max + MaxDiff_c)^2, the bound of every error and of every sum of w s^2, and every
+  // squared difference below 2^24 (its row sums split the terms into two 32-bit parts)
+  int64_t bound = 0, dmax2 = 0;
+  for(int c = 0; c < 3; c++)
+  {
+    const int64_t m = (int64_t)S.maxv + std::abs((int64_t)a.maxdiff[c]);
+    bound += (int64_t)prm.cws[c] * m * m;
+    dmax2 = std::max(dmax2, m * m);
+  }
+  const bool key = (prm.invalid_pel_action == QMIV_PEL_STOP || prm.invalid_pel_action == QMIV_PEL_CNCL) &&
+                   2 * bound < (int64_t)((1u << 25) - 1u) && dmax2 < ((int64_t)1 << 24);
+  a.key_off = (uint32_t)(key ? bound : 0);
+  a.kscale = 128u;
+  const int R = prm.search_range;
   cudaError_t e;
-  if(S.esz == 1) { e = mesz == 1 ? launch_masked_t<uint8_t, uint8_t>(a, prm.search_range, s) : launch_masked_t<uint8_t, uint16_t>(a, prm.search_range, s); }
-  else { e = mesz == 1 ? launch_masked_t<uint16_t, uint8_t>(a, prm.search_range, s) : launch_masked_t<uint16_t, uint16_t>(a, prm.search_range, s); }
+  if(S.esz == 1) { e = mesz == 1 ? launch_masked_t<uint8_t, uint8_t>(a, R, key, s) : launch_masked_t<uint8_t, uint16_t>(a, R, key, s); }
+  else { e = mesz == 1 ? launch_masked_t<uint16_t, uint8_t>(a, R, key, s) : launch_masked_t<uint16_t, uint16_t>(a, R, key, s); }
   if(e != cudaSuccess) { return cuda_fail(e, "masked launches"); }
   QMIV_CUDA(cudaMemcpyAsync(h_out_, out_.p, sizeof(MaskOut), cudaMemcpyDeviceToHost, s));
   QMIV_CUDA(cudaStreamSynchronize(s));

@@ -105,3 +105,56 @@ def test_masked_errors(qctx):
         # the calc still works after the refusals
         got, nnm = calc.compute_masked(f0, f1, m, 8)
         assert nnm == int((m != 0).sum())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(640, 360, 10, 420, 2, 8, "weights"), (352, 288, 8, 444, 5, 10, "binary"),
+                                   (258, 130, 10, 422, 4, 12, "sparse"), (200, 100, 10, 420, 1, 8, "weights")])
+def test_masked_search_forms_agree(shape, qctx, oracle_lib):
+    """The masked search has two kernels: exact integer keys, four pixels per thread, where the bit
+    depth, weights and GCD range bound every error and samples are in range (STOP, CNCL), and the
+    plain per-candidate integer loop otherwise (SKIP, WARN). On in-range frames every action gives
+    the same values, and both equal the C restatement."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    W, H, bd, cf, R, mbd, kind = shape
+    f0, f1 = synth.make_pair(W, H, bd, seed=W * 7 + R, chroma_format=cf)
+    m = det_mask(W, H, mbd, W + 11 * H, kind)
+    p = oracle.make_params(W, H, bd, cf, search_range=R, erp=True)
+    exp, n_exp = oracle_lib.compute_pair_masked(p, f0, f1, m, mbd)
+    sse = []
+    for act in (qmiv_b200.PEL_STOP, qmiv_b200.PEL_CNCL, qmiv_b200.PEL_SKIP, qmiv_b200.PEL_WARN):
+        with qmiv_b200.Calc(qctx, W, H, bd, cf, search_range=R, erp=True, invalid_pel_action=act) as calc:
+            got, nnm = calc.compute_masked(f0, f1, m, mbd)
+        assert nnm == n_exp
+        for k in ["gcd_r2t", "psnr", "wspsnr"]:
+            assert list(got[k][:3]) == list(exp[k][:3]), (act, k)
+        for k in ["psnr_pic", "wspsnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"]:
+            assert got[k] == exp[k], (act, k)
+        sse.append((list(got["cps_sse_r2t"][:3]), list(got["cps_sse_t2r"][:3])))
+    assert all(v == sse[0] for v in sse), sse      # the per-direction uint64 search sums of both kernels
+
+
+@pytest.mark.gpu
+def test_masked_out_of_range_samples_skip(qctx, oracle_lib):
+    """Under SKIP, samples above the bit depth's maximum are searched as they are (the integer-loop
+    kernel); the results equal the C restatement's on the same frames."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    W, H, bd = 160, 96, 10
+    f0, f1 = synth.make_pair(W, H, bd, seed=99)
+    f1 = tuple(np.array(pl, copy=True) for pl in f1)
+    f1[0][10, 17] = 1500
+    f1[1][5, 9] = 1200
+    m = det_mask(W, H, 8, 5, "weights")
+    p = oracle.make_params(W, H, bd, 420, search_range=2, erp=False)   # the restatement computes on raw samples
+    exp, n_exp = oracle_lib.compute_pair_masked(p, f0, f1, m, 8)
+    with qmiv_b200.Calc(qctx, W, H, bd, search_range=2, invalid_pel_action=qmiv_b200.PEL_SKIP) as calc:
+        got, nnm = calc.compute_masked(f0, f1, m, 8)
+    assert nnm == n_exp
+    for k in ["gcd_r2t", "psnr"]:
+        assert list(got[k][:3]) == list(exp[k][:3]), k
+    for k in ["psnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"]:
+        assert got[k] == exp[k], k
