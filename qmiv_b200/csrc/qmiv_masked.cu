@@ -2,7 +2,7 @@
 // mask picture's luma weights every sample of PSNR, WS-PSNR and IV-PSNR (the STD-only *M processor
 // calls; the app refuses the SSIM family with a mask, :360-365).
 //
-//   k_mask_prepass   one warp per 4:4:4 row: sum of (In1 - In0) * M (GCD-M), sum of (In1 - In0)^2 * M
+//   k_mask_prepass   one CTA per 4:4:4 row: sum of (In1 - In0) * M (GCD-M), sum of (In1 - In0)^2 * M
 //                    per row (PSNR-M, WS-PSNR-M), non-zero mask samples, exactness, largest samples
 //   k_mask_reduce    GCD-M (xGlobClrDiff.cpp:60-91): IEEE divide by NumNonMasked * MaskMax,
 //                    round half away, clip
@@ -76,29 +76,47 @@ __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v)
   return v;
 }
 
+// One CTA per 4:4:4 row: each thread takes four columns 256 apart per step, issuing all their loads
+// before any arithmetic, then the warps' sums meet in shared memory and one thread writes the row's
+// SSD and adds the row's totals.
 template <typename T, typename TM>
 __global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ MaskArgs a)
 {
-  const int lane = threadIdx.x & 31;
-  const int y = blockIdx.x * 8 + (threadIdx.x >> 5);
-  if(y >= a.H) { return; }                                   // whole warps: no block barrier follows
+  constexpr int U = 4;
+  __shared__ uint64_t red[8][6];
+  __shared__ uint32_t redu[8][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int y = blockIdx.x;
   int64_t  sd[3] = { 0, 0, 0 };
   uint64_t ssd[3] = { 0, 0, 0 };
   uint32_t nnm = 0, dif = 0, mx0 = 0, mx1 = 0;
-  for(int x = lane; x < a.W; x += 32)
+  for(int xb = threadIdx.x; xb < a.W; xb += 256 * U)
   {
-    const int32_t m = mask_at<TM>(a, x, y);
-    nnm += m != 0;
+    int32_t  m[U];
+    uint32_t va[U][3], vb[U][3];
     #pragma unroll
-    for(int c = 0; c < 3; c++)
+    for(int u = 0; u < U; u++)
     {
-      uint32_t va = (uint32_t)fetch<T>(a.in0, c, x, y), vb = (uint32_t)fetch<T>(a.in1, c, x, y);
-      mx0 = max(mx0, va); mx1 = max(mx1, vb);
-      va = min(va, a.clip); vb = min(vb, a.clip);
-      const int32_t d = (int32_t)vb - (int32_t)va;
-      sd[c] += (int64_t)(d * m);                             // int32 product, xDistortionSTD.cpp:50
-      ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)(uint32_t)m;    // xDistortionSTD.cpp:62
-      dif |= (d != 0 ? 1u : 0u) << c;
+      const int x = min(xb + u * 256, a.W - 1);              // columns past the row repeat the last one, masked out below
+      m[u] = xb + u * 256 < a.W ? mask_at<TM>(a, x, y) : 0;
+      #pragma unroll
+      for(int c = 0; c < 3; c++) { va[u][c] = (uint32_t)fetch<T>(a.in0, c, x, y); vb[u][c] = (uint32_t)fetch<T>(a.in1, c, x, y); }
+    }
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      if(xb + u * 256 >= a.W) { continue; }
+      nnm += m[u] != 0;
+      #pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        mx0 = max(mx0, va[u][c]); mx1 = max(mx1, vb[u][c]);
+        const uint32_t p0 = min(va[u][c], a.clip), p1 = min(vb[u][c], a.clip);
+        const int32_t d = (int32_t)p1 - (int32_t)p0;
+        sd[c] += (int64_t)(d * m[u]);                          // int32 product, xDistortionSTD.cpp:50
+        ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)(uint32_t)m[u];    // xDistortionSTD.cpp:62
+        dif |= (d != 0 ? 1u : 0u) << c;
+      }
     }
   }
   #pragma unroll
@@ -113,19 +131,33 @@ __global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ Ma
   mx1 = __reduce_max_sync(0xffffffffu, mx1);
   if(lane == 0)
   {
-    MaskOut* o = a.out;
     #pragma unroll
-    for(int c = 0; c < 3; c++)
-    {
-      a.row_ssd[(size_t)c * a.H + y] = ssd[c];
-      atomicAdd(reinterpret_cast<unsigned long long*>(&o->sd[c]), (unsigned long long)sd[c]);
-      atomicAdd(reinterpret_cast<unsigned long long*>(&o->ssd[c]), (unsigned long long)ssd[c]);
-      if(dif & (1u << c)) { atomicOr(&o->differs[c], 1u); }
-    }
-    atomicAdd(&o->nnm, (int32_t)nnm);
-    atomicMax(&o->max_sample[0], mx0);
-    atomicMax(&o->max_sample[1], mx1);
+    for(int c = 0; c < 3; c++) { red[warp][c] = (uint64_t)sd[c]; red[warp][3 + c] = ssd[c]; }
+    redu[warp][0] = nnm; redu[warp][1] = dif; redu[warp][2] = mx0; redu[warp][3] = mx1;
   }
+  __syncthreads();
+  if(threadIdx.x != 0) { return; }
+  uint64_t t[6] = { 0, 0, 0, 0, 0, 0 };
+  nnm = 0; dif = 0; mx0 = 0; mx1 = 0;
+  #pragma unroll
+  for(int w = 0; w < 8; w++)
+  {
+    #pragma unroll
+    for(int k = 0; k < 6; k++) { t[k] += red[w][k]; }
+    nnm += redu[w][0]; dif |= redu[w][1]; mx0 = max(mx0, redu[w][2]); mx1 = max(mx1, redu[w][3]);
+  }
+  MaskOut* o = a.out;
+  #pragma unroll
+  for(int c = 0; c < 3; c++)
+  {
+    a.row_ssd[(size_t)c * a.H + y] = t[3 + c];
+    atomicAdd(reinterpret_cast<unsigned long long*>(&o->sd[c]), (unsigned long long)t[c]);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&o->ssd[c]), (unsigned long long)t[3 + c]);
+    if(dif & (1u << c)) { atomicOr(&o->differs[c], 1u); }
+  }
+  atomicAdd(&o->nnm, (int32_t)nnm);
+  atomicMax(&o->max_sample[0], mx0);
+  atomicMax(&o->max_sample[1], mx1);
 }
 
 // GCD-M, xGlobClrDiff.cpp:60-91 (called with swapped pictures, xGlobClrDiff.h:42: mean of In1 - In0)
@@ -261,31 +293,35 @@ __global__ void __launch_bounds__(256, 4) k_cps_masked_key(const __grid_constant
   {
     const int ly = e / SW, lx = e - ly * SW;
     const int gx = clampi(x0 - R + lx, 0, a.W - 1), gy = clampi(y0 - R + ly, 0, a.H - 1);
-    int4 v = make_int4(0, 0, 0, (int32_t)kMaskedT);
-    if(mask_at<TM>(a, gx, gy) != 0)
-    {
-      const uint32_t r0 = min((uint32_t)fetch<T>(ref, 0, gx, gy), a.clip);
-      const uint32_t r1 = min((uint32_t)fetch<T>(ref, 1, gx, gy), a.clip);
-      const uint32_t r2 = min((uint32_t)fetch<T>(ref, 2, gx, gy), a.clip);
-      v = make_int4((int32_t)r0, (int32_t)r1, (int32_t)r2, (int32_t)(a.key_off + w0 * r0 * r0 + w1 * r1 * r1 + w2 * r2 * r2));
-    }
-    st[ly][lx] = v;
+    // branch-free: every sample is read, a masked one is replaced by the sentinel
+    const int32_t  mk = mask_at<TM>(a, gx, gy);
+    const uint32_t r0 = min((uint32_t)fetch<T>(ref, 0, gx, gy), a.clip);
+    const uint32_t r1 = min((uint32_t)fetch<T>(ref, 1, gx, gy), a.clip);
+    const uint32_t r2 = min((uint32_t)fetch<T>(ref, 2, gx, gy), a.clip);
+    const uint32_t q = a.key_off + w0 * r0 * r0 + w1 * r1 * r1 + w2 * r2 * r2;
+    st[ly][lx] = make_int4(mk ? (int32_t)r0 : 0, mk ? (int32_t)r1 : 0, mk ? (int32_t)r2 : 0, (int32_t)(mk ? q : kMaskedT));
   }
   __syncthreads();
+  // candidates in column pairs: one three-input minimum takes two keys
+  auto key = [&](const int4& r, int p, int k) -> uint32_t {
+    const uint32_t t = (uint32_t)r.w + (uint32_t)(c0[p] * r.x) + (uint32_t)(c1[p] * r.y) + (uint32_t)(c2[p] * r.z);
+    return t * a.kscale + (uint32_t)k;
+  };
   #pragma unroll
   for(int j = 0; j < D + P - 1; j++)
   {
     #pragma unroll
-    for(int dx = 0; dx < D; dx++)
+    for(int dx = 0; dx < D; dx += 2)
     {
-      const int4 r = st[ty * P + j][tx + dx];
+      const int4 ra = st[ty * P + j][tx + dx];
+      const int4 rb = st[ty * P + j][tx + min(dx + 1, D - 1)];
       #pragma unroll
       for(int p = 0; p < P; p++)
       {
         const int dy = j - p;
         if(dy < 0 || dy >= D) { continue; }                  // resolved at compile time
-        const uint32_t t = (uint32_t)r.w + (uint32_t)(c0[p] * r.x) + (uint32_t)(c1[p] * r.y) + (uint32_t)(c2[p] * r.z);
-        best[p] = min(best[p], t * a.kscale + (uint32_t)(dy * D + dx));
+        if(dx + 1 < D) { best[p] = __vimin3_u32(best[p], key(ra, p, dy * D + dx), key(rb, p, dy * D + dx + 1)); }
+        else { best[p] = min(best[p], key(ra, p, dy * D + dx)); }
       }
     }
   }
@@ -378,7 +414,7 @@ __global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ M
 template <typename T, typename TM>
 cudaError_t launch_masked_t(const MaskArgs& a, int R, bool key, cudaStream_t s)
 {
-  k_mask_prepass<T, TM><<<(a.H + 7) / 8, 256, 0, s>>>(a);
+  k_mask_prepass<T, TM><<<a.H, 256, 0, s>>>(a);
   k_mask_reduce<<<1, 32, 0, s>>>(a);
   const dim3 grid((a.W + 31) / 32, (a.H + 7) / 8, 2);
   const dim3 grid_key((a.W + 31) / 32, (a.H + 31) / 32, 2);
