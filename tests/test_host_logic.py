@@ -96,3 +96,45 @@ def test_fp32_keys_order_like_int32_errors(bd, w, g):
     bits = e.view(np.uint32).astype(np.uint64)
     key = ((bits - 0x49800000) << 7) + np.arange(25, dtype=np.uint64)[None, :]
     assert np.array_equal(np.argmin(key, axis=1), best_ref)
+
+
+@pytest.mark.parametrize("bd,w,g,R", [(10, (4, 1, 1), 10, 2), (8, (4, 1, 1), 3, 5), (10, (4, 1, 1), 10, 4),
+                                      (9, (6, 2, 3), 5, 3)])
+def test_masked_integer_keys_order_like_int32_errors(bd, w, g, R):
+    """The masked search's key form: t = B + sum w r^2 + sum (-2 w s) r in uint32 is the error shifted
+    by a per-pixel constant into [0, 2B]; t * 128 + raster index, with masked candidates staged as
+    (0, 0, 0, 2^25 - 1), picks the reference's first strict minimum over unmasked candidates. The row-sum
+    split of d^2 M into 16 low bits and the rest sums exactly in 32 bits over 32 pixels."""
+    rng = np.random.default_rng(bd * 31 + R)
+    maxv = (1 << bd) - 1
+    D = 2 * R + 1
+    n = 8000
+    wi = np.array(w, np.int64)
+    B = int((wi * (maxv + g) ** 2).sum())
+    assert 2 * B < (1 << 25) - 1 and (maxv + g) ** 2 < (1 << 24)    # the host's condition for this form
+    s = rng.integers(-g, maxv + g + 1, (n, 3)).astype(np.int64)
+    r = rng.integers(0, maxv + 1, (n, D * D, 3)).astype(np.int64)
+    r[:, 5] = r[:, 1]                                                  # ties
+    masked = rng.random((n, D * D)) < 0.4
+    masked[:, (D * D) // 2] = False                                    # the centre of a searched pixel is unmasked
+    err = ((s[:, None, :] - r) ** 2 * wi).sum(-1)
+    best_ref = np.argmin(np.where(masked, np.iinfo(np.int64).max, err), axis=1)   # first strict minimum
+    u32 = np.uint64(0xffffffff)
+    q = (B + (wi * r * r).sum(-1)).astype(np.uint64)
+    a = (-2 * wi * s).astype(np.int64)
+    t = q.copy()
+    for c in range(3):
+        t = (t + ((a[:, None, c] * r[..., c]) & 0xffffffff).astype(np.uint64)) & u32
+    t = np.where(masked, np.uint64((1 << 25) - 1), t)
+    real = ~masked
+    assert t[real].max() <= 2 * B and np.array_equal(t[real].astype(np.int64), (err + B - (wi * s * s).sum(-1)[:, None])[real])
+    key = (t * np.uint64(128) + np.arange(D * D, dtype=np.uint64)[None, :]) & u32
+    assert np.array_equal(np.argmin(key, axis=1), best_ref)
+    # row sums: d^2 M split into low 16 bits and the rest, each summed over 32 pixels in 32 bits
+    m = rng.integers(0, 1 << 14, (n // 32, 32)).astype(np.uint64)
+    d2 = rng.integers(0, (maxv + g) ** 2 + 1, (n // 32, 32)).astype(np.uint64)
+    v = d2 * m
+    lo = (v & np.uint64(0xffff)).sum(1)
+    hi = (v >> np.uint64(16)).sum(1)
+    assert lo.max() < (1 << 32) and hi.max() < (1 << 32)
+    assert np.array_equal((hi << np.uint64(16)) + lo, v.sum(1))
