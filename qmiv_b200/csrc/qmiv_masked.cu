@@ -9,8 +9,9 @@
 //   k_cps_masked     the masked search (xCorrespPixelShiftSTD.cpp:151-215), both directions: masked
 //                    test pixels and masked candidates are skipped, the winner's squared differences
 //                    are weighted by the test pixel's mask value and summed per row in uint64;
-//                    k_cps_masked_key is the same search by exact integer keys, four pixels per
-//                    thread, where the bit depth, weights and GCD range bound every error
+//                    k_cps_masked_key is the same search by exact integer keys, both directions
+//                    per CTA, four pixels per thread, where the bit depth, weights and GCD range
+//                    bound every error
 //   k_mask_finalize  the ordered compensated sums (xKBNS.h:36-43) of the ERP row weights and the
 //                    row totals, one CTA per chain (terms staged in shared memory, one thread sums)
 // dB values, exact-component fake values and the picture averages are formed on the host in
@@ -257,51 +258,72 @@ __global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ Mask
 // pixel exactly as e does. The key t * 128 + k (k the raster index of the candidate) then orders them
 // as (error, raster index), so one unsigned minimum per candidate keeps the reference's first strict
 // minimum. A masked reference sample is staged as (0, 0, 0, 2^25 - 1): its key is above every real
-// one, so it never wins. Each thread searches four vertically adjacent pixels, so one staged sample
-// read from shared memory feeds up to four candidates.
-template <typename T, typename TM, int R>
-__global__ void __launch_bounds__(256, 4) k_cps_masked_key(const __grid_constant__ MaskArgs a)
+// one, so it never wins.
+// A CTA takes a 32 x 32 tile in both directions: it stages both pictures with an R halo (and the
+// tile's mask values) once; warps 0-7 search In1's pixels in In0 (R2T, -GCD), warps 8-15 In0's in In1
+// (T2R, +GCD), each thread four vertically adjacent pixels, so one staged sample read from shared
+// memory feeds up to four candidates. A test pixel's own samples come from the other picture's staged
+// tile (a masked one reads the sentinel, and its weight M = 0 discards the result).
+template <int R>
+struct MaskKeyGeo
 {
-  constexpr int P = 4, TW = 32, TH = 8 * P, SW = TW + 2 * R, SH = TH + 2 * R, D = 2 * R + 1;
+  static constexpr int P = 4, TW = 32, TH = 8 * P, SW = TW + 2 * R, SH = TH + 2 * R, D = 2 * R + 1;
+  static constexpr size_t kSmem = sizeof(int4) * 2 * SH * SW + sizeof(int32_t) * TH * TW;
+};
+
+template <typename T, typename TM, int R>
+__global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant__ MaskArgs a)
+{
+  using G = MaskKeyGeo<R>;
+  constexpr int P = G::P, TW = G::TW, TH = G::TH, SW = G::SW, SH = G::SH, D = G::D;
   constexpr uint32_t kMaskedT = (1u << 25) - 1u;
   static_assert(D * D <= 128, "the raster index must fit the key's low 7 bits");
-  __shared__ int4 st[SH][SW];                                // (Y, Cb, Cr, B + sum w r^2)
-  const int dir = blockIdx.z;
-  const Img& tst = dir ? a.in0 : a.in1;
-  const Img& ref = dir ? a.in1 : a.in0;
+  extern __shared__ int4 smem[];
+  int4* st0 = smem;                                          // In0: (Y, Cb, Cr, B + sum w r^2)
+  int4* st1 = smem + SH * SW;                                // In1
+  int32_t* mk = reinterpret_cast<int32_t*>(smem + 2 * SH * SW);   // M of the tile's pixels, 0 outside the picture
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
   const uint32_t w0 = (uint32_t)a.cws[0], w1 = (uint32_t)a.cws[1], w2 = (uint32_t)a.cws[2];
-  // the test pixels are read before the tile is staged so that their loads overlap the staging
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int x = x0 + tx, xc = min(x, a.W - 1);
+  for(int e = threadIdx.x; e < SH * SW; e += 512)
+  {
+    const int ly = e / SW, lx = e - ly * SW;
+    const int ux = x0 - R + lx, uy = y0 - R + ly;
+    const int gx = clampi(ux, 0, a.W - 1), gy = clampi(uy, 0, a.H - 1);
+    // branch-free: every sample is read, a masked one is replaced by the sentinel
+    const int32_t  mv = mask_at<TM>(a, gx, gy);
+    const uint32_t p0 = min((uint32_t)fetch<T>(a.in0, 0, gx, gy), a.clip);
+    const uint32_t p1 = min((uint32_t)fetch<T>(a.in0, 1, gx, gy), a.clip);
+    const uint32_t p2 = min((uint32_t)fetch<T>(a.in0, 2, gx, gy), a.clip);
+    const uint32_t q0 = min((uint32_t)fetch<T>(a.in1, 0, gx, gy), a.clip);
+    const uint32_t q1 = min((uint32_t)fetch<T>(a.in1, 1, gx, gy), a.clip);
+    const uint32_t q2 = min((uint32_t)fetch<T>(a.in1, 2, gx, gy), a.clip);
+    const uint32_t k0 = a.key_off + w0 * p0 * p0 + w1 * p1 * p1 + w2 * p2 * p2;
+    const uint32_t k1 = a.key_off + w0 * q0 * q0 + w1 * q1 * q1 + w2 * q2 * q2;
+    st0[e] = make_int4(mv ? (int32_t)p0 : 0, mv ? (int32_t)p1 : 0, mv ? (int32_t)p2 : 0, (int32_t)(mv ? k0 : kMaskedT));
+    st1[e] = make_int4(mv ? (int32_t)q0 : 0, mv ? (int32_t)q1 : 0, mv ? (int32_t)q2 : 0, (int32_t)(mv ? k1 : kMaskedT));
+    if(ly >= R && ly < R + TH && lx >= R && lx < R + TW) { mk[(ly - R) * TW + (lx - R)] = (ux < a.W && uy < a.H) ? mv : 0; }
+  }
+  __syncthreads();
+  const int dir = threadIdx.x >> 8;                          // warp-uniform
+  const int4* ref = dir ? st1 : st0;
+  const int4* tst = dir ? st0 : st1;
+  const int tx = threadIdx.x & 31, ty = (threadIdx.x & 255) >> 5;
   const int32_t sg = dir ? 1 : -1;
   int32_t s[P][3], c0[P], c1[P], c2[P], m[P];
   uint32_t best[P];
   #pragma unroll
   for(int p = 0; p < P; p++)
   {
-    const int y = y0 + ty * P + p, yc = min(y, a.H - 1);     // rows past the picture search a clamped pixel, discarded below
-    #pragma unroll
-    for(int c = 0; c < 3; c++) { s[p][c] = (int32_t)min((uint32_t)fetch<T>(tst, c, xc, yc), a.clip) + sg * a.out->gcd[c]; }
+    const int4 t = tst[(ty * P + p + R) * SW + tx + R];
+    s[p][0] = t.x + sg * a.out->gcd[0];
+    s[p][1] = t.y + sg * a.out->gcd[1];
+    s[p][2] = t.z + sg * a.out->gcd[2];
     c0[p] = -2 * (int32_t)w0 * s[p][0];
     c1[p] = -2 * (int32_t)w1 * s[p][1];
     c2[p] = -2 * (int32_t)w2 * s[p][2];
-    m[p] = (x < a.W && y < a.H) ? mask_at<TM>(a, x, y) : 0;  // 0 for masked and out-of-picture pixels
+    m[p] = mk[(ty * P + p) * TW + tx];
     best[p] = 0xffffffffu;
   }
-  for(int e = threadIdx.x; e < SH * SW; e += 256)
-  {
-    const int ly = e / SW, lx = e - ly * SW;
-    const int gx = clampi(x0 - R + lx, 0, a.W - 1), gy = clampi(y0 - R + ly, 0, a.H - 1);
-    // branch-free: every sample is read, a masked one is replaced by the sentinel
-    const int32_t  mk = mask_at<TM>(a, gx, gy);
-    const uint32_t r0 = min((uint32_t)fetch<T>(ref, 0, gx, gy), a.clip);
-    const uint32_t r1 = min((uint32_t)fetch<T>(ref, 1, gx, gy), a.clip);
-    const uint32_t r2 = min((uint32_t)fetch<T>(ref, 2, gx, gy), a.clip);
-    const uint32_t q = a.key_off + w0 * r0 * r0 + w1 * r1 * r1 + w2 * r2 * r2;
-    st[ly][lx] = make_int4(mk ? (int32_t)r0 : 0, mk ? (int32_t)r1 : 0, mk ? (int32_t)r2 : 0, (int32_t)(mk ? q : kMaskedT));
-  }
-  __syncthreads();
   // candidates in column pairs: one three-input minimum takes two keys
   auto key = [&](const int4& r, int p, int k) -> uint32_t {
     const uint32_t t = (uint32_t)r.w + (uint32_t)(c0[p] * r.x) + (uint32_t)(c1[p] * r.y) + (uint32_t)(c2[p] * r.z);
@@ -313,8 +335,8 @@ __global__ void __launch_bounds__(256, 4) k_cps_masked_key(const __grid_constant
     #pragma unroll
     for(int dx = 0; dx < D; dx += 2)
     {
-      const int4 ra = st[ty * P + j][tx + dx];
-      const int4 rb = st[ty * P + j][tx + min(dx + 1, D - 1)];
+      const int4 ra = ref[(ty * P + j) * SW + tx + dx];
+      const int4 rb = ref[(ty * P + j) * SW + tx + min(dx + 1, D - 1)];
       #pragma unroll
       for(int p = 0; p < P; p++)
       {
@@ -326,8 +348,8 @@ __global__ void __launch_bounds__(256, 4) k_cps_masked_key(const __grid_constant
     }
   }
   // Row sums. Each term d^2 M is below 2^38 here (d^2 < 2^24 is checked with the key bound, M < 2^14),
-  // so its low 16 bits and the rest (< 2^22) are summed over the warp's 32 pixels of a row in 32 bits each, exactly, by one
-  // redux.sync apiece.
+  // so its low 16 bits and the rest (< 2^22) are summed over the warp's 32 pixels of a row in 32 bits
+  // each, exactly, by one redux.sync apiece.
   uint32_t lo[P][3], hi[P][3];
   #pragma unroll
   for(int p = 0; p < P; p++)
@@ -335,7 +357,7 @@ __global__ void __launch_bounds__(256, 4) k_cps_masked_key(const __grid_constant
     // the minimum is always some candidate's key (no key has low bits 127), so k < D * D; the clamp
     // keeps the read in the tile whatever the data
     const int k = min((int)(best[p] & 127u), D * D - 1);
-    const int4 bp = st[ty * P + p + k / D][tx + k % D];
+    const int4 bp = ref[(ty * P + p + k / D) * SW + tx + k % D];
     const int32_t d[3] = { s[p][0] - bp.x, s[p][1] - bp.y, s[p][2] - bp.z };
     #pragma unroll
     for(int c = 0; c < 3; c++)
@@ -360,6 +382,17 @@ __global__ void __launch_bounds__(256, 4) k_cps_masked_key(const __grid_constant
       }
     }
   }
+}
+
+template <typename T, typename TM, int R>
+cudaError_t launch_masked_key(const MaskArgs& a, cudaStream_t s)
+{
+  constexpr size_t smem = MaskKeyGeo<R>::kSmem;
+  const cudaError_t e = cudaFuncSetAttribute(k_cps_masked_key<T, TM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if(e != cudaSuccess) { return e; }
+  const dim3 grid((a.W + MaskKeyGeo<R>::TW - 1) / MaskKeyGeo<R>::TW, (a.H + MaskKeyGeo<R>::TH - 1) / MaskKeyGeo<R>::TH);
+  k_cps_masked_key<T, TM, R><<<grid, 512, smem, s>>>(a);
+  return cudaSuccess;
 }
 
 // Chains 0..2: WS rows of component c; chains 3..8: CPS rows of (direction, component). Each is the
@@ -417,18 +450,19 @@ cudaError_t launch_masked_t(const MaskArgs& a, int R, bool key, cudaStream_t s)
   k_mask_prepass<T, TM><<<a.H, 256, 0, s>>>(a);
   k_mask_reduce<<<1, 32, 0, s>>>(a);
   const dim3 grid((a.W + 31) / 32, (a.H + 7) / 8, 2);
-  const dim3 grid_key((a.W + 31) / 32, (a.H + 31) / 32, 2);
   if(key)
   {
+    cudaError_t e;
     switch(R)
     {
-    case 1: k_cps_masked_key<T, TM, 1><<<grid_key, 256, 0, s>>>(a); break;
-    case 2: k_cps_masked_key<T, TM, 2><<<grid_key, 256, 0, s>>>(a); break;
-    case 3: k_cps_masked_key<T, TM, 3><<<grid_key, 256, 0, s>>>(a); break;
-    case 4: k_cps_masked_key<T, TM, 4><<<grid_key, 256, 0, s>>>(a); break;
-    case 5: k_cps_masked_key<T, TM, 5><<<grid_key, 256, 0, s>>>(a); break;
+    case 1: e = launch_masked_key<T, TM, 1>(a, s); break;
+    case 2: e = launch_masked_key<T, TM, 2>(a, s); break;
+    case 3: e = launch_masked_key<T, TM, 3>(a, s); break;
+    case 4: e = launch_masked_key<T, TM, 4>(a, s); break;
+    case 5: e = launch_masked_key<T, TM, 5>(a, s); break;
     default: return cudaErrorInvalidValue;
     }
+    if(e != cudaSuccess) { return e; }
   }
   else switch(R)
   {
