@@ -3,7 +3,8 @@
 // calls; the app refuses the SSIM family with a mask, :360-365).
 //
 //   k_mask_prepass   one CTA per 4:4:4 row: sum of (In1 - In0) * M (GCD-M), sum of (In1 - In0)^2 * M
-//                    per row (PSNR-M, WS-PSNR-M), non-zero mask samples, exactness, largest samples
+//                    per row (PSNR-M, WS-PSNR-M), non-zero mask samples, exactness, largest samples;
+//                    k_mask_prepass420v the same for aligned 4:2:0 frames with vector loads
 //   k_mask_reduce    GCD-M (xGlobClrDiff.cpp:60-91): IEEE divide by NumNonMasked * MaskMax,
 //                    round half away, clip
 //   k_cps_masked     the masked search (xCorrespPixelShiftSTD.cpp:151-215), both directions: masked
@@ -77,49 +78,14 @@ __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v)
   return v;
 }
 
-// One CTA per 4:4:4 row: each thread takes four columns 256 apart per step, issuing all their loads
-// before any arithmetic, then the warps' sums meet in shared memory and one thread writes the row's
-// SSD and adds the row's totals.
-template <typename T, typename TM>
-__global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ MaskArgs a)
+// The row's sums: warp sums meet in shared memory, one thread writes the row's SSD and adds the
+// row's totals (called by all 256 threads of the CTA).
+__device__ __forceinline__ void mask_prepass_row_tail(const MaskArgs& a, int y, int64_t sd[3], uint64_t ssd[3], uint32_t nnm,
+                                                      uint32_t dif, uint32_t mx0, uint32_t mx1)
 {
-  constexpr int U = 4;
   __shared__ uint64_t red[8][6];
   __shared__ uint32_t redu[8][4];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int y = blockIdx.x;
-  int64_t  sd[3] = { 0, 0, 0 };
-  uint64_t ssd[3] = { 0, 0, 0 };
-  uint32_t nnm = 0, dif = 0, mx0 = 0, mx1 = 0;
-  for(int xb = threadIdx.x; xb < a.W; xb += 256 * U)
-  {
-    int32_t  m[U];
-    uint32_t va[U][3], vb[U][3];
-    #pragma unroll
-    for(int u = 0; u < U; u++)
-    {
-      const int x = min(xb + u * 256, a.W - 1);              // columns past the row repeat the last one, masked out below
-      m[u] = xb + u * 256 < a.W ? mask_at<TM>(a, x, y) : 0;
-      #pragma unroll
-      for(int c = 0; c < 3; c++) { va[u][c] = (uint32_t)fetch<T>(a.in0, c, x, y); vb[u][c] = (uint32_t)fetch<T>(a.in1, c, x, y); }
-    }
-    #pragma unroll
-    for(int u = 0; u < U; u++)
-    {
-      if(xb + u * 256 >= a.W) { continue; }
-      nnm += m[u] != 0;
-      #pragma unroll
-      for(int c = 0; c < 3; c++)
-      {
-        mx0 = max(mx0, va[u][c]); mx1 = max(mx1, vb[u][c]);
-        const uint32_t p0 = min(va[u][c], a.clip), p1 = min(vb[u][c], a.clip);
-        const int32_t d = (int32_t)p1 - (int32_t)p0;
-        sd[c] += (int64_t)(d * m[u]);                          // int32 product, xDistortionSTD.cpp:50
-        ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)(uint32_t)m[u];    // xDistortionSTD.cpp:62
-        dif |= (d != 0 ? 1u : 0u) << c;
-      }
-    }
-  }
   #pragma unroll
   for(int c = 0; c < 3; c++)
   {
@@ -159,6 +125,147 @@ __global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ Ma
   atomicAdd(&o->nnm, (int32_t)nnm);
   atomicMax(&o->max_sample[0], mx0);
   atomicMax(&o->max_sample[1], mx1);
+}
+
+
+// One CTA per 4:4:4 row: each thread takes four columns 256 apart per step, issuing all their loads
+// before any arithmetic, then the warps' sums meet in shared memory and one thread writes the row's
+// SSD and adds the row's totals.
+template <typename T, typename TM>
+__global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ MaskArgs a)
+{
+  constexpr int U = 4;
+  const int y = blockIdx.x;
+  int64_t  sd[3] = { 0, 0, 0 };
+  uint64_t ssd[3] = { 0, 0, 0 };
+  uint32_t nnm = 0, dif = 0, mx0 = 0, mx1 = 0;
+  for(int xb = threadIdx.x; xb < a.W; xb += 256 * U)
+  {
+    int32_t  m[U];
+    uint32_t va[U][3], vb[U][3];
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      const int x = min(xb + u * 256, a.W - 1);              // columns past the row repeat the last one, masked out below
+      m[u] = xb + u * 256 < a.W ? mask_at<TM>(a, x, y) : 0;
+      #pragma unroll
+      for(int c = 0; c < 3; c++) { va[u][c] = (uint32_t)fetch<T>(a.in0, c, x, y); vb[u][c] = (uint32_t)fetch<T>(a.in1, c, x, y); }
+    }
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      if(xb + u * 256 >= a.W) { continue; }
+      nnm += m[u] != 0;
+      #pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        mx0 = max(mx0, va[u][c]); mx1 = max(mx1, vb[u][c]);
+        const uint32_t p0 = min(va[u][c], a.clip), p1 = min(vb[u][c], a.clip);
+        const int32_t d = (int32_t)p1 - (int32_t)p0;
+        sd[c] += (int64_t)(d * m[u]);                          // int32 product, xDistortionSTD.cpp:50
+        ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)(uint32_t)m[u];    // xDistortionSTD.cpp:62
+        dif |= (d != 0 ? 1u : 0u) << c;
+      }
+    }
+  }
+  mask_prepass_row_tail(a, y, sd, ssd, nnm, dif, mx0, mx1);
+}
+
+// 4:2:0 rows whose planes and mask are aligned for vector loads (checked on the host): a thread
+// takes four adjacent pixels per group, read as one 4-sample load per luma plane, one 2-sample
+// load per chroma plane and one 4-sample load of the mask; two groups 1024 pixels apart are in
+// flight per step. The sums are the same integers as the generic kernel's.
+__device__ __forceinline__ void ld4(const uint8_t* p, uint32_t v[4])
+{
+  const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(p));
+  v[0] = w & 0xffu; v[1] = (w >> 8) & 0xffu; v[2] = (w >> 16) & 0xffu; v[3] = w >> 24;
+}
+__device__ __forceinline__ void ld4(const uint16_t* p, uint32_t v[4])
+{
+  const uint2 w = __ldg(reinterpret_cast<const uint2*>(p));
+  v[0] = w.x & 0xffffu; v[1] = w.x >> 16; v[2] = w.y & 0xffffu; v[3] = w.y >> 16;
+}
+__device__ __forceinline__ void ld2(const uint8_t* p, uint32_t v[2])
+{
+  const uint32_t w = __ldg(reinterpret_cast<const unsigned short*>(p));
+  v[0] = w & 0xffu; v[1] = w >> 8;
+}
+__device__ __forceinline__ void ld2(const uint16_t* p, uint32_t v[2])
+{
+  const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(p));
+  v[0] = w & 0xffffu; v[1] = w >> 16;
+}
+
+template <typename T, typename TM>
+__global__ void __launch_bounds__(256) k_mask_prepass420v(const __grid_constant__ MaskArgs a)
+{
+  constexpr int U = 2;
+  const int y = blockIdx.x;
+  const int ng = a.W >> 2;                                    // groups of four pixels in the row
+  const T* l0 = static_cast<const T*>(a.in0.p[0]) + (size_t)y * a.in0.pitch[0];
+  const T* l1 = static_cast<const T*>(a.in1.p[0]) + (size_t)y * a.in1.pitch[0];
+  const T* u0 = static_cast<const T*>(a.in0.p[1]) + (size_t)(y >> 1) * a.in0.pitch[1];
+  const T* v0 = static_cast<const T*>(a.in0.p[2]) + (size_t)(y >> 1) * a.in0.pitch[2];
+  const T* u1 = static_cast<const T*>(a.in1.p[1]) + (size_t)(y >> 1) * a.in1.pitch[1];
+  const T* v1 = static_cast<const T*>(a.in1.p[2]) + (size_t)(y >> 1) * a.in1.pitch[2];
+  const TM* mr = static_cast<const TM*>(a.mask) + (size_t)y * a.mpitch;
+  int64_t  sd[3] = { 0, 0, 0 };
+  uint64_t ssd[3] = { 0, 0, 0 };
+  uint32_t nnm = 0, dif = 0, mx0 = 0, mx1 = 0;
+  for(int gb = threadIdx.x; gb < ng; gb += 256 * U)
+  {
+    uint32_t m[U][4], ya[U][4], yb[U][4], ca[U][2][2], cb[U][2][2];
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      const int g = min(gb + u * 256, ng - 1);               // groups past the row repeat the last one, skipped below
+      const int x = g << 2, xc = g << 1;
+      ld4(mr + x, m[u]);
+      ld4(l0 + x, ya[u]); ld4(l1 + x, yb[u]);
+      ld2(u0 + xc, ca[u][0]); ld2(v0 + xc, ca[u][1]);
+      ld2(u1 + xc, cb[u][0]); ld2(v1 + xc, cb[u][1]);
+    }
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      if(gb + u * 256 >= ng) { continue; }
+      #pragma unroll
+      for(int i = 0; i < 4; i++)
+      {
+        const int32_t mi = (int32_t)m[u][i];
+        nnm += mi != 0;
+        #pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          const uint32_t va = c ? ca[u][c - 1][i >> 1] : ya[u][i], vb = c ? cb[u][c - 1][i >> 1] : yb[u][i];
+          mx0 = max(mx0, va); mx1 = max(mx1, vb);
+          const uint32_t p0 = min(va, a.clip), p1 = min(vb, a.clip);
+          const int32_t d = (int32_t)p1 - (int32_t)p0;
+          sd[c] += (int64_t)(d * mi);                          // int32 product, xDistortionSTD.cpp:50
+          ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)(uint32_t)mi;    // xDistortionSTD.cpp:62
+          dif |= (d != 0 ? 1u : 0u) << c;
+        }
+      }
+    }
+  }
+  mask_prepass_row_tail(a, y, sd, ssd, nnm, dif, mx0, mx1);
+}
+
+// The vector loads of k_mask_prepass420v need 4:2:0, a width divisible by 4, luma rows of both frames
+// and mask rows starting on 4-sample boundaries and chroma rows on 2-sample boundaries.
+bool mask_prepass_vec_ok(const MaskArgs& a, size_t esz, size_t mesz)
+{
+  auto al = [](const void* p, size_t n) { return (reinterpret_cast<uintptr_t>(p) % n) == 0; };
+  if(a.W % 4 != 0 || a.mpitch % 4 != 0 || !al(a.mask, 4 * mesz)) { return false; }
+  const Img* ims[2] = { &a.in0, &a.in1 };
+  for(const Img* im : ims)
+  {
+    if(im->sx[0] != 0 || im->sy[0] != 0) { return false; }
+    for(int c = 1; c < 3; c++) { if(im->sx[c] != 1 || im->sy[c] != 1) { return false; } }
+    if(im->pitch[0] % 4 != 0 || !al(im->p[0], 4 * esz)) { return false; }
+    for(int c = 1; c < 3; c++) { if(im->pitch[c] % 2 != 0 || !al(im->p[c], 2 * esz)) { return false; } }
+  }
+  return true;
 }
 
 // GCD-M, xGlobClrDiff.cpp:60-91 (called with swapped pictures, xGlobClrDiff.h:42: mean of In1 - In0)
@@ -447,7 +554,8 @@ __global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ M
 template <typename T, typename TM>
 cudaError_t launch_masked_t(const MaskArgs& a, int R, bool key, cudaStream_t s)
 {
-  k_mask_prepass<T, TM><<<a.H, 256, 0, s>>>(a);
+  if(mask_prepass_vec_ok(a, sizeof(T), sizeof(TM))) { k_mask_prepass420v<T, TM><<<a.H, 256, 0, s>>>(a); }
+  else { k_mask_prepass<T, TM><<<a.H, 256, 0, s>>>(a); }
   k_mask_reduce<<<1, 32, 0, s>>>(a);
   const dim3 grid((a.W + 31) / 32, (a.H + 7) / 8, 2);
   if(key)
