@@ -74,3 +74,43 @@ def test_null_arguments_are_rejected():
     assert lib.qmiv_frame_pair_compute(None, None, None, 0, None) == 1
     assert lib.qmiv_calc_destroy(None) == 1
     assert lib.qmiv_batch_destroy(None) == 1
+
+
+def test_every_handle_entry_point_rejects_null():
+    """Each entry point checks its handle and pointers before any device work: a null handle gives
+    QMIV_ERR_INVALID_ARG (1) and a message, never a crash (the reference asserts instead)."""
+    import ctypes
+    import qmiv_b200
+    lib = qmiv_b200.library()
+    ms, nl, g4 = (ctypes.c_double * 8)(), (ctypes.c_uint64 * 8)(), (ctypes.c_int32 * 4)()
+    calls = {
+        "qmiv_ctx_destroy": lambda: lib.qmiv_ctx_destroy(None),
+        "qmiv_ctx_memory": lambda: lib.qmiv_ctx_memory(None, None, None),
+        "qmiv_ctx_set_profiling": lambda: lib.qmiv_ctx_set_profiling(None, 1),
+        "qmiv_ctx_stage_times": lambda: lib.qmiv_ctx_stage_times(None, ms, nl, 0),
+        "qmiv_frame_pair_submit": lambda: lib.qmiv_frame_pair_submit(None, None, None, 0),
+        "qmiv_frame_pair_wait": lambda: lib.qmiv_frame_pair_wait(None, 0, None),
+        "qmiv_frame_pair_compute_masked": lambda: lib.qmiv_frame_pair_compute_masked(None, None, None, None, 8, 0, None, None),
+        "qmiv_calc_set_color_space": lambda: lib.qmiv_calc_set_color_space(None, 0, 0),
+        "qmiv_calc_gcd": lambda: lib.qmiv_calc_gcd(None, None, None, g4),
+        "qmiv_calc_scp": lambda: lib.qmiv_calc_scp(None, None, None, None, None, None, 0),
+        "qmiv_calc_set_gcd": lambda: lib.qmiv_calc_set_gcd(None, None),
+        "qmiv_calc_cps_rows": lambda: lib.qmiv_calc_cps_rows(None, None, None),
+        "qmiv_calc_stream": lambda: lib.qmiv_calc_stream(None, None),
+        "qmiv_frame_pair_compute_static": lambda: lib.qmiv_frame_pair_compute_static(None, None, 64, 64, 8, 420, None, 1,
+                                                                                      None, None),
+        "qmiv_batch_create": lambda: lib.qmiv_batch_create(None, 4, 1 << 20, None, 0, None),
+        "qmiv_batch_compute": lambda: lib.qmiv_batch_compute(None, None, 0, None),
+        "qmiv_batch_submit": lambda: lib.qmiv_batch_submit(None, None, 0, None),
+        "qmiv_batch_wait": lambda: lib.qmiv_batch_wait(None, 0, None),
+        "qmiv_batch_stream": lambda: lib.qmiv_batch_stream(None, None),
+        "qmiv_batch_tuning": lambda: lib.qmiv_batch_tuning(None, 64, 64, 8, 2, None, None, None),
+        "qmiv_server_create": lambda: lib.qmiv_server_create(None, None, 4, 1 << 20, 1, None),
+        "qmiv_server_destroy": lambda: lib.qmiv_server_destroy(None),
+        "qmiv_server_submit": lambda: lib.qmiv_server_submit(None, None, None),
+        "qmiv_server_wait": lambda: lib.qmiv_server_wait(None, 0, 0, None, None),
+        "qmiv_server_stats": lambda: lib.qmiv_server_stats(None, None, None, None, None, 0),
+    }
+    for name, call in calls.items():
+        assert call() == 1, name
+        assert lib.qmiv_last_error(), name
