@@ -64,6 +64,7 @@ struct Geo
   static constexpr int Q  = Q0 + (12 - Q0 % 8) % 8;   // smallest >= Q0 with Q % 8 == 4
   static constexpr int RP = 2 * Q;                    // row pitch in float4
   static constexpr uint32_t kTileBytes = (uint32_t)SH * RP * 16u;
+  static constexpr uint32_t kCodeBytes = 2u * TH * TW; // winners' candidate codes [dir][TH][TW]
 };
 
 struct CpsGeomArgs
@@ -239,6 +240,65 @@ __device__ void convert(const CpsArgs& a, const CpsGeomArgs& g, const unsigned c
   }
 }
 
+// Two neighbouring samples of a raw row, as one 32-bit word (2-byte samples) or the low half of one
+// (1-byte samples); the address is even in samples.
+template <typename T>
+__device__ __forceinline__ uint32_t load_pair(const T* p)
+{
+  if constexpr(sizeof(T) == 2) { return *reinterpret_cast<const uint32_t*>(p); }
+  else { return *reinterpret_cast<const uint16_t*>(p); }
+}
+// Byte selectors placing the first / second sample of a pair into the low bits of 0x4B000000
+// (2^23), whose float value minus 2^23 is then the sample itself.
+template <typename T> struct PairSel;
+template <> struct PairSel<uint16_t> { static constexpr uint32_t lo = 0x7410u, hi = 0x7432u; };
+template <> struct PairSel<uint8_t>  { static constexpr uint32_t lo = 0x7440u, hi = 0x7441u; };
+__device__ __forceinline__ float pair_f(uint32_t pr, uint32_t sel) { return __uint_as_float(__byte_perm(pr, kBiasBits, sel)) - kBias; }
+
+// raw boxes -> float4 tiles for 4:2:0 pictures and an even search range. The staged samples then
+// start at even picture coordinates and fall into 2x2 units that share one chroma sample; a thread
+// converts whole units: each unit row's two luma samples from one load, the chroma pair and the
+// chroma part of q (w1 Cb^2 + w2 Cr^2 + 2^23) once. Coordinates are clamped as in `convert`: a unit
+// lies either wholly inside or wholly outside the picture in each direction (even W and H), and the
+// clamped column pair and the selectors reproduce the edge replication. The float4 values are those
+// of `convert`: every term is an integer below 2^24, so the changed order of the sums is exact.
+template <typename T, int R, int WY>
+__device__ void convert420(const CpsArgs& a, const CpsGeomArgs& g, const unsigned char* raw, float4* F0, float4* F1,
+                           int x0, int y0)
+{
+  using G = Geo<R, WY>;
+  static_assert(R % 2 == 0, "units start at even coordinates");
+  constexpr int UC = G::SW / 2, UR = G::SH / 2, NU = UC * UR;
+  const int W = a.W, H = a.H;
+  const int cw = W >> 1, chh = H >> 1;
+  const int xl = x0 - g.ax, yl = y0 - R, xc = (x0 >> 1) - g.ax, yc = (y0 - R) >> 1;
+  const float w0 = a.wf[0], w1 = a.wf[1], w2 = a.wf[2];
+  #pragma unroll 1
+  for(int u = threadIdx.x; u < 2 * NU; u += G::NT)
+  {
+    const int f = u >= NU ? 1 : 0;
+    const int r = u - f * NU;
+    const int ur = r / UC, uc = r - ur * UC;
+    const int gx = x0 - R + 2 * uc, gy = y0 - R + 2 * ur;
+    const int px = clampi(gx, 0, W - 2);
+    const uint32_t s0 = gx < W ? PairSel<T>::lo : PairSel<T>::hi;
+    const uint32_t s1 = gx >= 0 ? PairSel<T>::hi : PairSel<T>::lo;
+    const int gy0 = clampi(gy, 0, H - 1), gy1 = clampi(gy + 1, 0, H - 1);
+    const T* rl = reinterpret_cast<const T*>(raw + g.off[f][0]) + (px - xl);
+    const uint32_t l0 = load_pair<T>(rl + (gy0 - yl) * g.bwl), l1 = load_pair<T>(rl + (gy1 - yl) * g.bwl);
+    const int co = (clampi(gy >> 1, 0, chh - 1) - yc) * g.bwc + clampi(gx >> 1, 0, cw - 1) - xc;
+    const float cu = u2f_exact(reinterpret_cast<const T*>(raw + g.off[f][1])[co]);
+    const float cv = u2f_exact(reinterpret_cast<const T*>(raw + g.off[f][2])[co]);
+    const float qc = fmaf(w2, cv * cv, fmaf(w1, cu * cu, kBias));
+    const float y00 = pair_f(l0, s0), y01 = pair_f(l0, s1), y10 = pair_f(l1, s0), y11 = pair_f(l1, s1);
+    float4* d = (f ? F1 : F0) + 2 * ur * G::RP + uc;
+    d[0]             = make_float4(y00, cu, cv, fmaf(w0, y00 * y00, qc));
+    d[G::Q]          = make_float4(y01, cu, cv, fmaf(w0, y01 * y01, qc));
+    d[G::RP]         = make_float4(y10, cu, cv, fmaf(w0, y10 * y10, qc));
+    d[G::RP + G::Q]  = make_float4(y11, cu, cv, fmaf(w0, y11 * y11, qc));
+  }
+}
+
 // ---- search ---------------------------------------------------------------------------------
 // Thread (warp w, lane L) owns rows 4 * (w >> 1) + i (i < 4) of columns 64 * (w & 1) + 2L + j
 // (j < 2); p = 2 * i + j indexes its eight pixels.
@@ -378,113 +438,7 @@ __device__ __forceinline__ void search_int(const Thr& th, const float4* tst, con
   }
 }
 
-// ---- epilogue ---------------------------------------------------------------------------------
-// Winner of every pixel: per-component squared difference into the 32-bit row sums, SCP store,
-// and the SSIM moments of (test picture, SCP) of the 4x4 block the thread shares with its lane
-// neighbour.
-//
-// fp32 path: all values are integers below 2^24 (path condition), so float arithmetic is exact.
-// Tiles that reach past the picture (EDGE) weight every pixel by 1 (inside) or 0 (outside).
-template <int R, int WY, typename T, bool EDGE, bool MOM, bool SCP>
-__device__ __forceinline__ void epilogue_fp(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref,
-                                            const uint32_t idx[8], int dir, int x0, int y0, int ga, int gb, int gc)
-{
-  using G = Geo<R, WY>;
-  using C = Code<R>;
-  uint32_t* rows = a.rows + (size_t)dir * a.H * 3;
-  T* scp = static_cast<T*>(dir ? a.scp0 : a.scp1);
-  const size_t plane = (size_t)a.W * a.H;
-  const int xb = x0 + 2 * th.hx, yb = y0 + th.y0;
-  const float fg[3] = { (float)ga, (float)gb, (float)gc };
-  const float fmax = (float)a.maxv;
-  const float4* rrow = ref + th.y0 * G::RP + th.hx;
-  const float4* trow = tst + (th.y0 + R) * G::RP + th.hx;
-  float cm[2] = { 1.f, 1.f };
-  if(EDGE) { cm[0] = xb < a.W ? 1.f : 0.f; cm[1] = xb + 1 < a.W ? 1.f : 0.f; }
-  float mm[3][5];
-  #pragma unroll
-  for(int c = 0; c < 3; c++)
-  {
-    #pragma unroll
-    for(int m = 0; m < 5; m++) { mm[c][m] = 0.f; }
-  }
-  uint32_t rs[12];
-  #pragma unroll
-  for(int i = 0; i < 4; i++)
-  {
-    const int y = yb + i;
-    const float rmask = (!EDGE || y < a.H) ? 1.f : 0.f;
-    float frs[3] = { 0.f, 0.f, 0.f };
-    #pragma unroll
-    for(int j = 0; j < 2; j++)
-    {
-      const uint32_t k = idx[2 * i + j];
-      const int dyi = C::dy(k), dx = j + C::dx(k);
-      const float4 r = rrow[(i + dyi) * G::RP + (dx & 1) * G::Q + (dx >> 1)];
-      const float4 t = trow[i * G::RP + ((j + R) & 1) * G::Q + ((j + R) >> 1)];
-      const float m = EDGE ? rmask * cm[j] : 1.f;
-      const float rv[3] = { r.x, r.y, r.z }, tv[3] = { t.x, t.y, t.z };
-      #pragma unroll
-      for(int c = 0; c < 3; c++)
-      {
-        const float rg = rv[c] - fg[c];
-        const float d = tv[c] - rg;
-        const float b = fminf(fmaxf(rg, 0.f), fmax);
-        frs[c] = fmaf(EDGE ? d * m : d, d, frs[c]);
-        if(MOM)
-        {
-          const float tm = EDGE ? tv[c] * m : tv[c], bm = EDGE ? b * m : b;
-          mm[c][0] += tm;
-          mm[c][1] += bm;
-          mm[c][2] = fmaf(tm, tv[c], mm[c][2]);
-          mm[c][3] = fmaf(bm, b, mm[c][3]);
-          mm[c][4] = fmaf(tm, b, mm[c][4]);
-        }
-        if(SCP && (!EDGE || m != 0.f)) { scp[(size_t)c * plane + (size_t)y * a.W + xb + j] = (T)f2i_exact(b); }
-      }
-    }
-    #pragma unroll
-    for(int c = 0; c < 3; c++)
-    {
-      // 2^23 + (a sum below 2^23) has the sum in its low bits; 32 lanes add 32 x 0x4B000000
-      rs[3 * i + c] = __reduce_add_sync(kFull, __float_as_uint(frs[c] + kBias)) - 32u * kBiasBits;
-    }
-  }
-  // the warp's twelve row sums (row yb + i, component c) go out in one atomic: lane 3 i + c adds
-  // rs[3 i + c] to rows[(yb + i) * 3 + c]
-  if(th.lane < 12)
-  {
-    uint32_t v = rs[0];
-    #pragma unroll
-    for(int q = 1; q < 12; q++) { v = th.lane == q ? rs[q] : v; }
-    if(!EDGE || yb + ((th.lane * 11) >> 5) < a.H) { atomicAdd(rows + (size_t)yb * 3 + th.lane, v); }
-  }
-  if(MOM)
-  {
-    // lanes 2m and 2m + 1 hold the two column halves of block bx; all shuffles first, then the even
-    // lanes store the fifteen moment planes' values
-    const Moments mom = a.mom[dir];
-    const int bx = xb >> 2, by = yb >> 2;
-    uint32_t mv[15];
-    #pragma unroll
-    for(int c = 0; c < 3; c++)
-    {
-      #pragma unroll
-      for(int m = 0; m < 5; m++)
-      {
-        mv[5 * c + m] = __float2uint_rn(mm[c][m] + __shfl_xor_sync(kFull, mm[c][m], 1));   // exact: integers below 2^24
-      }
-    }
-    if((th.lane & 1) == 0 && bx < mom.nbx && by < mom.nby)
-    {
-      uint32_t* q = mom.p + (size_t)by * mom.pitch + bx;
-      const size_t plane = mom.plane();
-      #pragma unroll
-      for(int k = 0; k < 15; k++) { q[0] = mv[k]; q += plane; }
-    }
-  }
-}
-
+// ---- epilogue of the int32 path ----------------------------------------------------------------
 // int32 path: the SSE path's wrap-around arithmetic
 template <int R, int WY, typename T>
 __device__ __forceinline__ void epilogue_int(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref,
@@ -572,23 +526,163 @@ __device__ __noinline__ void direction_int(const Thr& th, const CpsArgs& a, cons
   epilogue_int<R, WY, T>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc);
 }
 
-template <int R, int WY, typename T>
-__device__ __forceinline__ void epilogue_dispatch(const Thr& th, const CpsArgs& a, const float4* tst, const float4* ref,
-                                                  const uint32_t idx[8], int dir, int x0, int y0, int ga, int gb, int gc)
+// ---- block epilogue (fp32 path) -------------------------------------------------------------------
+// After both searches the winners' codes sit in shared memory ([dir][TH][TW] bytes) and the threads
+// are re-dealt: warp w takes direction w / WY and the 4x4 blocks of tile rows 4 (w % WY) .. + 3,
+// lane L the block of columns 4 L .. 4 L + 3. A thread then holds a whole SSIM sub-block (its moments
+// need no exchange between lanes and leave as one coalesced store per moment plane), and a warp
+// holds whole tile rows (one warp reduction per row and component).
+//
+// Staged position of candidate k of pixel (i, j) relative to the block's first candidate:
+// i RP + off[j & 1][k] + (j >> 1), off[p][k] = dy RP + ((p + dx) & 1) Q + ((p + dx) >> 1) for the
+// parity-split rows. Codes that no search produces map to 0 (never read, kept in bounds).
+template <int R, int WY>
+__device__ __forceinline__ void build_offsets(int16_t* off)
 {
   using G = Geo<R, WY>;
+  using C = Code<R>;
+  for(int e = threadIdx.x; e < 256; e += G::NT)
+  {
+    const int p = e >> 7, k = e & 127;
+    const int dy = C::dy((uint32_t)k), dx = C::dx((uint32_t)k);
+    const bool valid = k <= (int)C::kMax && dy < G::D && dx < G::D;
+    off[e] = valid ? (int16_t)(dy * G::RP + ((p + dx) & 1) * G::Q + ((p + dx) >> 1)) : (int16_t)0;
+  }
+}
+
+// the eight codes a search thread owns: row 4 (w >> 1) + i, columns 64 (w & 1) + 2 L + j
+template <int R, int WY>
+__device__ __forceinline__ void store_codes(const Thr& th, uint8_t* codes, int dir, const uint32_t idx[8])
+{
+  using G = Geo<R, WY>;
+  uint8_t* cw = codes + dir * (G::TH * G::TW) + th.y0 * G::TW + 2 * th.hx;
+  #pragma unroll
+  for(int i = 0; i < 4; i++) { *reinterpret_cast<uint16_t*>(cw + i * G::TW) = (uint16_t)(idx[2 * i] | (idx[2 * i + 1] << 8)); }
+}
+
+// fp32 path: every value is an integer below 2^24 (path condition), so the float arithmetic is exact;
+// a row's four squared differences add below 2^23. Tiles that reach past the picture (EDGE) weight
+// every pixel by 1 (inside) or 0 (outside).
+template <int R, int WY, typename T, bool EDGE, bool MOM, bool SCP>
+__device__ __forceinline__ void epilogue_blk(const CpsArgs& a, const float4* F0, const float4* F1, const uint8_t* codes,
+                                             const int16_t* off, int dir, int x0, int y0, int g0, int g1, int g2)
+{
+  using G = Geo<R, WY>;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int by = warp - dir * WY, bx = lane;
+  const float4* tst = dir ? F1 : F0;
+  const float4* ref = dir ? F0 : F1;
+  uint32_t* rows = a.rows + (size_t)dir * a.H * 3;
+  T* scp = static_cast<T*>(dir ? a.scp0 : a.scp1);
+  const size_t plane = (size_t)a.W * a.H;
+  const int xb = x0 + 4 * bx, yb = y0 + 4 * by;
+  const float sg = dir ? -1.f : 1.f;
+  const float fg[3] = { sg * (float)g0, sg * (float)g1, sg * (float)g2 };
+  const float fmax = (float)a.maxv;
+  const float4* rb = ref + 4 * by * G::RP + 2 * bx;
+  const float4* tb = tst + (4 * by + R) * G::RP + 2 * bx;
+  const uint8_t* cb = codes + dir * (G::TH * G::TW) + 4 * by * G::TW + 4 * bx;
+  float cm[4] = { 1.f, 1.f, 1.f, 1.f };
+  if(EDGE)
+  {
+    #pragma unroll
+    for(int j = 0; j < 4; j++) { cm[j] = xb + j < a.W ? 1.f : 0.f; }
+  }
+  float mm[3][5];
+  #pragma unroll
+  for(int c = 0; c < 3; c++)
+  {
+    #pragma unroll
+    for(int m = 0; m < 5; m++) { mm[c][m] = 0.f; }
+  }
+  uint32_t rs[12];
+  #pragma unroll
+  for(int i = 0; i < 4; i++)
+  {
+    const int y = yb + i;
+    const float rmask = (!EDGE || y < a.H) ? 1.f : 0.f;
+    const uint32_t c4 = *reinterpret_cast<const uint32_t*>(cb + i * G::TW);
+    float frs[3] = { 0.f, 0.f, 0.f };
+    #pragma unroll
+    for(int j = 0; j < 4; j++)
+    {
+      const uint32_t k = (c4 >> (8 * j)) & 0xffu;
+      const float4 r = rb[i * G::RP + off[(j & 1) * 128 + k] + (j >> 1)];
+      const float4 t = tb[i * G::RP + ((j + R) & 1) * G::Q + ((j + R) >> 1)];
+      const float m = EDGE ? rmask * cm[j] : 1.f;
+      const float rv[3] = { r.x, r.y, r.z }, tv[3] = { t.x, t.y, t.z };
+      #pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const float rg = rv[c] - fg[c];
+        const float d = tv[c] - rg;
+        const float b = fminf(fmaxf(rg, 0.f), fmax);
+        frs[c] = fmaf(EDGE ? d * m : d, d, frs[c]);
+        if(MOM)
+        {
+          const float tm = EDGE ? tv[c] * m : tv[c], bm = EDGE ? b * m : b;
+          mm[c][0] += tm;
+          mm[c][1] += bm;
+          mm[c][2] = fmaf(tm, tv[c], mm[c][2]);
+          mm[c][3] = fmaf(bm, b, mm[c][3]);
+          mm[c][4] = fmaf(tm, b, mm[c][4]);
+        }
+        if(SCP && (!EDGE || m != 0.f)) { scp[(size_t)c * plane + (size_t)y * a.W + xb + j] = (T)f2i_exact(b); }
+      }
+    }
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      // 2^23 + (a sum below 2^23) has the sum in its low bits; 32 lanes add 32 x 0x4B000000
+      rs[3 * i + c] = __reduce_add_sync(kFull, __float_as_uint(frs[c] + kBias)) - 32u * kBiasBits;
+    }
+  }
+  // the warp's twelve row sums (row yb + i, component c) go out in one atomic: lane 3 i + c adds
+  // rs[3 i + c] to rows[(yb + i) * 3 + c]
+  if(lane < 12)
+  {
+    uint32_t v = rs[0];
+    #pragma unroll
+    for(int q = 1; q < 12; q++) { v = lane == q ? rs[q] : v; }
+    if(!EDGE || yb + ((lane * 11) >> 5) < a.H) { atomicAdd(rows + (size_t)yb * 3 + lane, v); }
+  }
+  if(MOM)
+  {
+    const Moments mom = a.mom[dir];
+    const int bxg = xb >> 2, byg = yb >> 2;
+    if(bxg < mom.nbx && byg < mom.nby)
+    {
+      uint32_t* q = mom.p + (size_t)byg * mom.pitch + bxg;
+      const size_t mplane = mom.plane();
+      #pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        #pragma unroll
+        for(int m = 0; m < 5; m++) { q[0] = __float2uint_rn(mm[c][m]); q += mplane; }   // exact: integers below 2^24
+      }
+    }
+  }
+}
+
+template <int R, int WY, typename T>
+__device__ __forceinline__ void epilogue_blk_dispatch(const CpsArgs& a, const float4* F0, const float4* F1,
+                                                      const uint8_t* codes, const int16_t* off, int x0, int y0,
+                                                      int g0, int g1, int g2)
+{
+  using G = Geo<R, WY>;
+  const int dir = (int)(threadIdx.x >> 5) >= WY ? 1 : 0;
   const int sel = ((x0 + G::TW > a.W || y0 + G::TH > a.H) ? 4 : 0) | (a.mom[dir].p != nullptr ? 2 : 0) |
                   ((dir ? a.scp0 : a.scp1) != nullptr ? 1 : 0);
   switch(sel)
   {
-  case 0: epilogue_fp<R, WY, T, false, false, false>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
-  case 1: epilogue_fp<R, WY, T, false, false, true>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
-  case 2: epilogue_fp<R, WY, T, false, true, false>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
-  case 3: epilogue_fp<R, WY, T, false, true, true>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
-  case 4: epilogue_fp<R, WY, T, true, false, false>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
-  case 5: epilogue_fp<R, WY, T, true, false, true>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
-  case 6: epilogue_fp<R, WY, T, true, true, false>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
-  default: epilogue_fp<R, WY, T, true, true, true>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc); break;
+  case 0: epilogue_blk<R, WY, T, false, false, false>(a, F0, F1, codes, off, dir, x0, y0, g0, g1, g2); break;
+  case 1: epilogue_blk<R, WY, T, false, false, true>(a, F0, F1, codes, off, dir, x0, y0, g0, g1, g2); break;
+  case 2: epilogue_blk<R, WY, T, false, true, false>(a, F0, F1, codes, off, dir, x0, y0, g0, g1, g2); break;
+  case 3: epilogue_blk<R, WY, T, false, true, true>(a, F0, F1, codes, off, dir, x0, y0, g0, g1, g2); break;
+  case 4: epilogue_blk<R, WY, T, true, false, false>(a, F0, F1, codes, off, dir, x0, y0, g0, g1, g2); break;
+  case 5: epilogue_blk<R, WY, T, true, false, true>(a, F0, F1, codes, off, dir, x0, y0, g0, g1, g2); break;
+  case 6: epilogue_blk<R, WY, T, true, true, false>(a, F0, F1, codes, off, dir, x0, y0, g0, g1, g2); break;
+  default: epilogue_blk<R, WY, T, true, true, true>(a, F0, F1, codes, off, dir, x0, y0, g0, g1, g2); break;
   }
 }
 
@@ -609,15 +703,18 @@ __device__ __forceinline__ void cps_loop(int ntiles, const Locate& locate, uint3
   unsigned char* base = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);   // TMA boxes: 128-byte aligned
   float4* F0 = reinterpret_cast<float4*>(base);
   float4* F1 = F0 + G::SH * G::RP;
-  unsigned char* raw = base + 2 * G::kTileBytes;
+  uint8_t* codes = reinterpret_cast<uint8_t*>(base + 2 * G::kTileBytes);
+  unsigned char* raw = base + 2 * G::kTileBytes + G::kCodeBytes;
   uint64_t* bar = reinterpret_cast<uint64_t*>(raw + raw_cap);
   const Thr th;
   // the current pair's arguments, copied to shared memory whenever the work list enters a new pair
   __shared__ __align__(16) CpsArgs s_a;
   __shared__ __align__(16) CpsGeomArgs s_g;
+  __shared__ int16_t s_off[256];
   static_assert(sizeof(CpsArgs) % 4 == 0 && sizeof(CpsGeomArgs) % 4 == 0, "word copies");
 
   if(threadIdx.x == 0) { mbar_init(bar, 1); fence_barrier_init(); }
+  build_offsets<R, WY>(s_off);
   __syncthreads();
   int t = blockIdx.x;
   if(t < ntiles && threadIdx.x == 0)
@@ -659,7 +756,15 @@ __device__ __forceinline__ void cps_loop(int ntiles, const Locate& locate, uint3
       __syncthreads();
     }
     if(a.clip < (sizeof(T) == 1 ? 0xffu : 0xffffu)) { convert<T, R, WY, true>(a, g, raw, F0, F1, x0, y0); }
-    else { convert<T, R, WY, false>(a, g, raw, F0, F1, x0, y0); }
+    else
+    {
+      if constexpr(R % 2 == 0)
+      {
+        if(g.sx == 1 && g.sy == 1) { convert420<T, R, WY>(a, g, raw, F0, F1, x0, y0); }
+        else { convert<T, R, WY, false>(a, g, raw, F0, F1, x0, y0); }
+      }
+      else { convert<T, R, WY, false>(a, g, raw, F0, F1, x0, y0); }
+    }
     __syncthreads();
     // the raw boxes are free again: the next tile's copies overlap this tile's search
     const int tn = t + (int)gridDim.x;
@@ -674,22 +779,29 @@ __device__ __forceinline__ void cps_loop(int ntiles, const Locate& locate, uint3
     }
     const int g0 = a.gcd_src->gcd[0], g1 = a.gcd_src->gcd[1], g2 = a.gcd_src->gcd[2];
     const bool int_path = (a.gcd_src->flags & 4) != 0;
-    #pragma unroll 1
-    for(int dir = 0; dir < 2; dir++)
+    // dir 0 (R2T): test = In0 + GCD searched in In1 -> rows[0], SCP1 = clip(In1[best] - GCD)
+    // dir 1 (T2R): test = In1 - GCD searched in In0 -> rows[1], SCP0 = clip(In0[best] + GCD)
+    if(!int_path)
     {
-      // dir 0 (R2T): test = In0 + GCD searched in In1 -> rows[0], SCP1 = clip(In1[best] - GCD)
-      // dir 1 (T2R): test = In1 - GCD searched in In0 -> rows[1], SCP0 = clip(In0[best] + GCD)
-      const float4* tst = dir ? F1 : F0;
-      const float4* ref = dir ? F0 : F1;
-      const int sg = dir ? -1 : 1;
-      const int ga = sg * g0, gb = sg * g1, gc = sg * g2;
-      if(!int_path)
+      #pragma unroll 1
+      for(int dir = 0; dir < 2; dir++)
       {
+        const float sg = dir ? -1.f : 1.f;
         uint32_t idx[8];
-        search_fp32<R, WY>(th, tst, ref, a.wf, (float)ga, (float)gb, (float)gc, idx);
-        epilogue_dispatch<R, WY, T>(th, a, tst, ref, idx, dir, x0, y0, ga, gb, gc);
+        search_fp32<R, WY>(th, dir ? F1 : F0, dir ? F0 : F1, a.wf, sg * (float)g0, sg * (float)g1, sg * (float)g2, idx);
+        store_codes<R, WY>(th, codes, dir, idx);
       }
-      else { direction_int<R, WY, T>(th, a, tst, ref, dir, x0, y0, ga, gb, gc); }
+      __syncthreads();
+      epilogue_blk_dispatch<R, WY, T>(a, F0, F1, codes, s_off, x0, y0, g0, g1, g2);
+    }
+    else
+    {
+      #pragma unroll 1
+      for(int dir = 0; dir < 2; dir++)
+      {
+        const int sg = dir ? -1 : 1;
+        direction_int<R, WY, T>(th, a, dir ? F1 : F0, dir ? F0 : F1, dir, x0, y0, sg * g0, sg * g1, sg * g2);
+      }
     }
     __syncthreads();
   }
@@ -697,14 +809,14 @@ __device__ __forceinline__ void cps_loop(int ntiles, const Locate& locate, uint3
 
 // one frame pair, arguments in parameter space
 template <int R, int WY, typename T>
-__global__ void __launch_bounds__(64 * WY, 1) k_cps(const __grid_constant__ CpsKernelArgs k)
+__global__ void __launch_bounds__(64 * WY, WY == 4 ? 2 : 1) k_cps(const __grid_constant__ CpsKernelArgs k)
 {
   cps_loop<R, WY, T, false>(k.g.ntiles, [&](int t) { return TileRef{ &k, t }; }, k.g.raw_bytes);
 }
 
 // work list over the tiles of many frame pairs: pair p owns tiles [prefix[p], prefix[p + 1])
 template <int R, int WY, typename T>
-__global__ void __launch_bounds__(64 * WY, 1) k_cps_multi(const CpsKernelArgs* __restrict__ descs,
+__global__ void __launch_bounds__(64 * WY, WY == 4 ? 2 : 1) k_cps_multi(const CpsKernelArgs* __restrict__ descs,
                                                           const int32_t* __restrict__ prefix, int npairs, int ntiles,
                                                           uint32_t raw_cap)
 {
@@ -797,7 +909,7 @@ size_t plan(CpsGeomArgs& g, int esz, int sx, int sy)
   }
   g.raw_bytes = cur;
   g.tx_bytes = (uint32_t)(2 * (g.bwl * g.bhl + 2 * g.bwc * g.bhc) * esz);
-  return kAlign + 2 * (size_t)G::kTileBytes + cur + 16;
+  return kAlign + 2 * (size_t)G::kTileBytes + G::kCodeBytes + cur + 16;
 }
 
 template <int R, int WY>
