@@ -1,8 +1,8 @@
 // Corresponding-pixel-shift search (libs/pmbb-ivqm/src/xCorrespPixelShiftSSE.cpp:18-127) for
-// sm_100a: persistent CTAs, TMA tile loads, 4 x 2 pixels per thread.
+// sm_100a: persistent CTAs, TMA tile loads, 4 x 2 pixels per thread in the search.
 //
-// Per tile of 128 x TH output pixels (TH = 32, or 16 when shared memory is short) a CTA of
-// 2 x TH / 4 warps
+// Per tile of 128 x TH output pixels (TH = 32, or 16 when shared memory is short or the autotuner
+// prefers two CTAs per SM) a CTA of 2 x TH / 4 warps
 //   1. receives both pictures' raw samples of the tile plus an R-pixel halo (luma box and the
 //      two chroma boxes of each picture) through TMA into shared memory; the copies of tile n+1
 //      are issued as soon as tile n's raw samples are converted, so they land during its search;
@@ -10,9 +10,13 @@
 //      reading every sample at its clamped picture coordinate (the reference's edge-replicated
 //      margin, apps/QMIV/src/xAppQMIV.cpp:353 and :899) and the chroma of 4:2:0 / 4:2:2 at
 //      (x >> sx, y >> sy) (the nearest upsampling of libs/pmbb-core/src/xPixelOpsSTD.cpp:30-87);
+//      4:2:0 tiles at an even search range are converted as 2x2 units sharing one chroma sample;
 //   3. searches both directions. A thread owns 4 rows x 2 columns of output pixels, so each
-//      staged reference pixel is loaded once per thread for up to 8 of its pixels; two lanes
-//      together hold one 4x4 SSIM sub-block.
+//      staged reference pixel is loaded once per thread for up to 8 of its pixels; the winners'
+//      candidate codes go to shared memory;
+//   4. re-deals the threads for the epilogue: one thread per 4x4 block and direction gathers its
+//      16 winners, adds their squared differences to the 32-bit row sums, writes the shift-
+//      compensated samples (SCP) or the IV-SSIM sub-block moments of (test picture, SCP).
 //
 // Exact fp32 keys: for a test pixel s (test + GCD, unclipped) and candidate r,
 //     e - sum_c w_c s_c^2 + 2^23 = (q(r) + 2^23) + sum_c (-2 w_c s_c) r_c
@@ -260,9 +264,10 @@ __device__ __forceinline__ float pair_f(uint32_t pr, uint32_t sel) { return __ui
 // converts whole units: each unit row's two luma samples from one load, the chroma pair and the
 // chroma part of q (w1 Cb^2 + w2 Cr^2 + 2^23) once. Coordinates are clamped as in `convert`: a unit
 // lies either wholly inside or wholly outside the picture in each direction (even W and H), and the
-// clamped column pair and the selectors reproduce the edge replication. The float4 values are those
-// of `convert`: every term is an integer below 2^24, so the changed order of the sums is exact.
-template <typename T, int R, int WY>
+// clamped column pair and the selectors reproduce the edge replication; tiles whose halo lies inside
+// the picture (INTERIOR) skip the clamps. The float4 values are those of `convert`: every term is an
+// integer below 2^24, so the changed order of the sums is exact.
+template <typename T, int R, int WY, bool INTERIOR>
 __device__ void convert420(const CpsArgs& a, const CpsGeomArgs& g, const unsigned char* raw, float4* F0, float4* F1,
                            int x0, int y0)
 {
@@ -279,16 +284,32 @@ __device__ void convert420(const CpsArgs& a, const CpsGeomArgs& g, const unsigne
     const int f = u >= NU ? 1 : 0;
     const int r = u - f * NU;
     const int ur = r / UC, uc = r - ur * UC;
-    const int gx = x0 - R + 2 * uc, gy = y0 - R + 2 * ur;
-    const int px = clampi(gx, 0, W - 2);
-    const uint32_t s0 = gx < W ? PairSel<T>::lo : PairSel<T>::hi;
-    const uint32_t s1 = gx >= 0 ? PairSel<T>::hi : PairSel<T>::lo;
-    const int gy0 = clampi(gy, 0, H - 1), gy1 = clampi(gy + 1, 0, H - 1);
-    const T* rl = reinterpret_cast<const T*>(raw + g.off[f][0]) + (px - xl);
-    const uint32_t l0 = load_pair<T>(rl + (gy0 - yl) * g.bwl), l1 = load_pair<T>(rl + (gy1 - yl) * g.bwl);
-    const int co = (clampi(gy >> 1, 0, chh - 1) - yc) * g.bwc + clampi(gx >> 1, 0, cw - 1) - xc;
-    const float cu = u2f_exact(reinterpret_cast<const T*>(raw + g.off[f][1])[co]);
-    const float cv = u2f_exact(reinterpret_cast<const T*>(raw + g.off[f][2])[co]);
+    const T* rl = reinterpret_cast<const T*>(raw + g.off[f][0]);
+    const T* ru = reinterpret_cast<const T*>(raw + g.off[f][1]);
+    const T* rv = reinterpret_cast<const T*>(raw + g.off[f][2]);
+    uint32_t l0, l1, s0 = PairSel<T>::lo, s1 = PairSel<T>::hi;
+    int co;
+    if(INTERIOR)
+    {
+      // the tile and its halo lie inside the picture: unit (ur, uc) is raw luma (2 ur, ax - R + 2 uc)
+      // and raw chroma (ur, ax - R / 2 + uc)
+      const T* p = rl + 2 * ur * g.bwl + (g.ax - R) + 2 * uc;
+      l0 = load_pair<T>(p);
+      l1 = load_pair<T>(p + g.bwl);
+      co = ur * g.bwc + (g.ax - R / 2) + uc;
+    }
+    else
+    {
+      const int gx = x0 - R + 2 * uc, gy = y0 - R + 2 * ur;
+      const int px = clampi(gx, 0, W - 2);
+      s0 = gx < W ? PairSel<T>::lo : PairSel<T>::hi;
+      s1 = gx >= 0 ? PairSel<T>::hi : PairSel<T>::lo;
+      const int gy0 = clampi(gy, 0, H - 1), gy1 = clampi(gy + 1, 0, H - 1);
+      l0 = load_pair<T>(rl + (gy0 - yl) * g.bwl + (px - xl));
+      l1 = load_pair<T>(rl + (gy1 - yl) * g.bwl + (px - xl));
+      co = (clampi(gy >> 1, 0, chh - 1) - yc) * g.bwc + clampi(gx >> 1, 0, cw - 1) - xc;
+    }
+    const float cu = u2f_exact(ru[co]), cv = u2f_exact(rv[co]);
     const float qc = fmaf(w2, cv * cv, fmaf(w1, cu * cu, kBias));
     const float y00 = pair_f(l0, s0), y01 = pair_f(l0, s1), y10 = pair_f(l1, s0), y11 = pair_f(l1, s1);
     float4* d = (f ? F1 : F0) + 2 * ur * G::RP + uc;
@@ -595,20 +616,24 @@ __device__ __forceinline__ void epilogue_blk(const CpsArgs& a, const float4* F0,
     #pragma unroll
     for(int m = 0; m < 5; m++) { mm[c][m] = 0.f; }
   }
-  uint32_t rs[12];
-  #pragma unroll
+  // the four rows run as a loop (not unrolled) to keep the kernel's hot code small; lanes 0-2 add
+  // the warp's row sums of components 0-2 to rows[y * 3 + c]
+  const bool l1 = lane == 1, l2 = lane == 2;
+  #pragma unroll 1
   for(int i = 0; i < 4; i++)
   {
     const int y = yb + i;
     const float rmask = (!EDGE || y < a.H) ? 1.f : 0.f;
     const uint32_t c4 = *reinterpret_cast<const uint32_t*>(cb + i * G::TW);
+    const float4* rr = rb + i * G::RP;
+    const float4* tr = tb + i * G::RP;
     float frs[3] = { 0.f, 0.f, 0.f };
     #pragma unroll
     for(int j = 0; j < 4; j++)
     {
       const uint32_t k = (c4 >> (8 * j)) & 0xffu;
-      const float4 r = rb[i * G::RP + off[(j & 1) * 128 + k] + (j >> 1)];
-      const float4 t = tb[i * G::RP + ((j + R) & 1) * G::Q + ((j + R) >> 1)];
+      const float4 r = rr[off[(j & 1) * 128 + k] + (j >> 1)];
+      const float4 t = tr[((j + R) & 1) * G::Q + ((j + R) >> 1)];
       const float m = EDGE ? rmask * cm[j] : 1.f;
       const float rv[3] = { r.x, r.y, r.z }, tv[3] = { t.x, t.y, t.z };
       #pragma unroll
@@ -630,21 +655,11 @@ __device__ __forceinline__ void epilogue_blk(const CpsArgs& a, const float4* F0,
         if(SCP && (!EDGE || m != 0.f)) { scp[(size_t)c * plane + (size_t)y * a.W + xb + j] = (T)f2i_exact(b); }
       }
     }
-    #pragma unroll
-    for(int c = 0; c < 3; c++)
-    {
-      // 2^23 + (a sum below 2^23) has the sum in its low bits; 32 lanes add 32 x 0x4B000000
-      rs[3 * i + c] = __reduce_add_sync(kFull, __float_as_uint(frs[c] + kBias)) - 32u * kBiasBits;
-    }
-  }
-  // the warp's twelve row sums (row yb + i, component c) go out in one atomic: lane 3 i + c adds
-  // rs[3 i + c] to rows[(yb + i) * 3 + c]
-  if(lane < 12)
-  {
-    uint32_t v = rs[0];
-    #pragma unroll
-    for(int q = 1; q < 12; q++) { v = lane == q ? rs[q] : v; }
-    if(!EDGE || yb + ((lane * 11) >> 5) < a.H) { atomicAdd(rows + (size_t)yb * 3 + lane, v); }
+    // 2^23 + (a sum below 2^23) has the sum in its low bits; 32 lanes add 32 x 0x4B000000
+    const uint32_t s0 = __reduce_add_sync(kFull, __float_as_uint(frs[0] + kBias)) - 32u * kBiasBits;
+    const uint32_t s1 = __reduce_add_sync(kFull, __float_as_uint(frs[1] + kBias)) - 32u * kBiasBits;
+    const uint32_t s2 = __reduce_add_sync(kFull, __float_as_uint(frs[2] + kBias)) - 32u * kBiasBits;
+    if(lane < 3 && (!EDGE || y < a.H)) { atomicAdd(rows + (size_t)y * 3 + lane, l2 ? s2 : (l1 ? s1 : s0)); }
   }
   if(MOM)
   {
@@ -760,7 +775,11 @@ __device__ __forceinline__ void cps_loop(int ntiles, const Locate& locate, uint3
     {
       if constexpr(R % 2 == 0)
       {
-        if(g.sx == 1 && g.sy == 1) { convert420<T, R, WY>(a, g, raw, F0, F1, x0, y0); }
+        if(g.sx == 1 && g.sy == 1)
+        {
+          if(x0 >= R && y0 >= R && x0 + G::TW + R <= a.W && y0 + G::TH + R <= a.H) { convert420<T, R, WY, true>(a, g, raw, F0, F1, x0, y0); }
+          else { convert420<T, R, WY, false>(a, g, raw, F0, F1, x0, y0); }
+        }
         else { convert<T, R, WY, false>(a, g, raw, F0, F1, x0, y0); }
       }
       else { convert<T, R, WY, false>(a, g, raw, F0, F1, x0, y0); }
