@@ -352,9 +352,13 @@ def build_oracle():
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
 
 
-def build_reference(ref_root="/root/reference", jobs=8):
-    """Compile the reference from its own sources into oracle/_ref (only where they exist)."""
-    if not os.path.isdir(ref_root):
+def build_reference(ref_root=None, jobs=8):
+    """Compile the reference from its own sources into oracle/_ref (only where they exist).
+
+    ref_root: the reference's source tree; QMIV_REFERENCE_ROOT is read when it is not given. Without
+    either, nothing is built."""
+    ref_root = ref_root or os.environ.get("QMIV_REFERENCE_ROOT")
+    if not ref_root or not os.path.isdir(ref_root):
         return False
     subprocess.run(["make", "-s", "-C", HERE, f"-j{jobs}", "ref", f"REF={ref_root}"], check=True)
     return True
