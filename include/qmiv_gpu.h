@@ -267,13 +267,16 @@ QMIV_API qmiv_status qmiv_calc_stream(qmiv_calc calc, void** cuda_stream);
    theirs to use (allocating there could deadlock or break a memory budget). It computes PSNR,
    WS-PSNR and IV-PSNR (the metrics in `metric_mask`, others are rejected) of one frame pair whose
    planes are already in device memory, enqueued on `cuda_stream` (0 = default stream), and blocks
-   until the result is in `out`. It calls no cudaMalloc, cudaFree or other allocating routine: its
-   scratch is one fixed file-scope device array (about 350 KB, held by every GPU that loads the
-   library until exit), which limits the picture height to QMIV_STATIC_MAX_HEIGHT rows; taller
-   pictures are rejected with QMIV_ERR_UNSUPPORTED. The first call on a device looks up that
-   array's device address (with the device current); make that first call before any stream
-   capture. All calls share the one array: calls that overlap on the GPU (from different threads or
-   streams) race, so serialise them. */
+   until the result is in `out`; it synchronises that stream and copies from pageable host memory, so
+   it must not be called on a stream that is being captured into a CUDA graph. It calls no
+   cudaMalloc, cudaFree or other allocating routine: its scratch is one fixed file-scope device array
+   (about 350 KB per GPU), which limits the picture height to QMIV_STATIC_MAX_HEIGHT rows; taller
+   pictures are rejected with QMIV_ERR_UNSUPPORTED. The array comes with the library's device code:
+   with CUDA's lazy module loading (the default) it is placed on a GPU at this entry point's first
+   call there, and it stays until the process exits, so a caller that may not allocate after
+   start-up makes one call on each GPU during start-up. Each call looks up the array's address in the
+   context current at the call. All calls share the one array: calls that overlap on the GPU (from
+   different threads or streams) race, so serialise them. */
 #define QMIV_STATIC_MAX_HEIGHT 4352
 QMIV_API qmiv_status qmiv_frame_pair_compute_static(const qmiv_frame* in0, const qmiv_frame* in1, int32_t width,
                                                     int32_t height, int32_t bitdepth, int32_t chroma_format,

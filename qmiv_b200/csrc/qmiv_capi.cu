@@ -87,12 +87,11 @@ int32_t round_f32_half_away(float f)  // xHelpersFLT.h:32
   return (int32_t)t;
 }
 
-void ws_weights(int32_t H, int32_t lat_range, std::vector<double>& w, double& correction)  // xWeightedSpherically.cpp:13-29
+void ws_weights(int32_t H, int32_t lat_range, double* w, double& correction)  // xWeightedSpherically.cpp:13-29
 {
   const double pi  = 3.14159265358979323846;
   const double heq = 180.0 * (double)H / (double)lat_range;
   const double off = (heq - H) / 2.0;
-  w.resize(H);
   double s = 0.0, c = 0.0;  // KBNS (xKBNS.h:36-43)
   for(int32_t h = 0; h < H; h++)
   {
@@ -102,6 +101,12 @@ void ws_weights(int32_t H, int32_t lat_range, std::vector<double>& w, double& co
     s = t;
   }
   correction = H / (s + c);
+}
+
+void ws_weights(int32_t H, int32_t lat_range, std::vector<double>& w, double& correction)
+{
+  w.resize(H);
+  ws_weights(H, lat_range, w.data(), correction);
 }
 
 // per-picture average of a per-component metric, xMetricQMIV.cpp:91-97

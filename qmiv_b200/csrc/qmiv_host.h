@@ -79,6 +79,8 @@ struct FinishInfo
 double  psnr_from_ssd(double ssd, int64_t area, int32_t bitdepth);
 int32_t num_scales(int32_t W, int32_t H);
 int32_t round_f32_half_away(float f);
+// equirectangular row weights w[0..H) and the WS-PSNR correction H / sum(w)
+void    ws_weights(int32_t H, int32_t lat_range, double* w, double& correction);
 void    ws_weights(int32_t H, int32_t lat_range, std::vector<double>& w, double& correction);
 void    finish_result(const PairOut& o, const FinishInfo& fi, qmiv_result* r);
 // Status of a finished pair from its device flags: a CPS tile load that did not complete, then

@@ -6,14 +6,17 @@
 // WS-PSNR and IV-PSNR of one device-resident frame pair, with all of its scratch in one file-scope
 // device array of fixed size, and calls no cudaMalloc, cudaFree or other allocating routine.
 //
-// The array is a host-side stand-in in host code: its device address is looked up once per device
-// with cudaGetSymbolAddress (device current) and passed to the kernels. Every call shares the
-// array; calls that overlap on the GPU race, so callers must serialise them.
+// In host code the array's name is a host-side stand-in, not a device address. Every call looks up
+// the array's device address with cudaGetSymbolAddress for the device (and context) current at the
+// call and passes it to the kernels; the lookup allocates nothing once the library's module is
+// loaded on that device, so a context created by the caller or a context re-created after
+// cudaDeviceReset is always given its own copy's address. With CUDA's lazy module loading the module,
+// and with it the array, is loaded on a device at the first call there: callers that may not allocate
+// later make one call during start-up. Every call shares the array; calls that overlap on the GPU
+// race, so callers must serialise them.
 #include "qmiv_host.h"
 
-#include <cmath>
 #include <cstring>
-#include <mutex>
 
 using namespace qmiv;
 
@@ -34,21 +37,13 @@ constexpr size_t kScratchBytes = kOffWs + align_up(sizeof(double) * kMaxH);
 
 static __device__ __align__(256) unsigned char g_static_scratch[kScratchBytes];
 
-std::mutex g_addr_mu;
-void*      g_addr[256] = {};  // device address of g_static_scratch per device ordinal
-
-qmiv_status scratch_address(int device, char** out)
+// device address of g_static_scratch in the current device's context
+qmiv_status scratch_address(char** out)
 {
-  std::lock_guard<std::mutex> lk(g_addr_mu);
-  if(device < 0 || device >= 256) { return fail(QMIV_ERR_UNSUPPORTED, "device ordinal too large"); }
-  if(!g_addr[device])
-  {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);  // the current device is `device`
-    if(e != cudaSuccess || p == nullptr) { return cuda_fail(e == cudaSuccess ? cudaErrorInvalidSymbol : e, "cudaGetSymbolAddress"); }
-    g_addr[device] = p;
-  }
-  *out = static_cast<char*>(g_addr[device]);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if(e != cudaSuccess || p == nullptr) { return cuda_fail(e == cudaSuccess ? cudaErrorInvalidSymbol : e, "cudaGetSymbolAddress"); }
+  *out = static_cast<char*>(p);
   return QMIV_OK;
 }
 
@@ -130,10 +125,8 @@ extern "C" qmiv_status qmiv_frame_pair_compute_static(const qmiv_frame* in0, con
   Shape S;
   QMIV_TRY(S.init(width, height, bitdepth, chroma_format));
 
-  int device = 0;
-  QMIV_CUDA(cudaGetDevice(&device));
   char* base = nullptr;
-  QMIV_TRY(scratch_address(device, &base));
+  QMIV_TRY(scratch_address(&base));
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
 
   // frames: device pointers used in place
@@ -159,18 +152,7 @@ extern "C" qmiv_status qmiv_frame_pair_compute_static(const qmiv_frame* in0, con
   const bool need_ws = prm.erp && (metric_mask & (QMIV_WSPSNR | QMIV_IVPSNR));
   if(need_ws)
   {
-    const double pi  = 3.14159265358979323846;  // xWeightedSpherically.cpp:13-29
-    const double heq = 180.0 * (double)S.H / (double)prm.lat_range_deg;
-    const double off = (heq - S.H) / 2.0;
-    double ks = 0.0, kc = 0.0;
-    for(int32_t h = 0; h < S.H; h++)
-    {
-      ws_host[h] = cos((h + off - (heq / 2 - 0.5)) * pi / heq);
-      const double t = ks + ws_host[h];
-      if(std::fabs(ks) >= std::fabs(ws_host[h])) { kc += ((ks - t) + ws_host[h]); } else { kc += ((ws_host[h] - t) + ks); }
-      ks = t;
-    }
-    ws_corr = S.H / (ks + kc);
+    ws_weights(S.H, prm.lat_range_deg, ws_host, ws_corr);
     QMIV_CUDA(cudaMemcpyAsync(base + kOffWs, ws_host, sizeof(double) * S.H, cudaMemcpyHostToDevice, s));
   }
 
