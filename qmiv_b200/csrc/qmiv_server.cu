@@ -2,12 +2,15 @@
 // continuously batched over worker engines.
 //
 //   submit   validates the request and queues it (rejects one larger than the whole budget)
-//   admit    a worker moves queued requests, in arrival order, to the admitted set while their
-//            resident frames fit the budget: host frames are copied into device memory counted
-//            against the context's budget, device frames are used in place
-//   batch    each worker takes the next pending pairs of all admitted requests, in arrival order,
+//   ingest   one thread admits queued requests in arrival order while their resident frames fit the
+//            budget (host frames need device copies counted against the context's budget; device
+//            frames are used in place), then uploads a request's host frames pair by pair on its own
+//            copy stream, outside the scheduler lock, and publishes each pair once its copies have
+//            landed; a request that does not fit waits for finished requests to release theirs
+//   batch    each worker takes the next landed pairs of all admitted requests, in arrival order,
 //            up to max_batch_pairs / max_batch_pixels, and runs them through its own engine
-//            (own stream), so two workers keep two launch sequences in flight
+//            (own stream), so two workers keep two launch sequences in flight while the ingest
+//            thread keeps the host link busy
 //   finish   when a request's last pair is done its resident frames are freed, the sequence means
 //            are formed, and waiters are woken
 #include "qmiv_engine.h"
@@ -34,6 +37,7 @@ struct Request
   DevMem       resident;                  // device copies of host frames
   size_t       resident_bytes = 0;
   int32_t      next = 0;                  // next pair to schedule
+  int32_t      landed = 0;                // pairs whose frames are in device memory
   int32_t      done = 0;                  // pairs finished
   int32_t      batches = 0;
   bool         admitted = false, finished = false;
@@ -74,6 +78,9 @@ struct qmiv_server_s
   bool         stopping = false;
   std::vector<std::unique_ptr<Engine>> engines;
   std::vector<std::thread> workers;
+  std::thread  ingest_thread;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t  copy_event[2] = { nullptr, nullptr };
   // statistics since the last reset
   std::vector<double> latencies;
   int64_t      pairs_done = 0;
@@ -82,61 +89,111 @@ struct qmiv_server_s
 
   double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
   void   worker(int w);
-  bool   admit_locked();
+  void   ingest();
+  // admits the front of the queue; false while the budget is full (mu held)
+  bool   admit_front_locked(std::shared_ptr<Request>& out);
+  qmiv_status upload_pair(Request& r, const Shape& S, int i, cudaEvent_t ev);
 };
 
 static size_t frame_device_bytes(const Shape& S) { return 2 * S.staged_frame_bytes(); }
 
-// Moves queued requests into the admitted set while their resident frames fit. Called with mu held.
-bool qmiv_server_s::admit_locked()
+// Admits the front of the queue: allocates its resident frames if it has host frames. Returns false
+// (and admits nothing) while the budget is full and admitted requests will still release memory.
+bool qmiv_server_s::admit_front_locked(std::shared_ptr<Request>& out)
 {
-  bool any = false;
-  while(!queued.empty())
+  std::shared_ptr<Request> r = queued.front();
+  if(r->resident_bytes > 0 && r->resident.alloc(ctx, r->resident_bytes) != QMIV_OK)
   {
-    std::shared_ptr<Request> r = queued.front();
+    bool busy = false;
+    for(auto& a : admitted) { busy = busy || !a->finished; }
+    if(busy) { return false; }   // budget full: wait for admitted requests to free memory, keep the order
+    // nothing admitted will free memory: the request cannot fit beside the engines' working memory
+    r->status = fail(QMIV_ERR_BUDGET, "request frames do not fit the HBM budget beside the engines' working memory");
+    r->resident_bytes = 0;
+  }
+  queued.pop_front();
+  r->admitted = true;
+  r->admit_ms = now_ms();
+  if(r->resident_bytes == 0) { r->landed = r->desc.num_pairs; }   // device frames, or failed: nothing to upload
+  admitted.push_back(r);
+  out = r;
+  return true;
+}
+
+// Enqueues the copies of pair i's host frames into the request's resident memory on the copy stream
+// and records `ev` after them. Frame descriptors are rewritten to the device copies, which workers
+// read only once the pair is published.
+qmiv_status qmiv_server_s::upload_pair(Request& r, const Shape& S, int i, cudaEvent_t ev)
+{
+  char* base = r.resident.as<char>();
+  for(int f = 0; f < 2; f++)
+  {
+    qmiv_frame& fr = f ? r.in1[i] : r.in0[i];
+    if(fr.mem != QMIV_MEM_HOST) { continue; }
+    size_t off = ((size_t)i * 2 + f) * S.staged_frame_bytes();
+    for(int c = 0; c < 3; c++)
+    {
+      char* dst = base + off;
+      const size_t row = S.plane_cols(c) * S.esz;
+      QMIV_CUDA(cudaMemcpy2DAsync(dst, S.staged_pitch(c), fr.plane[c], (size_t)fr.pitch[c], row, S.plane_rows(c),
+                                  cudaMemcpyHostToDevice, copy_stream));
+      fr.plane[c] = dst;
+      fr.pitch[c] = (int64_t)S.staged_pitch(c);
+      off += S.staged_plane_bytes(c);
+    }
+    fr.mem = QMIV_MEM_DEVICE;
+  }
+  QMIV_CUDA(cudaEventRecord(ev, copy_stream));
+  return QMIV_OK;
+}
+
+// Admission and upload thread. Pair i + 1's copies are enqueued before pair i is waited for, so
+// the copy stream always has work while pairs are published.
+void qmiv_server_s::ingest()
+{
+  cudaSetDevice(ctx->device);
+  for(;;)
+  {
+    std::shared_ptr<Request> r;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      for(;;)
+      {
+        if(queued.empty())
+        {
+          if(stopping) { return; }
+          cv_work.wait_for(lk, std::chrono::milliseconds(5));
+          continue;
+        }
+        if(admit_front_locked(r)) { break; }
+        cv_done.wait_for(lk, std::chrono::milliseconds(2));   // a finishing request releases memory
+      }
+    }
+    cv_work.notify_all();
+    if(r->landed == r->desc.num_pairs) { continue; }
     Shape S;
     S.init(r->desc.width, r->desc.height, r->desc.bitdepth, r->desc.chroma_format);
-    if(r->resident_bytes > 0 && r->resident.alloc(ctx, r->resident_bytes) != QMIV_OK)
+    qmiv_status st = QMIV_OK;
+    const int n = r->desc.num_pairs;
+    for(int i = 0; i < n && st == QMIV_OK; i++)
     {
-      bool busy = false;
-      for(auto& a : admitted) { busy = busy || !a->finished; }
-      if(busy) { break; }   // budget full: wait for admitted requests to free memory, keep the order
-      // nothing admitted will free memory: the request cannot fit beside the engines' working memory
-      r->status = fail(QMIV_ERR_BUDGET, "request frames do not fit the HBM budget beside the engines' working memory");
-      r->resident_bytes = 0;
-    }
-    if(r->resident_bytes > 0)
-    {
-      char* base = r->resident.as<char>();
-      cudaError_t e = cudaSuccess;
-      for(int i = 0; i < r->desc.num_pairs && e == cudaSuccess; i++)
+      st = upload_pair(*r, S, i, copy_event[i & 1]);
+      if(st == QMIV_OK && i > 0 && cudaEventSynchronize(copy_event[(i - 1) & 1]) != cudaSuccess) { st = cuda_fail(cudaErrorUnknown, "server frame upload"); }
+      if(st == QMIV_OK && i > 0)
       {
-        for(int f = 0; f < 2 && e == cudaSuccess; f++)
-        {
-          qmiv_frame& fr = f ? r->in1[i] : r->in0[i];
-          if(fr.mem != QMIV_MEM_HOST) { continue; }
-          size_t off = ((size_t)i * 2 + f) * S.staged_frame_bytes();
-          for(int c = 0; c < 3 && e == cudaSuccess; c++)
-          {
-            char* dst = base + off;
-            const size_t row = S.plane_cols(c) * S.esz;
-            e = cudaMemcpy2D(dst, S.staged_pitch(c), fr.plane[c], (size_t)fr.pitch[c], row, S.plane_rows(c), cudaMemcpyHostToDevice);
-            fr.plane[c] = dst;
-            fr.pitch[c] = (int64_t)S.staged_pitch(c);
-            off += S.staged_plane_bytes(c);
-          }
-          fr.mem = QMIV_MEM_DEVICE;
-        }
+        std::lock_guard<std::mutex> lk(mu);
+        r->landed = i;
       }
-      if(e != cudaSuccess) { r->status = cuda_fail(e, "server frame upload"); }
+      if(i > 0) { cv_work.notify_all(); }
     }
-    queued.pop_front();
-    r->admitted = true;
-    r->admit_ms = now_ms();
-    admitted.push_back(r);
-    any = true;
+    if(st == QMIV_OK && cudaEventSynchronize(copy_event[(n - 1) & 1]) != cudaSuccess) { st = cuda_fail(cudaErrorUnknown, "server frame upload"); }
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if(st != QMIV_OK && r->status == QMIV_OK) { r->status = st; }
+      r->landed = n;
+    }
+    cv_work.notify_all();
   }
-  return any;
 }
 
 void qmiv_server_s::worker(int w)
@@ -154,15 +211,14 @@ void qmiv_server_s::worker(int w)
       std::unique_lock<std::mutex> lk(mu);
       for(;;)
       {
-        admit_locked();
-        // next pending pairs of the admitted requests, in arrival order
+        // next landed pairs of the admitted requests, in arrival order
         int64_t px = 0;
         for(auto& r : admitted)
         {
           if(r->status != QMIV_OK) { continue; }
           const int64_t ppx = (int64_t)r->desc.width * r->desc.height;
           bool counted = false;
-          while(r->next < r->desc.num_pairs && (int)descs.size() < max_batch_pairs && px + ppx <= max_batch_pixels)
+          while(r->next < r->landed && (int)descs.size() < max_batch_pairs && px + ppx <= max_batch_pixels)
           {
             qmiv_pair_desc d{};
             d.in0 = r->in0[r->next]; d.in1 = r->in1[r->next];
@@ -176,10 +232,11 @@ void qmiv_server_s::worker(int w)
           }
           if((int)descs.size() >= max_batch_pairs) { break; }
         }
-        // requests that failed at admission finish without running
+        // requests that failed at admission or upload finish without running (once no pair of
+        // theirs is still running on a worker)
         for(auto& r : admitted)
         {
-          if(r->status != QMIV_OK && !r->finished)
+          if(r->status != QMIV_OK && !r->finished && r->landed == r->desc.num_pairs && r->done == r->next)
           {
             r->finished = true;
             r->done_ms = now_ms();
@@ -194,7 +251,7 @@ void qmiv_server_s::worker(int w)
           for(auto& r : admitted) { busy = busy || !r->finished; }
           if(!busy) { return; }
         }
-        cv_work.wait_for(lk, std::chrono::milliseconds(2));
+        cv_work.wait_for(lk, std::chrono::milliseconds(1));
       }
     }
     out.assign(descs.size(), qmiv_result{});
@@ -249,8 +306,12 @@ qmiv_status qmiv_server_create(qmiv_ctx ctx, const qmiv_params* params, int32_t 
     s->engines.emplace_back(new Engine());
     QMIV_TRY(s->engines.back()->init(ctx, prm, max_batch_pairs, max_batch_pixels, QMIV_BATCH_GRAPH | QMIV_BATCH_AUTOTUNE));
   }
+  QMIV_CUDA(cudaSetDevice(ctx->device));
+  QMIV_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+  for(int k = 0; k < 2; k++) { QMIV_CUDA(cudaEventCreateWithFlags(&s->copy_event[k], cudaEventDisableTiming)); }
   qmiv_server_s* sp = s.get();
   for(int w = 0; w < workers; w++) { s->workers.emplace_back([sp, w] { sp->worker(w); }); }
+  s->ingest_thread = std::thread([sp] { sp->ingest(); });
   *out_server = s.release();
   return QMIV_OK;
 }
@@ -263,7 +324,10 @@ qmiv_status qmiv_server_destroy(qmiv_server s)
     s->stopping = true;
   }
   s->cv_work.notify_all();
+  if(s->ingest_thread.joinable()) { s->ingest_thread.join(); }
   for(std::thread& t : s->workers) { t.join(); }
+  for(int k = 0; k < 2; k++) { if(s->copy_event[k]) { cudaEventDestroy(s->copy_event[k]); } }
+  if(s->copy_stream) { cudaStreamDestroy(s->copy_stream); }
   delete s;
   return QMIV_OK;
 }
