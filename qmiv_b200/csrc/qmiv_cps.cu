@@ -367,7 +367,7 @@ __device__ __forceinline__ void search_fp32(const Thr& th, const float4* tst, co
   using C = Code<R>;
   constexpr int D = G::D;
   float c0[8], c1[8], c2[8];
-  uint32_t best[8];
+  uint32_t best[8], pend[8];
   // c = -2 w (t + g) = (-2 w) t + (-2 w g): integers below 2^24, exact in one FFMA
   const float m0 = -2.0f * wf[0], m1 = -2.0f * wf[1], m2 = -2.0f * wf[2];
   const float o0 = m0 * ga, o1 = m1 * gb, o2 = m2 * gc;
@@ -412,8 +412,15 @@ __device__ __forceinline__ void search_fp32(const Thr& th, const float4* tst, co
           const uint32_t ka = (kShared ? C::of(ry, rx) : C::of(dyi, rx - j)) - (kKeyBase << 7);
           const uint32_t kc = (kShared ? C::of(ry, rx + 1) : C::of(dyi, rx + 1 - j)) - (kKeyBase << 7);
           if(va && vc) { best[p] = __vimin3_u32(best[p], key(ra, p, ka), key(rc, p, kc)); }
-          else if(va) { best[p] = min(best[p], key(ra, p, ka)); }
-          else if(vc) { best[p] = min(best[p], key(rc, p, kc)); }
+          else if(va || vc)
+          {
+            // a pixel's one leftover candidate per search row: rows dyi and dyi + 1 share a
+            // three-input minimum, the last row's goes alone
+            const uint32_t ks = va ? key(ra, p, ka) : key(rc, p, kc);
+            if(dyi == D - 1) { best[p] = min(best[p], ks); }
+            else if((dyi & 1) == 0) { pend[p] = ks; }
+            else { best[p] = __vimin3_u32(best[p], pend[p], ks); }
+          }
         }
       }
     }

@@ -79,8 +79,9 @@ struct qmiv_server_s
   std::vector<std::unique_ptr<Engine>> engines;
   std::vector<std::thread> workers;
   std::thread  ingest_thread;
-  cudaStream_t copy_stream = nullptr;
-  cudaEvent_t  copy_event[2] = { nullptr, nullptr };
+  static constexpr int kInFlight = 8;     // pairs whose uploads are in flight at once
+  cudaStream_t copy_stream[2] = { nullptr, nullptr };
+  cudaEvent_t  copy_event[kInFlight] = {};
   // statistics since the last reset
   std::vector<double> latencies;
   int64_t      pairs_done = 0;
@@ -92,7 +93,7 @@ struct qmiv_server_s
   void   ingest();
   // admits the front of the queue; false while the budget is full (mu held)
   bool   admit_front_locked(std::shared_ptr<Request>& out);
-  qmiv_status upload_pair(Request& r, const Shape& S, int i, cudaEvent_t ev);
+  qmiv_status upload_pair(Request& r, const Shape& S, int i, cudaStream_t cs, cudaEvent_t ev);
 };
 
 static size_t frame_device_bytes(const Shape& S) { return 2 * S.staged_frame_bytes(); }
@@ -120,10 +121,10 @@ bool qmiv_server_s::admit_front_locked(std::shared_ptr<Request>& out)
   return true;
 }
 
-// Enqueues the copies of pair i's host frames into the request's resident memory on the copy stream
+// Enqueues the copies of pair i's host frames into the request's resident memory on copy stream `cs`
 // and records `ev` after them. Frame descriptors are rewritten to the device copies, which workers
 // read only once the pair is published.
-qmiv_status qmiv_server_s::upload_pair(Request& r, const Shape& S, int i, cudaEvent_t ev)
+qmiv_status qmiv_server_s::upload_pair(Request& r, const Shape& S, int i, cudaStream_t cs, cudaEvent_t ev)
 {
   char* base = r.resident.as<char>();
   for(int f = 0; f < 2; f++)
@@ -136,63 +137,94 @@ qmiv_status qmiv_server_s::upload_pair(Request& r, const Shape& S, int i, cudaEv
       char* dst = base + off;
       const size_t row = S.plane_cols(c) * S.esz;
       QMIV_CUDA(cudaMemcpy2DAsync(dst, S.staged_pitch(c), fr.plane[c], (size_t)fr.pitch[c], row, S.plane_rows(c),
-                                  cudaMemcpyHostToDevice, copy_stream));
+                                  cudaMemcpyHostToDevice, cs));
       fr.plane[c] = dst;
       fr.pitch[c] = (int64_t)S.staged_pitch(c);
       off += S.staged_plane_bytes(c);
     }
     fr.mem = QMIV_MEM_DEVICE;
   }
-  QMIV_CUDA(cudaEventRecord(ev, copy_stream));
+  QMIV_CUDA(cudaEventRecord(ev, cs));
   return QMIV_OK;
 }
 
-// Admission and upload thread. Pair i + 1's copies are enqueued before pair i is waited for, so
-// the copy stream always has work while pairs are published.
+// Admission and upload thread. Up to kInFlight pairs, across request boundaries, have their copies
+// in flight, alternating between two copy streams (both copy engines busy); pairs are published in
+// order as their copies land.
 void qmiv_server_s::ingest()
 {
   cudaSetDevice(ctx->device);
-  for(;;)
+  struct Flight
   {
     std::shared_ptr<Request> r;
-    {
-      std::unique_lock<std::mutex> lk(mu);
-      for(;;)
-      {
-        if(queued.empty())
-        {
-          if(stopping) { return; }
-          cv_work.wait_for(lk, std::chrono::milliseconds(5));
-          continue;
-        }
-        if(admit_front_locked(r)) { break; }
-        cv_done.wait_for(lk, std::chrono::milliseconds(2));   // a finishing request releases memory
-      }
-    }
-    cv_work.notify_all();
-    if(r->landed == r->desc.num_pairs) { continue; }
-    Shape S;
-    S.init(r->desc.width, r->desc.height, r->desc.bitdepth, r->desc.chroma_format);
-    qmiv_status st = QMIV_OK;
-    const int n = r->desc.num_pairs;
-    for(int i = 0; i < n && st == QMIV_OK; i++)
-    {
-      st = upload_pair(*r, S, i, copy_event[i & 1]);
-      if(st == QMIV_OK && i > 0 && cudaEventSynchronize(copy_event[(i - 1) & 1]) != cudaSuccess) { st = cuda_fail(cudaErrorUnknown, "server frame upload"); }
-      if(st == QMIV_OK && i > 0)
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        r->landed = i;
-      }
-      if(i > 0) { cv_work.notify_all(); }
-    }
-    if(st == QMIV_OK && cudaEventSynchronize(copy_event[(n - 1) & 1]) != cudaSuccess) { st = cuda_fail(cudaErrorUnknown, "server frame upload"); }
+    int                      i;
+    cudaEvent_t              ev;
+  };
+  std::deque<Flight> flight;
+  std::vector<cudaEvent_t> free_ev(copy_event, copy_event + kInFlight);
+  std::shared_ptr<Request> cur;     // the admitted request whose pairs are being issued
+  Shape S;
+  int next_pair = 0;
+  uint64_t issued = 0;
+  // publishes the oldest pair in flight once its copies have landed
+  auto retire = [&]() {
+    Flight f = flight.front();
+    flight.pop_front();
+    const cudaError_t e = cudaEventSynchronize(f.ev);
+    free_ev.push_back(f.ev);
     {
       std::lock_guard<std::mutex> lk(mu);
-      if(st != QMIV_OK && r->status == QMIV_OK) { r->status = st; }
-      r->landed = n;
+      if(e != cudaSuccess && f.r->status == QMIV_OK) { f.r->status = cuda_fail(e, "server frame upload"); }
+      f.r->landed = std::max(f.r->landed, f.i + 1);
     }
     cv_work.notify_all();
+  };
+  for(;;)
+  {
+    if(!cur)
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      if(queued.empty())
+      {
+        if(!flight.empty()) { lk.unlock(); retire(); continue; }
+        if(stopping) { return; }
+        cv_work.wait_for(lk, std::chrono::milliseconds(5));
+        continue;
+      }
+      std::shared_ptr<Request> r;
+      if(!admit_front_locked(r))
+      {
+        if(!flight.empty()) { lk.unlock(); retire(); continue; }
+        cv_done.wait_for(lk, std::chrono::milliseconds(2));   // a finishing request releases memory
+        continue;
+      }
+      lk.unlock();
+      cv_work.notify_all();
+      if(r->landed == r->desc.num_pairs) { continue; }     // nothing to upload
+      cur = r;
+      S.init(r->desc.width, r->desc.height, r->desc.bitdepth, r->desc.chroma_format);
+      next_pair = 0;
+    }
+    if(flight.size() == (size_t)kInFlight) { retire(); continue; }
+    cudaEvent_t ev = free_ev.back();
+    free_ev.pop_back();
+    const qmiv_status st = upload_pair(*cur, S, next_pair, copy_stream[issued++ & 1], ev);
+    if(st != QMIV_OK)
+    {
+      // the pairs in flight land first; then the request is failed and marked fully landed
+      free_ev.push_back(ev);
+      while(!flight.empty()) { retire(); }
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        if(cur->status == QMIV_OK) { cur->status = st; }
+        cur->landed = cur->desc.num_pairs;
+      }
+      cv_work.notify_all();
+      cur.reset();
+      continue;
+    }
+    flight.push_back(Flight{ cur, next_pair, ev });
+    if(++next_pair == cur->desc.num_pairs) { cur.reset(); }
   }
 }
 
@@ -307,8 +339,8 @@ qmiv_status qmiv_server_create(qmiv_ctx ctx, const qmiv_params* params, int32_t 
     QMIV_TRY(s->engines.back()->init(ctx, prm, max_batch_pairs, max_batch_pixels, QMIV_BATCH_GRAPH | QMIV_BATCH_AUTOTUNE));
   }
   QMIV_CUDA(cudaSetDevice(ctx->device));
-  QMIV_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
-  for(int k = 0; k < 2; k++) { QMIV_CUDA(cudaEventCreateWithFlags(&s->copy_event[k], cudaEventDisableTiming)); }
+  for(int k = 0; k < 2; k++) { QMIV_CUDA(cudaStreamCreateWithFlags(&s->copy_stream[k], cudaStreamNonBlocking)); }
+  for(int k = 0; k < qmiv_server_s::kInFlight; k++) { QMIV_CUDA(cudaEventCreateWithFlags(&s->copy_event[k], cudaEventDisableTiming)); }
   qmiv_server_s* sp = s.get();
   for(int w = 0; w < workers; w++) { s->workers.emplace_back([sp, w] { sp->worker(w); }); }
   s->ingest_thread = std::thread([sp] { sp->ingest(); });
@@ -326,8 +358,8 @@ qmiv_status qmiv_server_destroy(qmiv_server s)
   s->cv_work.notify_all();
   if(s->ingest_thread.joinable()) { s->ingest_thread.join(); }
   for(std::thread& t : s->workers) { t.join(); }
-  for(int k = 0; k < 2; k++) { if(s->copy_event[k]) { cudaEventDestroy(s->copy_event[k]); } }
-  if(s->copy_stream) { cudaStreamDestroy(s->copy_stream); }
+  for(int k = 0; k < qmiv_server_s::kInFlight; k++) { if(s->copy_event[k]) { cudaEventDestroy(s->copy_event[k]); } }
+  for(int k = 0; k < 2; k++) { if(s->copy_stream[k]) { cudaStreamDestroy(s->copy_stream[k]); } }
   delete s;
   return QMIV_OK;
 }
