@@ -607,14 +607,23 @@ __device__ __forceinline__ void epilogue_blk(const CpsArgs& a, const float4* F0,
   const float sg = dir ? -1.f : 1.f;
   const float fg[3] = { sg * (float)g0, sg * (float)g1, sg * (float)g2 };
   const float fmax = (float)a.maxv;
+  // Bank spreading: a float4 of column 4 bx + j sits 2 bx + const float4 from the row start, so lanes
+  // visiting the same j would hit only four of the eight 16-byte bank groups. Lanes with bit 2 of bx
+  // set visit the block's columns in the order j ^ 2, one float4 off (+1 for j < 2, -1 for j >= 2),
+  // which puts the eight lanes of every shared-memory phase on eight different groups.
+  const int sw = (bx >> 2) & 1;
   const float4* rb = ref + 4 * by * G::RP + 2 * bx;
   const float4* tb = tst + (4 * by + R) * G::RP + 2 * bx;
+  const float4* rbs[2] = { rb + sw, rb - sw };   // j < 2, j >= 2
+  const float4* tbs[2] = { tb + sw, tb - sw };
   const uint8_t* cb = codes + dir * (G::TH * G::TW) + 4 * by * G::TW + 4 * bx;
+  int xj[4];                                      // picture column of visit j
   float cm[4] = { 1.f, 1.f, 1.f, 1.f };
-  if(EDGE)
+  #pragma unroll
+  for(int j = 0; j < 4; j++)
   {
-    #pragma unroll
-    for(int j = 0; j < 4; j++) { cm[j] = xb + j < a.W ? 1.f : 0.f; }
+    xj[j] = xb + (j ^ (2 * sw));
+    if(EDGE) { cm[j] = xj[j] < a.W ? 1.f : 0.f; }
   }
   float mm[3][5];
   #pragma unroll
@@ -631,16 +640,16 @@ __device__ __forceinline__ void epilogue_blk(const CpsArgs& a, const float4* F0,
   {
     const int y = yb + i;
     const float rmask = (!EDGE || y < a.H) ? 1.f : 0.f;
-    const uint32_t c4 = *reinterpret_cast<const uint32_t*>(cb + i * G::TW);
-    const float4* rr = rb + i * G::RP;
-    const float4* tr = tb + i * G::RP;
+    // the four codes of the row, rotated so that byte j is the code of visit j
+    const uint32_t c4 = __funnelshift_l(*reinterpret_cast<const uint32_t*>(cb + i * G::TW),
+                                        *reinterpret_cast<const uint32_t*>(cb + i * G::TW), 16 * sw);
     float frs[3] = { 0.f, 0.f, 0.f };
     #pragma unroll
     for(int j = 0; j < 4; j++)
     {
       const uint32_t k = (c4 >> (8 * j)) & 0xffu;
-      const float4 r = rr[off[(j & 1) * 128 + k] + (j >> 1)];
-      const float4 t = tr[((j + R) & 1) * G::Q + ((j + R) >> 1)];
+      const float4 r = rbs[j >> 1][i * G::RP + off[(j & 1) * 128 + k] + (j >> 1)];
+      const float4 t = tbs[j >> 1][i * G::RP + ((j + R) & 1) * G::Q + ((j + R) >> 1)];
       const float m = EDGE ? rmask * cm[j] : 1.f;
       const float rv[3] = { r.x, r.y, r.z }, tv[3] = { t.x, t.y, t.z };
       #pragma unroll
@@ -659,7 +668,7 @@ __device__ __forceinline__ void epilogue_blk(const CpsArgs& a, const float4* F0,
           mm[c][3] = fmaf(bm, b, mm[c][3]);
           mm[c][4] = fmaf(tm, b, mm[c][4]);
         }
-        if(SCP && (!EDGE || m != 0.f)) { scp[(size_t)c * plane + (size_t)y * a.W + xb + j] = (T)f2i_exact(b); }
+        if(SCP && (!EDGE || m != 0.f)) { scp[(size_t)c * plane + (size_t)y * a.W + xj[j]] = (T)f2i_exact(b); }
       }
     }
     // 2^23 + (a sum below 2^23) has the sum in its low bits; 32 lanes add 32 x 0x4B000000
