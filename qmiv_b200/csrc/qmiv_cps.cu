@@ -276,27 +276,31 @@ __device__ void convert420(const CpsArgs& a, const CpsGeomArgs& g, const unsigne
   constexpr int UC = G::SW / 2, UR = G::SH / 2, NU = UC * UR;
   const int W = a.W, H = a.H;
   const int cw = W >> 1, chh = H >> 1;
-  const int xl = x0 - g.ax, yl = y0 - R, xc = (x0 >> 1) - g.ax, yc = (y0 - R) >> 1;
+  const int ax = g.ax, bwl = g.bwl, bwc = g.bwc;
+  const int xl = x0 - ax, yl = y0 - R, xc = (x0 >> 1) - ax, yc = (y0 - R) >> 1;
   const float w0 = a.wf[0], w1 = a.wf[1], w2 = a.wf[2];
+  // the geometry is read once: the tile stores below could alias the shared argument copy
+  const uint32_t offl[2] = { g.off[0][0], g.off[1][0] }, offu[2] = { g.off[0][1], g.off[1][1] },
+                 offv[2] = { g.off[0][2], g.off[1][2] };
   #pragma unroll 1
   for(int u = threadIdx.x; u < 2 * NU; u += G::NT)
   {
     const int f = u >= NU ? 1 : 0;
     const int r = u - f * NU;
     const int ur = r / UC, uc = r - ur * UC;
-    const T* rl = reinterpret_cast<const T*>(raw + g.off[f][0]);
-    const T* ru = reinterpret_cast<const T*>(raw + g.off[f][1]);
-    const T* rv = reinterpret_cast<const T*>(raw + g.off[f][2]);
+    const T* rl = reinterpret_cast<const T*>(raw + (f ? offl[1] : offl[0]));
+    const T* ru = reinterpret_cast<const T*>(raw + (f ? offu[1] : offu[0]));
+    const T* rv = reinterpret_cast<const T*>(raw + (f ? offv[1] : offv[0]));
     uint32_t l0, l1, s0 = PairSel<T>::lo, s1 = PairSel<T>::hi;
     int co;
     if(INTERIOR)
     {
       // the tile and its halo lie inside the picture: unit (ur, uc) is raw luma (2 ur, ax - R + 2 uc)
       // and raw chroma (ur, ax - R / 2 + uc)
-      const T* p = rl + 2 * ur * g.bwl + (g.ax - R) + 2 * uc;
+      const T* p = rl + 2 * ur * bwl + (ax - R) + 2 * uc;
       l0 = load_pair<T>(p);
-      l1 = load_pair<T>(p + g.bwl);
-      co = ur * g.bwc + (g.ax - R / 2) + uc;
+      l1 = load_pair<T>(p + bwl);
+      co = ur * bwc + (ax - R / 2) + uc;
     }
     else
     {
@@ -305,9 +309,9 @@ __device__ void convert420(const CpsArgs& a, const CpsGeomArgs& g, const unsigne
       s0 = gx < W ? PairSel<T>::lo : PairSel<T>::hi;
       s1 = gx >= 0 ? PairSel<T>::hi : PairSel<T>::lo;
       const int gy0 = clampi(gy, 0, H - 1), gy1 = clampi(gy + 1, 0, H - 1);
-      l0 = load_pair<T>(rl + (gy0 - yl) * g.bwl + (px - xl));
-      l1 = load_pair<T>(rl + (gy1 - yl) * g.bwl + (px - xl));
-      co = (clampi(gy >> 1, 0, chh - 1) - yc) * g.bwc + clampi(gx >> 1, 0, cw - 1) - xc;
+      l0 = load_pair<T>(rl + (gy0 - yl) * bwl + (px - xl));
+      l1 = load_pair<T>(rl + (gy1 - yl) * bwl + (px - xl));
+      co = (clampi(gy >> 1, 0, chh - 1) - yc) * bwc + clampi(gx >> 1, 0, cw - 1) - xc;
     }
     const float cu = u2f_exact(ru[co]), cv = u2f_exact(rv[co]);
     const float qc = fmaf(w2, cv * cv, fmaf(w1, cu * cu, kBias));
@@ -957,7 +961,8 @@ void plan_pair(CpsGeomArgs& g, size_t& smem, int esz, int sx, int sy, int W, int
 }
 
 // runtime (R, WY) -> plan_pair; false for combinations that are never instantiated (R = 5 with
-// 128 x 32 tiles never fits shared memory)
+// 128 x 32 or 128 x 24 tiles never fits shared memory; 128 x 24 tiles exist in the work-list form
+// only, where the autotuner picks them)
 bool plan_any(int R, int wy, CpsGeomArgs& g, size_t& smem, int esz, int sx, int sy, int W, int H)
 {
   switch(R * 16 + wy)
@@ -966,6 +971,10 @@ bool plan_any(int R, int wy, CpsGeomArgs& g, size_t& smem, int esz, int sx, int 
   case 2 * 16 + 8: plan_pair<2, 8>(g, smem, esz, sx, sy, W, H); return true;
   case 3 * 16 + 8: plan_pair<3, 8>(g, smem, esz, sx, sy, W, H); return true;
   case 4 * 16 + 8: plan_pair<4, 8>(g, smem, esz, sx, sy, W, H); return true;
+  case 1 * 16 + 6: plan_pair<1, 6>(g, smem, esz, sx, sy, W, H); return true;
+  case 2 * 16 + 6: plan_pair<2, 6>(g, smem, esz, sx, sy, W, H); return true;
+  case 3 * 16 + 6: plan_pair<3, 6>(g, smem, esz, sx, sy, W, H); return true;
+  case 4 * 16 + 6: plan_pair<4, 6>(g, smem, esz, sx, sy, W, H); return true;
   case 1 * 16 + 4: plan_pair<1, 4>(g, smem, esz, sx, sy, W, H); return true;
   case 2 * 16 + 4: plan_pair<2, 4>(g, smem, esz, sx, sy, W, H); return true;
   case 3 * 16 + 4: plan_pair<3, 4>(g, smem, esz, sx, sy, W, H); return true;
@@ -1065,6 +1074,7 @@ cudaError_t launch_multi_r(const CpsKernelArgs* d, const int32_t* prefix, int np
   if constexpr(R <= 4)
   {
     if(wy == 8) { return launch_multi_inst<R, 8, T>(d, prefix, npairs, ntiles, raw_cap, smem, dev, s); }
+    if(wy == 6) { return launch_multi_inst<R, 6, T>(d, prefix, npairs, ntiles, raw_cap, smem, dev, s); }
   }
   if(wy == 4) { return launch_multi_inst<R, 4, T>(d, prefix, npairs, ntiles, raw_cap, smem, dev, s); }
   return cudaErrorInvalidConfiguration;

@@ -94,65 +94,84 @@ qmiv_status Engine::kind_for(const qmiv_pair_desc& d, PairKind*& out)
   return QMIV_OK;
 }
 
-// Times the candidate CPS tile heights on one real pair of the kind (GCD 0, results discarded)
-// and keeps the faster one.
+// Times the candidate CPS tile shapes (128 x 32 with 16 warps, 128 x 24 with 12, 128 x 16 with 8 at
+// two CTAs per SM; those that fit shared memory) on one real pair of the kind (GCD 0, results
+// discarded) and keeps the fastest. The candidates take turns over several rounds and each keeps its
+// fastest launch, so a clock ramp or another stream's burst during one round does not decide.
 qmiv_status Engine::autotune(PairKind& k, const Img& in0, const Img& in1, cudaStream_t s)
 {
   k.tuned = true;
-  const int cands[2] = { 8, 4 };
-  const bool valid[2] = { cps_tile_fits(k.R, 8, (int)k.S.esz, k.S.sx, k.S.sy),
-                          cps_tile_fits(k.R, 4, (int)k.S.esz, k.S.sx, k.S.sy) };
-  if(!(valid[0] && valid[1])) { return QMIV_OK; }   // one candidate only: nothing to tune
+  constexpr int kCands = 3, kRounds = 5;
+  const int cands[kCands] = { 8, 6, 4 };
+  int wys[kCands], n = 0;
+  for(int c = 0; c < kCands; c++)
+  {
+    if(cps_tile_fits(k.R, cands[c], (int)k.S.esz, k.S.sx, k.S.sy)) { wys[n++] = cands[c]; }
+  }
+  if(n < 2) { return QMIV_OK; }   // one candidate only: nothing to tune
   const Shape& S = k.S;
   const size_t out_b = align_sz(sizeof(PairOut), kRegionAlign);
   const size_t rows_b = align_sz((size_t)2 * S.H * 3 * sizeof(uint32_t), kRegionAlign);
   const size_t desc_b = align_sz(cps_desc_bytes(), kRegionAlign);
-  QMIV_TRY(tune_scratch_.ensure(ctx_, out_b + rows_b + desc_b + kRegionAlign));
+  QMIV_TRY(tune_scratch_.ensure(ctx_, out_b + rows_b + kCands * (desc_b + kRegionAlign)));
   char* base = tune_scratch_.as<char>();
   PairOut* dout = reinterpret_cast<PairOut*>(base);
   uint32_t* rows = reinterpret_cast<uint32_t*>(base + out_b);
-  void* ddesc = base + out_b + rows_b;
-  int32_t* dprefix = reinterpret_cast<int32_t*>(base + out_b + rows_b + desc_b);
   QMIV_CUDA(cudaMemsetAsync(base, 0, out_b + rows_b, s));
   CpsArgs ca{};
   ca.in0 = in0; ca.in1 = in1; ca.W = S.W; ca.H = S.H; ca.maxv = S.maxv; ca.clip = 0xffffu;
   for(int c = 0; c < 3; c++) { ca.wi[c] = prm_.cws[c]; ca.wf[c] = (float)prm_.cws[c]; }
   ca.gcd_src = dout; ca.rows = rows;
+  alignas(64) static thread_local unsigned char host_desc[4096];
+  if(cps_desc_bytes() > sizeof(host_desc)) { return QMIV_OK; }
+  CpsPairPlan plan[kCands]{};
+  void* ddesc[kCands];
+  int32_t* dprefix[kCands];
+  bool ok[kCands] = {};
+  for(int c = 0; c < n; c++)
+  {
+    ddesc[c] = base + out_b + rows_b + c * (desc_b + kRegionAlign);
+    dprefix[c] = reinterpret_cast<int32_t*>(static_cast<char*>(ddesc[c]) + desc_b);
+    if(cps_describe(host_desc, ca, k.R, (int)S.esz, wys[c], &plan[c]) != cudaSuccess) { continue; }
+    const int32_t prefix[2] = { 0, plan[c].ntiles };
+    QMIV_CUDA(cudaMemcpyAsync(ddesc[c], host_desc, cps_desc_bytes(), cudaMemcpyHostToDevice, s));
+    QMIV_CUDA(cudaMemcpyAsync(dprefix[c], prefix, sizeof(prefix), cudaMemcpyHostToDevice, s));
+    QMIV_CUDA(cudaStreamSynchronize(s));   // host_desc is reused for the next candidate
+    ok[c] = true;
+  }
   cudaEvent_t e0, e1;
   QMIV_CUDA(cudaEventCreate(&e0));
   QMIV_CUDA(cudaEventCreate(&e1));
-  float best_ms = 1e30f;
-  int best = k.wy;
-  alignas(64) static thread_local unsigned char host_desc[4096];
-  for(int i = 0; i < 2 && cps_desc_bytes() <= sizeof(host_desc); i++)
+  float best_ms[kCands];
+  for(int c = 0; c < kCands; c++) { best_ms[c] = 1e30f; }
+  cudaError_t e = cudaSuccess;
+  for(int round = 0; round <= kRounds && e == cudaSuccess; round++)   // round 0 warms every candidate up
   {
-    const int wy = cands[i];
-    CpsPairPlan plan{};
-    if(cps_describe(host_desc, ca, k.R, (int)S.esz, wy, &plan) != cudaSuccess) { continue; }
-    const int32_t prefix[2] = { 0, plan.ntiles };
-    cudaError_t e = cudaMemcpyAsync(ddesc, host_desc, cps_desc_bytes(), cudaMemcpyHostToDevice, s);
-    if(e == cudaSuccess) { e = cudaMemcpyAsync(dprefix, prefix, sizeof(prefix), cudaMemcpyHostToDevice, s); }
-    float ms = 0.f;
-    for(int rep = 0; rep < 3 && e == cudaSuccess; rep++)
+    for(int c = 0; c < n && e == cudaSuccess; c++)
     {
+      if(!ok[c]) { continue; }
       e = cudaEventRecord(e0, s);
-      if(e == cudaSuccess) { e = launch_cps_multi(ddesc, dprefix, 1, plan.ntiles, k.R, wy, (int)S.esz, plan.raw_bytes, plan.smem, s); }
+      if(e == cudaSuccess) { e = launch_cps_multi(ddesc[c], dprefix[c], 1, plan[c].ntiles, k.R, wys[c], (int)S.esz, plan[c].raw_bytes, plan[c].smem, s); }
       if(e == cudaSuccess) { e = cudaEventRecord(e1, s); }
       if(e == cudaSuccess) { e = cudaEventSynchronize(e1); }
-      if(e == cudaSuccess && rep > 0)
+      if(e == cudaSuccess && round > 0)
       {
         float t = 0.f;
         cudaEventElapsedTime(&t, e0, e1);
-        ms += t;
+        best_ms[c] = std::min(best_ms[c], t);
       }
     }
-    if(e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return cuda_fail(e, "CPS autotuning launch"); }
-    k.tune_ms[i] = ms / 2;
-    if(ms < best_ms) { best_ms = ms; best = wy; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  k.wy = best;
+  if(e != cudaSuccess) { return cuda_fail(e, "CPS autotuning launch"); }
+  int best = -1;
+  for(int c = 0; c < n; c++)
+  {
+    for(int q = 0; q < kCands; q++) { if(cands[q] == wys[c]) { k.tune_ms[q] = ok[c] ? best_ms[c] : 0.f; } }
+    if(ok[c] && (best < 0 || best_ms[c] < best_ms[best])) { best = c; }
+  }
+  if(best >= 0) { k.wy = wys[best]; }
   return QMIV_OK;
 }
 

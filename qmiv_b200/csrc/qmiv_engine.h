@@ -26,7 +26,7 @@ struct PairKind
   DevMem      ws_dev;
   int32_t     wy = 8;          // CPS tile height / 4
   bool        tuned = false;
-  float       tune_ms[2] = { 0.f, 0.f };
+  float       tune_ms[3] = { 0.f, 0.f, 0.f };   // fastest launch of 128 x 32, 128 x 24, 128 x 16 tiles
 };
 
 struct KindKey

@@ -107,7 +107,7 @@ def test_batch_autotune(qctx):
             assert batch.compute([_desc(s, *f) for s, f in zip(specs, frames)]) == plain
         for W, H, bd, cf, R, _ in specs:
             tw, th, rows = batch.tuning(W, H, bd, R)
-            assert tw == 128 and th in (16, 32) and rows == 4
+            assert tw == 128 and th in (16, 24, 32) and rows == 4
             if R == 5:
                 assert th == 16
         with pytest.raises(qmiv_b200.QmivError):
