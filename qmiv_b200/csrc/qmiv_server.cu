@@ -34,8 +34,8 @@ struct Request
   uint64_t     ticket = 0;
   qmiv_request desc{};
   std::vector<qmiv_frame> in0, in1;       // caller frames (or resident copies after admission)
-  DevMem       resident;                  // device copies of host frames
-  size_t       resident_bytes = 0;
+  char*        resident = nullptr;        // device copies of host frames (from the server's memory pool)
+  size_t       resident_bytes = 0;        // bytes the request needs there (counted against the budget)
   int32_t      next = 0;                  // next pair to schedule
   int32_t      landed = 0;                // pairs whose frames are in device memory
   int32_t      done = 0;                  // pairs finished
@@ -82,6 +82,10 @@ struct qmiv_server_s
   static constexpr int kInFlight = 8;     // pairs whose uploads are in flight at once
   cudaStream_t copy_stream[2] = { nullptr, nullptr };
   cudaEvent_t  copy_event[kInFlight] = {};
+  cudaEvent_t  alloc_event = nullptr;     // orders a fresh allocation before the second copy stream
+  // Resident frames come from a stream-ordered pool that keeps its memory: allocating and freeing a
+  // request's frames never synchronises the device (cudaFree would wait for every worker's kernels).
+  cudaMemPool_t pool = nullptr;
   // statistics since the last reset
   std::vector<double> latencies;
   int64_t      pairs_done = 0;
@@ -94,6 +98,9 @@ struct qmiv_server_s
   // admits the front of the queue; false while the budget is full (mu held)
   bool   admit_front_locked(std::shared_ptr<Request>& out);
   qmiv_status upload_pair(Request& r, const Shape& S, int i, cudaStream_t cs, cudaEvent_t ev);
+  // resident memory of a request: budget first, then the pool (ingest thread); release at finish
+  qmiv_status alloc_resident(Request& r);
+  void        free_resident(Request& r);
 };
 
 static size_t frame_device_bytes(const Shape& S) { return 2 * S.staged_frame_bytes(); }
@@ -103,7 +110,7 @@ static size_t frame_device_bytes(const Shape& S) { return 2 * S.staged_frame_byt
 bool qmiv_server_s::admit_front_locked(std::shared_ptr<Request>& out)
 {
   std::shared_ptr<Request> r = queued.front();
-  if(r->resident_bytes > 0 && r->resident.alloc(ctx, r->resident_bytes) != QMIV_OK)
+  if(r->resident_bytes > 0 && alloc_resident(*r) != QMIV_OK)
   {
     bool busy = false;
     for(auto& a : admitted) { busy = busy || !a->finished; }
@@ -121,12 +128,42 @@ bool qmiv_server_s::admit_front_locked(std::shared_ptr<Request>& out)
   return true;
 }
 
+qmiv_status qmiv_server_s::alloc_resident(Request& r)
+{
+  if(!ctx->reserve(r.resident_bytes)) { return fail(QMIV_ERR_BUDGET, "HBM budget exceeded"); }
+  void* p = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, r.resident_bytes, pool, copy_stream[0]);
+  if(e == cudaSuccess) { e = cudaEventRecord(alloc_event, copy_stream[0]); }
+  if(e == cudaSuccess) { e = cudaStreamWaitEvent(copy_stream[1], alloc_event, 0); }
+  if(e != cudaSuccess)
+  {
+    if(p) { cudaFreeAsync(p, copy_stream[0]); }
+    cudaGetLastError();
+    ctx->unreserve(r.resident_bytes);
+    return cuda_fail(e, "server frame memory");
+  }
+  r.resident = static_cast<char*>(p);
+  return QMIV_OK;
+}
+
+// Called when every pair of the request is done (the workers' engines have synchronised their
+// streams), so the memory is free for the next allocation in copy-stream order.
+void qmiv_server_s::free_resident(Request& r)
+{
+  if(r.resident)
+  {
+    cudaFreeAsync(r.resident, copy_stream[0]);
+    ctx->unreserve(r.resident_bytes);
+    r.resident = nullptr;
+  }
+}
+
 // Enqueues the copies of pair i's host frames into the request's resident memory on copy stream `cs`
 // and records `ev` after them. Frame descriptors are rewritten to the device copies, which workers
 // read only once the pair is published.
 qmiv_status qmiv_server_s::upload_pair(Request& r, const Shape& S, int i, cudaStream_t cs, cudaEvent_t ev)
 {
-  char* base = r.resident.as<char>();
+  char* base = r.resident;
   for(int f = 0; f < 2; f++)
   {
     qmiv_frame& fr = f ? r.in1[i] : r.in0[i];
@@ -272,7 +309,7 @@ void qmiv_server_s::worker(int w)
           {
             r->finished = true;
             r->done_ms = now_ms();
-            r->resident.release();
+            free_resident(*r);
             cv_done.notify_all();
           }
         }
@@ -302,7 +339,7 @@ void qmiv_server_s::worker(int w)
         {
           r.finished = true;
           r.done_ms = t;
-          r.resident.release();
+          free_resident(r);
           latencies.push_back(r.done_ms - r.submit_ms);
           last_done_ms = t;
         }
@@ -341,6 +378,14 @@ qmiv_status qmiv_server_create(qmiv_ctx ctx, const qmiv_params* params, int32_t 
   QMIV_CUDA(cudaSetDevice(ctx->device));
   for(int k = 0; k < 2; k++) { QMIV_CUDA(cudaStreamCreateWithFlags(&s->copy_stream[k], cudaStreamNonBlocking)); }
   for(int k = 0; k < qmiv_server_s::kInFlight; k++) { QMIV_CUDA(cudaEventCreateWithFlags(&s->copy_event[k], cudaEventDisableTiming)); }
+  QMIV_CUDA(cudaEventCreateWithFlags(&s->alloc_event, cudaEventDisableTiming));
+  cudaMemPoolProps pp{};
+  pp.allocType = cudaMemAllocationTypePinned;
+  pp.location.type = cudaMemLocationTypeDevice;
+  pp.location.id = ctx->device;
+  QMIV_CUDA(cudaMemPoolCreate(&s->pool, &pp));
+  uint64_t keep = UINT64_MAX;   // the pool keeps what it has reserved: no release to the driver between requests
+  QMIV_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   qmiv_server_s* sp = s.get();
   for(int w = 0; w < workers; w++) { s->workers.emplace_back([sp, w] { sp->worker(w); }); }
   s->ingest_thread = std::thread([sp] { sp->ingest(); });
@@ -358,6 +403,10 @@ qmiv_status qmiv_server_destroy(qmiv_server s)
   s->cv_work.notify_all();
   if(s->ingest_thread.joinable()) { s->ingest_thread.join(); }
   for(std::thread& t : s->workers) { t.join(); }
+  for(auto& kv : s->by_ticket) { s->free_resident(*kv.second); }   // requests never waited on
+  if(s->copy_stream[0]) { cudaStreamSynchronize(s->copy_stream[0]); }
+  if(s->pool) { cudaMemPoolDestroy(s->pool); }
+  if(s->alloc_event) { cudaEventDestroy(s->alloc_event); }
   for(int k = 0; k < qmiv_server_s::kInFlight; k++) { if(s->copy_event[k]) { cudaEventDestroy(s->copy_event[k]); } }
   for(int k = 0; k < 2; k++) { if(s->copy_stream[k]) { cudaStreamDestroy(s->copy_stream[k]); } }
   delete s;
