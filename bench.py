@@ -34,8 +34,9 @@ W, H, BD, CF = 4096, 2048, 10, 420
 PAIRS_PER_STEP = 8
 METRIC_NAME = "IV-PSNR frame-pairs/s @4096x2048 10b"
 # DRAM bytes of one 8-pair k_cps_multi launch: ncu dram__bytes_read.sum + dram__bytes_write.sum of a
-# 2-pair launch of the same kernel (100.8 MB + 86.0 MB) times the ratio of pairs, 4
-CPS_TRAFFIC_BYTES = 4 * (100.8e6 + 86.0e6)
+# one-pair launch of the same kernel (50.4 MB of frames read, 71.2 MB of IV-SSIM sub-block moments and
+# row sums written) times the 8 pairs; every pair is read once and its moments written once
+CPS_TRAFFIC_BYTES = 8 * (50.45e6 + 71.17e6)
 METRICS = ("IVPSNR", "WSPSNR", "IVSSIM")
 # values of the headline pair compared with the reference library's
 PARITY_KEYS = ("gcd_r2t", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r", "wspsnr_pic", "ivssim", "ivssim_r2t", "ivssim_t2r")
@@ -310,7 +311,7 @@ def run_qmiv(args, world, rank, local):
 
     ctx = qmiv_b200.Context(local)
     batch = qmiv_b200.Batch(ctx, max_pairs=PAIRS_PER_STEP, max_pixels=PAIRS_PER_STEP * W * H, erp=True, graph=True,
-                            autotune=True)
+                            autotune=not args.no_autotune)
     stream = torch.cuda.ExternalStream(batch.stream(), device=f"cuda:{local}")
     dev_desc, host_desc = descs(dev_pairs), descs(host_np)
 
@@ -741,6 +742,9 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the 1080p 8-bit and the MS-SSIM workloads")
     ap.add_argument("--size", default=None, help="WxH of a smaller profiling case (not a bench line)")
     ap.add_argument("--pairs", type=int, default=None, help="pairs per step of a smaller profiling case")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="profiling case: the default 128x32 CPS tile for the timed workload instead of the autotuner's "
+                         "pick (a profiler's replay skews the timings the autotuner compares)")
     args = ap.parse_args()
     global W, H, PAIRS_PER_STEP
     if args.size:
