@@ -361,4 +361,12 @@ def build_reference(ref_root=None, jobs=8):
     if not ref_root or not os.path.isdir(ref_root):
         return False
     subprocess.run(["make", "-s", "-C", HERE, f"-j{jobs}", "ref", f"REF={ref_root}"], check=True)
+    if os.path.exists(os.path.join(os.path.dirname(HERE), "qmiv_b200", "libqmiv_b200.so")):
+        subprocess.run(["make", "-s", "-C", HERE, f"-j{jobs}", "shimcheck", f"REF={ref_root}"], check=True)
     return True
+
+
+def shim_check_path(arch=None):
+    """The drop-in adapter's check program (oracle/Makefile shimcheck), or None where it is not built."""
+    p = os.path.join(reference_dir(arch), "shim_check")
+    return p if os.path.exists(p) else None

@@ -162,6 +162,33 @@ def test_full_size_erp_4096x2048_10bit(qctx, oracle_lib):
         assert got[k] == exp[k], k
 
 
+def test_msssim_workload_2048_blurred(qctx, oracle_lib):
+    """The MS-SSIM workload's shape: 2048x2048 10-bit 4:2:0 pairs with a seeded blur, 5 scales,
+    MS-SSIM and IV-MS-SSIM through the plain and the batched form, bit-exact against the C restatement
+    and, where it is built here, the compiled reference library."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    W = H = 2048
+    pairs = [synth.make_pair(W, H, 10, seed=2000 + i, blur_sigma=s) for i, s in enumerate((0.7, 1.8))]
+    mask = qmiv_b200.MSSSIM | qmiv_b200.IVMSSSIM
+    keys = ["gcd_r2t", "msssim", "msssim_pic", "ivmsssim", "ivmsssim_r2t", "ivmsssim_t2r"]
+    p = oracle.make_params(W, H, 10, 420)
+    exp = [oracle_lib.compute_pair(p, a, b, mask) for a, b in pairs]
+    with qmiv_b200.Calc(qctx, W, H, 10, 420) as calc:
+        plain = [calc.compute(a, b, mask) for a, b in pairs]
+    descs = [dict(frame0=a, frame1=b, width=W, height=H, bitdepth=10, search_range=2, metrics=mask) for a, b in pairs]
+    with qmiv_b200.Batch(qctx, 2, 2 * W * H, graph=True, autotune=True) as batch:
+        batched = batch.compute(descs)
+    for k in keys:
+        for i in range(len(pairs)):
+            assert plain[i][k] == exp[i][k], (i, k)
+            assert batched[i][k] == exp[i][k], (i, k)
+    if oracle.reference_available():
+        ref = oracle.Reference().compute_pair(p, *pairs[0], mask)
+        for k in keys:
+            assert plain[0][k] == ref[k], k
+
+
 def test_full_size_properties(qctx):
     """Size-independent properties at 4096x2048: identical frames give SSE 0, GCD 0, SSIM 1, and the
     result does not depend on the order the pairs are computed in."""
