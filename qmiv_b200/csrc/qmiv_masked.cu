@@ -59,7 +59,6 @@ struct MaskArgs
   uint64_t*   row_cps;         // [2][H][3]
   const double* ws;            // [H] or null
   MaskOut*    out;
-  uint32_t    key_off;         // k_cps_masked_key: bound B of every error and every sum of w s^2
   uint32_t    kscale;          // 128, read from the parameter bank so the key stays one integer multiply-add
 };
 
@@ -357,25 +356,31 @@ __global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ Mask
   }
 }
 
-// The same search where every error and every sum of w s^2 is at most B with 2B < 2^25 - 1 (the host
-// checks this from the bit depth, weights and GCD clip range; samples are in range under STOP and CNCL).
-// Expanding e = sum_c w_c (s_c - r_c)^2 = K_s + q_r + sum_c a_c r_c with K_s = sum w s^2 (constant per
-// test pixel), q_r = sum w r^2 (staged once per reference sample) and a_c = -2 w_c s_c gives
-// t = B + q_r + sum_c a_c r_c = e + (B - K_s), an integer in [0, 2B] that orders the candidates of a
-// pixel exactly as e does. The key t * 128 + k (k the raster index of the candidate) then orders them
-// as (error, raster index), so one unsigned minimum per candidate keeps the reference's first strict
-// minimum. A masked reference sample is staged as (0, 0, 0, 2^25 - 1): its key is above every real
-// one, so it never wins.
+// The same search by exact fp32 keys, the form of the unmasked search (qmiv_cps.cu): for a test pixel
+// s (test + GCD) and a candidate r, e - K_s + 2^23 = (q_r + 2^23) + sum_c (-2 w_c s_c) r_c with
+// K_s = sum_c w_c s_c^2 and q_r = sum_c w_c r_c^2 is three FFMAs. Where the host's check holds (the
+// bit depth, weights and GCD range keep every partial sum an integer below 2^24, the same condition as
+// the unmasked search, and 2^23 + B <= 2^24 - 2 with B = sum_c w_c (Max + MaxDiff_c)^2 the bound of
+// every error), the value lies in [2^20, 2^24 - 2], its bit pattern grows with it, and the key
+// (bits - bits(2^20)) * 128 + k (k the raster index of the candidate) orders candidates as (error,
+// raster index), the reference's first strict minimum. A masked reference sample is staged as
+// (0, 0, 0, 2^24 - 1): its value is that constant, above every real one, so it never wins against an
+// unmasked candidate (with every candidate masked the raster-first one is taken, as the integer
+// kernels do).
 // A CTA takes a 32 x 32 tile in both directions: it stages both pictures with an R halo (and the
 // tile's mask values) once; warps 0-7 search In1's pixels in In0 (R2T, -GCD), warps 8-15 In0's in In1
 // (T2R, +GCD), each thread four vertically adjacent pixels, so one staged sample read from shared
 // memory feeds up to four candidates. A test pixel's own samples come from the other picture's staged
 // tile (a masked one reads the sentinel, and its weight M = 0 discards the result).
+constexpr float    kMaskBias    = 8388608.0f;        // 2^23
+constexpr float    kMaskedValue = 16777215.0f;       // 2^24 - 1: the staged value of a masked sample
+constexpr uint32_t kMaskKeyBase = 0x49800000u;       // bit pattern of 2^20f
+
 template <int R>
 struct MaskKeyGeo
 {
   static constexpr int P = 4, TW = 32, TH = 8 * P, SW = TW + 2 * R, SH = TH + 2 * R, D = 2 * R + 1;
-  static constexpr size_t kSmem = sizeof(int4) * 2 * SH * SW + sizeof(int32_t) * TH * TW;
+  static constexpr size_t kSmem = sizeof(float4) * 2 * SH * SW + sizeof(int32_t) * TH * TW;
 };
 
 template <typename T, typename TM, int R>
@@ -383,58 +388,58 @@ __global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant
 {
   using G = MaskKeyGeo<R>;
   constexpr int P = G::P, TW = G::TW, TH = G::TH, SW = G::SW, SH = G::SH, D = G::D;
-  constexpr uint32_t kMaskedT = (1u << 25) - 1u;
   static_assert(D * D <= 128, "the raster index must fit the key's low 7 bits");
-  extern __shared__ int4 smem[];
-  int4* st0 = smem;                                          // In0: (Y, Cb, Cr, B + sum w r^2)
-  int4* st1 = smem + SH * SW;                                // In1
+  extern __shared__ float4 smem[];
+  float4* st0 = smem;                                         // In0: (Y, Cb, Cr, 2^23 + sum w r^2)
+  float4* st1 = smem + SH * SW;                               // In1
   int32_t* mk = reinterpret_cast<int32_t*>(smem + 2 * SH * SW);   // M of the tile's pixels, 0 outside the picture
   const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
-  const uint32_t w0 = (uint32_t)a.cws[0], w1 = (uint32_t)a.cws[1], w2 = (uint32_t)a.cws[2];
+  const float w0 = (float)a.cws[0], w1 = (float)a.cws[1], w2 = (float)a.cws[2];
   for(int e = threadIdx.x; e < SH * SW; e += 512)
   {
     const int ly = e / SW, lx = e - ly * SW;
     const int ux = x0 - R + lx, uy = y0 - R + ly;
     const int gx = clampi(ux, 0, a.W - 1), gy = clampi(uy, 0, a.H - 1);
     // branch-free: every sample is read, a masked one is replaced by the sentinel
-    const int32_t  mv = mask_at<TM>(a, gx, gy);
-    const uint32_t p0 = min((uint32_t)fetch<T>(a.in0, 0, gx, gy), a.clip);
-    const uint32_t p1 = min((uint32_t)fetch<T>(a.in0, 1, gx, gy), a.clip);
-    const uint32_t p2 = min((uint32_t)fetch<T>(a.in0, 2, gx, gy), a.clip);
-    const uint32_t q0 = min((uint32_t)fetch<T>(a.in1, 0, gx, gy), a.clip);
-    const uint32_t q1 = min((uint32_t)fetch<T>(a.in1, 1, gx, gy), a.clip);
-    const uint32_t q2 = min((uint32_t)fetch<T>(a.in1, 2, gx, gy), a.clip);
-    const uint32_t k0 = a.key_off + w0 * p0 * p0 + w1 * p1 * p1 + w2 * p2 * p2;
-    const uint32_t k1 = a.key_off + w0 * q0 * q0 + w1 * q1 * q1 + w2 * q2 * q2;
-    st0[e] = make_int4(mv ? (int32_t)p0 : 0, mv ? (int32_t)p1 : 0, mv ? (int32_t)p2 : 0, (int32_t)(mv ? k0 : kMaskedT));
-    st1[e] = make_int4(mv ? (int32_t)q0 : 0, mv ? (int32_t)q1 : 0, mv ? (int32_t)q2 : 0, (int32_t)(mv ? k1 : kMaskedT));
+    const int32_t mv = mask_at<TM>(a, gx, gy);
+    const float p0 = u2f_exact(min((uint32_t)fetch<T>(a.in0, 0, gx, gy), a.clip));
+    const float p1 = u2f_exact(min((uint32_t)fetch<T>(a.in0, 1, gx, gy), a.clip));
+    const float p2 = u2f_exact(min((uint32_t)fetch<T>(a.in0, 2, gx, gy), a.clip));
+    const float q0 = u2f_exact(min((uint32_t)fetch<T>(a.in1, 0, gx, gy), a.clip));
+    const float q1 = u2f_exact(min((uint32_t)fetch<T>(a.in1, 1, gx, gy), a.clip));
+    const float q2 = u2f_exact(min((uint32_t)fetch<T>(a.in1, 2, gx, gy), a.clip));
+    const float k0 = fmaf(w2, p2 * p2, fmaf(w1, p1 * p1, fmaf(w0, p0 * p0, kMaskBias)));
+    const float k1 = fmaf(w2, q2 * q2, fmaf(w1, q1 * q1, fmaf(w0, q0 * q0, kMaskBias)));
+    st0[e] = mv ? make_float4(p0, p1, p2, k0) : make_float4(0.f, 0.f, 0.f, kMaskedValue);
+    st1[e] = mv ? make_float4(q0, q1, q2, k1) : make_float4(0.f, 0.f, 0.f, kMaskedValue);
     if(ly >= R && ly < R + TH && lx >= R && lx < R + TW) { mk[(ly - R) * TW + (lx - R)] = (ux < a.W && uy < a.H) ? mv : 0; }
   }
   __syncthreads();
   const int dir = threadIdx.x >> 8;                          // warp-uniform
-  const int4* ref = dir ? st1 : st0;
-  const int4* tst = dir ? st0 : st1;
+  const float4* ref = dir ? st1 : st0;
+  const float4* tst = dir ? st0 : st1;
   const int tx = threadIdx.x & 31, ty = (threadIdx.x & 255) >> 5;
-  const int32_t sg = dir ? 1 : -1;
-  int32_t s[P][3], c0[P], c1[P], c2[P], m[P];
+  const float sg = dir ? 1.f : -1.f;
+  float s[P][3], c0[P], c1[P], c2[P];
+  int32_t m[P];
   uint32_t best[P];
   #pragma unroll
   for(int p = 0; p < P; p++)
   {
-    const int4 t = tst[(ty * P + p + R) * SW + tx + R];
-    s[p][0] = t.x + sg * a.out->gcd[0];
-    s[p][1] = t.y + sg * a.out->gcd[1];
-    s[p][2] = t.z + sg * a.out->gcd[2];
-    c0[p] = -2 * (int32_t)w0 * s[p][0];
-    c1[p] = -2 * (int32_t)w1 * s[p][1];
-    c2[p] = -2 * (int32_t)w2 * s[p][2];
+    const float4 t = tst[(ty * P + p + R) * SW + tx + R];
+    s[p][0] = fmaf(sg, (float)a.out->gcd[0], t.x);
+    s[p][1] = fmaf(sg, (float)a.out->gcd[1], t.y);
+    s[p][2] = fmaf(sg, (float)a.out->gcd[2], t.z);
+    c0[p] = -2.0f * w0 * s[p][0];
+    c1[p] = -2.0f * w1 * s[p][1];
+    c2[p] = -2.0f * w2 * s[p][2];
     m[p] = mk[(ty * P + p) * TW + tx];
     best[p] = 0xffffffffu;
   }
   // candidates in column pairs: one three-input minimum takes two keys
-  auto key = [&](const int4& r, int p, int k) -> uint32_t {
-    const uint32_t t = (uint32_t)r.w + (uint32_t)(c0[p] * r.x) + (uint32_t)(c1[p] * r.y) + (uint32_t)(c2[p] * r.z);
-    return t * a.kscale + (uint32_t)k;
+  auto key = [&](const float4& r, int p, int k) -> uint32_t {
+    const float t = fmaf(c2[p], r.z, fmaf(c1[p], r.y, fmaf(c0[p], r.x, r.w)));
+    return __float_as_uint(t) * a.kscale + ((uint32_t)k - (kMaskKeyBase << 7));
   };
   #pragma unroll
   for(int j = 0; j < D + P - 1; j++)
@@ -442,8 +447,8 @@ __global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant
     #pragma unroll
     for(int dx = 0; dx < D; dx += 2)
     {
-      const int4 ra = ref[(ty * P + j) * SW + tx + dx];
-      const int4 rb = ref[(ty * P + j) * SW + tx + min(dx + 1, D - 1)];
+      const float4 ra = ref[(ty * P + j) * SW + tx + dx];
+      const float4 rb = ref[(ty * P + j) * SW + tx + min(dx + 1, D - 1)];
       #pragma unroll
       for(int p = 0; p < P; p++)
       {
@@ -464,12 +469,12 @@ __global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant
     // the minimum is always some candidate's key (no key has low bits 127), so k < D * D; the clamp
     // keeps the read in the tile whatever the data
     const int k = min((int)(best[p] & 127u), D * D - 1);
-    const int4 bp = ref[(ty * P + p + k / D) * SW + tx + k % D];
-    const int32_t d[3] = { s[p][0] - bp.x, s[p][1] - bp.y, s[p][2] - bp.z };
+    const float4 bp = ref[(ty * P + p + k / D) * SW + tx + k % D];
+    const float d[3] = { s[p][0] - bp.x, s[p][1] - bp.y, s[p][2] - bp.z };   // exact integers
     #pragma unroll
     for(int c = 0; c < 3; c++)
     {
-      const uint64_t t = (uint64_t)(uint32_t)(d[c] * d[c]) * (uint64_t)(uint32_t)m[p];
+      const uint64_t t = (uint64_t)__float2uint_rn(d[c] * d[c]) * (uint64_t)(uint32_t)m[p];   // d^2 < 2^24: exact
       lo[p][c] = __reduce_add_sync(0xffffffffu, (uint32_t)t & 0xffffu);
       hi[p][c] = __reduce_add_sync(0xffffffffu, (uint32_t)(t >> 16));
     }
@@ -649,9 +654,10 @@ qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const 
   a.out = out_.as<MaskOut>();
   QMIV_CUDA(cudaMemsetAsync(out_.p, 0, sizeof(MaskOut), s));
   QMIV_CUDA(cudaMemsetAsync(a.row_cps, 0, (size_t)6 * S.H * sizeof(uint64_t), s));
-  // the key search needs samples in range (STOP fails on any other, CNCL clips), 2B < 2^25 - 1 with
-  // B = sum_c w_c (Max + MaxDiff_c)^2, the bound of every error and of every sum of w s^2, and every
-  // squared difference below 2^24 (its row sums split the terms into two 32-bit parts)
+  // the key search needs samples in range (STOP fails on any other, CNCL clips), the fp32 exactness of
+  // the unmasked search, 2^23 + B <= 2^24 - 2 with B = sum_c w_c (Max + MaxDiff_c)^2, the bound of every
+  // error (so that the masked sentinel 2^24 - 1 is above every real value), and every squared
+  // difference below 2^24 (its row sums split the terms into two 32-bit parts)
   int64_t bound = 0, dmax2 = 0;
   for(int c = 0; c < 3; c++)
   {
@@ -660,8 +666,8 @@ qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const 
     dmax2 = std::max(dmax2, m * m);
   }
   const bool key = (prm.invalid_pel_action == QMIV_PEL_STOP || prm.invalid_pel_action == QMIV_PEL_CNCL) &&
-                   2 * bound < (int64_t)((1u << 25) - 1u) && dmax2 < ((int64_t)1 << 24);
-  a.key_off = (uint32_t)(key ? bound : 0);
+                   cps_fp32_exact(S.maxv, prm.cws, a.maxdiff) && ((int64_t)1 << 23) + bound <= ((int64_t)1 << 24) - 2 &&
+                   dmax2 < ((int64_t)1 << 24);
   a.kscale = 128u;
   const int R = prm.search_range;
   cudaError_t e;
