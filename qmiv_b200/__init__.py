@@ -360,6 +360,24 @@ class Batch:
         check(self._lib.qmiv_batch_compute(self.handle, descs, len(pairs), out), "qmiv_batch_compute")
         return [out[i].as_dict() for i in range(len(pairs))]
 
+    def compute_masked(self, pairs: Iterable[dict], masks, mask_bitdepths) -> tuple[list[dict], list[int]]:
+        """Mask mode for many pairs (qmiv_batch_compute_masked): pairs as for compute() (metrics from
+        PSNR, WSPSNR, IVPSNR), masks the mask pictures' luma planes (uint8 for bit depth 8, else uint16;
+        host arrays or CUDA tensors), mask_bitdepths one per pair. Returns (result dicts, numbers of
+        non-zero mask samples)."""
+        pairs = list(pairs)
+        n = len(pairs)
+        descs, keep = self._descs(pairs)
+        fm = (_lib.QmivFrame * max(1, n))()
+        for i, m in enumerate(masks):
+            fm[i], k = make_frame((m, m, m))
+            keep.append(k)
+        bds = (ctypes.c_int32 * max(1, n))(*mask_bitdepths)
+        out = (_lib.QmivResult * max(1, n))()
+        nnm = (ctypes.c_int32 * max(1, n))()
+        check(self._lib.qmiv_batch_compute_masked(self.handle, descs, fm, bds, n, out, nnm), "qmiv_batch_compute_masked")
+        return [out[i].as_dict() for i in range(n)], [int(nnm[i]) for i in range(n)]
+
     def submit(self, pairs: Iterable[dict]) -> int:
         """Asynchronous compute (qmiv_batch_submit): returns a ticket for wait(); up to two in flight.
         The frames must stay alive and unchanged until the wait."""

@@ -131,6 +131,9 @@ SIGNATURES = {
     "qmiv_batch_destroy": (ctypes.c_int, [_P]),
     "qmiv_batch_stream": (ctypes.c_int, [_P, _PP]),
     "qmiv_batch_compute": (ctypes.c_int, [_P, ctypes.POINTER(QmivPairDesc), ctypes.c_int32, ctypes.POINTER(QmivResult)]),
+    "qmiv_batch_compute_masked": (ctypes.c_int, [_P, ctypes.POINTER(QmivPairDesc), ctypes.POINTER(QmivFrame),
+                                                 ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.POINTER(QmivResult),
+                                                 ctypes.POINTER(ctypes.c_int32)]),
     "qmiv_batch_submit": (ctypes.c_int, [_P, ctypes.POINTER(QmivPairDesc), ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
     "qmiv_batch_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(QmivResult)]),
     "qmiv_batch_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -16,6 +16,7 @@ struct qmiv_batch_s
   uint64_t     ticket[2] = { 0, 0 };            // submission held by each slot, 0 = none
   uint64_t     next_ticket = 1;
   Engine& slot(int k) { return k == 0 ? engine : *engine2; }
+  std::unique_ptr<MaskedBatch> masked;          // mask-mode calls, created on first use
 };
 
 extern "C" {
@@ -84,6 +85,17 @@ qmiv_status qmiv_batch_wait(qmiv_batch b, uint64_t ticket, qmiv_result* out)
     }
   }
   return fail(QMIV_ERR_INVALID_ARG, "unknown ticket");
+}
+
+qmiv_status qmiv_batch_compute_masked(qmiv_batch b, const qmiv_pair_desc* pairs, const qmiv_frame* masks,
+                                      const int32_t* mask_bitdepths, int32_t n, qmiv_result* out, int32_t* num_non_masked)
+{
+  if(!b || !pairs || !masks || !mask_bitdepths || n <= 0) { return fail(QMIV_ERR_INVALID_ARG, "null argument or no pairs"); }
+  if(n > b->max_pairs) { return fail(QMIV_ERR_INVALID_ARG, "more pairs than the batch was created for"); }
+  if(b->ticket[0] || b->ticket[1]) { return fail(QMIV_ERR_BUSY, "a submission is in flight; wait for it first"); }
+  QMIV_CUDA(cudaSetDevice(b->ctx->device));
+  if(!b->masked) { b->masked.reset(new MaskedBatch()); }
+  return b->masked->run(b->ctx, b->prm, b->engine.stream(), pairs, masks, mask_bitdepths, n, out, num_non_masked);
 }
 
 qmiv_status qmiv_batch_stream(qmiv_batch b, void** cuda_stream)

@@ -218,12 +218,10 @@ qmiv_status PairPipeline::prepare(uint32_t mask, bool want_scp, bool host_frames
   return QMIV_OK;
 }
 
-qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cudaStream_t s)
+qmiv_status resolve_frame(const Shape& S, const qmiv_frame* f, char* staging, Img& out, cudaStream_t s)
 {
-  const Shape& S = shape_;
   if(!f) { return fail(QMIV_ERR_INVALID_ARG, "frame is null"); }
-  size_t off = (size_t)which * S.staged_frame_bytes();
-  const int tok = f->mem == QMIV_MEM_HOST ? prof_begin(s) : -1;
+  size_t off = 0;
   for(int c = 0; c < 3; c++)
   {
     if(!f->plane[c]) { return fail(QMIV_ERR_INVALID_ARG, "frame plane is null"); }
@@ -238,8 +236,8 @@ qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cuda
     }
     else if(f->mem == QMIV_MEM_HOST)
     {
-      if(!staging_.p) { return fail(QMIV_ERR_INVALID_ARG, "staging not prepared"); }
-      char* dst = staging_.as<char>() + off;
+      if(!staging) { return fail(QMIV_ERR_INVALID_ARG, "staging not prepared"); }
+      char* dst = staging + off;
       if((size_t)f->pitch[c] == row_bytes && S.staged_pitch(c) == row_bytes)
       {
         QMIV_CUDA(cudaMemcpyAsync(dst, f->plane[c], row_bytes * S.plane_rows(c), cudaMemcpyHostToDevice, s));
@@ -255,6 +253,15 @@ qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cuda
     }
     else { return fail(QMIV_ERR_INVALID_ARG, "frame mem must be QMIV_MEM_HOST or QMIV_MEM_DEVICE"); }
   }
+  return QMIV_OK;
+}
+
+qmiv_status PairPipeline::resolve(const qmiv_frame* f, int which, Img& out, cudaStream_t s)
+{
+  if(!f) { return fail(QMIV_ERR_INVALID_ARG, "frame is null"); }
+  const int tok = f->mem == QMIV_MEM_HOST ? prof_begin(s) : -1;
+  char* stage = staging_.p ? staging_.as<char>() + (size_t)which * shape_.staged_frame_bytes() : nullptr;
+  QMIV_TRY(resolve_frame(shape_, f, stage, out, s));
   prof_end(s, QMIV_STAGE_H2D, tok);
   return QMIV_OK;
 }

@@ -108,6 +108,10 @@ struct Shape
 
 qmiv_status validate_params(const qmiv_params& p);
 
+// The device view of a frame of shape S: device planes are used in place, host planes are copied into
+// `staging` (S.staged_frame_bytes(), rows padded to 16 bytes) on stream s.
+qmiv_status resolve_frame(const Shape& S, const qmiv_frame* f, char* staging, Img& out, cudaStream_t s);
+
 // Structural similarity options of a parameter set (xSSIM::setStructSimParams, xSSIM.cpp:86-113).
 constexpr uint32_t kSsimFamily = QMIV_SSIM | QMIV_MSSSIM | QMIV_IVSSIM | QMIV_IVMSSSIM;
 inline bool    ssim_regular(int32_t mode) { return mode >= QMIV_SSM_REGULAR_GAUSSIAN_FLT && mode <= QMIV_SSM_REGULAR_AVERAGED; }
@@ -239,6 +243,22 @@ private:
 };
 
 // Mask mode of one calc (qmiv_masked.cu): its scratch and the synchronous run.
+// Mask mode for many frame pairs of uneven shape (qmiv_batch_compute_masked): every stage one launch
+// per group of pairs with the same sample sizes, search range and search form.
+class MaskedBatch
+{
+public:
+  qmiv_status run(qmiv_ctx_s* ctx, const qmiv_params& prm, cudaStream_t s, const qmiv_pair_desc* pairs,
+                  const qmiv_frame* masks, const int32_t* mask_bitdepths, int32_t n, qmiv_result* out,
+                  int32_t* num_non_masked);
+  ~MaskedBatch();
+
+private:
+  DevMem arena_;
+  void*  h_ = nullptr;        // pinned mirror of the argument tables and the results
+  size_t h_bytes_ = 0;
+};
+
 class MaskedPipeline
 {
 public:

@@ -27,6 +27,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
 
 namespace qmiv {
 
@@ -61,6 +64,26 @@ struct MaskArgs
   MaskOut*    out;
   uint32_t    kscale;          // 128, read from the parameter bank so the key stays one integer multiply-add
 };
+
+// Host-side description of one masked frame pair: its shape and parameters and what follows from them
+// (the GCD-M clip range, which search form applies, the ERP row weights and their correction).
+struct MaskPlan
+{
+  Shape               S;
+  qmiv_params         prm{};
+  int32_t             mbd = 8;       // mask bit depth
+  size_t              mesz = 1;      // bytes per mask sample
+  int32_t             maxdiff[4] = { 0, 0, 0, 0 };
+  bool                key = false;   // the exact-key search applies (k_cps_masked_key)
+  double              ws_corr = 1.0;
+  std::vector<double> ws;            // [H] with ERP
+};
+qmiv_status plan_masked(const Shape& S, const qmiv_params& prm, const qmiv_frame* mask, int32_t mask_bitdepth, MaskPlan& P);
+qmiv_status resolve_mask(const MaskPlan& P, const qmiv_frame* mask, char* staging, MaskArgs& a, cudaStream_t s);
+void        fill_mask_args(const MaskPlan& P, const Img& a0, const Img& a1, uint64_t* rows, const double* ws, MaskOut* out,
+                           MaskArgs& a);
+qmiv_status masked_status(const MaskOut& o, const MaskPlan& P);
+void        finish_masked(const MaskOut& o, const MaskPlan& P, uint32_t metrics, qmiv_result* out);
 
 namespace {
 
@@ -131,10 +154,10 @@ __device__ __forceinline__ void mask_prepass_row_tail(const MaskArgs& a, int y, 
 // before any arithmetic, then the warps' sums meet in shared memory and one thread writes the row's
 // SSD and adds the row's totals.
 template <typename T, typename TM>
-__global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ MaskArgs a)
+__device__ __forceinline__ void mask_prepass_body(const MaskArgs& a, int row)
 {
   constexpr int U = 4;
-  const int y = blockIdx.x;
+  const int y = row;
   int64_t  sd[3] = { 0, 0, 0 };
   uint64_t ssd[3] = { 0, 0, 0 };
   uint32_t nnm = 0, dif = 0, mx0 = 0, mx1 = 0;
@@ -196,10 +219,10 @@ __device__ __forceinline__ void ld2(const uint16_t* p, uint32_t v[2])
 }
 
 template <typename T, typename TM>
-__global__ void __launch_bounds__(256) k_mask_prepass420v(const __grid_constant__ MaskArgs a)
+__device__ __forceinline__ void mask_prepass420v_body(const MaskArgs& a, int row)
 {
   constexpr int U = 2;
-  const int y = blockIdx.x;
+  const int y = row;
   const int ng = a.W >> 2;                                    // groups of four pixels in the row
   const T* l0 = static_cast<const T*>(a.in0.p[0]) + (size_t)y * a.in0.pitch[0];
   const T* l1 = static_cast<const T*>(a.in1.p[0]) + (size_t)y * a.in1.pitch[0];
@@ -268,7 +291,7 @@ bool mask_prepass_vec_ok(const MaskArgs& a, size_t esz, size_t mesz)
 }
 
 // GCD-M, xGlobClrDiff.cpp:60-91 (called with swapped pictures, xGlobClrDiff.h:42: mean of In1 - In0)
-__global__ void k_mask_reduce(const __grid_constant__ MaskArgs a)
+__device__ __forceinline__ void mask_reduce_body(const MaskArgs& a)
 {
   if(threadIdx.x != 0) { return; }
   MaskOut* o = a.out;
@@ -288,14 +311,14 @@ __global__ void k_mask_reduce(const __grid_constant__ MaskArgs a)
 // reference samples and mask of the tile plus an R halo at clamped coordinates (the reference's
 // edge-extended margin). Candidates run in raster order with a strict minimum of the int32 error.
 template <typename T, typename TM, int R>
-__global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ MaskArgs a)
+__device__ __forceinline__ void cps_masked_body(const MaskArgs& a, int bx, int by, int bz)
 {
   constexpr int TW = 32, TH = 8, SW = TW + 2 * R, SH = TH + 2 * R;
   __shared__ int4 st[SH][SW];                                // (Y, Cb, Cr, mask)
-  const int dir = blockIdx.z;
+  const int dir = bz;
   const Img& tst = dir ? a.in0 : a.in1;
   const Img& ref = dir ? a.in1 : a.in0;
-  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  const int x0 = bx * TW, y0 = by * TH;
   for(int e = threadIdx.x; e < SH * SW; e += 256)
   {
     const int ly = e / SW, lx = e - ly * SW;
@@ -384,7 +407,7 @@ struct MaskKeyGeo
 };
 
 template <typename T, typename TM, int R>
-__global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant__ MaskArgs a)
+__device__ __forceinline__ void cps_masked_key_body(const MaskArgs& a, int bx, int by)
 {
   using G = MaskKeyGeo<R>;
   constexpr int P = G::P, TW = G::TW, TH = G::TH, SW = G::SW, SH = G::SH, D = G::D;
@@ -393,7 +416,7 @@ __global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant
   float4* st0 = smem;                                         // In0: (Y, Cb, Cr, 2^23 + sum w r^2)
   float4* st1 = smem + SH * SW;                               // In1
   int32_t* mk = reinterpret_cast<int32_t*>(smem + 2 * SH * SW);   // M of the tile's pixels, 0 outside the picture
-  const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+  const int x0 = bx * TW, y0 = by * TH;
   const float w0 = (float)a.cws[0], w1 = (float)a.cws[1], w2 = (float)a.cws[2];
   for(int e = threadIdx.x; e < SH * SW; e += 512)
   {
@@ -496,28 +519,17 @@ __global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant
   }
 }
 
-template <typename T, typename TM, int R>
-cudaError_t launch_masked_key(const MaskArgs& a, cudaStream_t s)
-{
-  constexpr size_t smem = MaskKeyGeo<R>::kSmem;
-  const cudaError_t e = cudaFuncSetAttribute(k_cps_masked_key<T, TM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if(e != cudaSuccess) { return e; }
-  const dim3 grid((a.W + MaskKeyGeo<R>::TW - 1) / MaskKeyGeo<R>::TW, (a.H + MaskKeyGeo<R>::TH - 1) / MaskKeyGeo<R>::TH);
-  k_cps_masked_key<T, TM, R><<<grid, 512, smem, s>>>(a);
-  return cudaSuccess;
-}
-
 // Chains 0..2: WS rows of component c; chains 3..8: CPS rows of (direction, component). Each is the
 // reference's row-order compensated sum; the CPS chains also form the plain uint64 totals. One CTA per
 // chain: all threads stage a chunk of the chain's terms (the products with the ERP weights, the same
 // doubles the serial loop would form) in shared memory, then thread 0 adds them in row order, so the
 // serial chain never waits on global memory.
 constexpr int kMaskFinChunk = 4096;
-__global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ MaskArgs a)
+__device__ __forceinline__ void mask_finalize_body(const MaskArgs& a, int chain)
 {
   __shared__ double vals[kMaskFinChunk];
   __shared__ unsigned long long tot;
-  const int k = blockIdx.x;
+  const int k = chain;
   if(k < 3 && !a.ws) { return; }                              // uniform over the CTA
   MaskOut* o = a.out;
   const int H = a.H;
@@ -554,6 +566,58 @@ __global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ M
     o->cps_ws[d][c] = a.ws ? s.result() : 0.0;
   }
   else { o->ws_err[k] = s.result(); }
+}
+
+// ---- kernels: one frame pair (arguments in parameter space) and many (a device table of arguments,
+// one grid dimension indexing the pair; CTAs beyond their pair's extent return) -----------------
+template <typename T, typename TM>
+__global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ MaskArgs a) { mask_prepass_body<T, TM>(a, blockIdx.x); }
+template <typename T, typename TM>
+__global__ void __launch_bounds__(256) k_mask_prepass420v(const __grid_constant__ MaskArgs a) { mask_prepass420v_body<T, TM>(a, blockIdx.x); }
+__global__ void k_mask_reduce(const __grid_constant__ MaskArgs a) { mask_reduce_body(a); }
+template <typename T, typename TM, int R>
+__global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ MaskArgs a) { cps_masked_body<T, TM, R>(a, blockIdx.x, blockIdx.y, blockIdx.z); }
+template <typename T, typename TM, int R>
+__global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant__ MaskArgs a) { cps_masked_key_body<T, TM, R>(a, blockIdx.x, blockIdx.y); }
+__global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ MaskArgs a) { mask_finalize_body(a, blockIdx.x); }
+
+// jobs: the pairs of one launch group; vec: the group's pairs take the vector-load prepass
+template <typename T, typename TM, bool VEC>
+__global__ void __launch_bounds__(256) k_mask_prepass_multi(const MaskArgs* __restrict__ jobs, const int32_t* __restrict__ idx)
+{
+  const MaskArgs& a = jobs[idx[blockIdx.y]];
+  if((int)blockIdx.x >= a.H) { return; }
+  if(VEC) { mask_prepass420v_body<T, TM>(a, blockIdx.x); } else { mask_prepass_body<T, TM>(a, blockIdx.x); }
+}
+__global__ void k_mask_reduce_multi(const MaskArgs* __restrict__ jobs) { mask_reduce_body(jobs[blockIdx.x]); }
+template <typename T, typename TM, int R>
+__global__ void __launch_bounds__(256) k_cps_masked_multi(const MaskArgs* __restrict__ jobs, const int32_t* __restrict__ idx)
+{
+  const MaskArgs& a = jobs[idx[blockIdx.z >> 1]];
+  if((int)blockIdx.x * 32 >= a.W || (int)blockIdx.y * 8 >= a.H) { return; }
+  cps_masked_body<T, TM, R>(a, blockIdx.x, blockIdx.y, blockIdx.z & 1);
+}
+template <typename T, typename TM, int R>
+__global__ void __launch_bounds__(512, 2) k_cps_masked_key_multi(const MaskArgs* __restrict__ jobs, const int32_t* __restrict__ idx)
+{
+  const MaskArgs& a = jobs[idx[blockIdx.z]];
+  if((int)blockIdx.x * MaskKeyGeo<R>::TW >= a.W || (int)blockIdx.y * MaskKeyGeo<R>::TH >= a.H) { return; }
+  cps_masked_key_body<T, TM, R>(a, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(256) k_mask_finalize_multi(const MaskArgs* __restrict__ jobs)
+{
+  mask_finalize_body(jobs[blockIdx.x / 9], blockIdx.x % 9);
+}
+
+template <typename T, typename TM, int R>
+cudaError_t launch_masked_key(const MaskArgs& a, cudaStream_t s)
+{
+  constexpr size_t smem = MaskKeyGeo<R>::kSmem;
+  const cudaError_t e = cudaFuncSetAttribute(k_cps_masked_key<T, TM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if(e != cudaSuccess) { return e; }
+  const dim3 grid((a.W + MaskKeyGeo<R>::TW - 1) / MaskKeyGeo<R>::TW, (a.H + MaskKeyGeo<R>::TH - 1) / MaskKeyGeo<R>::TH);
+  k_cps_masked_key<T, TM, R><<<grid, 512, smem, s>>>(a);
+  return cudaSuccess;
 }
 
 template <typename T, typename TM>
@@ -600,60 +664,20 @@ double psnr_masked(double ssd, int32_t nnm, int32_t bitdepth_pic, int32_t bitdep
 
 }  // namespace
 
-MaskedPipeline::~MaskedPipeline()
+// ---- host side, shared by the one-pair call and the batched form ---------------------------------
+qmiv_status plan_masked(const Shape& S, const qmiv_params& prm, const qmiv_frame* mask, int32_t mask_bitdepth, MaskPlan& P)
 {
-  if(h_out_) { cudaFreeHost(h_out_); }
-}
-
-qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const qmiv_frame* in1, const qmiv_frame* mask,
-                                int32_t mask_bitdepth, uint32_t metrics, qmiv_result* out, int32_t* num_non_masked)
-{
-  PairPipeline& pipe = calc->pipe;
-  const Shape& S = pipe.shape();
-  const qmiv_params& prm = calc->prm;
-  cudaStream_t s = calc->stream;
   if(mask_bitdepth < 8 || mask_bitdepth > 14) { return fail(QMIV_ERR_INVALID_ARG, "mask bit depth must be in 8..14"); }
   if(!mask || !mask->plane[0]) { return fail(QMIV_ERR_INVALID_ARG, "mask plane is null"); }
-  const size_t mesz = mask_bitdepth <= 8 ? 1 : 2;
-  const size_t mrow = (size_t)S.W * mesz;
-  if(mask->pitch[0] < (int64_t)mrow || (mask->pitch[0] % (int64_t)mesz) != 0) { return fail(QMIV_ERR_INVALID_ARG, "bad mask pitch"); }
+  if(mask->mem != QMIV_MEM_HOST && mask->mem != QMIV_MEM_DEVICE) { return fail(QMIV_ERR_INVALID_ARG, "mask mem must be QMIV_MEM_HOST or QMIV_MEM_DEVICE"); }
+  P.mesz = mask_bitdepth <= 8 ? 1 : 2;
+  const size_t mrow = (size_t)S.W * P.mesz;
+  if(mask->pitch[0] < (int64_t)mrow || (mask->pitch[0] % (int64_t)P.mesz) != 0) { return fail(QMIV_ERR_INVALID_ARG, "bad mask pitch"); }
   if(S.bitdepth > 14) { return fail(QMIV_ERR_UNSUPPORTED, "mask mode needs bit depth <= 14"); }
-
-  const bool host = in0->mem == QMIV_MEM_HOST || in1->mem == QMIV_MEM_HOST;
-  QMIV_TRY(pipe.prepare(QMIV_PSNR, false, host));           // staging for host frames, ERP weights on the device
-  Img a0{}, a1{};
-  QMIV_TRY(pipe.resolve(in0, 0, a0, s));
-  QMIV_TRY(pipe.resolve(in1, 1, a1, s));
-
-  QMIV_TRY(out_.ensure(calc->ctx, sizeof(MaskOut)));
-  QMIV_TRY(rows_.ensure(calc->ctx, (size_t)9 * S.H * sizeof(uint64_t)));
-  if(!h_out_) { QMIV_CUDA(cudaMallocHost(&h_out_, sizeof(MaskOut))); }
-  MaskArgs a{};
-  a.in0 = a0; a.in1 = a1;
-  if(mask->mem == QMIV_MEM_DEVICE)
-  {
-    a.mask = mask->plane[0];
-    a.mpitch = (int32_t)(mask->pitch[0] / (int64_t)mesz);
-  }
-  else if(mask->mem == QMIV_MEM_HOST)
-  {
-    QMIV_TRY(stage_.ensure(calc->ctx, mrow * S.H));
-    QMIV_CUDA(cudaMemcpy2DAsync(stage_.p, mrow, mask->plane[0], (size_t)mask->pitch[0], mrow, S.H, cudaMemcpyHostToDevice, s));
-    a.mask = stage_.p;
-    a.mpitch = S.W;
-  }
-  else { return fail(QMIV_ERR_INVALID_ARG, "mask mem must be QMIV_MEM_HOST or QMIV_MEM_DEVICE"); }
-  a.W = S.W; a.H = S.H;
-  a.clip = prm.invalid_pel_action == QMIV_PEL_CNCL ? (uint32_t)S.maxv : 0xffffu;
-  a.maxv = S.maxv; a.mask_max = (1 << mask_bitdepth) - 1;
-  for(int c = 0; c < 4; c++) { a.maxdiff[c] = pipe.maxdiff()[c]; }
-  for(int c = 0; c < 3; c++) { a.cws[c] = prm.cws[c]; }
-  a.row_ssd = rows_.as<uint64_t>();
-  a.row_cps = rows_.as<uint64_t>() + (size_t)3 * S.H;
-  a.ws = prm.erp ? pipe.ws_device() : nullptr;
-  a.out = out_.as<MaskOut>();
-  QMIV_CUDA(cudaMemsetAsync(out_.p, 0, sizeof(MaskOut), s));
-  QMIV_CUDA(cudaMemsetAsync(a.row_cps, 0, (size_t)6 * S.H * sizeof(uint64_t), s));
+  P.S = S;
+  P.prm = prm;
+  P.mbd = mask_bitdepth;
+  for(int c = 0; c < 4; c++) { P.maxdiff[c] = round_f32_half_away(prm.unc[c] * (float)S.maxv); }   // xGlobClrDiff.cpp:76
   // the key search needs samples in range (STOP fails on any other, CNCL clips), the fp32 exactness of
   // the unmasked search, 2^23 + B <= 2^24 - 2 with B = sum_c w_c (Max + MaxDiff_c)^2, the bound of every
   // error (so that the masked sentinel 2^24 - 1 is above every real value), and every squared
@@ -661,34 +685,69 @@ qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const 
   int64_t bound = 0, dmax2 = 0;
   for(int c = 0; c < 3; c++)
   {
-    const int64_t m = (int64_t)S.maxv + std::abs((int64_t)a.maxdiff[c]);
+    const int64_t m = (int64_t)S.maxv + std::abs((int64_t)P.maxdiff[c]);
     bound += (int64_t)prm.cws[c] * m * m;
     dmax2 = std::max(dmax2, m * m);
   }
-  const bool key = (prm.invalid_pel_action == QMIV_PEL_STOP || prm.invalid_pel_action == QMIV_PEL_CNCL) &&
-                   cps_fp32_exact(S.maxv, prm.cws, a.maxdiff) && ((int64_t)1 << 23) + bound <= ((int64_t)1 << 24) - 2 &&
-                   dmax2 < ((int64_t)1 << 24);
-  a.kscale = 128u;
-  const int R = prm.search_range;
-  cudaError_t e;
-  if(S.esz == 1) { e = mesz == 1 ? launch_masked_t<uint8_t, uint8_t>(a, R, key, s) : launch_masked_t<uint8_t, uint16_t>(a, R, key, s); }
-  else { e = mesz == 1 ? launch_masked_t<uint16_t, uint8_t>(a, R, key, s) : launch_masked_t<uint16_t, uint16_t>(a, R, key, s); }
-  if(e != cudaSuccess) { return cuda_fail(e, "masked launches"); }
-  QMIV_CUDA(cudaMemcpyAsync(h_out_, out_.p, sizeof(MaskOut), cudaMemcpyDeviceToHost, s));
-  QMIV_CUDA(cudaStreamSynchronize(s));
-  const MaskOut& o = *static_cast<const MaskOut*>(h_out_);
+  P.key = (prm.invalid_pel_action == QMIV_PEL_STOP || prm.invalid_pel_action == QMIV_PEL_CNCL) &&
+          cps_fp32_exact(S.maxv, prm.cws, P.maxdiff) && ((int64_t)1 << 23) + bound <= ((int64_t)1 << 24) - 2 &&
+          dmax2 < ((int64_t)1 << 24);
+  P.ws.clear();
+  P.ws_corr = 1.0;
+  if(prm.erp) { ws_weights(S.H, prm.lat_range_deg, P.ws, P.ws_corr); }
+  return QMIV_OK;
+}
 
-  if(prm.invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3))
+qmiv_status resolve_mask(const MaskPlan& P, const qmiv_frame* mask, char* staging, MaskArgs& a, cudaStream_t s)
+{
+  const size_t mrow = (size_t)P.S.W * P.mesz;
+  if(mask->mem == QMIV_MEM_DEVICE)
+  {
+    a.mask = mask->plane[0];
+    a.mpitch = (int32_t)(mask->pitch[0] / (int64_t)P.mesz);
+    return QMIV_OK;
+  }
+  if(!staging) { return fail(QMIV_ERR_INVALID_ARG, "mask staging not prepared"); }
+  QMIV_CUDA(cudaMemcpy2DAsync(staging, mrow, mask->plane[0], (size_t)mask->pitch[0], mrow, P.S.H, cudaMemcpyHostToDevice, s));
+  a.mask = staging;
+  a.mpitch = P.S.W;
+  return QMIV_OK;
+}
+
+void fill_mask_args(const MaskPlan& P, const Img& a0, const Img& a1, uint64_t* rows, const double* ws, MaskOut* out, MaskArgs& a)
+{
+  const Shape& S = P.S;
+  a.in0 = a0; a.in1 = a1;
+  a.W = S.W; a.H = S.H;
+  a.clip = P.prm.invalid_pel_action == QMIV_PEL_CNCL ? (uint32_t)S.maxv : 0xffffu;
+  a.maxv = S.maxv; a.mask_max = (1 << P.mbd) - 1;
+  for(int c = 0; c < 4; c++) { a.maxdiff[c] = P.maxdiff[c]; }
+  for(int c = 0; c < 3; c++) { a.cws[c] = P.prm.cws[c]; }
+  a.row_ssd = rows;
+  a.row_cps = rows + (size_t)3 * S.H;
+  a.ws = P.prm.erp ? ws : nullptr;
+  a.out = out;
+  a.kscale = 128u;
+}
+
+qmiv_status masked_status(const MaskOut& o, const MaskPlan& P)
+{
+  if(P.prm.invalid_pel_action == QMIV_PEL_STOP && (o.flags & 3))
   {
     return fail(QMIV_ERR_INVALID_PIXEL, "input frame contains samples above the bit depth's maximum");
   }
   if(o.nnm == 0) { return fail(QMIV_ERR_INVALID_ARG, "the mask has no non-zero sample"); }
-  if(num_non_masked) { *num_non_masked = o.nnm; }
-  if(!out) { return QMIV_OK; }
+  return QMIV_OK;
+}
 
+// dB values with the reference's arithmetic and conventions
+void finish_masked(const MaskOut& o, const MaskPlan& P, uint32_t metrics, qmiv_result* out)
+{
+  const Shape& S = P.S;
+  const qmiv_params& prm = P.prm;
   std::memset(out, 0, sizeof(*out));
   const int64_t area = (int64_t)S.W * S.H;
-  const int32_t bd = S.bitdepth, mbd = mask_bitdepth;
+  const int32_t bd = S.bitdepth, mbd = P.mbd;
   for(int c = 0; c < 4; c++) { out->gcd_r2t[c] = o.gcd[c]; }
   for(int c = 0; c < 3; c++)
   {
@@ -712,7 +771,7 @@ qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const 
   {
     for(int c = 0; c < 3; c++)
     {
-      const double v = prm.erp ? psnr_masked(o.ws_err[c] * pipe.ws_corr(), o.nnm, bd, mbd) : psnr_masked((double)o.ssd[c], o.nnm, mbd, mbd);
+      const double v = prm.erp ? psnr_masked(o.ws_err[c] * P.ws_corr, o.nnm, bd, mbd) : psnr_masked((double)o.ssd[c], o.nnm, mbd, mbd);
       out->wspsnr[c] = out->exact[c] ? fake : v;
     }
     out->wspsnr_pic = per_pic3(out->wspsnr);
@@ -733,7 +792,225 @@ qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const 
     out->ivpsnr_r2t = q[0]; out->ivpsnr_t2r = q[1];
     out->ivpsnr = (q[1] < q[0]) ? q[1] : q[0];
   }
+}
+
+MaskedPipeline::~MaskedPipeline()
+{
+  if(h_out_) { cudaFreeHost(h_out_); }
+}
+
+qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const qmiv_frame* in1, const qmiv_frame* mask,
+                                int32_t mask_bitdepth, uint32_t metrics, qmiv_result* out, int32_t* num_non_masked)
+{
+  PairPipeline& pipe = calc->pipe;
+  const Shape& S = pipe.shape();
+  cudaStream_t s = calc->stream;
+  MaskPlan P;
+  QMIV_TRY(plan_masked(S, calc->prm, mask, mask_bitdepth, P));
+  const bool host = in0->mem == QMIV_MEM_HOST || in1->mem == QMIV_MEM_HOST;
+  QMIV_TRY(pipe.prepare(QMIV_PSNR, false, host));           // staging for host frames, ERP weights on the device
+  Img a0{}, a1{};
+  QMIV_TRY(pipe.resolve(in0, 0, a0, s));
+  QMIV_TRY(pipe.resolve(in1, 1, a1, s));
+  QMIV_TRY(out_.ensure(calc->ctx, sizeof(MaskOut)));
+  QMIV_TRY(rows_.ensure(calc->ctx, (size_t)9 * S.H * sizeof(uint64_t)));
+  if(!h_out_) { QMIV_CUDA(cudaMallocHost(&h_out_, sizeof(MaskOut))); }
+  MaskArgs a{};
+  if(mask->mem == QMIV_MEM_HOST) { QMIV_TRY(stage_.ensure(calc->ctx, (size_t)S.W * P.mesz * S.H)); }
+  QMIV_TRY(resolve_mask(P, mask, stage_.as<char>(), a, s));
+  fill_mask_args(P, a0, a1, rows_.as<uint64_t>(), pipe.ws_device(), out_.as<MaskOut>(), a);
+  QMIV_CUDA(cudaMemsetAsync(out_.p, 0, sizeof(MaskOut), s));
+  QMIV_CUDA(cudaMemsetAsync(a.row_cps, 0, (size_t)6 * S.H * sizeof(uint64_t), s));
+  const int R = P.prm.search_range;
+  cudaError_t e;
+  if(S.esz == 1) { e = P.mesz == 1 ? launch_masked_t<uint8_t, uint8_t>(a, R, P.key, s) : launch_masked_t<uint8_t, uint16_t>(a, R, P.key, s); }
+  else { e = P.mesz == 1 ? launch_masked_t<uint16_t, uint8_t>(a, R, P.key, s) : launch_masked_t<uint16_t, uint16_t>(a, R, P.key, s); }
+  if(e != cudaSuccess) { return cuda_fail(e, "masked launches"); }
+  QMIV_CUDA(cudaMemcpyAsync(h_out_, out_.p, sizeof(MaskOut), cudaMemcpyDeviceToHost, s));
+  QMIV_CUDA(cudaStreamSynchronize(s));
+  const MaskOut& o = *static_cast<const MaskOut*>(h_out_);
+  QMIV_TRY(masked_status(o, P));
+  if(num_non_masked) { *num_non_masked = o.nnm; }
+  if(out) { finish_masked(o, P, metrics, out); }
   return QMIV_OK;
+}
+
+// ---- batched form ---------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kMaskAlign = 256;
+inline size_t malign(size_t v) { return (v + kMaskAlign - 1) & ~(kMaskAlign - 1); }
+
+template <typename T, typename TM>
+void launch_prepass_group(const MaskArgs* d, const int32_t* idx, int count, int max_h, bool vec, cudaStream_t s)
+{
+  const dim3 grid(max_h, count);
+  if(vec) { k_mask_prepass_multi<T, TM, true><<<grid, 256, 0, s>>>(d, idx); }
+  else { k_mask_prepass_multi<T, TM, false><<<grid, 256, 0, s>>>(d, idx); }
+}
+
+template <typename T, typename TM, int R>
+cudaError_t launch_search_group_r(const MaskArgs* d, const int32_t* idx, int count, int max_w, int max_h, bool key, cudaStream_t s)
+{
+  if(key)
+  {
+    using G = MaskKeyGeo<R>;
+    const cudaError_t e = cudaFuncSetAttribute(k_cps_masked_key_multi<T, TM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::kSmem);
+    if(e != cudaSuccess) { return e; }
+    const dim3 grid((max_w + G::TW - 1) / G::TW, (max_h + G::TH - 1) / G::TH, count);
+    k_cps_masked_key_multi<T, TM, R><<<grid, 512, G::kSmem, s>>>(d, idx);
+  }
+  else
+  {
+    const dim3 grid((max_w + 31) / 32, (max_h + 7) / 8, 2 * count);
+    k_cps_masked_multi<T, TM, R><<<grid, 256, 0, s>>>(d, idx);
+  }
+  return cudaSuccess;
+}
+
+template <typename T, typename TM>
+cudaError_t launch_search_group(const MaskArgs* d, const int32_t* idx, int count, int max_w, int max_h, int R, bool key, cudaStream_t s)
+{
+  switch(R)
+  {
+  case 1: return launch_search_group_r<T, TM, 1>(d, idx, count, max_w, max_h, key, s);
+  case 2: return launch_search_group_r<T, TM, 2>(d, idx, count, max_w, max_h, key, s);
+  case 3: return launch_search_group_r<T, TM, 3>(d, idx, count, max_w, max_h, key, s);
+  case 4: return launch_search_group_r<T, TM, 4>(d, idx, count, max_w, max_h, key, s);
+  case 5: return launch_search_group_r<T, TM, 5>(d, idx, count, max_w, max_h, key, s);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+struct GroupInfo
+{
+  std::vector<int32_t> pairs;
+  int max_w = 0, max_h = 0;
+};
+
+}  // namespace
+
+MaskedBatch::~MaskedBatch()
+{
+  if(h_) { cudaFreeHost(h_); }
+}
+
+// One call: plans every pair (as the one-pair call does), lays out one device arena (results, row
+// sums, ERP weights, host-frame and host-mask staging, the argument table and the groups' pair
+// indices), copies the tables with one H2D, launches prepass / reduce / search / finalize each once per
+// group, and reads every pair's result block back with one D2H.
+qmiv_status MaskedBatch::run(qmiv_ctx_s* ctx, const qmiv_params& prm0, cudaStream_t s, const qmiv_pair_desc* pairs,
+                             const qmiv_frame* masks, const int32_t* mask_bitdepths, int32_t n, qmiv_result* out,
+                             int32_t* num_non_masked)
+{
+  std::vector<MaskPlan> P(n);
+  size_t off_out = 0, off_rows = malign(sizeof(MaskOut) * n), cur = 0;
+  std::vector<size_t> o_rows(n), o_ws(n), o_stage(n), o_mstage(n);
+  cur = off_rows;
+  for(int i = 0; i < n; i++)
+  {
+    const qmiv_pair_desc& d = pairs[i];
+    if((d.metric_mask & ~(uint32_t)(QMIV_PSNR | QMIV_WSPSNR | QMIV_IVPSNR)) != 0 || d.metric_mask == 0)
+    {
+      return fail(QMIV_ERR_UNSUPPORTED, "mask mode computes PSNR, WS-PSNR and IV-PSNR only (as the reference)");
+    }
+    Shape S;
+    QMIV_TRY(S.init(d.width, d.height, d.bitdepth, d.chroma_format));
+    qmiv_params prm = prm0;
+    prm.search_range = d.search_range;
+    QMIV_TRY(validate_params(prm));
+    QMIV_TRY(plan_masked(S, prm, &masks[i], mask_bitdepths[i], P[i]));
+    o_rows[i] = cur; cur += malign(sizeof(uint64_t) * 9 * S.H);
+    o_ws[i] = cur; cur += prm.erp ? malign(sizeof(double) * S.H) : 0;
+    const bool host = d.in0.mem == QMIV_MEM_HOST || d.in1.mem == QMIV_MEM_HOST;
+    o_stage[i] = cur; cur += host ? malign(2 * S.staged_frame_bytes()) : 0;
+    o_mstage[i] = cur; cur += masks[i].mem == QMIV_MEM_HOST ? malign((size_t)S.W * P[i].mesz * S.H) : 0;
+  }
+  // groups: prepass by (sample sizes, vector loads), search by (sample sizes, R, search form)
+  std::map<std::tuple<int, int, int>, GroupInfo> pre;
+  std::map<std::tuple<int, int, int, int>, GroupInfo> srch;
+  const size_t off_args = cur;
+  cur += malign(sizeof(MaskArgs) * n);
+  const size_t off_idx = cur;
+  cur += malign(sizeof(int32_t) * 2 * n);
+  const size_t total = cur;
+  QMIV_TRY(arena_.ensure(ctx, total));
+  const size_t hbytes = (total - off_args) + sizeof(MaskOut) * n;
+  if(h_bytes_ < hbytes)
+  {
+    if(h_) { cudaFreeHost(h_); h_ = nullptr; h_bytes_ = 0; }
+    QMIV_CUDA(cudaMallocHost(&h_, hbytes));
+    h_bytes_ = hbytes;
+  }
+  char* dbase = arena_.as<char>();
+  MaskArgs* hargs = reinterpret_cast<MaskArgs*>(static_cast<char*>(h_));
+  int32_t* hidx = reinterpret_cast<int32_t*>(static_cast<char*>(h_) + (off_idx - off_args));
+  MaskOut* hout = reinterpret_cast<MaskOut*>(static_cast<char*>(h_) + (total - off_args));
+  QMIV_CUDA(cudaMemsetAsync(dbase, 0, off_args, s));      // results and row sums start at zero
+  for(int i = 0; i < n; i++)
+  {
+    const MaskPlan& p = P[i];
+    const Shape& S = p.S;
+    char* stage = dbase + o_stage[i];
+    Img a0{}, a1{};
+    QMIV_TRY(resolve_frame(S, &pairs[i].in0, stage, a0, s));
+    QMIV_TRY(resolve_frame(S, &pairs[i].in1, stage + S.staged_frame_bytes(), a1, s));
+    MaskArgs& a = hargs[i];
+    a = MaskArgs{};
+    QMIV_TRY(resolve_mask(p, &masks[i], dbase + o_mstage[i], a, s));
+    double* ws = reinterpret_cast<double*>(dbase + o_ws[i]);
+    if(p.prm.erp) { QMIV_CUDA(cudaMemcpyAsync(ws, p.ws.data(), sizeof(double) * S.H, cudaMemcpyHostToDevice, s)); }
+    fill_mask_args(p, a0, a1, reinterpret_cast<uint64_t*>(dbase + o_rows[i]), ws,
+                   reinterpret_cast<MaskOut*>(dbase + off_out) + i, a);
+    const int t = (int)S.esz, tm = (int)p.mesz;
+    GroupInfo& gp = pre[std::make_tuple(t, tm, (int)mask_prepass_vec_ok(a, S.esz, p.mesz))];
+    gp.pairs.push_back(i); gp.max_h = std::max(gp.max_h, S.H); gp.max_w = std::max(gp.max_w, S.W);
+    GroupInfo& gs = srch[std::make_tuple(t, tm, p.prm.search_range, (int)p.key)];
+    gs.pairs.push_back(i); gs.max_h = std::max(gs.max_h, S.H); gs.max_w = std::max(gs.max_w, S.W);
+  }
+  int k = 0;
+  std::vector<int> pre_first, srch_first;
+  for(auto& g : pre) { pre_first.push_back(k); for(int32_t i : g.second.pairs) { hidx[k++] = i; } }
+  for(auto& g : srch) { srch_first.push_back(k); for(int32_t i : g.second.pairs) { hidx[k++] = i; } }
+  QMIV_CUDA(cudaMemcpyAsync(dbase + off_args, h_, total - off_args, cudaMemcpyHostToDevice, s));
+  const MaskArgs* dargs = reinterpret_cast<const MaskArgs*>(dbase + off_args);
+  const int32_t* didx = reinterpret_cast<const int32_t*>(dbase + off_idx);
+  int gi = 0;
+  for(auto& g : pre)
+  {
+    const int t = std::get<0>(g.first), tm = std::get<1>(g.first);
+    const bool vec = std::get<2>(g.first) != 0;
+    const int32_t* ix = didx + pre_first[gi++];
+    const int cnt = (int)g.second.pairs.size(), mh = g.second.max_h;
+    if(t == 1) { if(tm == 1) { launch_prepass_group<uint8_t, uint8_t>(dargs, ix, cnt, mh, vec, s); } else { launch_prepass_group<uint8_t, uint16_t>(dargs, ix, cnt, mh, vec, s); } }
+    else { if(tm == 1) { launch_prepass_group<uint16_t, uint8_t>(dargs, ix, cnt, mh, vec, s); } else { launch_prepass_group<uint16_t, uint16_t>(dargs, ix, cnt, mh, vec, s); } }
+  }
+  k_mask_reduce_multi<<<n, 32, 0, s>>>(dargs);
+  gi = 0;
+  for(auto& g : srch)
+  {
+    const int t = std::get<0>(g.first), tm = std::get<1>(g.first), R = std::get<2>(g.first);
+    const bool key = std::get<3>(g.first) != 0;
+    const int32_t* ix = didx + srch_first[gi++];
+    const int cnt = (int)g.second.pairs.size(), mw = g.second.max_w, mh = g.second.max_h;
+    cudaError_t e;
+    if(t == 1) { e = tm == 1 ? launch_search_group<uint8_t, uint8_t>(dargs, ix, cnt, mw, mh, R, key, s) : launch_search_group<uint8_t, uint16_t>(dargs, ix, cnt, mw, mh, R, key, s); }
+    else { e = tm == 1 ? launch_search_group<uint16_t, uint8_t>(dargs, ix, cnt, mw, mh, R, key, s) : launch_search_group<uint16_t, uint16_t>(dargs, ix, cnt, mw, mh, R, key, s); }
+    if(e != cudaSuccess) { return cuda_fail(e, "masked search launch"); }
+  }
+  k_mask_finalize_multi<<<9 * n, 256, 0, s>>>(dargs);
+  QMIV_CUDA(cudaGetLastError());
+  QMIV_CUDA(cudaMemcpyAsync(hout, dbase + off_out, sizeof(MaskOut) * n, cudaMemcpyDeviceToHost, s));
+  QMIV_CUDA(cudaStreamSynchronize(s));
+  qmiv_status first = QMIV_OK;
+  for(int i = 0; i < n; i++)
+  {
+    const qmiv_status st = masked_status(hout[i], P[i]);
+    if(st != QMIV_OK && first == QMIV_OK) { first = st; }
+    if(num_non_masked) { num_non_masked[i] = hout[i].nnm; }
+    if(out) { finish_masked(hout[i], P[i], pairs[i].metric_mask, &out[i]); }
+  }
+  return first;
 }
 
 }  // namespace qmiv

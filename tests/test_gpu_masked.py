@@ -158,3 +158,38 @@ def test_masked_out_of_range_samples_skip(qctx, oracle_lib):
         assert list(got[k][:3]) == list(exp[k][:3]), k
     for k in ["psnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"]:
         assert got[k] == exp[k], k
+
+
+@pytest.mark.parametrize("erp", [False, True])
+def test_masked_batched_equals_one_pair_calls(erp, golden_masked, qctx):
+    """The batched mask mode (qmiv_batch_compute_masked) on an uneven set: every golden case (8/10/12-bit
+    pictures, 8-14-bit masks, R 1-5, 4:2:0/4:2:2/4:4:4 as the fixtures have them) plus seeded
+    1920x1080 and 4096x2048 pairs, host and device frames mixed, in one call. Each pair's result
+    equals the one-pair call's; the golden cases also equal the compiled reference's fixtures."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    cases = [c for c in golden_masked if bool(c["erp"]) == erp]
+    items = []
+    for k, c in enumerate(cases):
+        f0, f1, m = masked_case_inputs(c)
+        if k % 2:
+            f0, f1, m = tuple(_dev(p) for p in f0), tuple(_dev(p) for p in f1), _dev(m)
+        items.append((c["width"], c["height"], c["bitdepth"], c["chroma_format"], c["search_range"], f0, f1, m,
+                      c["mask_bitdepth"], c))
+    for W, H, bd, R, mbd in [(1920, 1080, 8, 2, 8), (4096, 2048, 10, 2, 10)]:
+        f0, f1 = synth.make_pair(W, H, bd, seed=W + bd)
+        m = det_mask(W, H, mbd, W + H, "weights")
+        items.append((W, H, bd, 420, R, tuple(_dev(p) for p in f0), tuple(_dev(p) for p in f1), _dev(m), mbd, None))
+    mask = qmiv_b200.PSNR | qmiv_b200.WSPSNR | qmiv_b200.IVPSNR
+    pairs = [dict(frame0=f0, frame1=f1, width=W, height=H, bitdepth=bd, chroma_format=cf, search_range=R, metrics=mask)
+             for W, H, bd, cf, R, f0, f1, m, mbd, c in items]
+    with qmiv_b200.Batch(qctx, len(pairs), sum(p["width"] * p["height"] for p in pairs), erp=erp) as batch:
+        for _ in range(2):   # the second call reuses the batch's arena
+            got, nnm = batch.compute_masked(pairs, [it[7] for it in items], [it[8] for it in items])
+            for i, (W, H, bd, cf, R, f0, f1, m, mbd, c) in enumerate(items):
+                with qmiv_b200.Calc(qctx, W, H, bd, cf, search_range=R, erp=erp) as calc:
+                    one, one_nnm = calc.compute_masked(f0, f1, m, mbd)
+                assert got[i] == one and nnm[i] == one_nnm, (i, W, H, bd, R)
+                if c is not None:
+                    assert compare_masked(got[i], nnm[i], c["expected"]) == []
