@@ -14,6 +14,7 @@ from its sources into oracle/_ref by oracle/Makefile) on the same workload, on r
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import re
@@ -415,15 +416,20 @@ def run_qmiv(args, world, rank, local):
 
     solo = world == 1
     side = max(3, args.steps // 4)
-    mixed = run_mixed(ctx, side, int_peak.value) if (solo and not args.no_mixed) else None
-    serve = None
-    if solo and args.serve_seconds > 0:
-        serve = {"host": run_serve(ctx, args.serve_seconds, host=True),
-                 "device": run_serve(ctx, args.serve_seconds, host=False)}
-    masked = run_masked(ctx, side) if (solo and not args.no_masked) else None
-    ssim_modes = run_ssim_modes(ctx, side) if (solo and not args.no_ssim_modes) else None
-    c0 = run_config0(ctx, side) if (solo and not args.no_configs) else None
-    c2 = run_config2(ctx, side, hbm_peak()) if (solo and not args.no_configs) else None
+
+    def leg(name, fn, on):
+        if not (solo and on):
+            return None
+        log(f"[bench] {name}")
+        return fn()
+
+    mixed = leg("mixed set", lambda: run_mixed(ctx, side, int_peak.value), not args.no_mixed)
+    serve = leg("serving", lambda: {"host": run_serve(ctx, args.serve_seconds, host=True),
+                                    "device": run_serve(ctx, args.serve_seconds, host=False)}, args.serve_seconds > 0)
+    masked = leg("mask mode", lambda: run_masked(ctx, side), not args.no_masked)
+    ssim_modes = leg("ssim options", lambda: run_ssim_modes(ctx, side), not args.no_ssim_modes)
+    c0 = leg("1080p 8-bit", lambda: run_config0(ctx, side), not args.no_configs)
+    c2 = leg("MS-SSIM workload", lambda: run_config2(ctx, side, hbm_peak()), not args.no_configs)
 
     batch.close()
     ctx.close()
@@ -489,6 +495,19 @@ def run_reference_app(n_frames, threads, seed=0, shape=None, metrics=METRICS, er
     ivpsnr = re.search(r"Average\s+IVPSNR\s+([0-9.]+)", out)
     return dict(value=n_frames / secs, secs=secs, frames=n_frames, threads=threads,
                 ivpsnr=float(ivpsnr.group(1)) if ivpsnr else None)
+
+
+def in_child(fn, *args, timeout=600):
+    """fn(*args) in a spawned child process: the reference library runs its own thread pool in native
+    code, and a crash there ends only the child (the value is then None and the reason is logged)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        try:
+            return pool.apply_async(fn, args).get(timeout)
+        except Exception as e:  # the child died or timed out: this field stays empty
+            log(f"{fn.__name__} failed in its child process: {e!r}")
+            return None
 
 
 def reference_parity(frame0, frame1, shape, search_range, erp, mask, gpu, keys, threads):
@@ -739,6 +758,7 @@ def host_threads():
 
 
 def main():
+    faulthandler.enable()   # a crash in native code prints the Python stack of every thread to stderr
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -817,36 +837,36 @@ def main():
             if c:
                 cpu = {"value": c["value"], "unit": "frame-pairs/s", "cores": c["threads"], "kind": "reference",
                        "sample": f"{c['frames']} pairs of the workload, QMIV app -nth {c['threads']}, {c['secs']:.2f} s"}
-            parity["headline"] = reference_parity(*synth.make_pair(W, H, BD, seed=0), (W, H, BD), 2, True, 7 | 32,
-                                                  r["sample"], PARITY_KEYS, threads)
+            parity["headline"] = in_child(reference_parity, *synth.make_pair(W, H, BD, seed=0), (W, H, BD), 2, True,
+                                          7 | 32, r["sample"], PARITY_KEYS, threads)
         except Exception as e:  # the GPU number stands without the CPU baseline
             log("cpu baseline failed:", e)
         if c0 is not None:
             try:
                 cr = run_reference_app(8, threads, seed=500, shape=C0, metrics=("IVPSNR",), erp=False)
                 c0["cpu_reference"] = {"value": cr["value"], "cores": threads, "ivpsnr_avg": cr["ivpsnr"]} if cr else None
-                parity["config0"] = reference_parity(*c0["pair0"], C0, 2, False, 4, c0["result0"],
-                                                     ("gcd_r2t", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"), threads)
+                parity["config0"] = in_child(reference_parity, *c0["pair0"], C0, 2, False, 4, c0["result0"],
+                                             ("gcd_r2t", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"), threads)
             except Exception as e:
                 log("config0 cpu baseline failed:", e)
         if c2 is not None:
             try:
                 cr = run_reference_app(2, threads, shape=C2, metrics=("MSSSIM", "IVMSSSIM"), erp=False, gen=c2["gen"])
                 c2["cpu_reference"] = {"value": cr["value"], "cores": threads, "sample": "2 pairs"} if cr else None
-                parity["config2"] = reference_parity(*c2["pair0"], C2, 2, False, 16 | 64, c2["result0"],
-                                                     ("msssim", "msssim_pic", "ivmsssim"), threads)
+                parity["config2"] = in_child(reference_parity, *c2["pair0"], C2, 2, False, 16 | 64, c2["result0"],
+                                             ("msssim", "msssim_pic", "ivmsssim"), threads)
             except Exception as e:
                 log("config2 cpu baseline failed:", e)
         if r["masked"] is not None:
             try:
-                cm = run_reference_masked(threads)
+                cm = in_child(run_reference_masked, threads)
                 if cm:
                     r["masked"]["cpu_reference"] = {"value": cm["value"], "cores": cm["threads"], "ivpsnr": cm["ivpsnr"]}
             except Exception as e:
                 log("masked cpu baseline failed:", e)
         if r["ssim_modes"] is not None:
             try:
-                cs = run_reference_ssim_option(threads, SSIM_OPTIONS[0])
+                cs = in_child(run_reference_ssim_option, threads, SSIM_OPTIONS[0])
                 if cs:
                     r["ssim_modes"]["options"][0]["cpu_reference"] = {"value": cs["value"], "cores": cs["threads"],
                                                                       "ivssim": cs["ivssim"]}
