@@ -17,6 +17,10 @@
 /* ----------------------------------------------------------------------------------------------- */
 
 static inline int32_t qo_clampi(int32_t v, int32_t lo, int32_t hi) { return v < lo ? lo : (v > hi ? hi : v); }
+/* The reference's int32 products and sums where they may wrap (two's complement), formed in unsigned
+   arithmetic: a signed overflow is undefined in C and lets the compiler widen the result. */
+static inline int32_t qo_mul_wrap(int32_t a, int32_t b) { return (int32_t)((uint32_t)a * (uint32_t)b); }
+static inline int32_t qo_add_wrap(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
 static inline int32_t qo_max_value(int32_t bitdepth) { return (1 << bitdepth) - 1; } /* xCommonDefCORE.h:156 */
 
 /* Round half away from zero by adding +-0.5 and truncating, as xRoundF32ToI32 / xRoundF64ToI32
@@ -176,12 +180,12 @@ void qo_cps_rows_std(const uint16_t* tst, const uint16_t* ref, int32_t W, int32_
           {
             pel[c] = ref[c * pl + (size_t)yy * W + xx];
             const int32_t d = s[c] - pel[c];
-            err += d * d * cws[c];
+            err = qo_add_wrap(err, qo_mul_wrap(qo_mul_wrap(d, d), cws[c]));
           }
           if(err < best_err) { best_err = err; for(int32_t c = 0; c < 3; c++) { best_pel[c] = pel[c]; } }
         }
       }
-      for(int32_t c = 0; c < 3; c++) { const int32_t d = s[c] - best_pel[c]; rowsum[c] += (uint64_t)(int64_t)(d * d); }
+      for(int32_t c = 0; c < 3; c++) { const int32_t d = s[c] - best_pel[c]; rowsum[c] += (uint64_t)(int64_t)qo_mul_wrap(d, d); }
     }
     for(int32_t c = 0; c < 3; c++) { row_sse[(size_t)y * 3 + c] = rowsum[c]; }
   }
@@ -661,7 +665,7 @@ void qo_gcd_masked(const uint16_t* tst, const uint16_t* ref, const uint16_t* msk
   {
     const uint16_t* t = tst + (size_t)c * W * H;
     const uint16_t* r = ref + (size_t)c * W * H;
-    for(size_t i = 0; i < (size_t)W * H; i++) { sd[c] += ((int32_t)t[i] - (int32_t)r[i]) * (int32_t)msk[i]; }
+    for(size_t i = 0; i < (size_t)W * H; i++) { sd[c] += qo_mul_wrap((int32_t)t[i] - (int32_t)r[i], (int32_t)msk[i]); }
   }
   const double den = (double)((int64_t)nnm * (int64_t)qo_max_value(mask_bitdepth));
   for(int32_t c = 0; c < 4; c++)
@@ -701,7 +705,7 @@ void qo_cps_masked(const uint16_t* tst, const uint16_t* ref, const uint16_t* msk
           {
             pel[c] = ref[c * pl + (size_t)yy * W + xx];
             const int32_t d = s[c] - pel[c];
-            err += (uint32_t)(d * d) * (uint32_t)cws[c];
+            err += (uint32_t)qo_mul_wrap(d, d) * (uint32_t)cws[c];
           }
           if((int32_t)err < best_err) { best_err = (int32_t)err; for(int32_t c = 0; c < 3; c++) { best_pel[c] = pel[c]; } }
         }
@@ -709,7 +713,7 @@ void qo_cps_masked(const uint16_t* tst, const uint16_t* ref, const uint16_t* msk
       for(int32_t c = 0; c < 3; c++)
       {
         const int32_t d = s[c] - best_pel[c];
-        rowsum[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)m;
+        rowsum[c] += (uint64_t)(int64_t)qo_mul_wrap(d, d) * (uint64_t)m;
       }
     }
     for(int32_t c = 0; c < 3; c++) { row_sse[(size_t)y * 3 + c] = rowsum[c]; }
@@ -795,7 +799,7 @@ int qo_compute_pair_masked(const qo_params* p, const void* const planes0[3], con
     for(int32_t c = 0; c < 3; c++)
     {
       const uint16_t* a = P0 + (size_t)c * pl; const uint16_t* b = P1 + (size_t)c * pl;
-      for(size_t i = 0; i < pl; i++) { const int32_t d = (int32_t)a[i] - (int32_t)b[i]; ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)M[i]; }
+      for(size_t i = 0; i < pl; i++) { const int32_t d = (int32_t)a[i] - (int32_t)b[i]; ssd[c] += (uint64_t)(int64_t)qo_mul_wrap(d, d) * (uint64_t)M[i]; }
     }
     /* xPSNR::calcPicPSNRM, libs/pmbb-ivqm/src/xPSNR.cpp:54-66: the mask's bit depth stands for both
        the picture's and the mask's (CalcPSNRsFromMaskedSSDs(.., Msk->getBitDepth(), Msk->getBitDepth())) */
@@ -822,7 +826,7 @@ int qo_compute_pair_masked(const qo_params* p, const void* const planes0[3], con
             {
               const size_t i = (size_t)y * W + x;
               const int32_t d = (int32_t)b[i] - (int32_t)a[i];
-              rs += (uint64_t)(int64_t)(d * d) * (uint64_t)M[i];
+              rs += (uint64_t)(int64_t)qo_mul_wrap(d, d) * (uint64_t)M[i];
             }
             qo_kbns_add(&k, (double)rs * ws[y]);
           }

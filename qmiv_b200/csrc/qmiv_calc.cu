@@ -99,41 +99,49 @@ void ssim_line(const qmiv_params& p, int32_t len, int32_t& first_sample, int32_t
 PairPipeline::~PairPipeline()
 {
   if(h_out) { cudaFreeHost(h_out); h_out = nullptr; }
-  for(cudaEvent_t e : ev_pool_) { cudaEventDestroy(e); }
 }
 
-int PairPipeline::prof_begin(cudaStream_t s)
+int StageClock::begin(qmiv_ctx_s* ctx, cudaStream_t s)
 {
-  if(!ctx_ || !ctx_->profiling) { return -1; }
-  while(ev_pool_.size() < ev_used_ + 2)
+  if(!ctx || !ctx->profiling) { return -1; }
+  while(pool_.size() < used_ + 2)
   {
     cudaEvent_t e;
     if(cudaEventCreate(&e) != cudaSuccess) { return -1; }
-    ev_pool_.push_back(e);
+    pool_.push_back(e);
   }
-  const int tok = (int)ev_used_;
-  ev_used_ += 2;
-  cudaEventRecord(ev_pool_[tok], s);
+  const int tok = (int)used_;
+  used_ += 2;
+  cudaEventRecord(pool_[tok], s);
   return tok;
 }
 
-void PairPipeline::prof_end(cudaStream_t s, int stage, int tok)
+void StageClock::end(cudaStream_t s, int stage, int tok)
 {
   if(tok < 0) { return; }
-  cudaEventRecord(ev_pool_[tok + 1], s);
-  ev_pending_.emplace_back(stage, tok);
+  cudaEventRecord(pool_[tok + 1], s);
+  pending_.emplace_back(stage, tok);
 }
 
-void PairPipeline::harvest_profile()
+void StageClock::harvest(qmiv_ctx_s* ctx)
 {
-  for(const auto& p : ev_pending_)
+  for(const auto& p : pending_)
   {
     float ms = 0.f;
-    if(cudaEventElapsedTime(&ms, ev_pool_[p.second], ev_pool_[p.second + 1]) == cudaSuccess) { ctx_->add_stage(p.first, ms); }
+    if(ctx && cudaEventElapsedTime(&ms, pool_[p.second], pool_[p.second + 1]) == cudaSuccess) { ctx->add_stage(p.first, ms); }
   }
-  ev_pending_.clear();
-  ev_used_ = 0;
+  pending_.clear();
+  used_ = 0;
 }
+
+StageClock::~StageClock()
+{
+  for(cudaEvent_t e : pool_) { cudaEventDestroy(e); }
+}
+
+int PairPipeline::prof_begin(cudaStream_t s) { return clock_.begin(ctx_, s); }
+void PairPipeline::prof_end(cudaStream_t s, int stage, int tok) { clock_.end(s, stage, tok); }
+void PairPipeline::harvest_profile() { clock_.harvest(ctx_); }
 
 qmiv_status PairPipeline::configure(qmiv_ctx_s* ctx, const Shape& shape, const qmiv_params& prm, int32_t search_range)
 {

@@ -92,39 +92,6 @@ struct alignas(64) CpsKernelArgs
 };
 
 // ---- TMA / mbarrier ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-  uint32_t ok;
-  asm volatile(
-    "{\n\t.reg .pred p;\n\t"
-    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-    "selp.u32 %0, 1, 0, p;\n\t}"
-    : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
-  return ok != 0;
-}
-// Waits for the phase with the given parity; gives up (false) after about `limit` cycles.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit)
-{
-  if(mbar_try_wait(bar, parity)) { return true; }
-  const long long t0 = clock64();
-  do
-  {
-    if(mbar_try_wait(bar, parity)) { return true; }
-  } while(clock64() - t0 <= limit);
-  return false;
-}
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
 {
   asm volatile(

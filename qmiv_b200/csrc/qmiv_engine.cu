@@ -195,7 +195,6 @@ Engine::~Engine()
     if(cs) { cudaStreamSynchronize(cs); cudaStreamDestroy(cs); }
   }
   for(cudaEvent_t e : chunk_ready_) { cudaEventDestroy(e); }
-  for(cudaEvent_t e : ev_pool_) { cudaEventDestroy(e); }
   clear_graphs();
   if(host_mirror_) { cudaFreeHost(host_mirror_); }
   if(host_out_) { cudaFreeHost(host_out_); }
@@ -919,38 +918,9 @@ qmiv_status Engine::launch_all(const Tables& T, cudaStream_t s)
 }
 
 // ---- stage timing (not while a graph is replayed) -------------------------------------------------
-int Engine::prof_begin(cudaStream_t s)
-{
-  if(!ctx_->profiling) { return -1; }
-  while(ev_pool_.size() < ev_used_ + 2)
-  {
-    cudaEvent_t e;
-    if(cudaEventCreate(&e) != cudaSuccess) { return -1; }
-    ev_pool_.push_back(e);
-  }
-  const int tok = (int)ev_used_;
-  ev_used_ += 2;
-  cudaEventRecord(ev_pool_[tok], s);
-  return tok;
-}
-
-void Engine::prof_end(cudaStream_t s, int stage, int tok)
-{
-  if(tok < 0) { return; }
-  cudaEventRecord(ev_pool_[tok + 1], s);
-  ev_pending_.emplace_back(stage, tok);
-}
-
-void Engine::harvest_profile()
-{
-  for(const auto& p : ev_pending_)
-  {
-    float ms = 0.f;
-    if(cudaEventElapsedTime(&ms, ev_pool_[p.second], ev_pool_[p.second + 1]) == cudaSuccess) { ctx_->add_stage(p.first, ms); }
-  }
-  ev_pending_.clear();
-  ev_used_ = 0;
-}
+int Engine::prof_begin(cudaStream_t s) { return clock_.begin(ctx_, s); }
+void Engine::prof_end(cudaStream_t s, int stage, int tok) { clock_.end(s, stage, tok); }
+void Engine::harvest_profile() { clock_.harvest(ctx_); }
 
 bool Engine::tuning(int32_t W, int32_t H, int32_t bd, int32_t R, int32_t* tile_w, int32_t* tile_h, int32_t* rows) const
 {

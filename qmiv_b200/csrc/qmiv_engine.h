@@ -146,9 +146,7 @@ private:
   int          host_out_n_ = 0;
   std::map<std::string, cudaGraphExec_t> graphs_;
   std::map<std::string, int> seen_;
-  std::vector<cudaEvent_t> ev_pool_;
-  size_t ev_used_ = 0;
-  std::vector<std::pair<int, int>> ev_pending_;
+  StageClock   clock_;
   int          pend_n_ = -1;                   // pairs of the call in flight, -1 = none
   std::vector<PairKind*> pend_kind_;
   std::vector<uint32_t>  pend_mask_;

@@ -129,6 +129,23 @@ void ssim_line(const qmiv_params& p, int32_t len, int32_t& first_sample, int32_t
 qmiv_status check_metrics(const Shape& S, uint32_t mask, const qmiv_params& p);
 
 // The device pipeline of one frame pair of a fixed shape, with its scratch buffers.
+// Per-stage device timing: begin and end events on the launching stream, read once the stream has
+// synchronised and added to the context's totals (qmiv_ctx_stage_times). begin returns -1 (and end then
+// does nothing) while the context does not profile.
+class StageClock
+{
+public:
+  int  begin(qmiv_ctx_s* ctx, cudaStream_t s);
+  void end(cudaStream_t s, int stage, int tok);
+  void harvest(qmiv_ctx_s* ctx);
+  ~StageClock();
+
+private:
+  std::vector<cudaEvent_t> pool_;
+  size_t used_ = 0;
+  std::vector<std::pair<int, int>> pending_;     // (stage, index of the begin event)
+};
+
 class PairPipeline
 {
 public:
@@ -213,9 +230,7 @@ private:
   bool ws_uploaded_ = false;
   bool gcd_override_on_ = false;
   int32_t gcd_override_[4] = { 0, 0, 0, 0 };
-  std::vector<cudaEvent_t> ev_pool_;
-  size_t ev_used_ = 0;
-  std::vector<std::pair<int, int>> ev_pending_;  // (stage, index of the begin event)
+  StageClock clock_;
 };
 
 // Colour-space conversion of one calc (qmiv_colour.cu): the converted 4:4:4 planes of the current pair
@@ -257,6 +272,7 @@ private:
   DevMem arena_;
   void*  h_ = nullptr;        // pinned mirror of the argument tables and the results
   size_t h_bytes_ = 0;
+  StageClock clock_;
 };
 
 class MaskedPipeline

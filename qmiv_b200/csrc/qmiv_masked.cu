@@ -3,7 +3,8 @@
 // calls; the app refuses the SSIM family with a mask, :360-365).
 //
 //   k_mask_prepass   one CTA per 4:4:4 row: sum of (In1 - In0) * M (GCD-M), sum of (In1 - In0)^2 * M
-//                    per row (PSNR-M, WS-PSNR-M), non-zero mask samples, exactness, largest samples;
+//                    per row (PSNR-M, WS-PSNR-M), non-zero mask samples, exactness, samples above the
+//                    maximum (the OR of all samples exceeds 2^bd - 1 exactly when one sample does);
 //                    k_mask_prepass420v the same for aligned 4:2:0 frames with vector loads
 //   k_mask_reduce    GCD-M (xGlobClrDiff.cpp:60-91): IEEE divide by NumNonMasked * MaskMax,
 //                    round half away, clip
@@ -38,7 +39,7 @@ struct MaskOut
   int32_t  gcd[4];
   int32_t  flags;              // bit0 / bit1: frame 0 / 1 held samples above the maximum
   int32_t  nnm;                // non-zero mask samples (xPixelOpsSTD.cpp:273-284)
-  uint32_t max_sample[2];
+  uint32_t or_sample[2];       // OR of every sample per frame: above maxv (2^bd - 1) iff some sample is
   int64_t  sd[3];              // sum over 4:4:4 positions of (In1 - In0) * M
   uint64_t ssd[3];             // sum of (In1 - In0)^2 * M
   uint32_t differs[3];         // the component differs somewhere (whole-picture exactness)
@@ -116,8 +117,8 @@ __device__ __forceinline__ void mask_prepass_row_tail(const MaskArgs& a, int y, 
   }
   nnm = __reduce_add_sync(0xffffffffu, nnm);
   dif = __reduce_or_sync(0xffffffffu, dif);
-  mx0 = __reduce_max_sync(0xffffffffu, mx0);
-  mx1 = __reduce_max_sync(0xffffffffu, mx1);
+  mx0 = __reduce_or_sync(0xffffffffu, mx0);
+  mx1 = __reduce_or_sync(0xffffffffu, mx1);
   if(lane == 0)
   {
     #pragma unroll
@@ -133,7 +134,7 @@ __device__ __forceinline__ void mask_prepass_row_tail(const MaskArgs& a, int y, 
   {
     #pragma unroll
     for(int k = 0; k < 6; k++) { t[k] += red[w][k]; }
-    nnm += redu[w][0]; dif |= redu[w][1]; mx0 = max(mx0, redu[w][2]); mx1 = max(mx1, redu[w][3]);
+    nnm += redu[w][0]; dif |= redu[w][1]; mx0 |= redu[w][2]; mx1 |= redu[w][3];
   }
   MaskOut* o = a.out;
   #pragma unroll
@@ -145,8 +146,8 @@ __device__ __forceinline__ void mask_prepass_row_tail(const MaskArgs& a, int y, 
     if(dif & (1u << c)) { atomicOr(&o->differs[c], 1u); }
   }
   atomicAdd(&o->nnm, (int32_t)nnm);
-  atomicMax(&o->max_sample[0], mx0);
-  atomicMax(&o->max_sample[1], mx1);
+  atomicOr(&o->or_sample[0], mx0);
+  atomicOr(&o->or_sample[1], mx1);
 }
 
 
@@ -181,11 +182,11 @@ __device__ __forceinline__ void mask_prepass_body(const MaskArgs& a, int row)
       #pragma unroll
       for(int c = 0; c < 3; c++)
       {
-        mx0 = max(mx0, va[u][c]); mx1 = max(mx1, vb[u][c]);
+        mx0 |= va[u][c]; mx1 |= vb[u][c];
         const uint32_t p0 = min(va[u][c], a.clip), p1 = min(vb[u][c], a.clip);
         const int32_t d = (int32_t)p1 - (int32_t)p0;
-        sd[c] += (int64_t)(d * m[u]);                          // int32 product, xDistortionSTD.cpp:50
-        ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)(uint32_t)m[u];    // xDistortionSTD.cpp:62
+        sd[c] += (int64_t)mul_wrap(d, m[u]);                          // int32 product, xDistortionSTD.cpp:50
+        ssd[c] += (uint64_t)(int64_t)mul_wrap(d, d) * (uint64_t)(uint32_t)m[u];    // xDistortionSTD.cpp:62
         dif |= (d != 0 ? 1u : 0u) << c;
       }
     }
@@ -260,17 +261,202 @@ __device__ __forceinline__ void mask_prepass420v_body(const MaskArgs& a, int row
         for(int c = 0; c < 3; c++)
         {
           const uint32_t va = c ? ca[u][c - 1][i >> 1] : ya[u][i], vb = c ? cb[u][c - 1][i >> 1] : yb[u][i];
-          mx0 = max(mx0, va); mx1 = max(mx1, vb);
+          mx0 |= va; mx1 |= vb;
           const uint32_t p0 = min(va, a.clip), p1 = min(vb, a.clip);
           const int32_t d = (int32_t)p1 - (int32_t)p0;
-          sd[c] += (int64_t)(d * mi);                          // int32 product, xDistortionSTD.cpp:50
-          ssd[c] += (uint64_t)(int64_t)(d * d) * (uint64_t)(uint32_t)mi;    // xDistortionSTD.cpp:62
+          sd[c] += (int64_t)mul_wrap(d, mi);                          // int32 product, xDistortionSTD.cpp:50
+          ssd[c] += (uint64_t)(int64_t)mul_wrap(d, d) * (uint64_t)(uint32_t)mi;    // xDistortionSTD.cpp:62
           dif |= (d != 0 ? 1u : 0u) << c;
         }
       }
     }
   }
   mask_prepass_row_tail(a, y, sd, ssd, nnm, dif, mx0, mx1);
+}
+
+// One group of four 4:2:0 pixels as pairs of 16-bit samples: luma [0] = pixels 0-1 and [1] = pixels 2-3 of
+// each frame, one pair per chroma plane and frame (the two chroma samples under the four pixels) and the
+// four 8-bit mask samples.
+struct Grp16
+{
+  uint32_t l0[2], l1[2];
+  uint32_t c0[2], c1[2];       // [plane - 1]
+  uint32_t m;
+};
+
+__device__ __forceinline__ void ld_grp(const uint16_t* l0, const uint16_t* l1, const uint16_t* const ch0[2],
+                                       const uint16_t* const ch1[2], const uint8_t* mr, int g, Grp16& r)
+{
+  const uint2 a = __ldg(reinterpret_cast<const uint2*>(l0 + 4 * g)), b = __ldg(reinterpret_cast<const uint2*>(l1 + 4 * g));
+  r.l0[0] = a.x; r.l0[1] = a.y; r.l1[0] = b.x; r.l1[1] = b.y;
+  #pragma unroll
+  for(int p = 0; p < 2; p++)
+  {
+    r.c0[p] = __ldg(reinterpret_cast<const uint32_t*>(ch0[p] + 2 * g));
+    r.c1[p] = __ldg(reinterpret_cast<const uint32_t*>(ch1[p] + 2 * g));
+  }
+  r.m = __ldg(reinterpret_cast<const uint32_t*>(mr + 4 * g));
+}
+// 8-bit samples are spread to 16-bit pairs on loading (byte i of the word to half i of the pair)
+__device__ __forceinline__ void ld_grp(const uint8_t* l0, const uint8_t* l1, const uint8_t* const ch0[2],
+                                       const uint8_t* const ch1[2], const uint8_t* mr, int g, Grp16& r)
+{
+  const uint32_t a = __ldg(reinterpret_cast<const uint32_t*>(l0 + 4 * g)), b = __ldg(reinterpret_cast<const uint32_t*>(l1 + 4 * g));
+  r.l0[0] = __byte_perm(a, 0u, 0x4140u); r.l0[1] = __byte_perm(a, 0u, 0x4342u);
+  r.l1[0] = __byte_perm(b, 0u, 0x4140u); r.l1[1] = __byte_perm(b, 0u, 0x4342u);
+  #pragma unroll
+  for(int p = 0; p < 2; p++)
+  {
+    r.c0[p] = __byte_perm((uint32_t)__ldg(reinterpret_cast<const unsigned short*>(ch0[p] + 2 * g)), 0u, 0x4140u);
+    r.c1[p] = __byte_perm((uint32_t)__ldg(reinterpret_cast<const unsigned short*>(ch1[p] + 2 * g)), 0u, 0x4140u);
+  }
+  r.m = __ldg(reinterpret_cast<const uint32_t*>(mr + 4 * g));
+}
+
+// The differences of two clipped 16-bit pairs below 2^15: the 32-bit difference of the words holds the
+// low difference in its low half (two's complement) and the high difference times 2^16 once the low one
+// is taken off.
+template <bool CLIP>
+__device__ __forceinline__ void pair_diff(uint32_t w0, uint32_t w1, uint32_t clip2, uint32_t& dw, int32_t& dlo, int32_t& dhi)
+{
+  if(CLIP) { w0 = __vminu2(w0, clip2); w1 = __vminu2(w1, clip2); }
+  dw = w1 - w0;
+  dlo = (int32_t)(int16_t)(dw & 0xffffu);
+  dhi = (int32_t)(dw - (uint32_t)dlo) >> 16;
+}
+
+// A group's terms when every sample is below 2^15 and the mask below 2^8: the int32 products d * m of the
+// reference never overflow, so a chroma sample under two pixels of the row contributes d * (m0 + m1) and
+// d^2 * (m0 + m1) once (the square term formed as d * (d * m), one wide multiply-add), and the SD terms
+// of a step add up in int32 (below 2^27 for four groups). CLIP: concealment clips the samples first.
+__device__ __forceinline__ void word_terms(int32_t dlo, int32_t dhi, uint32_t m0, uint32_t m1, int32_t& sd, uint64_t& ssd)
+{
+  const int32_t a = dlo * (int32_t)m0, b = dhi * (int32_t)m1;
+  sd += a + b;
+  ssd += (uint64_t)((int64_t)dlo * a) + (uint64_t)((int64_t)dhi * b);
+}
+
+template <bool CLIP>
+__device__ __forceinline__ void grp_narrow(const Grp16& g, uint32_t clip2, int32_t sd[3], uint64_t ssd[3], uint32_t difw[3], uint32_t& nnm)
+{
+  const uint32_t mm[4] = { g.m & 0xffu, (g.m >> 8) & 0xffu, (g.m >> 16) & 0xffu, g.m >> 24 };
+  const uint32_t ms[2] = { mm[0] + mm[1], mm[2] + mm[3] };
+  nnm += __popc((((g.m & 0x7f7f7f7fu) + 0x7f7f7f7fu) | g.m) & 0x80808080u);    // non-zero mask bytes
+  #pragma unroll
+  for(int k = 0; k < 2; k++)
+  {
+    uint32_t dw; int32_t dlo, dhi;
+    pair_diff<CLIP>(g.l0[k], g.l1[k], clip2, dw, dlo, dhi);
+    difw[0] |= dw;
+    word_terms(dlo, dhi, mm[2 * k], mm[2 * k + 1], sd[0], ssd[0]);
+  }
+  #pragma unroll
+  for(int p = 0; p < 2; p++)
+  {
+    uint32_t dw; int32_t dlo, dhi;
+    pair_diff<CLIP>(g.c0[p], g.c1[p], clip2, dw, dlo, dhi);
+    difw[1 + p] |= dw;
+    word_terms(dlo, dhi, ms[0], ms[1], sd[1 + p], ssd[1 + p]);
+  }
+}
+
+// A step's OR of every sample of both frames (the above-maximum flags and the 2^15 test)
+__device__ __forceinline__ void grp_or(const Grp16& g, uint32_t& o0, uint32_t& o1)
+{
+  o0 |= g.l0[0] | g.l0[1]; o0 |= g.c0[0] | g.c0[1];
+  o1 |= g.l1[0] | g.l1[1]; o1 |= g.c1[0] | g.c1[1];
+}
+
+// The same group sample by sample with the reference's int32 products and 64-bit sums (a step that
+// holds a sample of 2^15 or more and is not clipped below it).
+__device__ __forceinline__ void grp_wide(const Grp16& g, uint32_t clip, int64_t sd[3], uint64_t ssd[3], uint32_t difw[3], uint32_t& nnm)
+{
+  #pragma unroll
+  for(int i = 0; i < 4; i++)
+  {
+    const int32_t mi = (int32_t)((g.m >> (8 * i)) & 0xffu);
+    nnm += mi != 0;
+    #pragma unroll
+    for(int c = 0; c < 3; c++)
+    {
+      const uint32_t w0 = c ? g.c0[c - 1] : g.l0[i >> 1], w1 = c ? g.c1[c - 1] : g.l1[i >> 1];
+      const int sh = c ? 16 * (i >> 1) : 16 * (i & 1);
+      const uint32_t p0 = min((w0 >> sh) & 0xffffu, clip), p1 = min((w1 >> sh) & 0xffffu, clip);
+      const int32_t d = (int32_t)p1 - (int32_t)p0;
+      sd[c] += (int64_t)mul_wrap(d, mi);                              // int32 product, xDistortionSTD.cpp:50
+      ssd[c] += (uint64_t)(int64_t)mul_wrap(d, d) * (uint64_t)(uint32_t)mi;      // xDistortionSTD.cpp:62
+      difw[c] |= (uint32_t)d;
+    }
+  }
+}
+
+// 4:2:0 rows as in mask_prepass420v_body with an 8-bit mask: four groups of four pixels per thread and
+// step, all loads issued first, the OR of the samples kept on the pairs, the terms by grp_narrow unless
+// the step holds an unclipped sample of 2^15 or more (then grp_wide). The sums are the same integers.
+template <typename T>
+__device__ __forceinline__ void mask_prepass420n_body(const MaskArgs& a, int row)
+{
+  constexpr int U = 4;
+  const int y = row;
+  const int ng = a.W >> 2;
+  const T* l0 = static_cast<const T*>(a.in0.p[0]) + (size_t)y * a.in0.pitch[0];
+  const T* l1 = static_cast<const T*>(a.in1.p[0]) + (size_t)y * a.in1.pitch[0];
+  const T* const ch0[2] = { static_cast<const T*>(a.in0.p[1]) + (size_t)(y >> 1) * a.in0.pitch[1],
+                            static_cast<const T*>(a.in0.p[2]) + (size_t)(y >> 1) * a.in0.pitch[2] };
+  const T* const ch1[2] = { static_cast<const T*>(a.in1.p[1]) + (size_t)(y >> 1) * a.in1.pitch[1],
+                            static_cast<const T*>(a.in1.p[2]) + (size_t)(y >> 1) * a.in1.pitch[2] };
+  const uint8_t* mr = static_cast<const uint8_t*>(a.mask) + (size_t)y * a.mpitch;
+  const uint32_t clip2 = a.clip | (a.clip << 16);
+  const bool chk = sizeof(T) == 2 && a.clip >= 0x8000u;       // unclipped 16-bit samples may reach 2^15
+  const bool clip_on = a.clip < (sizeof(T) == 1 ? 0xffu : 0xffffu);
+  int64_t  sd[3] = { 0, 0, 0 };
+  uint64_t ssd[3] = { 0, 0, 0 };
+  uint32_t difw[3] = { 0, 0, 0 };
+  uint32_t nnm = 0, mxw0 = 0, mxw1 = 0;
+  for(int gb = threadIdx.x; gb < ng; gb += 256 * U)
+  {
+    Grp16 g[U];
+    #pragma unroll
+    for(int u = 0; u < U; u++) { ld_grp(l0, l1, ch0, ch1, mr, min(gb + u * 256, ng - 1), g[u]); }   // past the row: repeats, skipped below
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      if(gb + u * 256 >= ng) { continue; }
+      grp_or(g[u], mxw0, mxw1);
+    }
+    if(chk && ((mxw0 | mxw1) & 0x80008000u) != 0)
+    {
+      #pragma unroll
+      for(int u = 0; u < U; u++) { if(gb + u * 256 < ng) { grp_wide(g[u], a.clip, sd, ssd, difw, nnm); } }
+      continue;
+    }
+    int32_t s32[3] = { 0, 0, 0 };
+    if(clip_on)
+    {
+      #pragma unroll
+      for(int u = 0; u < U; u++) { if(gb + u * 256 < ng) { grp_narrow<true>(g[u], clip2, s32, ssd, difw, nnm); } }
+    }
+    else
+    {
+      #pragma unroll
+      for(int u = 0; u < U; u++) { if(gb + u * 256 < ng) { grp_narrow<false>(g[u], clip2, s32, ssd, difw, nnm); } }
+    }
+    #pragma unroll
+    for(int c = 0; c < 3; c++) { sd[c] += s32[c]; }
+  }
+  const uint32_t dif = (difw[0] != 0 ? 1u : 0u) | (difw[1] != 0 ? 2u : 0u) | (difw[2] != 0 ? 4u : 0u);
+  const uint32_t mx0 = (mxw0 & 0xffffu) | (mxw0 >> 16), mx1 = (mxw1 & 0xffffu) | (mxw1 >> 16);
+  mask_prepass_row_tail(a, y, sd, ssd, nnm, dif, mx0, mx1);
+}
+
+constexpr int kPackPairs = 32;                                 // frame pairs per batched launch
+
+// The vector-load prepass: the narrow form for 8-bit masks, the sample-by-sample one otherwise.
+template <typename T, typename TM>
+__device__ __forceinline__ void mask_prepass420_body(const MaskArgs& a, int row)
+{
+  if constexpr(sizeof(TM) == 1) { mask_prepass420n_body<T>(a, row); }
+  else { mask_prepass420v_body<T, TM>(a, row); }
 }
 
 // The vector loads of k_mask_prepass420v need 4:2:0, a width divisible by 4, luma rows of both frames
@@ -303,7 +489,7 @@ __device__ __forceinline__ void mask_reduce_body(const MaskArgs& a)
     if(c < 3 && o->nnm > 0) { g = round_half_away(ddiv((double)o->sd[c], den)); }
     o->gcd[c] = min(max(g, -a.maxdiff[c]), a.maxdiff[c]);
   }
-  o->flags |= (o->max_sample[0] > (uint32_t)a.maxv ? 1 : 0) | (o->max_sample[1] > (uint32_t)a.maxv ? 2 : 0);
+  o->flags |= (o->or_sample[0] > (uint32_t)a.maxv ? 1 : 0) | (o->or_sample[1] > (uint32_t)a.maxv ? 2 : 0);
 }
 
 // The masked search. A CTA takes a 32 x 8 tile of test pixels of one direction (blockIdx.z: 0 = R2T,
@@ -354,16 +540,16 @@ __device__ __forceinline__ void cps_masked_body(const MaskArgs& a, int bx, int b
           const int4 r = st[ty + dy][tx + dx];
           if(r.w == 0) { continue; }
           const int32_t d0 = s[0] - r.x, d1 = s[1] - r.y, d2 = s[2] - r.z;
-          const uint32_t err = (uint32_t)(d0 * d0) * (uint32_t)a.cws[0] + (uint32_t)(d1 * d1) * (uint32_t)a.cws[1] +
-                               (uint32_t)(d2 * d2) * (uint32_t)a.cws[2];
+          const uint32_t err = (uint32_t)mul_wrap(d0, d0) * (uint32_t)a.cws[0] + (uint32_t)mul_wrap(d1, d1) * (uint32_t)a.cws[1] +
+                               (uint32_t)mul_wrap(d2, d2) * (uint32_t)a.cws[2];
           if((int32_t)err < best) { best = (int32_t)err; bidx = dy * D + dx; }
         }
       }
       const int4 bp = st[ty + bidx / D][tx + bidx % D];
       const int32_t d0 = s[0] - bp.x, d1 = s[1] - bp.y, d2 = s[2] - bp.z;
-      e[0] = (uint64_t)(int64_t)(d0 * d0) * (uint64_t)m;
-      e[1] = (uint64_t)(int64_t)(d1 * d1) * (uint64_t)m;
-      e[2] = (uint64_t)(int64_t)(d2 * d2) * (uint64_t)m;
+      e[0] = (uint64_t)(int64_t)mul_wrap(d0, d0) * (uint64_t)m;
+      e[1] = (uint64_t)(int64_t)mul_wrap(d1, d1) * (uint64_t)m;
+      e[2] = (uint64_t)(int64_t)mul_wrap(d2, d2) * (uint64_t)m;
     }
   }
   // a warp is 32 pixels of one row
@@ -573,7 +759,7 @@ __device__ __forceinline__ void mask_finalize_body(const MaskArgs& a, int chain)
 template <typename T, typename TM>
 __global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ MaskArgs a) { mask_prepass_body<T, TM>(a, blockIdx.x); }
 template <typename T, typename TM>
-__global__ void __launch_bounds__(256) k_mask_prepass420v(const __grid_constant__ MaskArgs a) { mask_prepass420v_body<T, TM>(a, blockIdx.x); }
+__global__ void __launch_bounds__(256, 3) k_mask_prepass420v(const __grid_constant__ MaskArgs a) { mask_prepass420_body<T, TM>(a, blockIdx.x); }
 __global__ void k_mask_reduce(const __grid_constant__ MaskArgs a) { mask_reduce_body(a); }
 template <typename T, typename TM, int R>
 __global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ MaskArgs a) { cps_masked_body<T, TM, R>(a, blockIdx.x, blockIdx.y, blockIdx.z); }
@@ -581,32 +767,40 @@ template <typename T, typename TM, int R>
 __global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant__ MaskArgs a) { cps_masked_key_body<T, TM, R>(a, blockIdx.x, blockIdx.y); }
 __global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ MaskArgs a) { mask_finalize_body(a, blockIdx.x); }
 
-// jobs: the pairs of one launch group; vec: the group's pairs take the vector-load prepass
+// The arguments of up to kPackPairs pairs of one launch group, passed by value: every CTA reads its
+// pair's arguments from the constant bank as the one-pair kernels do, without a dependent global load.
+struct MaskPack
+{
+  MaskArgs a[kPackPairs];
+};
+static_assert(sizeof(MaskPack) <= 32000, "kernel parameters are limited to 32 KB");
+
+// vec: the group's pairs take the vector-load prepass
 template <typename T, typename TM, bool VEC>
-__global__ void __launch_bounds__(256) k_mask_prepass_multi(const MaskArgs* __restrict__ jobs, const int32_t* __restrict__ idx)
+__global__ void __launch_bounds__(256, 3) k_mask_prepass_multi(const __grid_constant__ MaskPack pk)
 {
-  const MaskArgs& a = jobs[idx[blockIdx.y]];
+  const MaskArgs& a = pk.a[blockIdx.y];
   if((int)blockIdx.x >= a.H) { return; }
-  if(VEC) { mask_prepass420v_body<T, TM>(a, blockIdx.x); } else { mask_prepass_body<T, TM>(a, blockIdx.x); }
+  if(VEC) { mask_prepass420_body<T, TM>(a, blockIdx.x); } else { mask_prepass_body<T, TM>(a, blockIdx.x); }
 }
-__global__ void k_mask_reduce_multi(const MaskArgs* __restrict__ jobs) { mask_reduce_body(jobs[blockIdx.x]); }
+__global__ void k_mask_reduce_multi(const __grid_constant__ MaskPack pk) { mask_reduce_body(pk.a[blockIdx.x]); }
 template <typename T, typename TM, int R>
-__global__ void __launch_bounds__(256) k_cps_masked_multi(const MaskArgs* __restrict__ jobs, const int32_t* __restrict__ idx)
+__global__ void __launch_bounds__(256) k_cps_masked_multi(const __grid_constant__ MaskPack pk)
 {
-  const MaskArgs& a = jobs[idx[blockIdx.z >> 1]];
+  const MaskArgs& a = pk.a[blockIdx.z >> 1];
   if((int)blockIdx.x * 32 >= a.W || (int)blockIdx.y * 8 >= a.H) { return; }
   cps_masked_body<T, TM, R>(a, blockIdx.x, blockIdx.y, blockIdx.z & 1);
 }
 template <typename T, typename TM, int R>
-__global__ void __launch_bounds__(512, 2) k_cps_masked_key_multi(const MaskArgs* __restrict__ jobs, const int32_t* __restrict__ idx)
+__global__ void __launch_bounds__(512, 2) k_cps_masked_key_multi(const __grid_constant__ MaskPack pk)
 {
-  const MaskArgs& a = jobs[idx[blockIdx.z]];
+  const MaskArgs& a = pk.a[blockIdx.z];
   if((int)blockIdx.x * MaskKeyGeo<R>::TW >= a.W || (int)blockIdx.y * MaskKeyGeo<R>::TH >= a.H) { return; }
   cps_masked_key_body<T, TM, R>(a, blockIdx.x, blockIdx.y);
 }
-__global__ void __launch_bounds__(256) k_mask_finalize_multi(const MaskArgs* __restrict__ jobs)
+__global__ void __launch_bounds__(256) k_mask_finalize_multi(const __grid_constant__ MaskPack pk)
 {
-  mask_finalize_body(jobs[blockIdx.x / 9], blockIdx.x % 9);
+  mask_finalize_body(pk.a[blockIdx.x / 9], blockIdx.x % 9);
 }
 
 template <typename T, typename TM, int R>
@@ -620,12 +814,18 @@ cudaError_t launch_masked_key(const MaskArgs& a, cudaStream_t s)
   return cudaSuccess;
 }
 
+// pipe: the stage timers of the calling calc (events around each stage when its context profiles)
 template <typename T, typename TM>
-cudaError_t launch_masked_t(const MaskArgs& a, int R, bool key, cudaStream_t s)
+cudaError_t launch_masked_t(const MaskArgs& a, int R, bool key, PairPipeline& pipe, cudaStream_t s)
 {
+  int tok = pipe.prof_begin(s);
   if(mask_prepass_vec_ok(a, sizeof(T), sizeof(TM))) { k_mask_prepass420v<T, TM><<<a.H, 256, 0, s>>>(a); }
   else { k_mask_prepass<T, TM><<<a.H, 256, 0, s>>>(a); }
+  pipe.prof_end(s, QMIV_STAGE_PREPASS, tok);
+  tok = pipe.prof_begin(s);
   k_mask_reduce<<<1, 32, 0, s>>>(a);
+  pipe.prof_end(s, QMIV_STAGE_REDUCE, tok);
+  tok = pipe.prof_begin(s);
   const dim3 grid((a.W + 31) / 32, (a.H + 7) / 8, 2);
   if(key)
   {
@@ -650,7 +850,10 @@ cudaError_t launch_masked_t(const MaskArgs& a, int R, bool key, cudaStream_t s)
   case 5: k_cps_masked<T, TM, 5><<<grid, 256, 0, s>>>(a); break;
   default: return cudaErrorInvalidValue;
   }
+  pipe.prof_end(s, QMIV_STAGE_CPS, tok);
+  tok = pipe.prof_begin(s);
   k_mask_finalize<<<9, 256, 0, s>>>(a);
+  pipe.prof_end(s, QMIV_STAGE_FINALIZE, tok);
   return cudaGetLastError();
 }
 
@@ -823,11 +1026,14 @@ qmiv_status MaskedPipeline::run(qmiv_calc_s* calc, const qmiv_frame* in0, const 
   QMIV_CUDA(cudaMemsetAsync(a.row_cps, 0, (size_t)6 * S.H * sizeof(uint64_t), s));
   const int R = P.prm.search_range;
   cudaError_t e;
-  if(S.esz == 1) { e = P.mesz == 1 ? launch_masked_t<uint8_t, uint8_t>(a, R, P.key, s) : launch_masked_t<uint8_t, uint16_t>(a, R, P.key, s); }
-  else { e = P.mesz == 1 ? launch_masked_t<uint16_t, uint8_t>(a, R, P.key, s) : launch_masked_t<uint16_t, uint16_t>(a, R, P.key, s); }
+  if(S.esz == 1) { e = P.mesz == 1 ? launch_masked_t<uint8_t, uint8_t>(a, R, P.key, pipe, s) : launch_masked_t<uint8_t, uint16_t>(a, R, P.key, pipe, s); }
+  else { e = P.mesz == 1 ? launch_masked_t<uint16_t, uint8_t>(a, R, P.key, pipe, s) : launch_masked_t<uint16_t, uint16_t>(a, R, P.key, pipe, s); }
   if(e != cudaSuccess) { return cuda_fail(e, "masked launches"); }
+  const int tok = pipe.prof_begin(s);
   QMIV_CUDA(cudaMemcpyAsync(h_out_, out_.p, sizeof(MaskOut), cudaMemcpyDeviceToHost, s));
+  pipe.prof_end(s, QMIV_STAGE_D2H, tok);
   QMIV_CUDA(cudaStreamSynchronize(s));
+  pipe.harvest_profile();
   const MaskOut& o = *static_cast<const MaskOut*>(h_out_);
   QMIV_TRY(masked_status(o, P));
   if(num_non_masked) { *num_non_masked = o.nnm; }
@@ -841,16 +1047,18 @@ namespace {
 constexpr size_t kMaskAlign = 256;
 inline size_t malign(size_t v) { return (v + kMaskAlign - 1) & ~(kMaskAlign - 1); }
 
+// form: 1 = vector loads, 0 = generic
 template <typename T, typename TM>
-void launch_prepass_group(const MaskArgs* d, const int32_t* idx, int count, int max_h, bool vec, cudaStream_t s)
+cudaError_t launch_prepass_group(const MaskPack& pk, int count, int max_h, int form, cudaStream_t s)
 {
   const dim3 grid(max_h, count);
-  if(vec) { k_mask_prepass_multi<T, TM, true><<<grid, 256, 0, s>>>(d, idx); }
-  else { k_mask_prepass_multi<T, TM, false><<<grid, 256, 0, s>>>(d, idx); }
+  if(form == 1) { k_mask_prepass_multi<T, TM, true><<<grid, 256, 0, s>>>(pk); }
+  else { k_mask_prepass_multi<T, TM, false><<<grid, 256, 0, s>>>(pk); }
+  return cudaSuccess;
 }
 
 template <typename T, typename TM, int R>
-cudaError_t launch_search_group_r(const MaskArgs* d, const int32_t* idx, int count, int max_w, int max_h, bool key, cudaStream_t s)
+cudaError_t launch_search_group_r(const MaskPack& pk, int count, int max_w, int max_h, bool key, cudaStream_t s)
 {
   if(key)
   {
@@ -858,26 +1066,26 @@ cudaError_t launch_search_group_r(const MaskArgs* d, const int32_t* idx, int cou
     const cudaError_t e = cudaFuncSetAttribute(k_cps_masked_key_multi<T, TM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::kSmem);
     if(e != cudaSuccess) { return e; }
     const dim3 grid((max_w + G::TW - 1) / G::TW, (max_h + G::TH - 1) / G::TH, count);
-    k_cps_masked_key_multi<T, TM, R><<<grid, 512, G::kSmem, s>>>(d, idx);
+    k_cps_masked_key_multi<T, TM, R><<<grid, 512, G::kSmem, s>>>(pk);
   }
   else
   {
     const dim3 grid((max_w + 31) / 32, (max_h + 7) / 8, 2 * count);
-    k_cps_masked_multi<T, TM, R><<<grid, 256, 0, s>>>(d, idx);
+    k_cps_masked_multi<T, TM, R><<<grid, 256, 0, s>>>(pk);
   }
   return cudaSuccess;
 }
 
 template <typename T, typename TM>
-cudaError_t launch_search_group(const MaskArgs* d, const int32_t* idx, int count, int max_w, int max_h, int R, bool key, cudaStream_t s)
+cudaError_t launch_search_group(const MaskPack& pk, int count, int max_w, int max_h, int R, bool key, cudaStream_t s)
 {
   switch(R)
   {
-  case 1: return launch_search_group_r<T, TM, 1>(d, idx, count, max_w, max_h, key, s);
-  case 2: return launch_search_group_r<T, TM, 2>(d, idx, count, max_w, max_h, key, s);
-  case 3: return launch_search_group_r<T, TM, 3>(d, idx, count, max_w, max_h, key, s);
-  case 4: return launch_search_group_r<T, TM, 4>(d, idx, count, max_w, max_h, key, s);
-  case 5: return launch_search_group_r<T, TM, 5>(d, idx, count, max_w, max_h, key, s);
+  case 1: return launch_search_group_r<T, TM, 1>(pk, count, max_w, max_h, key, s);
+  case 2: return launch_search_group_r<T, TM, 2>(pk, count, max_w, max_h, key, s);
+  case 3: return launch_search_group_r<T, TM, 3>(pk, count, max_w, max_h, key, s);
+  case 4: return launch_search_group_r<T, TM, 4>(pk, count, max_w, max_h, key, s);
+  case 5: return launch_search_group_r<T, TM, 5>(pk, count, max_w, max_h, key, s);
   default: return cudaErrorInvalidValue;
   }
 }
@@ -885,7 +1093,6 @@ cudaError_t launch_search_group(const MaskArgs* d, const int32_t* idx, int count
 struct GroupInfo
 {
   std::vector<int32_t> pairs;
-  int max_w = 0, max_h = 0;
 };
 
 }  // namespace
@@ -926,16 +1133,12 @@ qmiv_status MaskedBatch::run(qmiv_ctx_s* ctx, const qmiv_params& prm0, cudaStrea
     o_stage[i] = cur; cur += host ? malign(2 * S.staged_frame_bytes()) : 0;
     o_mstage[i] = cur; cur += masks[i].mem == QMIV_MEM_HOST ? malign((size_t)S.W * P[i].mesz * S.H) : 0;
   }
-  // groups: prepass by (sample sizes, vector loads), search by (sample sizes, R, search form)
+  // groups: prepass by (sample sizes, prepass form), search by (sample sizes, R, search form)
   std::map<std::tuple<int, int, int>, GroupInfo> pre;
   std::map<std::tuple<int, int, int, int>, GroupInfo> srch;
-  const size_t off_args = cur;
-  cur += malign(sizeof(MaskArgs) * n);
-  const size_t off_idx = cur;
-  cur += malign(sizeof(int32_t) * 2 * n);
   const size_t total = cur;
   QMIV_TRY(arena_.ensure(ctx, total));
-  const size_t hbytes = (total - off_args) + sizeof(MaskOut) * n;
+  const size_t hbytes = sizeof(MaskOut) * n;
   if(h_bytes_ < hbytes)
   {
     if(h_) { cudaFreeHost(h_); h_ = nullptr; h_bytes_ = 0; }
@@ -943,10 +1146,9 @@ qmiv_status MaskedBatch::run(qmiv_ctx_s* ctx, const qmiv_params& prm0, cudaStrea
     h_bytes_ = hbytes;
   }
   char* dbase = arena_.as<char>();
-  MaskArgs* hargs = reinterpret_cast<MaskArgs*>(static_cast<char*>(h_));
-  int32_t* hidx = reinterpret_cast<int32_t*>(static_cast<char*>(h_) + (off_idx - off_args));
-  MaskOut* hout = reinterpret_cast<MaskOut*>(static_cast<char*>(h_) + (total - off_args));
-  QMIV_CUDA(cudaMemsetAsync(dbase, 0, off_args, s));      // results and row sums start at zero
+  std::vector<MaskArgs> hargs(n);
+  MaskOut* hout = static_cast<MaskOut*>(h_);
+  QMIV_CUDA(cudaMemsetAsync(dbase, 0, total, s));          // results and row sums start at zero
   for(int i = 0; i < n; i++)
   {
     const MaskPlan& p = P[i];
@@ -963,45 +1165,66 @@ qmiv_status MaskedBatch::run(qmiv_ctx_s* ctx, const qmiv_params& prm0, cudaStrea
     fill_mask_args(p, a0, a1, reinterpret_cast<uint64_t*>(dbase + o_rows[i]), ws,
                    reinterpret_cast<MaskOut*>(dbase + off_out) + i, a);
     const int t = (int)S.esz, tm = (int)p.mesz;
-    GroupInfo& gp = pre[std::make_tuple(t, tm, (int)mask_prepass_vec_ok(a, S.esz, p.mesz))];
-    gp.pairs.push_back(i); gp.max_h = std::max(gp.max_h, S.H); gp.max_w = std::max(gp.max_w, S.W);
-    GroupInfo& gs = srch[std::make_tuple(t, tm, p.prm.search_range, (int)p.key)];
-    gs.pairs.push_back(i); gs.max_h = std::max(gs.max_h, S.H); gs.max_w = std::max(gs.max_w, S.W);
+    const int form = mask_prepass_vec_ok(a, S.esz, p.mesz) ? 1 : 0;
+    pre[std::make_tuple(t, tm, form)].pairs.push_back(i);
+    srch[std::make_tuple(t, tm, p.prm.search_range, (int)p.key)].pairs.push_back(i);
   }
-  int k = 0;
-  std::vector<int> pre_first, srch_first;
-  for(auto& g : pre) { pre_first.push_back(k); for(int32_t i : g.second.pairs) { hidx[k++] = i; } }
-  for(auto& g : srch) { srch_first.push_back(k); for(int32_t i : g.second.pairs) { hidx[k++] = i; } }
-  QMIV_CUDA(cudaMemcpyAsync(dbase + off_args, h_, total - off_args, cudaMemcpyHostToDevice, s));
-  const MaskArgs* dargs = reinterpret_cast<const MaskArgs*>(dbase + off_args);
-  const int32_t* didx = reinterpret_cast<const int32_t*>(dbase + off_idx);
-  int gi = 0;
+  // launches over chunks of up to kPackPairs pairs, each chunk's arguments in the launch's parameters
+  std::vector<int32_t> all(n);
+  for(int i = 0; i < n; i++) { all[i] = i; }
+  MaskPack pk{};
+  int max_w = 0, max_h = 0;
+  auto pack = [&](const std::vector<int32_t>& ids, size_t first) -> int {
+    const int cnt = (int)std::min(ids.size() - first, (size_t)kPackPairs);
+    max_w = 0; max_h = 0;
+    for(int j = 0; j < cnt; j++)
+    {
+      pk.a[j] = hargs[ids[first + j]];
+      max_w = std::max(max_w, pk.a[j].W); max_h = std::max(max_h, pk.a[j].H);
+    }
+    return cnt;
+  };
+  int tok = clock_.begin(ctx, s);
   for(auto& g : pre)
   {
-    const int t = std::get<0>(g.first), tm = std::get<1>(g.first);
-    const bool vec = std::get<2>(g.first) != 0;
-    const int32_t* ix = didx + pre_first[gi++];
-    const int cnt = (int)g.second.pairs.size(), mh = g.second.max_h;
-    if(t == 1) { if(tm == 1) { launch_prepass_group<uint8_t, uint8_t>(dargs, ix, cnt, mh, vec, s); } else { launch_prepass_group<uint8_t, uint16_t>(dargs, ix, cnt, mh, vec, s); } }
-    else { if(tm == 1) { launch_prepass_group<uint16_t, uint8_t>(dargs, ix, cnt, mh, vec, s); } else { launch_prepass_group<uint16_t, uint16_t>(dargs, ix, cnt, mh, vec, s); } }
+    const int t = std::get<0>(g.first), tm = std::get<1>(g.first), form = std::get<2>(g.first);
+    for(size_t f = 0; f < g.second.pairs.size(); f += kPackPairs)
+    {
+      const int cnt = pack(g.second.pairs, f);
+      cudaError_t e;
+      if(t == 1) { e = tm == 1 ? launch_prepass_group<uint8_t, uint8_t>(pk, cnt, max_h, form, s) : launch_prepass_group<uint8_t, uint16_t>(pk, cnt, max_h, form, s); }
+      else { e = tm == 1 ? launch_prepass_group<uint16_t, uint8_t>(pk, cnt, max_h, form, s) : launch_prepass_group<uint16_t, uint16_t>(pk, cnt, max_h, form, s); }
+      if(e != cudaSuccess) { return cuda_fail(e, "masked prepass launch"); }
+    }
   }
-  k_mask_reduce_multi<<<n, 32, 0, s>>>(dargs);
-  gi = 0;
+  clock_.end(s, QMIV_STAGE_PREPASS, tok);
+  tok = clock_.begin(ctx, s);
+  for(size_t f = 0; f < all.size(); f += kPackPairs) { const int cnt = pack(all, f); k_mask_reduce_multi<<<cnt, 32, 0, s>>>(pk); }
+  clock_.end(s, QMIV_STAGE_REDUCE, tok);
+  tok = clock_.begin(ctx, s);
   for(auto& g : srch)
   {
     const int t = std::get<0>(g.first), tm = std::get<1>(g.first), R = std::get<2>(g.first);
     const bool key = std::get<3>(g.first) != 0;
-    const int32_t* ix = didx + srch_first[gi++];
-    const int cnt = (int)g.second.pairs.size(), mw = g.second.max_w, mh = g.second.max_h;
-    cudaError_t e;
-    if(t == 1) { e = tm == 1 ? launch_search_group<uint8_t, uint8_t>(dargs, ix, cnt, mw, mh, R, key, s) : launch_search_group<uint8_t, uint16_t>(dargs, ix, cnt, mw, mh, R, key, s); }
-    else { e = tm == 1 ? launch_search_group<uint16_t, uint8_t>(dargs, ix, cnt, mw, mh, R, key, s) : launch_search_group<uint16_t, uint16_t>(dargs, ix, cnt, mw, mh, R, key, s); }
-    if(e != cudaSuccess) { return cuda_fail(e, "masked search launch"); }
+    for(size_t f = 0; f < g.second.pairs.size(); f += kPackPairs)
+    {
+      const int cnt = pack(g.second.pairs, f);
+      cudaError_t e;
+      if(t == 1) { e = tm == 1 ? launch_search_group<uint8_t, uint8_t>(pk, cnt, max_w, max_h, R, key, s) : launch_search_group<uint8_t, uint16_t>(pk, cnt, max_w, max_h, R, key, s); }
+      else { e = tm == 1 ? launch_search_group<uint16_t, uint8_t>(pk, cnt, max_w, max_h, R, key, s) : launch_search_group<uint16_t, uint16_t>(pk, cnt, max_w, max_h, R, key, s); }
+      if(e != cudaSuccess) { return cuda_fail(e, "masked search launch"); }
+    }
   }
-  k_mask_finalize_multi<<<9 * n, 256, 0, s>>>(dargs);
+  clock_.end(s, QMIV_STAGE_CPS, tok);
+  tok = clock_.begin(ctx, s);
+  for(size_t f = 0; f < all.size(); f += kPackPairs) { const int cnt = pack(all, f); k_mask_finalize_multi<<<9 * cnt, 256, 0, s>>>(pk); }
+  clock_.end(s, QMIV_STAGE_FINALIZE, tok);
   QMIV_CUDA(cudaGetLastError());
+  tok = clock_.begin(ctx, s);
   QMIV_CUDA(cudaMemcpyAsync(hout, dbase + off_out, sizeof(MaskOut) * n, cudaMemcpyDeviceToHost, s));
+  clock_.end(s, QMIV_STAGE_D2H, tok);
   QMIV_CUDA(cudaStreamSynchronize(s));
+  clock_.harvest(ctx);
   qmiv_status first = QMIV_OK;
   for(int i = 0; i < n; i++)
   {

@@ -193,3 +193,71 @@ def test_masked_batched_equals_one_pair_calls(erp, golden_masked, qctx):
                 assert got[i] == one and nnm[i] == one_nnm, (i, W, H, bd, R)
                 if c is not None:
                     assert compare_masked(got[i], nnm[i], c["expected"]) == []
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bd", [10, 14])
+def test_masked_prepass_large_samples(bd, qctx, oracle_lib):
+    """The aligned 4:2:0 prepass with an 8-bit mask sums pairs of 16-bit samples in 32-bit words while
+    every sample of a thread's step is below 2^15, and sample by sample with the reference's int32
+    products otherwise. Frames with raw samples of 2^15 and above under SKIP give the C restatement's
+    sums at 10 bits and at 14 bits (the deepest mask mode takes); rows of 320 groups leave threads with
+    and without a large sample in the same row."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    W, H = 1280, 64
+    f0, f1 = synth.make_pair(W, H, bd, seed=5 + bd)
+    f0 = tuple(np.array(pl, copy=True) for pl in f0)
+    f1 = tuple(np.array(pl, copy=True) for pl in f1)
+    f1[0][3, 100] = 40000
+    f1[0][7, W - 1] = 65535
+    f1[2][10, 33] = 32768
+    f0[1][20, 600] = 50000
+    m = det_mask(W, H, 8, 17, "weights")
+    p = oracle.make_params(W, H, bd, 420, search_range=2, erp=True)
+    exp, n_exp = oracle_lib.compute_pair_masked(p, f0, f1, m, 8)
+    with qmiv_b200.Calc(qctx, W, H, bd, search_range=2, erp=True, invalid_pel_action=qmiv_b200.PEL_SKIP) as calc:
+        got, nnm = calc.compute_masked(f0, f1, m, 8)
+    assert nnm == n_exp
+    for k in ["gcd_r2t", "psnr", "wspsnr"]:
+        assert list(got[k][:3]) == list(exp[k][:3]), k
+    for k in ["psnr_pic", "wspsnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"]:
+        assert got[k] == exp[k], k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("erp", [False, True])
+def test_masked_staged_prepass_against_oracle(erp, qctx, oracle_lib):
+    """Aligned 4:2:0 pairs with 8-bit masks and widths divisible by 32 take the staged prepass: persistent
+    CTAs over the row pairs of every pair of a launch, each CTA's contiguous range crossing from one
+    pair into the next. Pairs of four widths (stage slots of different sizes), host and device frames,
+    in one batched call and one by one, give the C restatement's values."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    shapes = [(640, 360, 10, 2), (1280, 96, 8, 1), (2048, 130, 10, 3), (96, 34, 10, 2), (4096, 64, 8, 2)]
+    items = []
+    for k, (W, H, bd, R) in enumerate(shapes):
+        f0, f1 = synth.make_pair(W, H, bd, seed=31 * k + W)
+        m = det_mask(W, H, 8, 7 * k + H, "weights" if k % 2 else "sparse")
+        p = oracle.make_params(W, H, bd, 420, search_range=R, erp=erp)
+        exp, n_exp = oracle_lib.compute_pair_masked(p, f0, f1, m, 8)
+        if k % 2:
+            f0, f1, m = tuple(_dev(x) for x in f0), tuple(_dev(x) for x in f1), _dev(m)
+        items.append((W, H, bd, R, f0, f1, m, exp, n_exp))
+    keys3 = ["gcd_r2t", "psnr", "wspsnr"]
+    keys = ["psnr_pic", "wspsnr_pic", "ivpsnr", "ivpsnr_r2t", "ivpsnr_t2r"]
+    pairs = [dict(frame0=f0, frame1=f1, width=W, height=H, bitdepth=bd, search_range=R,
+                  metrics=qmiv_b200.PSNR | qmiv_b200.WSPSNR | qmiv_b200.IVPSNR) for W, H, bd, R, f0, f1, m, e, n in items]
+    with qmiv_b200.Batch(qctx, len(pairs), sum(W * H for W, H, *_ in items), erp=erp) as batch:
+        got, nnm = batch.compute_masked(pairs, [it[6] for it in items], [8] * len(items))
+    for i, (W, H, bd, R, f0, f1, m, exp, n_exp) in enumerate(items):
+        assert nnm[i] == n_exp, (W, H)
+        for k in keys3:
+            assert list(got[i][k][:3]) == list(exp[k][:3]), (W, H, k)
+        for k in keys:
+            assert got[i][k] == exp[k], (W, H, k)
+        with qmiv_b200.Calc(qctx, W, H, bd, search_range=R, erp=erp) as calc:
+            one, one_nnm = calc.compute_masked(f0, f1, m, 8)
+        assert one == got[i] and one_nnm == n_exp, (W, H)
