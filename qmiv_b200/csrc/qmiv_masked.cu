@@ -64,6 +64,7 @@ struct MaskArgs
   const double* ws;            // [H] or null
   MaskOut*    out;
   uint32_t    kscale;          // 128, read from the parameter bank so the key stays one integer multiply-add
+  int32_t     pairs420;        // 4:2:0 with luma and mask rows on 2-sample boundaries (two-sample loads)
 };
 
 // Host-side description of one masked frame pair: its shape and parameters and what follows from them
@@ -592,8 +593,80 @@ struct MaskKeyGeo
   static constexpr size_t kSmem = sizeof(float4) * 2 * SH * SW + sizeof(int32_t) * TH * TW;
 };
 
+// Two adjacent samples of one row (the host checked the alignment): low sample first
+__device__ __forceinline__ void ld_pair(const uint16_t* p, uint32_t& v0, uint32_t& v1)
+{
+  const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(p));
+  v0 = w & 0xffffu; v1 = w >> 16;
+}
+__device__ __forceinline__ void ld_pair(const uint8_t* p, uint32_t& v0, uint32_t& v1)
+{
+  const uint32_t w = __ldg(reinterpret_cast<const unsigned short*>(p));
+  v0 = w & 0xffu; v1 = w >> 8;
+}
+
+// The key search's staging for a tile whose halo lies inside a 4:2:0 picture, R even: the staged area
+// splits into 2 x 2 blocks at even picture coordinates, each under one chroma sample, read as two-sample
+// rows of luma and mask and one sample per chroma plane; the chroma part of the key, w1 Cb^2 + w2 Cr^2,
+// is formed once per block. Under the key search's bound every partial sum of the key is an integer
+// below 2^24, so the key equals the per-sample form's whatever the order of the additions.
 template <typename T, typename TM, int R>
-__device__ __forceinline__ void cps_masked_key_body(const MaskArgs& a, int bx, int by)
+__device__ __forceinline__ void stage_key420(const MaskArgs& a, float4* st0, float4* st1, int32_t* mk, int x0, int y0,
+                                             float w0, float w1, float w2)
+{
+  using G = MaskKeyGeo<R>;
+  constexpr int TW = G::TW, TH = G::TH, SW = G::SW, SH = G::SH, BW = SW / 2;
+  const bool clip_on = a.clip < (sizeof(T) == 1 ? 0xffu : 0xffffu);
+  for(int b = threadIdx.x; b < (SH / 2) * BW; b += 512)
+  {
+    const int by = b / BW, bx = b - by * BW;
+    const int ly = 2 * by, lx = 2 * bx;
+    const int ux = x0 - R + lx, uy = y0 - R + ly;             // even, the block inside the picture
+    uint32_t m[4];
+    {
+      const TM* mp = static_cast<const TM*>(a.mask) + (size_t)uy * a.mpitch + ux;
+      ld_pair(mp, m[0], m[1]);
+      ld_pair(mp + a.mpitch, m[2], m[3]);
+    }
+    const Img* im[2] = { &a.in0, &a.in1 };
+    float4* st[2] = { st0, st1 };
+    #pragma unroll
+    for(int f = 0; f < 2; f++)
+    {
+      const T* yp = static_cast<const T*>(im[f]->p[0]) + (size_t)uy * im[f]->pitch[0] + ux;
+      uint32_t v[4];
+      ld_pair(yp, v[0], v[1]);
+      ld_pair(yp + im[f]->pitch[0], v[2], v[3]);
+      uint32_t cb = __ldg(static_cast<const T*>(im[f]->p[1]) + (size_t)(uy >> 1) * im[f]->pitch[1] + (ux >> 1));
+      uint32_t cr = __ldg(static_cast<const T*>(im[f]->p[2]) + (size_t)(uy >> 1) * im[f]->pitch[2] + (ux >> 1));
+      if(clip_on)
+      {
+        cb = min(cb, a.clip); cr = min(cr, a.clip);
+        #pragma unroll
+        for(int i = 0; i < 4; i++) { v[i] = min(v[i], a.clip); }
+      }
+      const float fb = u2f_exact(cb), fr = u2f_exact(cr);
+      const float ct = fmaf(w2, fr * fr, fmaf(w1, fb * fb, kMaskBias));
+      #pragma unroll
+      for(int i = 0; i < 4; i++)
+      {
+        const float fy = u2f_exact(v[i]);
+        const int e = (ly + (i >> 1)) * SW + lx + (i & 1);
+        st[f][e] = m[i] ? make_float4(fy, fb, fr, fmaf(w0, fy * fy, ct)) : make_float4(0.f, 0.f, 0.f, kMaskedValue);
+      }
+    }
+    #pragma unroll
+    for(int i = 0; i < 4; i++)
+    {
+      const int ty = ly + (i >> 1) - R, tx = lx + (i & 1) - R;
+      if(ty >= 0 && ty < TH && tx >= 0 && tx < TW) { mk[ty * TW + tx] = (int32_t)m[i]; }
+    }
+  }
+}
+
+template <typename T, typename TM, int R>
+// kscale: 128 from a kernel parameter at a fixed offset (the key stays one multiply-add with a constant operand)
+__device__ __forceinline__ void cps_masked_key_body(const MaskArgs& a, int bx, int by, uint32_t kscale)
 {
   using G = MaskKeyGeo<R>;
   constexpr int P = G::P, TW = G::TW, TH = G::TH, SW = G::SW, SH = G::SH, D = G::D;
@@ -604,7 +677,16 @@ __device__ __forceinline__ void cps_masked_key_body(const MaskArgs& a, int bx, i
   int32_t* mk = reinterpret_cast<int32_t*>(smem + 2 * SH * SW);   // M of the tile's pixels, 0 outside the picture
   const int x0 = bx * TW, y0 = by * TH;
   const float w0 = (float)a.cws[0], w1 = (float)a.cws[1], w2 = (float)a.cws[2];
-  for(int e = threadIdx.x; e < SH * SW; e += 512)
+  bool staged = false;
+  if constexpr(R % 2 == 0)
+  {
+    if(a.pairs420 && x0 >= R && y0 >= R && x0 + TW + R <= a.W && y0 + TH + R <= a.H)
+    {
+      stage_key420<T, TM, R>(a, st0, st1, mk, x0, y0, w0, w1, w2);
+      staged = true;
+    }
+  }
+  for(int e = staged ? SH * SW : threadIdx.x; e < SH * SW; e += 512)
   {
     const int ly = e / SW, lx = e - ly * SW;
     const int ux = x0 - R + lx, uy = y0 - R + ly;
@@ -648,29 +730,39 @@ __device__ __forceinline__ void cps_masked_key_body(const MaskArgs& a, int bx, i
   // candidates in column pairs: one three-input minimum takes two keys
   auto key = [&](const float4& r, int p, int k) -> uint32_t {
     const float t = fmaf(c2[p], r.z, fmaf(c1[p], r.y, fmaf(c0[p], r.x, r.w)));
-    return __float_as_uint(t) * a.kscale + ((uint32_t)k - (kMaskKeyBase << 7));
+    return __float_as_uint(t) * kscale + ((uint32_t)k - (kMaskKeyBase << 7));
   };
+  // a warp whose 32 x P test pixels are all masked has nothing to search: every term it adds is
+  // multiplied by M = 0 (the reference skips masked test pixels, xCorrespPixelShiftSTD.cpp:151-215)
+  bool any = false;
   #pragma unroll
-  for(int j = 0; j < D + P - 1; j++)
+  for(int p = 0; p < P; p++) { any = any || m[p] != 0; }
+  if(__any_sync(0xffffffffu, any))
   {
     #pragma unroll
-    for(int dx = 0; dx < D; dx += 2)
+    for(int j = 0; j < D + P - 1; j++)
     {
-      const float4 ra = ref[(ty * P + j) * SW + tx + dx];
-      const float4 rb = ref[(ty * P + j) * SW + tx + min(dx + 1, D - 1)];
       #pragma unroll
-      for(int p = 0; p < P; p++)
+      for(int dx = 0; dx < D; dx += 2)
       {
-        const int dy = j - p;
-        if(dy < 0 || dy >= D) { continue; }                  // resolved at compile time
-        if(dx + 1 < D) { best[p] = __vimin3_u32(best[p], key(ra, p, dy * D + dx), key(rb, p, dy * D + dx + 1)); }
-        else { best[p] = min(best[p], key(ra, p, dy * D + dx)); }
+        const float4 ra = ref[(ty * P + j) * SW + tx + dx];
+        const float4 rb = ref[(ty * P + j) * SW + tx + min(dx + 1, D - 1)];
+        #pragma unroll
+        for(int p = 0; p < P; p++)
+        {
+          const int dy = j - p;
+          if(dy < 0 || dy >= D) { continue; }                  // resolved at compile time
+          if(dx + 1 < D) { best[p] = __vimin3_u32(best[p], key(ra, p, dy * D + dx), key(rb, p, dy * D + dx + 1)); }
+          else { best[p] = min(best[p], key(ra, p, dy * D + dx)); }
+        }
       }
     }
   }
-  // Row sums. Each term d^2 M is below 2^38 here (d^2 < 2^24 is checked with the key bound, M < 2^14),
-  // so its low 16 bits and the rest (< 2^22) are summed over the warp's 32 pixels of a row in 32 bits
-  // each, exactly, by one redux.sync apiece.
+  // Row sums. Each term d^2 M is below 2^38 here (|d| < 2^12: d^2 < 2^24 is checked with the key bound,
+  // M < 2^14). Over the warp's 32 pixels of a row the parts from bit 11 up (< 2^27 each) are summed in
+  // 32 bits, and the low 11 bits of two terms (sums below 2^16) share one 32-bit sum: 18 redux.sync per
+  // warp for its 4 rows x 3 components, every sum exact.
+  static_assert(P % 2 == 0, "low parts are reduced in pairs of rows");
   uint32_t lo[P][3], hi[P][3];
   #pragma unroll
   for(int p = 0; p < P; p++)
@@ -683,10 +775,23 @@ __device__ __forceinline__ void cps_masked_key_body(const MaskArgs& a, int bx, i
     #pragma unroll
     for(int c = 0; c < 3; c++)
     {
-      const uint64_t t = (uint64_t)__float2uint_rn(d[c] * d[c]) * (uint64_t)(uint32_t)m[p];   // d^2 < 2^24: exact
-      lo[p][c] = __reduce_add_sync(0xffffffffu, (uint32_t)t & 0xffffu);
-      hi[p][c] = __reduce_add_sync(0xffffffffu, (uint32_t)(t >> 16));
+      const int32_t di = f2i_exact(d[c] + 4096.0f) - 4096;   // d + 2^12 lies in (0, 2^13): exact
+      const uint64_t t = (uint64_t)(uint32_t)(di * di) * (uint64_t)(uint32_t)m[p];
+      hi[p][c] = __reduce_add_sync(0xffffffffu, (uint32_t)(t >> 11));
+      lo[p][c] = (uint32_t)t & 0x7ffu;
     }
+  }
+  #pragma unroll
+  for(int p = 0; p < P; p++)
+  {
+    const uint32_t s01 = __reduce_add_sync(0xffffffffu, lo[p][0] | (lo[p][1] << 16));
+    lo[p][0] = s01 & 0xffffu; lo[p][1] = s01 >> 16;
+  }
+  #pragma unroll
+  for(int p = 0; p < P; p += 2)
+  {
+    const uint32_t s2 = __reduce_add_sync(0xffffffffu, lo[p][2] | (lo[p + 1][2] << 16));
+    lo[p][2] = s2 & 0xffffu; lo[p + 1][2] = s2 >> 16;
   }
   if(tx == 0)
   {
@@ -698,7 +803,7 @@ __device__ __forceinline__ void cps_masked_key_body(const MaskArgs& a, int bx, i
       #pragma unroll
       for(int c = 0; c < 3; c++)
       {
-        const uint64_t v = ((uint64_t)hi[p][c] << 16) + lo[p][c];
+        const uint64_t v = ((uint64_t)hi[p][c] << 11) + lo[p][c];
         if(v) { atomicAdd(reinterpret_cast<unsigned long long*>(a.row_cps + ((size_t)dir * a.H + y) * 3 + c), (unsigned long long)v); }
       }
     }
@@ -764,7 +869,7 @@ __global__ void k_mask_reduce(const __grid_constant__ MaskArgs a) { mask_reduce_
 template <typename T, typename TM, int R>
 __global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ MaskArgs a) { cps_masked_body<T, TM, R>(a, blockIdx.x, blockIdx.y, blockIdx.z); }
 template <typename T, typename TM, int R>
-__global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant__ MaskArgs a) { cps_masked_key_body<T, TM, R>(a, blockIdx.x, blockIdx.y); }
+__global__ void __launch_bounds__(512, 2) k_cps_masked_key(const __grid_constant__ MaskArgs a) { cps_masked_key_body<T, TM, R>(a, blockIdx.x, blockIdx.y, a.kscale); }
 __global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ MaskArgs a) { mask_finalize_body(a, blockIdx.x); }
 
 // The arguments of up to kPackPairs pairs of one launch group, passed by value: every CTA reads its
@@ -772,6 +877,7 @@ __global__ void __launch_bounds__(256) k_mask_finalize(const __grid_constant__ M
 struct MaskPack
 {
   MaskArgs a[kPackPairs];
+  uint32_t kscale;             // 128, the key scale at a fixed parameter offset
 };
 static_assert(sizeof(MaskPack) <= 32000, "kernel parameters are limited to 32 KB");
 
@@ -796,7 +902,7 @@ __global__ void __launch_bounds__(512, 2) k_cps_masked_key_multi(const __grid_co
 {
   const MaskArgs& a = pk.a[blockIdx.z];
   if((int)blockIdx.x * MaskKeyGeo<R>::TW >= a.W || (int)blockIdx.y * MaskKeyGeo<R>::TH >= a.H) { return; }
-  cps_masked_key_body<T, TM, R>(a, blockIdx.x, blockIdx.y);
+  cps_masked_key_body<T, TM, R>(a, blockIdx.x, blockIdx.y, pk.kscale);
 }
 __global__ void __launch_bounds__(256) k_mask_finalize_multi(const __grid_constant__ MaskPack pk)
 {
@@ -931,6 +1037,14 @@ void fill_mask_args(const MaskPlan& P, const Img& a0, const Img& a1, uint64_t* r
   a.ws = P.prm.erp ? ws : nullptr;
   a.out = out;
   a.kscale = 128u;
+  auto al = [](const void* q, size_t n) { return (reinterpret_cast<uintptr_t>(q) % n) == 0; };
+  bool ok = a.mask != nullptr && a.mpitch % 2 == 0 && al(a.mask, 2 * P.mesz);
+  for(const Img* im : { &a.in0, &a.in1 })
+  {
+    ok = ok && im->sx[0] == 0 && im->sy[0] == 0 && im->pitch[0] % 2 == 0 && al(im->p[0], 2 * S.esz);
+    for(int c = 1; c < 3; c++) { ok = ok && im->sx[c] == 1 && im->sy[c] == 1; }
+  }
+  a.pairs420 = ok ? 1 : 0;
 }
 
 qmiv_status masked_status(const MaskOut& o, const MaskPlan& P)
@@ -1173,6 +1287,7 @@ qmiv_status MaskedBatch::run(qmiv_ctx_s* ctx, const qmiv_params& prm0, cudaStrea
   std::vector<int32_t> all(n);
   for(int i = 0; i < n; i++) { all[i] = i; }
   MaskPack pk{};
+  pk.kscale = 128u;
   int max_w = 0, max_h = 0;
   auto pack = [&](const std::vector<int32_t>& ids, size_t first) -> int {
     const int cnt = (int)std::min(ids.size() - first, (size_t)kPackPairs);
