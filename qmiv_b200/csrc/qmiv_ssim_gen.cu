@@ -14,10 +14,12 @@
 // roundings (separate multiply and add). The window formula uses separately rounded operations in the
 // reference's order, so every window value equals the portable reference's bit for bit.
 //
-// Two window kernels, both staging the samples a CTA's windows read in shared memory, both pictures
+// Three window kernels, all staging the samples a CTA's windows read in shared memory, both pictures
 // packed (a | b << 16) after clipping and margin extension:
 //   k_ssim_gen_rows (strides 1, 2, 4): each lane evaluates K neighbouring windows of a window row and
 //     walks that row's input rows; a sample loaded once feeds every window that covers it.
+//   k_ssim_box (averaged windows at strides 1, 2, 4): running column sums and box sums of the exact
+//     integer moments.
 //   k_ssim_gen (other strides): one window per thread.
 // Window values go to the band-transposed scratch [ny / 32][nx][32] that k_ssim_rows (qmiv_ssim.cu)
 // sums in x order, one lane per window row.
@@ -347,6 +349,94 @@ __global__ void __launch_bounds__(128) k_ssim_gen_rows(const __grid_constant__ S
   }
 }
 
+// Averaged windows (regular 11x11 and block 8 / 16 / 32) at strides 1, 2 and 4 by box sums. Their five
+// moments are exact integer sums (xStructSimSTD.cpp:155-193, :420-461), so any order of the additions
+// gives the same integers and the same window values. A CTA takes 32 window columns x kBoxRows window
+// rows: it stages the samples as the tap-by-tap kernels do (margin extension, clipping), then
+//   vertical: a thread per input column walks the tile's rows with running sums of the last N rows
+//     (the arriving row added, the leaving one subtracted; R, T in 32 bits, R^2, T^2, R T in 64) and
+//     stores them for each window row in shared memory, columns by phase modulo S so that the
+//     horizontal pass reads consecutive words;
+//   horizontal: a thread per window adds the N column sums of its window and evaluates it.
+// Per window this is about S^2 row steps and N column additions instead of N^2 taps.
+constexpr int kBoxRows = 8;
+
+struct BoxSums
+{
+  uint32_t r, t;
+  uint64_t rr, tt, rt;
+};
+
+template <int N, int S>
+__global__ void __launch_bounds__(32 * kBoxRows) k_ssim_box(const __grid_constant__ SsimGenArgs a)
+{
+  extern __shared__ __align__(16) unsigned char box_smem[];
+  const SsimGenJob& Jb = a.job[blockIdx.z];
+  const int wx0 = blockIdx.x * 32, wy0 = blockIdx.y * kBoxRows;
+  if(wx0 >= Jb.nx || wy0 >= Jb.ny) { return; }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tw = (min(32, Jb.nx - wx0) - 1) * S + N;
+  const int rows = min(kBoxRows, Jb.ny - wy0);
+  const int th = (rows - 1) * S + N;
+  const int cwp = a.cw;                                       // columns per phase: ceil(31 S + N, S)
+  uint32_t* tile = reinterpret_cast<uint32_t*>(box_smem);     // [th][tw]
+  const size_t tile_words = (size_t)((kBoxRows - 1) * S + N) * (31 * S + N);
+  // column sums [window row][S * cwp], one array per moment
+  uint64_t* c_rr = reinterpret_cast<uint64_t*>(box_smem + ((tile_words * 4 + 15) & ~(size_t)15));
+  uint64_t* c_tt = c_rr + kBoxRows * S * cwp;
+  uint64_t* c_rt = c_tt + kBoxRows * S * cwp;
+  uint32_t* c_r = reinterpret_cast<uint32_t*>(c_rt + kBoxRows * S * cwp);
+  uint32_t* c_t = c_r + kBoxRows * S * cwp;
+  stage_tile(Jb, a.border, Jb.x0 + wx0 * S, Jb.y0 + wy0 * S, tw, th, warp, kBoxRows, lane, tile, tw, [](int col) { return col; });
+  __syncthreads();
+
+  const int col = threadIdx.x;
+  if(col < tw)
+  {
+    BoxSums s{ 0u, 0u, 0ull, 0ull, 0ull };
+    const int slot = (col % S) * cwp + col / S;
+    for(int r = 0; r < th; r++)
+    {
+      const uint32_t v = tile[(size_t)r * tw + col];
+      const uint32_t t = v & 0xffffu, q = v >> 16;            // t = "Tst" (a), q = "Ref" (b)
+      s.r += q; s.t += t;
+      s.rr += (uint64_t)q * q; s.tt += (uint64_t)t * t; s.rt += (uint64_t)q * t;
+      if(r >= N)
+      {
+        const uint32_t u = tile[(size_t)(r - N) * tw + col];
+        const uint32_t tu = u & 0xffffu, qu = u >> 16;
+        s.r -= qu; s.t -= tu;
+        s.rr -= (uint64_t)qu * qu; s.tt -= (uint64_t)tu * tu; s.rt -= (uint64_t)qu * tu;
+      }
+      const int e = r - (N - 1);
+      if(e >= 0 && e % S == 0)
+      {
+        const int o = (e / S) * S * cwp + slot;
+        c_r[o] = s.r; c_t[o] = s.t; c_rr[o] = s.rr; c_tt[o] = s.tt; c_rt[o] = s.rt;
+      }
+    }
+  }
+  __syncthreads();
+
+  const int wr = warp, wx = wx0 + lane;
+  if(wr < rows && wx < Jb.nx)
+  {
+    const int base = wr * S * cwp;
+    uint64_t m2[3] = { 0ull, 0ull, 0ull };
+    uint32_t m1[2] = { 0u, 0u };
+    #pragma unroll
+    for(int dx = 0; dx < N; dx++)
+    {
+      const int o = base + (dx % S) * cwp + lane + dx / S;   // column lane S + dx
+      m1[0] += c_r[o]; m1[1] += c_t[o];
+      m2[0] += c_rr[o]; m2[1] += c_tt[o]; m2[2] += c_rt[o];
+    }
+    const double m[5] = { (double)m1[0], (double)m1[1], (double)m2[0], (double)m2[1], (double)m2[2] };   // exact: < 2^53
+    const int wy = wy0 + wr;
+    Jb.win[((size_t)(wy >> 5) * Jb.nx + wx) * 32 + (wy & 31)] = gen_window<kGenAvg, N>(m, a.inv, Jb.C1, Jb.C2, Jb.calc_l != 0);
+  }
+}
+
 // 2x2 mean of both pictures of a pair for the next MS-SSIM scale (xPixelOpsSTD.cpp:50-67), after clipping
 struct DownArgs
 {
@@ -481,6 +571,35 @@ cudaError_t gen_launch_k(const SsimGenArgs& a, const GenPlan& p, int S, int maxn
   return cudaGetLastError();
 }
 
+// shared memory of k_ssim_box<N, S>: the largest tile and the column sums of kBoxRows window rows
+constexpr size_t box_smem(int N, int S)
+{
+  const size_t tile = (size_t)((kBoxRows - 1) * S + N) * (31 * S + N) * 4;
+  const size_t cwp = (size_t)(31 * S + N + S - 1) / S;
+  return ((tile + 15) & ~(size_t)15) + (size_t)kBoxRows * S * cwp * (3 * 8 + 2 * 4);
+}
+
+template <int N, int S>
+cudaError_t box_launch_s(SsimGenArgs& a, int maxnx, int maxny, cudaStream_t s)
+{
+  constexpr size_t smem = box_smem(N, S);
+  static_assert(smem <= kGenSmemMax, "box tile too large");
+  const cudaError_t e = cudaFuncSetAttribute(k_ssim_box<N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if(e != cudaSuccess) { return e; }
+  a.cw = (31 * S + N + S - 1) / S;
+  const dim3 grid((maxnx + 31) / 32, (maxny + kBoxRows - 1) / kBoxRows, a.njobs);
+  k_ssim_box<N, S><<<grid, 32 * kBoxRows, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t box_launch(SsimGenArgs& a, int S, int maxnx, int maxny, cudaStream_t s)
+{
+  if(S == 1) { return box_launch_s<N, 1>(a, maxnx, maxny, s); }
+  if(S == 2) { return box_launch_s<N, 2>(a, maxnx, maxny, s); }
+  return box_launch_s<N, 4>(a, maxnx, maxny, s);
+}
+
 }  // namespace
 
 cudaError_t launch_ssim_gen(SsimGenArgs& a, int mode, int N, int S, int border, cudaStream_t s)
@@ -499,6 +618,7 @@ cudaError_t launch_ssim_gen(SsimGenArgs& a, int mode, int N, int S, int border, 
     maxnx = max(maxnx, J.nx); maxny = max(maxny, J.ny);
   }
   a.S = S; a.border = border; a.tw = p.tw; a.th = p.th; a.cw = p.cw; a.wr = p.wr;
+  const bool box = S == 1 || S == 2 || S == 4;                      // averaged windows by box sums
   switch(mode)
   {
   case QMIV_SSM_REGULAR_GAUSSIAN_FLT:
@@ -512,6 +632,7 @@ cudaError_t launch_ssim_gen(SsimGenArgs& a, int mode, int N, int S, int border, 
   case QMIV_SSM_REGULAR_AVERAGED:
     if(N != 11) { return cudaErrorInvalidValue; }
     a.coef = 0; a.inv = 1.0 / (double)121;                          // c_InvFltrArea
+    if(box) { return box_launch<11>(a, S, maxnx, maxny, s); }
     return gen_launch_k<kGenAvg, 11>(a, p, S, maxnx, maxny, s);
   case QMIV_SSM_BLOCK_GAUSSIAN_INT:
     a.inv = 1.0 / (double)(1 << 18);
@@ -520,6 +641,9 @@ cudaError_t launch_ssim_gen(SsimGenArgs& a, int mode, int N, int S, int border, 
     return cudaErrorInvalidValue;
   case QMIV_SSM_BLOCK_AVERAGED:
     a.coef = 0; a.inv = 1.0 / (double)(N * N);                      // c_InvBlockArea
+    if(box && N == 8) { return box_launch<8>(a, S, maxnx, maxny, s); }
+    if(box && N == 16) { return box_launch<16>(a, S, maxnx, maxny, s); }
+    if(box && N == 32) { return box_launch<32>(a, S, maxnx, maxny, s); }
     if(N == 8) { return gen_launch_k<kGenAvg, 8>(a, p, S, maxnx, maxny, s); }
     if(N == 16) { return gen_launch_k<kGenAvg, 16>(a, p, S, maxnx, maxny, s); }
     if(N == 32) { return gen_launch_k<kGenAvg, 32>(a, p, S, maxnx, maxny, s); }

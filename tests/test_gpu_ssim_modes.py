@@ -54,6 +54,12 @@ def test_ssim_modes_golden_device_frames(idx, golden_ssim_modes, qctx):
     (1280, 720, 10, 420, 2, True, 4, 0, 32, 4, oracle.SSIM | oracle.IVSSIM | oracle.MSSSIM),
     (300, 200, 14, 444, 2, False, 0, 4, 11, 11, oracle.SSIM | oracle.IVSSIM),
     (256, 256, 8, 420, 1, True, 4, 0, 8, 1, oracle.ALL),
+    # averaged windows at strides 1, 2, 4 take the box-sum kernel: 14-bit samples (the largest sums),
+    # partial tiles at odd sizes, margins, MS-SSIM scales
+    (320, 180, 14, 444, 2, False, 4, 0, 32, 1, oracle.SSIM | oracle.IVSSIM),
+    (510, 254, 10, 420, 2, True, 4, 0, 16, 2, oracle.SSIM | oracle.IVSSIM),
+    (333, 111, 12, 444, 2, False, 2, 1, 11, 4, oracle.SSIM | oracle.MSSSIM),
+    (300, 170, 14, 420, 2, True, 2, 5, 11, 2, oracle.SSIM | oracle.IVSSIM),
 ])
 def test_ssim_modes_against_oracle_seeded(shape, qctx, oracle_lib):
     """Seeded synthetic frames (the bench's generator) at sizes beyond the fixtures."""
