@@ -52,17 +52,18 @@ __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a,
 
 // Kahan-Babuska-Neumaier compensated sum (libs/pmbb-core/src/xKBNS.h:36-43).
 // The reference adds to c the rounding error of s + v, computed by Fast2Sum with the larger of the
-// two operands first. That error is exactly representable and unique, so Knuth's branch-free
-// TwoSum yields the same double; here it keeps the dependent chain free of branches.
+// two operands first: (big - t) + small. Here the operands are chosen by a compare and two selects
+// instead of a branch, four FP64 additions and one FP64 compare per term (Knuth's branch-free TwoSum,
+// which yields the same exactly representable error, takes six additions).
 struct Kbns
 {
   double s = 0.0, c = 0.0;
   __device__ __forceinline__ void add(double v)
   {
-    const double t  = dadd(s, v);
-    const double bv = dsub(t, s);
-    const double e  = dadd(dsub(s, dsub(t, bv)), dsub(v, bv));
-    c = dadd(c, e);
+    const double t = dadd(s, v);
+    const bool   sb = fabs(s) >= fabs(v);
+    const double big = sb ? s : v, small = sb ? v : s;
+    c = dadd(c, dadd(dsub(big, t), small));
     s = t;
   }
   __device__ __forceinline__ double result() const { return dadd(s, c); }

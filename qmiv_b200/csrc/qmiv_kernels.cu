@@ -243,7 +243,12 @@ __device__ __forceinline__ void finalize_body(const FinalizeArgs& a, int chain, 
       }
     }
     #pragma unroll
-    for(int k = 0; k < 6; k++) { atomicAdd(&acc[k], loc[k]); }
+    for(int k = 0; k < 6; k++)
+    {
+      #pragma unroll
+      for(int o2 = 16; o2 > 0; o2 >>= 1) { loc[k] += __shfl_down_sync(0xffffffffu, loc[k], o2); }
+      if((threadIdx.x & 31) == 0) { atomicAdd(&acc[k], loc[k]); }
+    }
     __syncthreads();
     if(threadIdx.x < 6) { o->cps_sum[threadIdx.x / 3][threadIdx.x % 3] = acc[threadIdx.x]; }
     return;
@@ -253,10 +258,24 @@ __device__ __forceinline__ void finalize_body(const FinalizeArgs& a, int chain, 
   const int len = ch.kind == kChainSsim ? a.slot[ch.a].ny : a.H;
   double* vals = stage;
   double* wts = stage + len;
-  for(int y = threadIdx.x; y < len; y += blockDim.x)
+  // eight rows per thread and pass with their loads issued together (one round trip per pass)
+  constexpr int U = 8;
+  for(int y0 = threadIdx.x; y0 < len; y0 += 256 * U)
   {
-    vals[y] = chain_value(a, ch, y);
-    if(wsum) { wts[y] = a.ws[a.slot[ch.a].ws_base + a.slot[ch.a].ws_step * y]; }
+    double v[U], w[U];
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      const int y = y0 + u * 256;
+      v[u] = y < len ? chain_value(a, ch, y) : 0.0;
+      w[u] = (wsum && y < len) ? a.ws[a.slot[ch.a].ws_base + a.slot[ch.a].ws_step * y] : 0.0;
+    }
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      const int y = y0 + u * 256;
+      if(y < len) { vals[y] = v[u]; if(wsum) { wts[y] = w[u]; } }
+    }
   }
   __syncthreads();
   if(threadIdx.x != 0) { return; }

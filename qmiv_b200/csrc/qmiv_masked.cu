@@ -835,11 +835,21 @@ __device__ __forceinline__ void mask_finalize_body(const MaskArgs& a, int chain)
   {
     const int n = min(kMaskFinChunk, H - base);
     __syncthreads();                                          // the previous chunk has been summed
-    for(int i = threadIdx.x; i < n; i += blockDim.x)
+    constexpr int U = kMaskFinChunk / 256;                    // a thread's loads all in flight at once
+    uint64_t v[U];
+    double w[U];
+    #pragma unroll
+    for(int u = 0; u < U; u++)
     {
-      const uint64_t v = r[(size_t)(base + i) * step];
-      loc += v;
-      vals[i] = a.ws ? dmul((double)v, a.ws[base + i]) : 0.0;
+      const int i = threadIdx.x + u * 256;
+      v[u] = i < n ? r[(size_t)(base + i) * step] : 0ull;
+      w[u] = (i < n && a.ws) ? a.ws[base + i] : 0.0;
+    }
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      const int i = threadIdx.x + u * 256;
+      if(i < n) { loc += v[u]; vals[i] = a.ws ? dmul((double)v[u], w[u]) : 0.0; }
     }
     __syncthreads();
     if(threadIdx.x == 0 && a.ws)
@@ -848,7 +858,8 @@ __device__ __forceinline__ void mask_finalize_body(const MaskArgs& a, int chain)
       for(int i = 0; i < n; i++) { s.add(vals[i]); }
     }
   }
-  atomicAdd(&tot, loc);                                       // exact: integer sum in any order
+  loc = warp_sum_u64(loc);                                    // exact: integer sum in any order
+  if((threadIdx.x & 31) == 0) { atomicAdd(&tot, loc); }
   __syncthreads();
   if(threadIdx.x != 0) { return; }
   if(cps)
