@@ -344,7 +344,7 @@ def run_qmiv(args, world, rank, local):
         batch.wait(ta)
         batch.wait(tb)
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
+    def pipelined_ms():
         barrier(world)
         torch.cuda.synchronize()
         ev0.record(stream)
@@ -357,7 +357,12 @@ def run_qmiv(args, world, rank, local):
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
-    ms_max = max_over_ranks(ev0.elapsed_time(ev1), world, local)
+        return max_over_ranks(ev0.elapsed_time(ev1), world, local)
+
+    with ClockSampler(local) as clocks:
+        ms_max = pipelined_ms()
+    # the same timed region repeated: the spread of the measurement (the headline value is the first)
+    rep_ms = [pipelined_ms() for _ in range(5)]
 
     # ---- per-stage kernel times: the same steps with the library's stage timers (CUDA events on the
     # batch stream around every stage's launch; graphs are not replayed while the timers are on) ----
@@ -446,7 +451,11 @@ def run_qmiv(args, world, rank, local):
     h2d = sum(frame_bytes(a) + frame_bytes(b) for a, b in pairs)
     d2h = PAIRS_PER_STEP * 632  # sizeof(PairOut), the device result block read back per pair
     value_sync = units / (ms_sync / 1e3)
+    rep = sorted(units / (m / 1e3) for m in rep_ms)
+    repeats = {"n": len(rep), "steps_each": args.steps, "pairs_s": [round(v, 1) for v in rep],
+               "median": rep[len(rep) // 2], "spread": (rep[-1] - rep[0]) / rep[len(rep) // 2]}
     return dict(value=value, value_sync=value_sync, ms=ms_max / args.steps, e2e=e2e_value, stage=stage, cps_avg_ms=cps_avg_ms,
+                repeats=repeats,
                 achieved=achieved, int_peak=int_peak.value, h2d=h2d, d2h=d2h, clocks=clocks.summary(),
                 sample=results[0], launches=int(round(launches_per_step * args.steps)), plain=plain_value,
                 cps_tile=cps_tile, mixed=mixed, serve=serve, masked=masked, ssim_modes=ssim_modes, c0=c0, c2=c2)
@@ -906,6 +915,7 @@ def main():
            "clocks": r["clocks"],
            "cpu_baseline": cpu,
            "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in r["stage"].items() if v[1]},
+           "repeats": r["repeats"],
            "one_batch_in_flight": r["value_sync"],
            "plain_form": r["plain"],
            "mixed_set": r["mixed"],
