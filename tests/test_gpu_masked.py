@@ -261,3 +261,29 @@ def test_masked_staged_prepass_against_oracle(erp, qctx, oracle_lib):
         with qmiv_b200.Calc(qctx, W, H, bd, search_range=R, erp=erp) as calc:
             one, one_nnm = calc.compute_masked(f0, f1, m, 8)
         assert one == got[i] and one_nnm == n_exp, (W, H)
+
+
+@pytest.mark.gpu
+def test_masked_batched_more_pairs_than_one_pack(qctx):
+    """A batched mask-mode call passes each launch group's arguments in packs of up to 32 pairs: 40
+    pairs of two sample sizes and two search ranges (groups that span two packs and groups that fit
+    one) equal their one-pair calls."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    shapes = [(64 + 32 * (i % 3), 32 + 16 * (i % 2), 8 if i % 4 else 10, 2 if i % 5 else 3) for i in range(40)]
+    items = []
+    for i, (W, H, bd, R) in enumerate(shapes):
+        f0, f1 = synth.make_pair(W, H, bd, seed=300 + i)
+        m = det_mask(W, H, 8, 5 + i, "weights" if i % 2 else "binary")
+        if i % 3 == 0:
+            f0, f1, m = tuple(_dev(x) for x in f0), tuple(_dev(x) for x in f1), _dev(m)
+        items.append((W, H, bd, R, f0, f1, m))
+    pairs = [dict(frame0=f0, frame1=f1, width=W, height=H, bitdepth=bd, search_range=R,
+                  metrics=qmiv_b200.PSNR | qmiv_b200.WSPSNR | qmiv_b200.IVPSNR) for W, H, bd, R, f0, f1, m in items]
+    with qmiv_b200.Batch(qctx, len(pairs), sum(W * H for W, H, *_ in items), erp=True) as batch:
+        got, nnm = batch.compute_masked(pairs, [it[6] for it in items], [8] * len(items))
+    for i, (W, H, bd, R, f0, f1, m) in enumerate(items):
+        with qmiv_b200.Calc(qctx, W, H, bd, search_range=R, erp=True) as calc:
+            one, one_nnm = calc.compute_masked(f0, f1, m, 8)
+        assert got[i] == one and nnm[i] == one_nnm, (i, W, H, bd, R)
