@@ -274,7 +274,22 @@ def run_mixed(ctx, steps, int_peak):
         torch.cuda.synchronize()
         out[name] = steps * len(specs) / (time.perf_counter() - t0)
         out[name + "_results"] = r
-    assert out.pop("plain_results") == out.pop("batched_results"), "plain and batched forms differ on the mixed set"
+    assert out.pop("plain_results") == out["batched_results"], "plain and batched forms differ on the mixed set"
+    # the batched form with two calls in flight (qmiv_batch_submit / qmiv_batch_wait), as the headline runs
+    for _ in range(2):
+        ta, tb = batch.submit(descs), batch.submit(descs)
+        batch.wait(ta)
+        batch.wait(tb)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ticket = batch.submit(descs)
+    for _ in range(steps - 1):
+        nxt = batch.submit(descs)
+        assert batch.wait(ticket) == out["batched_results"], "pipelined and synchronous batches differ"
+        ticket = nxt
+    assert batch.wait(ticket) == out.pop("batched_results"), "pipelined and synchronous batches differ"
+    torch.cuda.synchronize()
+    out["two_in_flight"] = steps * len(specs) / (time.perf_counter() - t0)
     # CPS search kernel per search range: the batched form on the pairs of one R with the stage timers on
     per_r = {}
     for R in sorted({s["search_range"] for s in specs}):
@@ -292,6 +307,7 @@ def run_mixed(ctx, steps, int_peak):
     for c in calcs.values():
         c.close()
     return {"plain_pairs_s": out["plain"], "batched_pairs_s": out["batched"], "cps_by_R": per_r,
+            "batched_two_in_flight_pairs_s": out["two_in_flight"], "two_in_flight_over_plain": out["two_in_flight"] / out["plain"],
             "batched_over_plain": out["batched"] / out["plain"]}
 
 
