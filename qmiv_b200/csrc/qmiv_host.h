@@ -7,6 +7,7 @@
 #include <mutex>
 #include <string>
 #include <memory>
+#include <map>
 #include <vector>
 
 struct qmiv_ctx_s
@@ -270,9 +271,10 @@ public:
 
 private:
   DevMem arena_;
-  void*  h_ = nullptr;        // pinned mirror of the argument tables and the results
+  void*  h_ = nullptr;        // pinned block of the results
   size_t h_bytes_ = 0;
   StageClock clock_;
+  std::map<std::pair<int32_t, int32_t>, DevMem> ws_dev_;   // ERP row weights by (height, latitude range)
 };
 
 class MaskedPipeline

@@ -29,6 +29,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <vector>
 
@@ -985,6 +986,25 @@ double psnr_masked(double ssd, int32_t nnm, int32_t bitdepth_pic, int32_t bitdep
 }  // namespace
 
 // ---- host side, shared by the one-pair call and the batched form ---------------------------------
+// ERP row weights and their correction for one height and latitude range (xWeightedSpherically.cpp:13-29),
+// computed once per process: mask-mode calls plan every call, and the weights depend on these two only.
+void ws_weights_cached(int32_t H, int32_t lat_range, std::vector<double>& w, double& correction)
+{
+  static std::mutex mu;
+  static std::map<std::pair<int32_t, int32_t>, std::pair<std::vector<double>, double>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(std::make_pair(H, lat_range));
+  if(it == cache.end())
+  {
+    if(cache.size() >= 64) { cache.clear(); }
+    std::pair<std::vector<double>, double> v;
+    ws_weights(H, lat_range, v.first, v.second);
+    it = cache.emplace(std::make_pair(H, lat_range), std::move(v)).first;
+  }
+  w = it->second.first;
+  correction = it->second.second;
+}
+
 qmiv_status plan_masked(const Shape& S, const qmiv_params& prm, const qmiv_frame* mask, int32_t mask_bitdepth, MaskPlan& P)
 {
   if(mask_bitdepth < 8 || mask_bitdepth > 14) { return fail(QMIV_ERR_INVALID_ARG, "mask bit depth must be in 8..14"); }
@@ -1014,7 +1034,7 @@ qmiv_status plan_masked(const Shape& S, const qmiv_params& prm, const qmiv_frame
           dmax2 < ((int64_t)1 << 24);
   P.ws.clear();
   P.ws_corr = 1.0;
-  if(prm.erp) { ws_weights(S.H, prm.lat_range_deg, P.ws, P.ws_corr); }
+  if(prm.erp) { ws_weights_cached(S.H, prm.lat_range_deg, P.ws, P.ws_corr); }
   return QMIV_OK;
 }
 
@@ -1237,7 +1257,7 @@ qmiv_status MaskedBatch::run(qmiv_ctx_s* ctx, const qmiv_params& prm0, cudaStrea
 {
   std::vector<MaskPlan> P(n);
   size_t off_out = 0, off_rows = malign(sizeof(MaskOut) * n), cur = 0;
-  std::vector<size_t> o_rows(n), o_ws(n), o_stage(n), o_mstage(n);
+  std::vector<size_t> o_rows(n), o_stage(n), o_mstage(n);
   cur = off_rows;
   for(int i = 0; i < n; i++)
   {
@@ -1253,7 +1273,6 @@ qmiv_status MaskedBatch::run(qmiv_ctx_s* ctx, const qmiv_params& prm0, cudaStrea
     QMIV_TRY(validate_params(prm));
     QMIV_TRY(plan_masked(S, prm, &masks[i], mask_bitdepths[i], P[i]));
     o_rows[i] = cur; cur += malign(sizeof(uint64_t) * 9 * S.H);
-    o_ws[i] = cur; cur += prm.erp ? malign(sizeof(double) * S.H) : 0;
     const bool host = d.in0.mem == QMIV_MEM_HOST || d.in1.mem == QMIV_MEM_HOST;
     o_stage[i] = cur; cur += host ? malign(2 * S.staged_frame_bytes()) : 0;
     o_mstage[i] = cur; cur += masks[i].mem == QMIV_MEM_HOST ? malign((size_t)S.W * P[i].mesz * S.H) : 0;
@@ -1285,8 +1304,18 @@ qmiv_status MaskedBatch::run(qmiv_ctx_s* ctx, const qmiv_params& prm0, cudaStrea
     MaskArgs& a = hargs[i];
     a = MaskArgs{};
     QMIV_TRY(resolve_mask(p, &masks[i], dbase + o_mstage[i], a, s));
-    double* ws = reinterpret_cast<double*>(dbase + o_ws[i]);
-    if(p.prm.erp) { QMIV_CUDA(cudaMemcpyAsync(ws, p.ws.data(), sizeof(double) * S.H, cudaMemcpyHostToDevice, s)); }
+    // ERP row weights: one device copy per (height, latitude range), uploaded on first use
+    double* ws = nullptr;
+    if(p.prm.erp)
+    {
+      DevMem& wd = ws_dev_[std::make_pair(S.H, p.prm.lat_range_deg)];
+      if(!wd.p)
+      {
+        QMIV_TRY(wd.alloc(ctx, sizeof(double) * S.H));
+        QMIV_CUDA(cudaMemcpy(wd.p, p.ws.data(), sizeof(double) * S.H, cudaMemcpyHostToDevice));
+      }
+      ws = wd.as<double>();
+    }
     fill_mask_args(p, a0, a1, reinterpret_cast<uint64_t*>(dbase + o_rows[i]), ws,
                    reinterpret_cast<MaskOut*>(dbase + off_out) + i, a);
     const int t = (int)S.esz, tm = (int)p.mesz;
