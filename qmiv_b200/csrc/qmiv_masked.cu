@@ -921,11 +921,28 @@ __global__ void __launch_bounds__(256) k_mask_finalize_multi(const __grid_consta
   mask_finalize_body(pk.a[blockIdx.x / 9], blockIdx.x % 9);
 }
 
+// A kernel's dynamic shared-memory limit, set once per kernel and device (not on every launch)
+template <typename F>
+cudaError_t smem_attr_once(F* fn, int bytes)
+{
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, bool> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess) { return e; }
+  std::lock_guard<std::mutex> lk(mu);
+  bool& d = done[std::make_pair(reinterpret_cast<const void*>(fn), dev)];
+  if(d) { return cudaSuccess; }
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if(e == cudaSuccess) { d = true; }
+  return e;
+}
+
 template <typename T, typename TM, int R>
 cudaError_t launch_masked_key(const MaskArgs& a, cudaStream_t s)
 {
   constexpr size_t smem = MaskKeyGeo<R>::kSmem;
-  const cudaError_t e = cudaFuncSetAttribute(k_cps_masked_key<T, TM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const cudaError_t e = smem_attr_once(k_cps_masked_key<T, TM, R>, (int)smem);
   if(e != cudaSuccess) { return e; }
   const dim3 grid((a.W + MaskKeyGeo<R>::TW - 1) / MaskKeyGeo<R>::TW, (a.H + MaskKeyGeo<R>::TH - 1) / MaskKeyGeo<R>::TH);
   k_cps_masked_key<T, TM, R><<<grid, 512, smem, s>>>(a);
@@ -1208,7 +1225,7 @@ cudaError_t launch_search_group_r(const MaskPack& pk, int count, int max_w, int 
   if(key)
   {
     using G = MaskKeyGeo<R>;
-    const cudaError_t e = cudaFuncSetAttribute(k_cps_masked_key_multi<T, TM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::kSmem);
+    const cudaError_t e = smem_attr_once(k_cps_masked_key_multi<T, TM, R>, (int)G::kSmem);
     if(e != cudaSuccess) { return e; }
     const dim3 grid((max_w + G::TW - 1) / G::TW, (max_h + G::TH - 1) / G::TH, count);
     k_cps_masked_key_multi<T, TM, R><<<grid, 512, G::kSmem, s>>>(pk);

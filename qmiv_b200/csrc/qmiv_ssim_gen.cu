@@ -584,8 +584,22 @@ cudaError_t box_launch_s(SsimGenArgs& a, int maxnx, int maxny, cudaStream_t s)
 {
   constexpr size_t smem = box_smem(N, S);
   static_assert(smem <= kGenSmemMax, "box tile too large");
-  const cudaError_t e = cudaFuncSetAttribute(k_ssim_box<N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if(e != cudaSuccess) { return e; }
+  {
+    // the shared-memory limit, once per device
+    static std::mutex mu;
+    static uint64_t done = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if(e != cudaSuccess) { return e; }
+    const uint64_t bit = 1ULL << (dev & 63);
+    std::lock_guard<std::mutex> lk(mu);
+    if(!(done & bit))
+    {
+      e = cudaFuncSetAttribute(k_ssim_box<N, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if(e != cudaSuccess) { return e; }
+      done |= bit;
+    }
+  }
   a.cw = (31 * S + N + S - 1) / S;
   const dim3 grid((maxnx + 31) / 32, (maxny + kBoxRows - 1) / kBoxRows, a.njobs);
   k_ssim_box<N, S><<<grid, 32 * kBoxRows, smem, s>>>(a);
