@@ -287,3 +287,40 @@ def test_masked_batched_more_pairs_than_one_pack(qctx):
         with qmiv_b200.Calc(qctx, W, H, bd, search_range=R, erp=True) as calc:
             one, one_nnm = calc.compute_masked(f0, f1, m, 8)
         assert got[i] == one and nnm[i] == one_nnm, (i, W, H, bd, R)
+
+
+@pytest.mark.gpu
+def test_masked_stage_timers(qctx):
+    """With the context's profiling on, a mask-mode call (one pair, then a batch of three) times each of
+    its stages once per call on the stream it runs on: prepass, reduce, search, finalize and read-back."""
+    import qmiv_b200
+    from qmiv_b200 import synth
+    from detgen import det_mask
+    W, H = 320, 192
+    f0, f1 = synth.make_pair(W, H, 10, seed=41)
+    m = det_mask(W, H, 8, 3, "weights")
+    stages = ("prepass", "reduce", "cps", "finalize", "d2h")
+    with qmiv_b200.Calc(qctx, W, H, 10, search_range=2, erp=True) as calc:
+        calc.compute_masked(f0, f1, m, 8)
+        qctx.stage_times(reset=True)
+        qctx.set_profiling(True)
+        try:
+            calc.compute_masked(f0, f1, m, 8)
+        finally:
+            qctx.set_profiling(False)
+        st = qctx.stage_times(reset=True)
+    for k in stages:
+        assert st[k][1] == 1 and st[k][0] > 0.0, (k, st[k])
+    pairs = [dict(frame0=f0, frame1=f1, width=W, height=H, bitdepth=10, search_range=2,
+                  metrics=qmiv_b200.PSNR | qmiv_b200.WSPSNR | qmiv_b200.IVPSNR)] * 3
+    with qmiv_b200.Batch(qctx, 3, 3 * W * H, erp=True) as batch:
+        batch.compute_masked(pairs, [m] * 3, [8] * 3)
+        qctx.stage_times(reset=True)
+        qctx.set_profiling(True)
+        try:
+            batch.compute_masked(pairs, [m] * 3, [8] * 3)
+        finally:
+            qctx.set_profiling(False)
+        st = qctx.stage_times(reset=True)
+    for k in stages:
+        assert st[k][1] == 1 and st[k][0] > 0.0, (k, st[k])
