@@ -315,6 +315,21 @@ __device__ __forceinline__ void ld_grp(const uint8_t* l0, const uint8_t* l1, con
   r.m = __ldg(reinterpret_cast<const uint32_t*>(mr + 4 * g));
 }
 
+// a row's luma of both frames and its mask for group g (the chroma words are the row pair's, loaded once)
+__device__ __forceinline__ void ld_luma_mask(const uint16_t* l0, const uint16_t* l1, const uint8_t* mr, int g, Grp16& r)
+{
+  const uint2 a = __ldg(reinterpret_cast<const uint2*>(l0 + 4 * g)), b = __ldg(reinterpret_cast<const uint2*>(l1 + 4 * g));
+  r.l0[0] = a.x; r.l0[1] = a.y; r.l1[0] = b.x; r.l1[1] = b.y;
+  r.m = __ldg(reinterpret_cast<const uint32_t*>(mr + 4 * g));
+}
+__device__ __forceinline__ void ld_luma_mask(const uint8_t* l0, const uint8_t* l1, const uint8_t* mr, int g, Grp16& r)
+{
+  const uint32_t a = __ldg(reinterpret_cast<const uint32_t*>(l0 + 4 * g)), b = __ldg(reinterpret_cast<const uint32_t*>(l1 + 4 * g));
+  r.l0[0] = __byte_perm(a, 0u, 0x4140u); r.l0[1] = __byte_perm(a, 0u, 0x4342u);
+  r.l1[0] = __byte_perm(b, 0u, 0x4140u); r.l1[1] = __byte_perm(b, 0u, 0x4342u);
+  r.m = __ldg(reinterpret_cast<const uint32_t*>(mr + 4 * g));
+}
+
 // The differences of two clipped 16-bit pairs below 2^15: the 32-bit difference of the words holds the
 // low difference in its low half (two's complement) and the high difference times 2^16 once the low one
 // is taken off.
@@ -392,6 +407,40 @@ __device__ __forceinline__ void grp_wide(const Grp16& g, uint32_t clip, int64_t 
   }
 }
 
+// grp_narrow for the two rows of a row pair sharing their chroma words: the chroma differences once,
+// each row's terms with its own mask sums, each row's SSD apart.
+template <bool CLIP>
+__device__ __forceinline__ void grp_pair_narrow(const Grp16 (&g)[2], uint32_t clip2, int32_t sd[3], uint64_t (*ssd)[3],
+                                                uint32_t difw[3], uint32_t& nnm)
+{
+  uint32_t ms[2][2];
+  #pragma unroll
+  for(int r = 0; r < 2; r++)
+  {
+    const uint32_t m = g[r].m;
+    const uint32_t mm[4] = { m & 0xffu, (m >> 8) & 0xffu, (m >> 16) & 0xffu, m >> 24 };
+    ms[r][0] = mm[0] + mm[1]; ms[r][1] = mm[2] + mm[3];
+    nnm += __popc((((m & 0x7f7f7f7fu) + 0x7f7f7f7fu) | m) & 0x80808080u);    // non-zero mask bytes
+    #pragma unroll
+    for(int k = 0; k < 2; k++)
+    {
+      uint32_t dw; int32_t dlo, dhi;
+      pair_diff<CLIP>(g[r].l0[k], g[r].l1[k], clip2, dw, dlo, dhi);
+      difw[0] |= dw;
+      word_terms(dlo, dhi, mm[2 * k], mm[2 * k + 1], sd[0], ssd[r][0]);
+    }
+  }
+  #pragma unroll
+  for(int p = 0; p < 2; p++)
+  {
+    uint32_t dw; int32_t dlo, dhi;
+    pair_diff<CLIP>(g[0].c0[p], g[0].c1[p], clip2, dw, dlo, dhi);
+    difw[1 + p] |= dw;
+    #pragma unroll
+    for(int r = 0; r < 2; r++) { word_terms(dlo, dhi, ms[r][0], ms[r][1], sd[1 + p], ssd[r][1 + p]); }
+  }
+}
+
 // 4:2:0 rows as in mask_prepass420v_body with an 8-bit mask: four groups of four pixels per thread and
 // step, all loads issued first, the OR of the samples kept on the pairs, the terms by grp_narrow unless
 // the step holds an unclipped sample of 2^15 or more (then grp_wide). The sums are the same integers.
@@ -451,15 +500,149 @@ __device__ __forceinline__ void mask_prepass420n_body(const MaskArgs& a, int row
   mask_prepass_row_tail(a, y, sd, ssd, nnm, dif, mx0, mx1);
 }
 
+// The sums of a row pair leave the CTA: warp sums meet in shared memory, one thread writes both rows'
+// SSD and adds the totals (called by all 256 threads).
+__device__ __forceinline__ void mask_prepass_pair_tail(const MaskArgs& a, int y0, int64_t sd[3], uint64_t ssd[2][3],
+                                                       uint32_t nnm, uint32_t dif, uint32_t mx0, uint32_t mx1)
+{
+  __shared__ uint64_t red[8][9];
+  __shared__ uint32_t redu[8][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t v[9];
+  #pragma unroll
+  for(int c = 0; c < 3; c++) { v[c] = (uint64_t)sd[c]; v[3 + c] = ssd[0][c]; v[6 + c] = ssd[1][c]; }
+  #pragma unroll
+  for(int k = 0; k < 9; k++) { v[k] = warp_sum_u64(v[k]); }
+  nnm = __reduce_add_sync(0xffffffffu, nnm);
+  dif = __reduce_or_sync(0xffffffffu, dif);
+  mx0 = __reduce_or_sync(0xffffffffu, mx0);
+  mx1 = __reduce_or_sync(0xffffffffu, mx1);
+  if(lane == 0)
+  {
+    #pragma unroll
+    for(int k = 0; k < 9; k++) { red[warp][k] = v[k]; }
+    redu[warp][0] = nnm; redu[warp][1] = dif; redu[warp][2] = mx0; redu[warp][3] = mx1;
+  }
+  __syncthreads();
+  if(threadIdx.x != 0) { return; }
+  uint64_t t[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+  nnm = 0; dif = 0; mx0 = 0; mx1 = 0;
+  #pragma unroll
+  for(int w = 0; w < 8; w++)
+  {
+    #pragma unroll
+    for(int k = 0; k < 9; k++) { t[k] += red[w][k]; }
+    nnm += redu[w][0]; dif |= redu[w][1]; mx0 |= redu[w][2]; mx1 |= redu[w][3];
+  }
+  MaskOut* o = a.out;
+  #pragma unroll
+  for(int c = 0; c < 3; c++)
+  {
+    a.row_ssd[(size_t)c * a.H + y0] = t[3 + c];
+    a.row_ssd[(size_t)c * a.H + y0 + 1] = t[6 + c];
+    atomicAdd(reinterpret_cast<unsigned long long*>(&o->sd[c]), (unsigned long long)t[c]);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&o->ssd[c]), (unsigned long long)(t[3 + c] + t[6 + c]));
+    if(dif & (1u << c)) { atomicOr(&o->differs[c], 1u); }
+  }
+  atomicAdd(&o->nnm, (int32_t)nnm);
+  atomicOr(&o->or_sample[0], mx0);
+  atomicOr(&o->or_sample[1], mx1);
+}
+
+// Luma rows 2 pr and 2 pr + 1 of an 8-bit-mask 4:2:0 picture (its height is even) in one CTA: the chroma
+// row under both is read once and its differences formed once, each row's chroma terms taking that
+// row's pixel-pair mask sums; two group columns per thread and step, all loads issued first. Each row
+// keeps its own SSD; the sums are the same integers as the one-row forms'.
+template <typename T>
+__device__ __forceinline__ void mask_prepass420p_body(const MaskArgs& a, int pr)
+{
+  constexpr int U = 2;
+  const int y0 = 2 * pr;
+  const int ng = a.W >> 2;
+  const T* const chs0[2] = { static_cast<const T*>(a.in0.p[1]) + (size_t)pr * a.in0.pitch[1],
+                             static_cast<const T*>(a.in0.p[2]) + (size_t)pr * a.in0.pitch[2] };
+  const T* const chs1[2] = { static_cast<const T*>(a.in1.p[1]) + (size_t)pr * a.in1.pitch[1],
+                             static_cast<const T*>(a.in1.p[2]) + (size_t)pr * a.in1.pitch[2] };
+  const T* lr0[2];
+  const T* lr1[2];
+  const uint8_t* mr[2];
+  #pragma unroll
+  for(int r = 0; r < 2; r++)
+  {
+    lr0[r] = static_cast<const T*>(a.in0.p[0]) + (size_t)(y0 + r) * a.in0.pitch[0];
+    lr1[r] = static_cast<const T*>(a.in1.p[0]) + (size_t)(y0 + r) * a.in1.pitch[0];
+    mr[r] = static_cast<const uint8_t*>(a.mask) + (size_t)(y0 + r) * a.mpitch;
+  }
+  const uint32_t clip2 = a.clip | (a.clip << 16);
+  const bool chk = sizeof(T) == 2 && a.clip >= 0x8000u;       // unclipped 16-bit samples may reach 2^15
+  const bool clip_on = a.clip < (sizeof(T) == 1 ? 0xffu : 0xffffu);
+  int64_t  sd[3] = { 0, 0, 0 };
+  uint64_t ssd[2][3] = { { 0, 0, 0 }, { 0, 0, 0 } };
+  uint32_t difw[3] = { 0, 0, 0 };
+  uint32_t nnm = 0, mxw0 = 0, mxw1 = 0;
+  for(int gb = threadIdx.x; gb < ng; gb += 256 * U)
+  {
+    Grp16 g[U][2];                                            // [group column][row]; the chroma words alike in both rows
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      const int gc = min(gb + u * 256, ng - 1);               // past the row: repeats, skipped below
+      ld_grp(lr0[0], lr1[0], chs0, chs1, mr[0], gc, g[u][0]);
+      g[u][1].c0[0] = g[u][0].c0[0]; g[u][1].c0[1] = g[u][0].c0[1];
+      g[u][1].c1[0] = g[u][0].c1[0]; g[u][1].c1[1] = g[u][0].c1[1];
+      ld_luma_mask(lr0[1], lr1[1], mr[1], gc, g[u][1]);
+    }
+    #pragma unroll
+    for(int u = 0; u < U; u++)
+    {
+      if(gb + u * 256 >= ng) { continue; }
+      grp_or(g[u][0], mxw0, mxw1);
+      mxw0 |= g[u][1].l0[0] | g[u][1].l0[1];
+      mxw1 |= g[u][1].l1[0] | g[u][1].l1[1];
+    }
+    if(chk && ((mxw0 | mxw1) & 0x80008000u) != 0)
+    {
+      #pragma unroll
+      for(int u = 0; u < U; u++)
+      {
+        if(gb + u * 256 >= ng) { continue; }
+        grp_wide(g[u][0], a.clip, sd, ssd[0], difw, nnm);
+        grp_wide(g[u][1], a.clip, sd, ssd[1], difw, nnm);
+      }
+      continue;
+    }
+    int32_t s32[3] = { 0, 0, 0 };
+    if(clip_on)
+    {
+      #pragma unroll
+      for(int u = 0; u < U; u++) { if(gb + u * 256 < ng) { grp_pair_narrow<true>(g[u], clip2, s32, ssd, difw, nnm); } }
+    }
+    else
+    {
+      #pragma unroll
+      for(int u = 0; u < U; u++) { if(gb + u * 256 < ng) { grp_pair_narrow<false>(g[u], clip2, s32, ssd, difw, nnm); } }
+    }
+    #pragma unroll
+    for(int c = 0; c < 3; c++) { sd[c] += s32[c]; }
+  }
+  const uint32_t dif = (difw[0] != 0 ? 1u : 0u) | (difw[1] != 0 ? 2u : 0u) | (difw[2] != 0 ? 4u : 0u);
+  const uint32_t mx0 = (mxw0 & 0xffffu) | (mxw0 >> 16), mx1 = (mxw1 & 0xffffu) | (mxw1 >> 16);
+  mask_prepass_pair_tail(a, y0, sd, ssd, nnm, dif, mx0, mx1);
+}
+
 constexpr int kPackPairs = 32;                                 // frame pairs per batched launch
 
-// The vector-load prepass: the narrow form for 8-bit masks, the sample-by-sample one otherwise.
+// The vector-load prepass: row pairs for 8-bit masks, sample by sample one row per CTA otherwise.
+// idx: the row pair (8-bit masks) or the row.
 template <typename T, typename TM>
-__device__ __forceinline__ void mask_prepass420_body(const MaskArgs& a, int row)
+__device__ __forceinline__ void mask_prepass420_body(const MaskArgs& a, int idx)
 {
-  if constexpr(sizeof(TM) == 1) { mask_prepass420n_body<T>(a, row); }
-  else { mask_prepass420v_body<T, TM>(a, row); }
+  if constexpr(sizeof(TM) == 1) { mask_prepass420p_body<T>(a, idx); }
+  else { mask_prepass420v_body<T, TM>(a, idx); }
 }
+// CTAs of the vector-load prepass for a picture of H rows
+template <typename TM>
+__host__ __device__ inline int prepass420_units(int H) { return sizeof(TM) == 1 ? H / 2 : H; }
 
 // The vector loads of k_mask_prepass420v need 4:2:0, a width divisible by 4, luma rows of both frames
 // and mask rows starting on 4-sample boundaries and chroma rows on 2-sample boundaries.
@@ -876,7 +1059,7 @@ __device__ __forceinline__ void mask_finalize_body(const MaskArgs& a, int chain)
 template <typename T, typename TM>
 __global__ void __launch_bounds__(256) k_mask_prepass(const __grid_constant__ MaskArgs a) { mask_prepass_body<T, TM>(a, blockIdx.x); }
 template <typename T, typename TM>
-__global__ void __launch_bounds__(256, 3) k_mask_prepass420v(const __grid_constant__ MaskArgs a) { mask_prepass420_body<T, TM>(a, blockIdx.x); }
+__global__ void __launch_bounds__(256, 2) k_mask_prepass420v(const __grid_constant__ MaskArgs a) { mask_prepass420_body<T, TM>(a, blockIdx.x); }
 __global__ void k_mask_reduce(const __grid_constant__ MaskArgs a) { mask_reduce_body(a); }
 template <typename T, typename TM, int R>
 __global__ void __launch_bounds__(256) k_cps_masked(const __grid_constant__ MaskArgs a) { cps_masked_body<T, TM, R>(a, blockIdx.x, blockIdx.y, blockIdx.z); }
@@ -895,10 +1078,10 @@ static_assert(sizeof(MaskPack) <= 32000, "kernel parameters are limited to 32 KB
 
 // vec: the group's pairs take the vector-load prepass
 template <typename T, typename TM, bool VEC>
-__global__ void __launch_bounds__(256, 3) k_mask_prepass_multi(const __grid_constant__ MaskPack pk)
+__global__ void __launch_bounds__(256, 2) k_mask_prepass_multi(const __grid_constant__ MaskPack pk)
 {
   const MaskArgs& a = pk.a[blockIdx.y];
-  if((int)blockIdx.x >= a.H) { return; }
+  if((int)blockIdx.x >= (VEC ? prepass420_units<TM>(a.H) : a.H)) { return; }
   if(VEC) { mask_prepass420_body<T, TM>(a, blockIdx.x); } else { mask_prepass_body<T, TM>(a, blockIdx.x); }
 }
 __global__ void k_mask_reduce_multi(const __grid_constant__ MaskPack pk) { mask_reduce_body(pk.a[blockIdx.x]); }
@@ -954,7 +1137,7 @@ template <typename T, typename TM>
 cudaError_t launch_masked_t(const MaskArgs& a, int R, bool key, PairPipeline& pipe, cudaStream_t s)
 {
   int tok = pipe.prof_begin(s);
-  if(mask_prepass_vec_ok(a, sizeof(T), sizeof(TM))) { k_mask_prepass420v<T, TM><<<a.H, 256, 0, s>>>(a); }
+  if(mask_prepass_vec_ok(a, sizeof(T), sizeof(TM))) { k_mask_prepass420v<T, TM><<<prepass420_units<TM>(a.H), 256, 0, s>>>(a); }
   else { k_mask_prepass<T, TM><<<a.H, 256, 0, s>>>(a); }
   pipe.prof_end(s, QMIV_STAGE_PREPASS, tok);
   tok = pipe.prof_begin(s);
@@ -1213,7 +1396,7 @@ inline size_t malign(size_t v) { return (v + kMaskAlign - 1) & ~(kMaskAlign - 1)
 template <typename T, typename TM>
 cudaError_t launch_prepass_group(const MaskPack& pk, int count, int max_h, int form, cudaStream_t s)
 {
-  const dim3 grid(max_h, count);
+  const dim3 grid(form == 1 ? prepass420_units<TM>(max_h) : max_h, count);
   if(form == 1) { k_mask_prepass_multi<T, TM, true><<<grid, 256, 0, s>>>(pk); }
   else { k_mask_prepass_multi<T, TM, false><<<grid, 256, 0, s>>>(pk); }
   return cudaSuccess;
