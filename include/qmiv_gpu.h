@@ -307,8 +307,8 @@ QMIV_API qmiv_status qmiv_batch_compute(qmiv_batch batch, const qmiv_pair_desc* 
    (apps/QMIV/src/xAppQMIV.cpp:900-1030; the reference runs them one frame at a time). pairs[i] as for
    qmiv_batch_compute, whose metric_mask may hold QMIV_PSNR, QMIV_WSPSNR and QMIV_IVPSNR; masks[i] the
    luma plane of pair i's mask picture (plane[0], pitch[0], mem; 1-byte samples for mask_bitdepths[i]
-   = 8, 2-byte above, up to 14). Every stage runs as one launch per group of pairs with the same sample
-   sizes and search range; each result equals qmiv_frame_pair_compute_masked's for that pair.
+   = 8, 2-byte above, up to 14). Every stage runs as one launch per group of up to 32 pairs with the
+   same sample sizes and search range; each result equals qmiv_frame_pair_compute_masked's for that pair.
    num_non_masked may be NULL. Returns the first failing pair's status (the others' results are still
    filled). Blocks until the results are on the host. */
 QMIV_API qmiv_status qmiv_batch_compute_masked(qmiv_batch batch, const qmiv_pair_desc* pairs, const qmiv_frame* masks,
