@@ -5,15 +5,16 @@
 //   k_mask_prepass   one CTA per 4:4:4 row: sum of (In1 - In0) * M (GCD-M), sum of (In1 - In0)^2 * M
 //                    per row (PSNR-M, WS-PSNR-M), non-zero mask samples, exactness, samples above the
 //                    maximum (the OR of all samples exceeds 2^bd - 1 exactly when one sample does);
-//                    k_mask_prepass420v the same for aligned 4:2:0 frames with vector loads
+//                    k_mask_prepass420v the same for aligned 4:2:0 frames with vector loads, one CTA
+//                    per luma row pair under an 8-bit mask (the shared chroma row read once)
 //   k_mask_reduce    GCD-M (xGlobClrDiff.cpp:60-91): IEEE divide by NumNonMasked * MaskMax,
 //                    round half away, clip
 //   k_cps_masked     the masked search (xCorrespPixelShiftSTD.cpp:151-215), both directions: masked
 //                    test pixels and masked candidates are skipped, the winner's squared differences
 //                    are weighted by the test pixel's mask value and summed per row in uint64;
-//                    k_cps_masked_key is the same search by exact integer keys, both directions
-//                    per CTA, four pixels per thread, where the bit depth, weights and GCD range
-//                    bound every error
+//                    k_cps_masked_key is the same search by exact fp32 keys, both directions per
+//                    CTA, four pixels per thread, where the bit depth, weights and GCD range bound
+//                    every error
 //   k_mask_finalize  the ordered compensated sums (xKBNS.h:36-43) of the ERP row weights and the
 //                    row totals, one CTA per chain (terms staged in shared memory, one thread sums)
 // dB values, exact-component fake values and the picture averages are formed on the host in
