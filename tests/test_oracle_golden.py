@@ -206,3 +206,28 @@ def test_ssim_mode_refusals(oracle_lib):
                 (0, 6, 11, 1)]:
         with pytest.raises(RuntimeError):
             oracle_lib.compute_pair_ssim(p, f0, f1, *cfg, mask=oracle.SSIM)
+
+
+def test_oracle_masked_ssd_wraps_like_the_reference(oracle_lib):
+    """The reference forms a masked squared difference as an int32 product that wraps (two's
+    complement) before widening to 64 bits (xDistortionSTD.cpp:62). The C restatement does the same in
+    defined arithmetic: one luma difference of 50000 (its square above 2^31) gives the SSD of the wrapped
+    product read as uint64, checked through PSNR-M = K - 10 log10(SSD) with K taken from a difference
+    of 46340, whose square does not wrap."""
+    import math
+    import numpy as np
+    W, H = 16, 8
+    p = oracle.make_params(W, H, 10, 420, search_range=1, erp=False)
+    m = np.ones((H, W), np.uint8)
+
+    def psnr_y(d):
+        f0 = tuple(np.zeros((h, w), np.uint16) for h, w in ((H, W), (H // 2, W // 2), (H // 2, W // 2)))
+        f1 = tuple(np.array(pl, copy=True) for pl in f0)
+        f1[0][2, 3] = d
+        r, _ = oracle_lib.compute_pair_masked(p, f0, f1, m, 8)
+        return r["psnr"][0]
+
+    k = psnr_y(46340) + 10.0 * math.log10(46340 * 46340)
+    sq = (50000 * 50000) & 0xffffffff                          # the int32 product's bits
+    wrapped = (sq - (1 << 32)) % (1 << 64) if sq >= (1 << 31) else sq   # sign-extended, read as uint64
+    assert math.isclose(psnr_y(50000), k - 10.0 * math.log10(wrapped), rel_tol=1e-12, abs_tol=1e-9)
