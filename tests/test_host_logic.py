@@ -138,3 +138,41 @@ def test_masked_integer_keys_order_like_int32_errors(bd, w, g, R):
     hi = (v >> np.uint64(16)).sum(1)
     assert lo.max() < (1 << 32) and hi.max() < (1 << 32)
     assert np.array_equal((hi << np.uint64(16)) + lo, v.sum(1))
+
+
+def test_pair_difference_decomposition():
+    """The mask prepass forms two sample differences from one 32-bit subtraction of 16-bit pairs below
+    2^15: the low half of the word difference, sign-extended, is the low difference, and the rest
+    shifted down (arithmetically) is the high one; the word difference is zero exactly when both are."""
+    import numpy as np
+    rng = np.random.default_rng(11)
+    v = rng.integers(0, 1 << 15, size=(200000, 4), dtype=np.int64)
+    v[:8] = [[0, 0, 0, 0], [0x7fff, 0, 0, 0x7fff], [0, 0x7fff, 0x7fff, 0], [5, 5, 5, 5],
+             [0x7fff, 0x7fff, 0, 0], [0, 0, 0x7fff, 0x7fff], [1, 0, 0, 1], [0, 1, 1, 0]]
+    w0 = v[:, 0] | (v[:, 1] << 16)
+    w1 = v[:, 2] | (v[:, 3] << 16)
+    dw = (w1 - w0) & 0xffffffff
+    dlo = ((dw & 0xffff) ^ 0x8000) - 0x8000
+    rest = (dw - dlo) & 0xffffffff
+    dhi = np.where(rest >= (1 << 31), rest - (1 << 32), rest) >> 16
+    assert np.array_equal(dlo, v[:, 2] - v[:, 0])
+    assert np.array_equal(dhi, v[:, 3] - v[:, 1])
+    assert np.array_equal(dw == 0, (v[:, 2] == v[:, 0]) & (v[:, 3] == v[:, 1]))
+
+
+def test_row_sum_split_of_squared_terms():
+    """The masked key search sums 32 terms d^2 M below 2^38 per row and component with 32-bit warp
+    reductions: the parts from bit 11 up stay below 2^27 (their sum below 2^32) and two low 11-bit parts
+    share one word (each sum below 2^16); the recombined sums are exact."""
+    import numpy as np
+    rng = np.random.default_rng(12)
+    for _ in range(200):
+        t = rng.integers(0, 1 << 38, size=(32, 2), dtype=np.uint64)
+        t[rng.integers(0, 32)] = (1 << 38) - 1
+        hi = (t >> np.uint64(11)).sum(axis=0)
+        lo_a, lo_b = (t[:, 0] & np.uint64(0x7ff)), (t[:, 1] & np.uint64(0x7ff))
+        packed = (lo_a | (lo_b << np.uint64(16))).sum()
+        assert int(hi.max()) < (1 << 32) and int(packed) < (1 << 32)
+        lo = [int(packed) & 0xffff, int(packed) >> 16]
+        for k in range(2):
+            assert (int(hi[k]) << 11) + lo[k] == int(t[:, k].sum())
