@@ -176,3 +176,40 @@ def test_row_sum_split_of_squared_terms():
         lo = [int(packed) & 0xffff, int(packed) >> 16]
         for k in range(2):
             assert (int(hi[k]) << 11) + lo[k] == int(t[:, k].sum())
+
+
+def test_fast2sum_with_select_equals_twosum_and_the_reference_branch():
+    """The compensated sums add the rounding error of s + v formed as (big - t) + small with the larger
+    operand chosen by a compare (xKBNS.h:36-43 branches on |s| >= |v|); Knuth's TwoSum yields the same
+    exactly representable error. Over mixed magnitudes, signs, ties and cancellations, both errors and
+    whole ordered sums agree bit for bit (IEEE double, round to nearest)."""
+    import numpy as np
+    rng = np.random.default_rng(13)
+    n = 20000
+    s = rng.standard_normal(n) * 10.0 ** rng.integers(-12, 13, n)
+    v = rng.standard_normal(n) * 10.0 ** rng.integers(-12, 13, n)
+    s[:6] = [1.0, -1.0, 1e16, 0.0, 3.0, -2.5]
+    v[:6] = [-1.0, 1e-16, 1.0, 0.0, 3.0, 2.5]
+    t = s + v
+    sb = np.abs(s) >= np.abs(v)
+    big, small = np.where(sb, s, v), np.where(sb, v, s)
+    e_fast = (big - t) + small
+    bv = t - s
+    e_two = (s - (t - bv)) + (v - bv)
+    assert np.array_equal(e_fast.view(np.int64), e_two.view(np.int64))
+
+    def kbns(vals, select):
+        acc, comp = 0.0, 0.0
+        for x in vals:
+            tt = acc + x
+            if select:
+                b, sm = (acc, x) if abs(acc) >= abs(x) else (x, acc)
+                comp += (b - tt) + sm
+            else:
+                bb = tt - acc
+                comp += (acc - (tt - bb)) + (x - bb)
+            acc = tt
+        return acc + comp
+    for k in range(20):
+        vals = (rng.standard_normal(300) * 10.0 ** rng.integers(-6, 7, 300)).tolist()
+        assert kbns(vals, True) == kbns(vals, False)
