@@ -213,3 +213,24 @@ def test_fast2sum_with_select_equals_twosum_and_the_reference_branch():
     for k in range(20):
         vals = (rng.standard_normal(300) * 10.0 ** rng.integers(-6, 7, 300)).tolist()
         assert kbns(vals, True) == kbns(vals, False)
+
+
+def test_mask_byte_count_and_or_flag():
+    """Two shortcuts of the mask prepass: the non-zero bytes of a 32-bit word of four 8-bit mask samples
+    are counted as popc((((m & 0x7f7f7f7f) + 0x7f7f7f7f) | m) & 0x80808080), and a picture holds a
+    sample above its maximum 2^bd - 1 exactly when the OR of all its samples exceeds that maximum."""
+    import numpy as np
+    rng = np.random.default_rng(14)
+    m = rng.integers(0, 1 << 32, size=100000, dtype=np.uint64)
+    m[:5] = [0, 0x80000000, 0x00ff0001, 0xffffffff, 0x01010100]
+    bits = ((((m & 0x7f7f7f7f) + 0x7f7f7f7f) | m) & 0x80808080).astype(np.uint64)
+    popc = np.array([bin(int(x)).count("1") for x in bits])
+    nonzero = sum(((m >> np.uint64(8 * k)) & np.uint64(0xff)) != 0 for k in range(4))
+    assert np.array_equal(popc, nonzero)
+    for bd in (8, 10, 12, 14):
+        maxv = (1 << bd) - 1
+        for _ in range(50):
+            x = rng.integers(0, maxv + 1, size=rng.integers(1, 64))
+            if rng.random() < 0.5:
+                x[rng.integers(0, x.size)] = rng.integers(maxv + 1, 1 << 16)
+            assert (np.bitwise_or.reduce(x) > maxv) == (x.max() > maxv)
